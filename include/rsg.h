@@ -1,0 +1,214 @@
+/*
+ * rsg.h -- C ABI of the B200 sparse linear-solve library (librsg.so).
+ *
+ * Plain C types only: pointers, sizes, status codes.  No exceptions cross this
+ * boundary.  Every entry point names the reference interface it replaces
+ * (paths relative to the reference project, Range-Software/range-solver-lib).
+ *
+ * Memory: arrays passed with RSG_MEM_HOST are caller-owned host buffers
+ * (copied during the call); arrays passed with RSG_MEM_DEVICE are device
+ * pointers on the context's GPU.  Matrices, preconditioners, assembly plans
+ * and learned models live in library-owned device memory behind opaque
+ * handles.  Each context owns one CUDA stream; calls on one context are
+ * serialised by the caller (like the reference, which is not re-entrant for
+ * one matrix); different contexts may be used from different threads.
+ */
+#ifndef RSG_H
+#define RSG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define RSG_API __attribute__((visibility("default")))
+#else
+#define RSG_API
+#endif
+
+typedef enum {
+    RSG_OK = 0,
+    RSG_NOT_CONVERGED = 1,      /* iteration limit reached (the reference returns silently) */
+    RSG_BREAKDOWN = 2,          /* non-finite residual / zero search direction */
+    RSG_ERR_INVALID_ARG = -1,
+    RSG_ERR_CUDA = -2,
+    RSG_ERR_OUT_OF_MEMORY = -3,
+    RSG_ERR_UNSUPPORTED = -4,
+    RSG_ERR_SINGULAR = -5,      /* singular block in block-Jacobi (RRMatrix::invert failure) */
+    RSG_ERR_TIMEOUT = -6
+} rsg_status;
+
+/* RMatrixSolverConf::Type (range-model-lib; used at src/rmatrixsolver.cpp:186-196) */
+typedef enum { RSG_SOLVER_CG = 0, RSG_SOLVER_GMRES = 1 } rsg_solver_type;
+
+/* RMatrixPreconditionerType (include/rmatrixpreconditioner.h:7-16), plus the learned one. */
+typedef enum {
+    RSG_PREC_NONE = 0,
+    RSG_PREC_JACOBI = 1,
+    RSG_PREC_BLOCK_JACOBI = 2,
+    RSG_PREC_LEARNED = 3
+} rsg_prec_type;
+
+typedef enum {
+    RSG_STOP_REFERENCE = 0,     /* RIterationInfo::hasConverged on ||r||/(||A||_F||x||+||b||) */
+    RSG_STOP_TRUE_RELRES = 1    /* FP64 true ||b-Ax||/||b|| <= rtol, recomputed before stopping */
+} rsg_stop_rule;
+
+typedef enum {
+    RSG_PRECISION_FP64 = 0,     /* everything in FP64 */
+    RSG_PRECISION_MIXED = 1     /* FP32 inner Krylov, FP64 residual/solution (reliable updates) */
+} rsg_precision;
+
+typedef enum { RSG_MEM_HOST = 0, RSG_MEM_DEVICE = 1 } rsg_memory;
+
+/* Mirrors RMatrixSolverConf fields read by src/rmatrixsolver.cpp:125-128 plus
+ * the GPU-specific options.  Fill with rsg_conf_default() first. */
+typedef struct {
+    int32_t  solver_type;       /* rsg_solver_type */
+    uint32_t n_outer;           /* nOuterIterations: CG iteration cap / GMRES restart cap */
+    uint32_t n_inner;           /* nInnerIterations: GMRES restart length */
+    double   cvg;               /* solverCvgValue (reference stopping rule) */
+    uint32_t output_frequency;  /* 0 = silent, like RIterationInfo */
+    const char *output_file;    /* convergence log "Iteration number|Solver residual|Solver convergence"; NULL = none */
+    double   eps;               /* stand-in for RConstants::eps (clamps and stagnation test) */
+    int32_t  stop_rule;         /* rsg_stop_rule */
+    double   rtol;              /* for RSG_STOP_TRUE_RELRES */
+    int32_t  precision;         /* rsg_precision */
+    int32_t  scale_equations;   /* 1 = reference's equation scaling 1e9*||A||_F/||b|| (src/rmatrixsolver.cpp:164-184) */
+    double   reliable_delta;    /* mixed precision: refresh the FP64 residual when ||r|| drops by this factor */
+    int32_t  flexible;          /* GMRES: store Z (flexible / variable preconditioner) */
+    int32_t  use_graph;         /* 1 = device-driven loop in one CUDA graph launch (default) */
+    uint32_t check_interval;    /* host-driven loop: iterations per convergence poll */
+    const void *learned;        /* rsg_learned* for RSG_PREC_LEARNED / learned initial guess */
+    int32_t  learned_initial_guess;
+    int32_t  reserved[7];
+} rsg_solver_conf;
+
+typedef struct {
+    uint32_t iterations;        /* CG iterations or GMRES inner steps in total */
+    uint32_t outer;             /* GMRES restarts / mixed-precision residual refreshes */
+    double   error;             /* last reference-style error */
+    double   trend;
+    double   true_relres;       /* FP64 ||b - A x|| / ||b|| of the returned x, recomputed on the GPU */
+    double   equation_scale;
+    double   norm_a;            /* ||A||_F */
+    double   norm_b;
+    double   seconds_setup;     /* preconditioner build, uploads (device-timed) */
+    double   seconds_solve;     /* iterations (device-timed) */
+    int32_t  converged;
+    int32_t  status;            /* rsg_status of the solve */
+    uint32_t fallbacks;         /* learned preconditioner: steps that fell back to Jacobi */
+    uint32_t reserved[5];
+} rsg_stats;
+
+typedef struct rsg_context rsg_context;
+typedef struct rsg_csr rsg_csr;
+typedef struct rsg_learned rsg_learned;
+
+/* ---- context ---- */
+RSG_API rsg_status rsg_context_create(int device, rsg_context **out);
+RSG_API void       rsg_context_destroy(rsg_context *ctx);
+RSG_API const char *rsg_status_string(rsg_status s);
+RSG_API const char *rsg_last_error(const rsg_context *ctx);
+RSG_API rsg_status rsg_context_set_stream(rsg_context *ctx, void *cuda_stream); /* NULL = own stream */
+RSG_API rsg_status rsg_synchronize(rsg_context *ctx);
+RSG_API void       rsg_conf_default(rsg_solver_conf *conf);
+
+/* ---- CSR matrices ----
+ * Replaces SparseMatrixCache + buildSparseMatrixCache (src/rmatrixsolver.cpp:14-54):
+ * upload the CSR once (uint32 row pointer and column indexes, FP64 values),
+ * compute ||A||_F, and derive the kernels' internal formats (FP32 values,
+ * 16-bit column offsets) on the GPU. */
+RSG_API rsg_status rsg_csr_create(rsg_context *ctx, uint32_t n_rows, const uint32_t *row_ptr,
+                                  const uint32_t *col_idx, const double *values, int32_t memory,
+                                  rsg_csr **out);
+/* Replaces refreshSparseMatrixCache (src/rmatrixsolver.cpp:56-97): same pattern, new values. */
+RSG_API rsg_status rsg_csr_update_values(rsg_context *ctx, rsg_csr *A, const double *values, int32_t memory);
+RSG_API void       rsg_csr_destroy(rsg_context *ctx, rsg_csr *A);
+RSG_API rsg_status rsg_csr_info(const rsg_csr *A, uint32_t *n_rows, uint64_t *nnz, double *frobenius);
+/* Device pointers to the stored CSR (row_ptr, col_idx, values) for callers that read it back. */
+RSG_API rsg_status rsg_csr_device_arrays(const rsg_csr *A, const uint32_t **row_ptr, const uint32_t **col_idx,
+                                         const double **values);
+
+/* Copy the stored CSR back to caller-owned host arrays (n_rows+1, nnz, nnz entries);
+ * the assembled system in the reference lives in host memory (RSparseMatrix). */
+RSG_API rsg_status rsg_csr_copy_to_host(rsg_context *ctx, const rsg_csr *A, uint32_t *row_ptr, uint32_t *col_idx,
+                                        double *values);
+
+/* y = A x in FP64 (multiplyRow, src/rmatrixsolver.cpp:111-119, over all rows).  Device pointers. */
+RSG_API rsg_status rsg_spmv(rsg_context *ctx, const rsg_csr *A, const double *x, double *y);
+/* y = A x with the FP32 copy of the values (mixed-precision inner product).  Device pointers. */
+RSG_API rsg_status rsg_spmv_f32(rsg_context *ctx, const rsg_csr *A, const float *x, float *y);
+/* Jacobi inverse diagonal d_i = 1/A_ii (0 when absent or zero): constructJacobi,
+ * src/rmatrixpreconditioner.cpp:78-94.  Device output. */
+RSG_API rsg_status rsg_jacobi_build(rsg_context *ctx, const rsg_csr *A, double *inv_diag);
+/* Block-Jacobi inverse blocks (n_rows x width, row-major per block row):
+ * constructBlockJacobi, src/rmatrixpreconditioner.cpp:96-148.  Device output. */
+RSG_API rsg_status rsg_block_jacobi_build(rsg_context *ctx, const rsg_csr *A, uint32_t block_size,
+                                          double *blocks, uint32_t *width_out);
+
+/* ---- solve ----
+ * Replaces RMatrixSolver::solve (src/rmatrixsolver.cpp:158-201) with its CG
+ * (:208-355) and GMRES (:357-581).  x is in/out: its incoming values are the
+ * initial guess, like the reference (callers zero it).  b and x are host or
+ * device arrays of n_rows doubles according to `memory`. */
+RSG_API rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_conf *conf, int32_t prec_type,
+                             uint32_t block_size, const double *b, double *x, int32_t memory, rsg_stats *stats);
+
+/* FP64 true relative residual ||b - A x|| / ||b|| (device pointers). */
+RSG_API rsg_status rsg_true_relres(rsg_context *ctx, const rsg_csr *A, const double *b, const double *x,
+                                   double *relres);
+
+/* ---- assembly (RSolverHeat / RSolverStress prepare + assemblyMatrix) ----
+ * A plan is the sparsity pattern of the free-DOF system plus the
+ * element-to-nonzero scatter map (the reference precedent is
+ * RSolverFluid::buildSparseMatrixPattern, src/rsolverfluid.cpp:2305-2397).  It
+ * is built once per mesh and node book; numeric assembly then runs on the GPU
+ * without atomics and in a fixed order, so repeated assemblies are bitwise
+ * identical. */
+typedef struct rsg_assembly rsg_assembly;
+
+typedef struct {
+    int32_t transient;   /* time solver enabled */
+    double  alpha;       /* time-march approximation coefficient (1 = backward Euler) */
+    double  dt;
+} rsg_time;
+
+/* Heat: 1 DOF per node; book[i] = free position or 0xffffffff (RSolverGeneric::generateNodeBook,
+ * src/rsolvergeneric.cpp:498-582).  All arrays host memory. */
+RSG_API rsg_status rsg_assembly_create_heat(rsg_context *ctx, uint32_t n_nodes, const double *xyz,
+                                            uint32_t n_tets, const uint32_t *tets, const uint32_t *book,
+                                            uint32_t n_free, rsg_assembly **out);
+/* Elasticity: 3 interleaved DOFs per node (RSolverStress::generateNodeBook,
+ * src/rsolverstress.cpp:1564-1652); traction triangles add RHS only. */
+RSG_API rsg_status rsg_assembly_create_stress(rsg_context *ctx, uint32_t n_nodes, const double *xyz,
+                                              uint32_t n_tets, const uint32_t *tets, uint32_t n_tris,
+                                              const uint32_t *tris, const uint32_t *book, uint32_t n_free,
+                                              rsg_assembly **out);
+RSG_API void       rsg_assembly_destroy(rsg_context *ctx, rsg_assembly *plan);
+RSG_API rsg_status rsg_assembly_info(const rsg_assembly *plan, uint32_t *n_free, uint64_t *nnz);
+
+/* Heat numeric assembly, src/rsolverheat.cpp:361-455 (element loop) and :755-820
+ * (theta scheme, Dirichlet lifting, scatter).  Per-tet arrays k_e, q_e, rhoc_e;
+ * per-node node_t (prescribed values at disabled nodes, previous T when
+ * transient).  Inputs in `memory`; writes the values of *A (created on the
+ * first call, same pattern afterwards) and b (device, n_free doubles). */
+RSG_API rsg_status rsg_assemble_heat(rsg_context *ctx, rsg_assembly *plan, const double *k_e, const double *q_e,
+                                     const double *rhoc_e, const double *node_t, const rsg_time *time,
+                                     int32_t memory, rsg_csr **A, double *b_device);
+
+/* Elasticity numeric assembly, src/rsolverstress.cpp:384-715 and :1654-1772.
+ * Per-tet e_mod, nu, rho_e, texp_e, dtemp_e; gravity[3]; per-triangle traction[3];
+ * node_u (3 per node: prescribed displacement / previous displacement). */
+RSG_API rsg_status rsg_assemble_stress(rsg_context *ctx, rsg_assembly *plan, const double *e_mod, const double *nu,
+                                       const double *rho_e, const double *gravity, const double *texp_e,
+                                       const double *dtemp_e, const double *traction, const double *node_u,
+                                       const rsg_time *time, int32_t memory, rsg_csr **A, double *b_device);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RSG_H */

@@ -1,0 +1,224 @@
+"""ctypes wrapper of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module, and only as the checker / the timed CPU baseline.  The CUDA library
+never calls it.  Build with `make -C oracle` (done by __graft_entry__.build()).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+EOD = 0xFFFFFFFF
+
+
+class OrcConf(C.Structure):
+    _fields_ = [
+        ("solver_type", C.c_int32),
+        ("n_outer", C.c_uint32),
+        ("n_inner", C.c_uint32),
+        ("cvg", C.c_double),
+        ("eps", C.c_double),
+        ("stop_rule", C.c_int32),
+        ("rtol", C.c_double),
+        ("scale_equations", C.c_int32),
+        ("n_threads", C.c_int32),
+    ]
+
+
+class OrcStats(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_uint32),
+        ("outer", C.c_uint32),
+        ("error", C.c_double),
+        ("trend", C.c_double),
+        ("true_relres", C.c_double),
+        ("equation_scale", C.c_double),
+        ("norm_a", C.c_double),
+        ("norm_b", C.c_double),
+        ("seconds", C.c_double),
+        ("converged", C.c_int32),
+        ("status", C.c_int32),
+    ]
+
+
+class OrcTime(C.Structure):
+    _fields_ = [("transient", C.c_int32), ("alpha", C.c_double), ("dt", C.c_double)]
+
+
+_P = C.c_void_p
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            raise RuntimeError("oracle not built: run `make -C oracle`")
+        L = C.CDLL(path)
+        L.orc_csr_frobenius.restype = C.c_double
+        L.orc_csr_frobenius.argtypes = [C.c_uint32, _P, _P]
+        L.orc_spmv.argtypes = [C.c_uint32, _P, _P, _P, _P, _P]
+        L.orc_jacobi_build.argtypes = [C.c_uint32, _P, _P, _P, _P]
+        L.orc_block_jacobi_build.restype = C.c_int
+        L.orc_block_jacobi_build.argtypes = [C.c_uint32, _P, _P, _P, C.c_uint32, _P, C.POINTER(C.c_uint32)]
+        L.orc_solve.restype = C.c_int
+        L.orc_solve.argtypes = [C.POINTER(OrcConf), C.c_uint32, _P, _P, _P, C.c_int32, C.c_uint32, _P, _P,
+                                C.POINTER(OrcStats)]
+        L.orc_true_relres.restype = C.c_double
+        L.orc_true_relres.argtypes = [C.c_uint32, _P, _P, _P, _P, _P]
+        L.orc_node_book.restype = C.c_uint32
+        L.orc_node_book.argtypes = [C.c_uint32, _P, _P]
+        L.orc_system_n.restype = C.c_uint32
+        L.orc_system_n.argtypes = [_P]
+        L.orc_system_nnz.restype = C.c_uint64
+        L.orc_system_nnz.argtypes = [_P]
+        L.orc_system_copy.argtypes = [_P, _P, _P, _P, _P]
+        L.orc_system_free.argtypes = [_P]
+        L.orc_assemble_heat.restype = _P
+        L.orc_assemble_heat.argtypes = [C.c_uint32, _P, C.c_uint32, _P, _P, _P, _P, _P, _P, C.c_uint32,
+                                        C.POINTER(OrcTime)]
+        L.orc_assemble_stress.restype = _P
+        L.orc_assemble_stress.argtypes = [C.c_uint32, _P, C.c_uint32, _P, _P, _P, _P, _P, _P, _P, C.c_uint32, _P,
+                                          _P, _P, _P, C.c_uint32, C.POINTER(OrcTime)]
+        _LIB = L
+    return _LIB
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+@dataclass
+class CSR:
+    n: int
+    rp: np.ndarray  # uint32 (n+1)
+    ci: np.ndarray  # uint32
+    val: np.ndarray  # float64
+
+    @property
+    def nnz(self) -> int:
+        return int(self.ci.shape[0])
+
+    def to_dense(self) -> np.ndarray:
+        A = np.zeros((self.n, self.n))
+        for i in range(self.n):
+            A[i, self.ci[self.rp[i]:self.rp[i + 1]]] += self.val[self.rp[i]:self.rp[i + 1]]
+        return A
+
+
+def csr_from_dense(A: np.ndarray) -> CSR:
+    n = A.shape[0]
+    rp = [0]
+    ci = []
+    val = []
+    for i in range(n):
+        for j in range(n):
+            if A[i, j] != 0.0:
+                ci.append(j)
+                val.append(A[i, j])
+        rp.append(len(ci))
+    return CSR(n, np.asarray(rp, np.uint32), np.asarray(ci, np.uint32), np.asarray(val, np.float64))
+
+
+def frobenius(A: CSR) -> float:
+    return lib().orc_csr_frobenius(A.n, _ptr(A.rp), _ptr(A.val))
+
+
+def spmv(A: CSR, x: np.ndarray) -> np.ndarray:
+    x = np.ascontiguousarray(x, np.float64)
+    y = np.empty(A.n)
+    lib().orc_spmv(A.n, _ptr(A.rp), _ptr(A.ci), _ptr(A.val), _ptr(x), _ptr(y))
+    return y
+
+
+def jacobi(A: CSR) -> np.ndarray:
+    d = np.empty(A.n)
+    lib().orc_jacobi_build(A.n, _ptr(A.rp), _ptr(A.ci), _ptr(A.val), _ptr(d))
+    return d
+
+
+def block_jacobi(A: CSR, block_size: int):
+    data = np.empty(A.n * max(block_size, 1))
+    w = C.c_uint32(0)
+    rc = lib().orc_block_jacobi_build(A.n, _ptr(A.rp), _ptr(A.ci), _ptr(A.val), block_size, _ptr(data), C.byref(w))
+    if rc != 0:
+        raise RuntimeError("singular diagonal block")
+    return data[: A.n * w.value].reshape(A.n, w.value), w.value
+
+
+def true_relres(A: CSR, b: np.ndarray, x: np.ndarray) -> float:
+    b = np.ascontiguousarray(b, np.float64)
+    x = np.ascontiguousarray(x, np.float64)
+    return lib().orc_true_relres(A.n, _ptr(A.rp), _ptr(A.ci), _ptr(A.val), _ptr(b), _ptr(x))
+
+
+def make_conf(solver: str = "cg", n_outer: int = 1000, n_inner: int = 30, cvg: float = 1e-13, eps: float = 1e-14,
+              stop_rule: str = "reference", rtol: float = 1e-10, scale: bool = True, threads: int = 0) -> OrcConf:
+    return OrcConf(0 if solver == "cg" else 1, n_outer, n_inner, cvg, eps, 0 if stop_rule == "reference" else 1,
+                   rtol, 1 if scale else 0, threads)
+
+
+def solve(A: CSR, b: np.ndarray, x0: np.ndarray | None = None, *, prec: int = 1, block_size: int = 1,
+          conf: OrcConf | None = None, **kw):
+    """RMatrixSolver::solve restated: returns (x, stats)."""
+    conf = conf or make_conf(**kw)
+    b = np.ascontiguousarray(b, np.float64)
+    x = np.zeros(A.n) if x0 is None else np.array(x0, np.float64, copy=True)
+    st = OrcStats()
+    rc = lib().orc_solve(C.byref(conf), A.n, _ptr(A.rp), _ptr(A.ci), _ptr(A.val), prec, block_size, _ptr(b), _ptr(x),
+                         C.byref(st))
+    if rc != 0:
+        raise RuntimeError(f"oracle solve failed: {rc}")
+    return x, st
+
+
+def _system(h) -> tuple[CSR, np.ndarray]:
+    L = lib()
+    n = L.orc_system_n(h)
+    nnz = L.orc_system_nnz(h)
+    rp = np.empty(n + 1, np.uint32)
+    ci = np.empty(nnz, np.uint32)
+    val = np.empty(nnz, np.float64)
+    b = np.empty(n, np.float64)
+    L.orc_system_copy(h, _ptr(rp), _ptr(ci), _ptr(val), _ptr(b))
+    L.orc_system_free(h)
+    return CSR(n, rp, ci, val), b
+
+
+def assemble_heat(p) -> tuple[CSR, np.ndarray]:
+    """RSolverHeat::prepare + assemblyMatrix restated for a rsg.workloads.HeatProblem."""
+    m = p.mesh
+    xyz = np.ascontiguousarray(m.xyz, np.float64)
+    tets = np.ascontiguousarray(m.tets, np.uint32)
+    k = np.ascontiguousarray(p.k_e, np.float64)
+    q = np.ascontiguousarray(p.q_e, np.float64)
+    rc = np.ascontiguousarray(p.rhoc_e, np.float64)
+    nt = np.ascontiguousarray(p.node_t, np.float64)
+    book = np.ascontiguousarray(p.book, np.uint32)
+    tm = OrcTime(1 if p.transient else 0, p.alpha, p.dt)
+    h = lib().orc_assemble_heat(m.n_nodes, _ptr(xyz), m.n_tets, _ptr(tets), _ptr(k), _ptr(q), _ptr(rc), _ptr(nt),
+                                _ptr(book), p.n_free, C.byref(tm))
+    return _system(h)
+
+
+def assemble_stress(p) -> tuple[CSR, np.ndarray]:
+    """RSolverStress::prepare + assemblyMatrix restated for a rsg.workloads.StressProblem."""
+    m = p.mesh
+    arrs = [np.ascontiguousarray(a, np.float64) for a in (m.xyz, p.e_mod, p.nu, p.rho_e, p.gravity, p.texp_e,
+                                                          p.dtemp_e, p.traction, p.node_u)]
+    xyz, e, nu, rho, g, te, dte, tr, nu_ = arrs
+    tets = np.ascontiguousarray(m.tets, np.uint32)
+    tris = np.ascontiguousarray(p.tris, np.uint32)
+    book = np.ascontiguousarray(p.book, np.uint32)
+    tm = OrcTime(1 if p.transient else 0, p.alpha, p.dt)
+    h = lib().orc_assemble_stress(m.n_nodes, _ptr(xyz), m.n_tets, _ptr(tets), _ptr(e), _ptr(nu), _ptr(rho), _ptr(g),
+                                  _ptr(te), _ptr(dte), tris.shape[0], _ptr(tris), _ptr(tr), _ptr(nu_), _ptr(book),
+                                  p.n_free, C.byref(tm))
+    return _system(h)

@@ -1,0 +1,677 @@
+// Preconditioned conjugate gradients on the GPU.
+//
+// Restates RMatrixSolver::solveCG (src/rmatrixsolver.cpp:208-355) with the
+// same recurrences, clamps and error measure, but fused so that one
+// iteration is two streaming kernels:
+//   dir:    p = z + beta p_old (computed on the fly inside the SpMV gather),
+//           q = A p, partial p^T q  -> last block: alpha = rho / clamp(p^T q)
+//   update: x += alpha p, r -= alpha q, z = P r (Jacobi / block Jacobi /
+//           none, src/rmatrixpreconditioner.cpp:150-190), partial r^T z,
+//           ||r||^2, ||x||^2  -> last block: beta, error, stopping rule
+// plus a check kernel that is a no-op unless the recurrence residual has
+// reached the tolerance, in which case it recomputes the FP64 true residual
+// b - A x (stop_rule TRUE_RELRES).
+//
+// Mixed precision (reliable updates, van der Vorst & Ye 2000): the matrix is
+// read as FP32 values with 16-bit column offsets, vectors are FP32 scaled by
+// sigma = 1/||b||, dot products are compensated FP32 (Dot2).  When the FP32
+// recurrence residual falls by `delta` (or reaches rtol) the check kernel
+// recomputes r = b - A (x + y) in FP64, folds the FP32 correction y into the
+// FP64 solution x and restarts the recurrence from the true residual while
+// keeping the search direction.
+//
+// The loop runs on the device: the kernels of two iterations form the body of
+// a CUDA graph `while` node whose condition the tail kernel sets from the
+// device state, so a whole solve is a single graph launch.  The tail kernel
+// also counts bodies and forces termination past a hard limit, so the loop
+// always ends even if the state were corrupted.
+#include "krylov.cuh"
+
+#include <cmath>
+
+namespace rsg {
+
+// ---------------- state transitions (thread 0 of the last block) ----------------
+
+__device__ void finalize_update64(CgState *st, double rz, double rr, double xx)
+{
+    st->rho_new = rz;
+    st->beta = rz / st->rho;
+    const double rn = sqrt(rr), xn = sqrt(xx);
+    st->rn = rn;
+    st->xn = xn;
+    double norm = st->an * xn + st->bn;
+    if (fabs(norm) < st->eps) norm = st->eps;
+    const double err = rn / norm;
+    st->trend = err - st->error;
+    st->error = err;
+    const uint32_t it = ++st->it;
+    if (st->history) {
+        st->history[it - 1] = err;
+        st->trend_hist[it - 1] = st->trend;
+    }
+    if (st->stop_rule == RSG_STOP_REFERENCE) {
+        // RIterationInfo::hasConverged, src/riterationinfo.cpp:90-109
+        const bool conv = !dev_isnormal(err) || !dev_isnormal(st->trend) || err < st->cvg ||
+                          fabs(st->trend) < st->eps * st->eps;
+        if (conv) {
+            st->done = 1;
+            st->converged = 1;
+            st->status = isfinite(err) ? RSG_OK : RSG_BREAKDOWN;
+        } else if (it >= st->max_it) {
+            st->done = 1;
+            st->status = RSG_NOT_CONVERGED;
+        }
+    } else {
+        if (!isfinite(rn)) {
+            st->done = 1;
+            st->status = RSG_BREAKDOWN;
+        } else if (rn <= st->rtol * st->bn) {
+            st->need_check = 1;
+        } else if (it >= st->max_it) {
+            st->done = 1;
+            st->status = RSG_NOT_CONVERGED;
+        }
+    }
+}
+
+__device__ void finalize_check64(CgState *st, double rz, double rn)
+{
+    st->n_updates++;
+    st->rn = rn;
+    if (!isfinite(rn)) {
+        st->done = 1;
+        st->status = RSG_BREAKDOWN;
+    } else if (rn <= st->rtol * st->bn) {
+        st->done = 1;
+        st->converged = 1;
+        st->status = RSG_OK;
+    } else {
+        // the recurrence drifted from the true residual: restart the direction
+        // (p = z) so that a tolerance below the attainable accuracy stagnates
+        // instead of diverging
+        st->rho_new = rz;
+        st->beta = 0.0;
+        st->need_check = 0;
+        if (st->it >= st->max_it) {
+            st->done = 1;
+            st->status = RSG_NOT_CONVERGED;
+        }
+    }
+}
+
+__device__ void finalize_update_mixed(CgState *st, double rz, double rr)
+{
+    st->rho_new = rz;
+    st->beta = rz / st->rho;
+    const double rn = sqrt(rr) / st->sigma;
+    st->rn = rn;
+    const uint32_t it = ++st->it;
+    const double rel = st->bn > 0.0 ? rn / st->bn : rn;
+    st->trend = rel - st->error;
+    st->error = rel;
+    if (st->history) {
+        st->history[it - 1] = rel;
+        st->trend_hist[it - 1] = st->trend;
+    }
+    if (!isfinite(rn) || rn <= st->rtol * st->bn || rn <= st->delta * st->max_r) st->need_check = 1;
+    else if (it >= st->max_it) {
+        st->done = 1;
+        st->status = RSG_NOT_CONVERGED;
+    }
+}
+
+__device__ void finalize_check_mixed(CgState *st, double rz, double rn)
+{
+    st->n_updates++;
+    st->fold = 1;
+    st->rn = rn;
+    if (!isfinite(rn)) {
+        st->done = 1;
+        st->status = RSG_BREAKDOWN;
+    } else if (rn <= st->rtol * st->bn) {
+        st->done = 1;
+        st->converged = 1;
+        st->status = RSG_OK;
+    } else {
+        st->max_r = rn;
+        st->rho_new = rz;
+        st->beta = rz / st->rho;
+        st->need_check = 0;
+        if (st->it >= st->max_it) {
+            st->done = 1;
+            st->status = RSG_NOT_CONVERGED;
+        }
+    }
+}
+
+__device__ __forceinline__ double clamp_pq(double pq, double eps)
+{
+    // src/rmatrixsolver.cpp:304-315
+    if (pq > 0.0) return fmax(pq, eps);
+    if (pq < 0.0) return fmin(pq, -eps);
+    return eps;
+}
+
+// ---------------- FP64 kernels ----------------
+
+template <int RPW>
+__global__ void __launch_bounds__(kBlock) k_cg_init_res(Csr<double> M, const double *__restrict__ b,
+                                                        const double *__restrict__ x, double *__restrict__ r,
+                                                        double *partials, CgState *st)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *prod = reinterpret_cast<double *>(smem_raw);
+    __shared__ double sh[64];
+    double acc[2] = {0.0, 0.0};
+    auto gx = [&](uint32_t c) { return x[c]; };
+    auto epi = [&](uint32_t row, double ax) {
+        const double ri = b[row] - ax;
+        r[row] = ri;
+        acc[0] += ri * ri;
+        acc[1] += b[row] * b[row];
+    };
+    for_rows<double, double, RPW>(M, gx, epi, prod);
+    double tot[2];
+    if (grid_sum<2>(acc, partials, &st->ticket[3], sh, tot) && threadIdx.x == 0) {
+        st->rn = sqrt(tot[0]);
+        st->bn = sqrt(tot[1]);
+        st->max_r = st->rn;
+    }
+}
+
+// z = P r for rows of groups [g*G, g*G+G); returns r^T z contribution.
+template <int PK>
+__device__ __forceinline__ double prec_group64(uint32_t g, uint32_t w, const double *__restrict__ d,
+                                               const double *rl, double *__restrict__ z)
+{
+    if (PK == 0) {
+        z[g] = rl[0];
+        return rl[0] * rl[0];
+    } else if (PK == 1) {
+        const double zi = d[g] * rl[0];
+        z[g] = zi;
+        return rl[0] * zi;
+    } else {
+        double s = 0.0;
+        for (uint32_t k = 0; k < w; k++) {
+            const double *row = d + (size_t(g) * w + k) * w;
+            double zk = 0.0;
+            for (uint32_t l = 0; l < w; l++) zk += row[l] * rl[l];
+            z[size_t(g) * w + k] = zk;
+            s += rl[k] * zk;
+        }
+        return s;
+    }
+}
+
+// z = P r from the stored r; finalizes init (mode 0) or a block-Jacobi check (mode 1).
+template <int PK>
+__global__ void __launch_bounds__(kBlock) k_cg_prec(uint32_t n, uint32_t w, const double *__restrict__ d,
+                                                    const double *__restrict__ r, double *__restrict__ z,
+                                                    double *partials, CgState *st, int mode)
+{
+    __shared__ double sh[32];
+    if (mode == 1 && (st->done || !st->need_check)) return;
+    const uint32_t G = PK == 2 ? w : 1, ng = n / G;
+    double acc[1] = {0.0};
+    double rl[kMaxBlock];
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
+        for (uint32_t k = 0; k < G; k++) rl[k] = r[size_t(g) * G + k];
+        acc[0] += prec_group64<PK>(g, w, d, rl, z);
+    }
+    double tot[1];
+    if (grid_sum<1>(acc, partials, &st->ticket[4], sh, tot) && threadIdx.x == 0) {
+        if (mode == 0) {
+            st->rho_new = tot[0];
+            st->rho = tot[0];
+            st->beta = 0.0;
+        } else {
+            finalize_check64(st, tot[0], st->check_rn);
+        }
+    }
+}
+
+template <int RPW>
+__global__ void __launch_bounds__(kBlock) k_cg_dir(Csr<double> M, const double *__restrict__ z,
+                                                   const double *__restrict__ p_old, double *__restrict__ p_new,
+                                                   double *__restrict__ q, double *partials, CgState *st)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *prod = reinterpret_cast<double *>(smem_raw);
+    __shared__ double sh[32];
+    if (st->done) return;
+    const double beta = st->beta;
+    double acc[1] = {0.0};
+    auto gx = [&](uint32_t c) { return fma(beta, p_old[c], z[c]); };
+    auto epi = [&](uint32_t row, double v) {
+        const double p = fma(beta, p_old[row], z[row]);
+        p_new[row] = p;
+        q[row] = v;
+        acc[0] += p * v;
+    };
+    for_rows<double, double, RPW>(M, gx, epi, prod);
+    double tot[1];
+    if (grid_sum<1>(acc, partials, &st->ticket[0], sh, tot) && threadIdx.x == 0) {
+        const double pq = clamp_pq(tot[0], st->eps);
+        st->pq = pq;
+        st->rho = st->rho_new;
+        st->alpha = st->rho / pq;
+    }
+}
+
+template <int PK>
+__global__ void __launch_bounds__(kBlock) k_cg_update(uint32_t n, uint32_t w, const double *__restrict__ d,
+                                                      const double *__restrict__ p, const double *__restrict__ q,
+                                                      double *__restrict__ x, double *__restrict__ r,
+                                                      double *__restrict__ z, double *partials, CgState *st)
+{
+    __shared__ double sh[96];
+    if (st->done) return;
+    const double alpha = st->alpha;
+    const uint32_t G = PK == 2 ? w : 1, ng = n / G;
+    double acc[3] = {0.0, 0.0, 0.0};
+    double rl[kMaxBlock];
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
+        for (uint32_t k = 0; k < G; k++) {
+            const size_t i = size_t(g) * G + k;
+            const double xi = fma(alpha, p[i], x[i]);
+            const double ri = fma(-alpha, q[i], r[i]);
+            x[i] = xi;
+            r[i] = ri;
+            acc[1] += ri * ri;
+            acc[2] += xi * xi;
+            rl[k] = ri;
+        }
+        acc[0] += prec_group64<PK>(g, w, d, rl, z);
+    }
+    double tot[3];
+    if (grid_sum<3>(acc, partials, &st->ticket[1], sh, tot) && threadIdx.x == 0)
+        finalize_update64(st, tot[0], tot[1], tot[2]);
+}
+
+template <int RPW, int PK>
+__global__ void __launch_bounds__(kBlock) k_cg_check(Csr<double> M, const double *__restrict__ d,
+                                                     const double *__restrict__ b, const double *__restrict__ x,
+                                                     double *__restrict__ r, double *__restrict__ z,
+                                                     double *partials, CgState *st)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *prod = reinterpret_cast<double *>(smem_raw);
+    __shared__ double sh[64];
+    if (st->done || !st->need_check) return;
+    double acc[2] = {0.0, 0.0};
+    auto gx = [&](uint32_t c) { return x[c]; };
+    auto epi = [&](uint32_t row, double ax) {
+        const double ri = b[row] - ax;
+        r[row] = ri;
+        acc[1] += ri * ri;
+        if (PK == 0) {
+            z[row] = ri;
+            acc[0] += ri * ri;
+        } else if (PK == 1) {
+            const double zi = d[row] * ri;
+            z[row] = zi;
+            acc[0] += ri * zi;
+        }
+    };
+    for_rows<double, double, RPW>(M, gx, epi, prod);
+    double tot[2];
+    if (grid_sum<2>(acc, partials, &st->ticket[2], sh, tot) && threadIdx.x == 0) {
+        if (PK == 2) st->check_rn = sqrt(tot[1]);
+        else finalize_check64(st, tot[0], sqrt(tot[1]));
+    }
+}
+
+// ---------------- mixed-precision kernels ----------------
+
+template <int PK>
+__device__ __forceinline__ void prec_group32(uint32_t g, uint32_t w, const float *__restrict__ d,
+                                             const float *rl, float *__restrict__ z, Dot2 &rz)
+{
+    if (PK == 0) {
+        z[g] = rl[0];
+        rz.add_prod(rl[0], rl[0]);
+    } else if (PK == 1) {
+        const float zi = d[g] * rl[0];
+        z[g] = zi;
+        rz.add_prod(rl[0], zi);
+    } else {
+        for (uint32_t k = 0; k < w; k++) {
+            const float *row = d + (size_t(g) * w + k) * w;
+            float zk = 0.f;
+            for (uint32_t l = 0; l < w; l++) zk = fmaf(row[l], rl[l], zk);
+            z[size_t(g) * w + k] = zk;
+            rz.add_prod(rl[k], zk);
+        }
+    }
+}
+
+// r32 = sigma * r64, z32 = P r32.  mode 0: init (sets sigma from ||b||); mode 1: block-Jacobi check tail.
+template <int PK>
+__global__ void __launch_bounds__(kBlock) k_mx_prec(uint32_t n, uint32_t w, const float *__restrict__ d,
+                                                    const double *__restrict__ r64, float *__restrict__ r32,
+                                                    float *__restrict__ z, double *partials, CgState *st, int mode)
+{
+    __shared__ double sh[32];
+    if (mode == 1 && (st->done || !st->need_check)) return;
+    const double sigma = mode == 0 ? (st->bn > 0.0 ? 1.0 / st->bn : 1.0) : st->sigma;
+    const uint32_t G = PK == 2 ? w : 1, ng = n / G;
+    Dot2 rz;
+    float rl[kMaxBlock];
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
+        for (uint32_t k = 0; k < G; k++) {
+            const size_t i = size_t(g) * G + k;
+            const float rf = mode == 0 ? float(r64[i] * sigma) : r32[i];
+            if (mode == 0) r32[i] = rf;
+            rl[k] = rf;
+        }
+        prec_group32<PK>(g, w, d, rl, z, rz);
+    }
+    double acc[1] = {rz.value()};
+    double tot[1];
+    if (grid_sum<1>(acc, partials, &st->ticket[4], sh, tot) && threadIdx.x == 0) {
+        if (mode == 0) {
+            st->sigma = sigma;
+            st->rho_new = tot[0];
+            st->rho = tot[0];
+            st->beta = 0.0;
+        } else {
+            finalize_check_mixed(st, tot[0], st->check_rn);
+        }
+    }
+}
+
+template <int RPW>
+__global__ void __launch_bounds__(kBlock) k_mx_dir(Csr<float> M, const float *__restrict__ z,
+                                                   const float *__restrict__ p_old, float *__restrict__ p_new,
+                                                   float *__restrict__ q, double *__restrict__ x,
+                                                   float *__restrict__ y, double *partials, CgState *st)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float *prod = reinterpret_cast<float *>(smem_raw);
+    __shared__ double sh[32];
+    if (st->done) return;
+    const float beta = float(st->beta);
+    const int fold = st->fold;
+    const double inv_sigma = 1.0 / st->sigma;
+    Dot2 pq;
+    auto gx = [&](uint32_t c) { return fmaf(beta, p_old[c], z[c]); };
+    auto epi = [&](uint32_t row, float v) {
+        const float p = fmaf(beta, p_old[row], z[row]);
+        p_new[row] = p;
+        q[row] = v;
+        pq.add_prod(p, v);
+        if (fold) {
+            x[row] = fma(double(y[row]), inv_sigma, x[row]);
+            y[row] = 0.f;
+        }
+    };
+    for_rows<float, float, RPW>(M, gx, epi, prod);
+    double acc[1] = {pq.value()};
+    double tot[1];
+    if (grid_sum<1>(acc, partials, &st->ticket[0], sh, tot) && threadIdx.x == 0) {
+        double d = tot[0];
+        if (d == 0.0 || !isfinite(d)) d = (d == 0.0) ? 1e-300 : d;
+        st->pq = d;
+        st->rho = st->rho_new;
+        st->alpha = st->rho / d;
+        st->fold = 0;
+    }
+}
+
+template <int PK>
+__global__ void __launch_bounds__(kBlock) k_mx_update(uint32_t n, uint32_t w, const float *__restrict__ d,
+                                                      const float *__restrict__ p, const float *__restrict__ q,
+                                                      float *__restrict__ y, float *__restrict__ r,
+                                                      float *__restrict__ z, double *partials, CgState *st)
+{
+    __shared__ double sh[64];
+    if (st->done) return;
+    const float alpha = float(st->alpha);
+    const uint32_t G = PK == 2 ? w : 1, ng = n / G;
+    Dot2 rz, rr;
+    float rl[kMaxBlock];
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
+        for (uint32_t k = 0; k < G; k++) {
+            const size_t i = size_t(g) * G + k;
+            y[i] = fmaf(alpha, p[i], y[i]);
+            const float ri = fmaf(-alpha, q[i], r[i]);
+            r[i] = ri;
+            rr.add_prod(ri, ri);
+            rl[k] = ri;
+        }
+        prec_group32<PK>(g, w, d, rl, z, rz);
+    }
+    double acc[2] = {rz.value(), rr.value()};
+    double tot[2];
+    if (grid_sum<2>(acc, partials, &st->ticket[1], sh, tot) && threadIdx.x == 0)
+        finalize_update_mixed(st, tot[0], tot[1]);
+}
+
+template <int RPW, int PK>
+__global__ void __launch_bounds__(kBlock) k_mx_check(Csr<double> M, const float *__restrict__ d,
+                                                     const double *__restrict__ b, const double *__restrict__ x,
+                                                     const float *__restrict__ y, float *__restrict__ r32,
+                                                     float *__restrict__ z, double *partials, CgState *st)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *prod = reinterpret_cast<double *>(smem_raw);
+    __shared__ double sh[64];
+    if (st->done || !st->need_check) return;
+    const double sigma = st->sigma, inv_sigma = 1.0 / sigma;
+    Dot2 rz;
+    double rr[1] = {0.0};
+    auto gx = [&](uint32_t c) { return fma(double(y[c]), inv_sigma, x[c]); };
+    auto epi = [&](uint32_t row, double ax) {
+        const double ri = b[row] - ax;
+        rr[0] += ri * ri;
+        const float rf = float(ri * sigma);
+        r32[row] = rf;
+        if (PK == 0) {
+            z[row] = rf;
+            rz.add_prod(rf, rf);
+        } else if (PK == 1) {
+            const float zf = d[row] * rf;
+            z[row] = zf;
+            rz.add_prod(rf, zf);
+        }
+    };
+    for_rows<double, double, RPW>(M, gx, epi, prod);
+    double acc[2] = {rz.value(), rr[0]};
+    double tot[2];
+    if (grid_sum<2>(acc, partials, &st->ticket[2], sh, tot) && threadIdx.x == 0) {
+        if (PK == 2) st->check_rn = sqrt(tot[1]);
+        else finalize_check_mixed(st, tot[0], sqrt(tot[1]));
+    }
+}
+
+__global__ void k_mx_fold(uint32_t n, double *__restrict__ x, float *__restrict__ y, const CgState *st)
+{
+    const double inv_sigma = 1.0 / st->sigma;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        x[i] = fma(double(y[i]), inv_sigma, x[i]);
+        y[i] = 0.f;
+    }
+}
+
+// Loop control: counts bodies, enforces the hard limit, drives the graph's while node.
+__global__ void k_tail(CgState *st, cudaGraphConditionalHandle h, int use_cond)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const uint32_t bc = ++st->body_count;
+    if (!st->done && bc >= st->body_limit) {
+        st->done = 1;
+        st->status = RSG_ERR_TIMEOUT;
+    }
+    if (use_cond) cudaGraphSetConditional(h, st->done ? 0u : 1u);
+}
+
+// ---------------- host driver ----------------
+
+namespace {
+
+template <typename K>
+void set_smem(K k, size_t smem)
+{
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+}
+
+struct Launch {
+    int g_spmv64, g_spmv32, g_vec;
+    size_t s64, s32;
+};
+
+template <int RPW, int PK>
+void launch_init(rsg_context *ctx, const CgArgs &a, const Launch &L)
+{
+    const Csr<double> M64 = view<double>(a.A, true);
+    k_cg_init_res<RPW><<<L.g_spmv64, kBlock, L.s64, ctx->stream>>>(M64, a.b, a.x, a.r, a.partials, a.st);
+    if (!a.mixed)
+        k_cg_prec<PK><<<L.g_vec, kBlock, 0, ctx->stream>>>(a.A->n, a.P.w, a.P.d, a.r, a.z, a.partials, a.st, 0);
+    else
+        k_mx_prec<PK><<<L.g_vec, kBlock, 0, ctx->stream>>>(a.A->n, a.P.w, a.P.d32, a.r, a.r32, a.z32, a.partials,
+                                                          a.st, 0);
+}
+
+template <int RPW, int PK>
+void launch_body(rsg_context *ctx, const CgArgs &a, const Launch &L, cudaGraphConditionalHandle h, int use_cond)
+{
+    const uint32_t n = a.A->n;
+    const Csr<double> M64 = view<double>(a.A, true);
+    if (!a.mixed) {
+        for (int half = 0; half < 2; half++) {
+            double *po = half ? a.p1 : a.p0, *pn = half ? a.p0 : a.p1;
+            k_cg_dir<RPW><<<L.g_spmv64, kBlock, L.s64, ctx->stream>>>(M64, a.z, po, pn, a.q, a.partials, a.st);
+            k_cg_update<PK><<<L.g_vec, kBlock, 0, ctx->stream>>>(n, a.P.w, a.P.d, pn, a.q, a.x, a.r, a.z, a.partials,
+                                                                a.st);
+            k_cg_check<RPW, PK><<<L.g_spmv64, kBlock, L.s64, ctx->stream>>>(M64, a.P.d, a.b, a.x, a.r, a.z,
+                                                                            a.partials, a.st);
+            if (PK == 2)
+                k_cg_prec<PK><<<L.g_vec, kBlock, 0, ctx->stream>>>(n, a.P.w, a.P.d, a.r, a.z, a.partials, a.st, 1);
+        }
+    } else {
+        const Csr<float> M32 = view<float>(a.A, true);
+        for (int half = 0; half < 2; half++) {
+            float *po = half ? a.p32b : a.p32a, *pn = half ? a.p32a : a.p32b;
+            k_mx_dir<RPW><<<L.g_spmv32, kBlock, L.s32, ctx->stream>>>(M32, a.z32, po, pn, a.q32, a.x, a.y32,
+                                                                      a.partials, a.st);
+            k_mx_update<PK><<<L.g_vec, kBlock, 0, ctx->stream>>>(n, a.P.w, a.P.d32, pn, a.q32, a.y32, a.r32, a.z32,
+                                                                a.partials, a.st);
+            k_mx_check<RPW, PK><<<L.g_spmv64, kBlock, L.s64, ctx->stream>>>(M64, a.P.d32, a.b, a.x, a.y32, a.r32,
+                                                                            a.z32, a.partials, a.st);
+            if (PK == 2)
+                k_mx_prec<PK><<<L.g_vec, kBlock, 0, ctx->stream>>>(n, a.P.w, a.P.d32, nullptr, a.r32, a.z32,
+                                                                  a.partials, a.st, 1);
+        }
+    }
+    k_tail<<<1, 32, 0, ctx->stream>>>(a.st, h, use_cond);
+}
+
+template <int RPW, int PK>
+rsg_status run_typed(rsg_context *ctx, const CgArgs &a, double *seconds)
+{
+    Launch L;
+    L.s64 = prod_smem<double>();
+    L.s32 = prod_smem<float>();
+    set_smem(k_cg_init_res<RPW>, L.s64);
+    set_smem(k_cg_dir<RPW>, L.s64);
+    set_smem(k_cg_check<RPW, PK>, L.s64);
+    set_smem(k_mx_dir<RPW>, L.s32);
+    set_smem(k_mx_check<RPW, PK>, L.s64);
+    const long long chunk_threads = (long long)a.A->n * 32 / RPW;
+    L.g_spmv64 = std::min(grid_for(ctx, (const void *)k_cg_dir<RPW>, kBlock, L.s64, chunk_threads), kMaxGrid);
+    L.g_spmv32 = std::min(grid_for(ctx, (const void *)k_mx_dir<RPW>, kBlock, L.s32, chunk_threads), kMaxGrid);
+    L.g_vec = std::min(grid_for(ctx, (const void *)k_cg_update<PK>, kBlock, 0, a.A->n), kMaxGrid);
+
+    RSG_CHECK_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
+    launch_init<RPW, PK>(ctx, a, L);
+    RSG_CHECK_CUDA(ctx, cudaGetLastError());
+
+    if (a.use_graph) {
+        cudaGraph_t graph = nullptr, body = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        cudaGraphConditionalHandle h;
+        RSG_CHECK_CUDA(ctx, cudaGraphCreate(&graph, 0));
+        rsg_status s = RSG_OK;
+        do {
+            if (cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
+                s = set_error(ctx, RSG_ERR_CUDA, "cudaGraphConditionalHandleCreate failed");
+                break;
+            }
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = h;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t node;
+            if (cudaGraphAddNode(&node, graph, nullptr, 0, &cp) != cudaSuccess) {
+                s = set_error(ctx, RSG_ERR_CUDA, "adding the while node failed");
+                break;
+            }
+            body = cp.conditional.phGraph_out[0];
+            if (cudaStreamBeginCaptureToGraph(ctx->stream, body, nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+                s = set_error(ctx, RSG_ERR_CUDA, "capture into the loop body failed");
+                break;
+            }
+            launch_body<RPW, PK>(ctx, a, L, h, 1);
+            cudaGraph_t captured = nullptr;
+            cudaError_t e = cudaStreamEndCapture(ctx->stream, &captured);
+            if (e != cudaSuccess) {
+                s = set_error(ctx, RSG_ERR_CUDA, "end capture: %s", cudaGetErrorString(e));
+                break;
+            }
+            e = cudaGraphInstantiate(&exec, graph, 0);
+            if (e != cudaSuccess) {
+                s = set_error(ctx, RSG_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+                break;
+            }
+            e = cudaGraphLaunch(exec, ctx->stream);
+            if (e != cudaSuccess) s = set_error(ctx, RSG_ERR_CUDA, "graph launch: %s", cudaGetErrorString(e));
+        } while (0);
+        if (s == RSG_OK && a.mixed)
+            k_mx_fold<<<L.g_vec, kBlock, 0, ctx->stream>>>(a.A->n, a.x, a.y32, a.st);
+        if (s == RSG_OK) {
+            cudaEventRecord(ctx->ev[1], ctx->stream);
+            cudaError_t e = cudaStreamSynchronize(ctx->stream);
+            if (e != cudaSuccess) s = set_error(ctx, RSG_ERR_CUDA, "solve: %s", cudaGetErrorString(e));
+        }
+        if (exec) cudaGraphExecDestroy(exec);
+        cudaGraphDestroy(graph);
+        if (s != RSG_OK) return s;
+    } else {
+        const uint32_t bodies_per_poll = std::max<uint32_t>(1, a.check_interval / 2);
+        int32_t *done_h = reinterpret_cast<int32_t *>(ctx->pinned);
+        for (;;) {
+            for (uint32_t k = 0; k < bodies_per_poll; k++) launch_body<RPW, PK>(ctx, a, L, 0, 0);
+            RSG_CHECK_CUDA(ctx, cudaGetLastError());
+            RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(done_h, &a.st->done, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                                ctx->stream));
+            RSG_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            if (*done_h) break;
+        }
+        if (a.mixed) k_mx_fold<<<L.g_vec, kBlock, 0, ctx->stream>>>(a.A->n, a.x, a.y32, a.st);
+        RSG_CHECK_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
+        RSG_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+    *seconds = ms * 1e-3;
+    return RSG_OK;
+}
+
+}  // namespace
+
+rsg_status cg_run(rsg_context *ctx, const CgArgs &a, double *seconds)
+{
+    const int rpw = pick_rpw(a.A);
+    switch (a.P.kind) {
+    case 0: RSG_RPW_DISPATCH(rpw, return (run_typed<RPW, 0>(ctx, a, seconds)));
+    case 1: RSG_RPW_DISPATCH(rpw, return (run_typed<RPW, 1>(ctx, a, seconds)));
+    default: RSG_RPW_DISPATCH(rpw, return (run_typed<RPW, 2>(ctx, a, seconds)));
+    }
+    return RSG_ERR_UNSUPPORTED;
+}
+
+}  // namespace rsg

@@ -1,0 +1,42 @@
+// Internal interface of the CSR module (used by the solvers and assembly).
+#pragma once
+
+#include "spmv.cuh"
+
+namespace rsg {
+
+constexpr uint32_t kMaxBlock = 8;   // largest block-Jacobi width handled on the GPU
+constexpr int kMaxGrid = 4096;      // upper bound on grid size of reduction kernels
+
+#define RSG_RPW_DISPATCH(rpw, ...)                 \
+    switch (rpw) {                                 \
+    case 32: {                                     \
+        constexpr int RPW = 32;                    \
+        __VA_ARGS__;                               \
+    } break;                                       \
+    case 16: {                                     \
+        constexpr int RPW = 16;                    \
+        __VA_ARGS__;                               \
+    } break;                                       \
+    case 8: {                                      \
+        constexpr int RPW = 8;                     \
+        __VA_ARGS__;                               \
+    } break;                                       \
+    default: {                                     \
+        constexpr int RPW = 4;                     \
+        __VA_ARGS__;                               \
+    } break;                                       \
+    }
+
+rsg_status spmv64(rsg_context *ctx, const rsg_csr *A, const double *x, double *y, bool off16);
+rsg_status spmv32(rsg_context *ctx, const rsg_csr *A, const float *x, float *y, bool off16);
+// Recompute ||A||_F and the FP32 copy after the values were rewritten in place.
+rsg_status csr_refresh(rsg_context *ctx, rsg_csr *A);
+rsg_status jacobi_build(rsg_context *ctx, const rsg_csr *A, double *d);
+uint32_t block_width(uint32_t n, uint32_t block_size);
+rsg_status block_jacobi_build(rsg_context *ctx, const rsg_csr *A, uint32_t w, double *blocks, unsigned int *flag);
+// out3 = {||b-Ax||, ||b||, relres}; partials >= 2*grid doubles.
+rsg_status true_residual(rsg_context *ctx, const rsg_csr *A, const double *b, const double *x, double *partials,
+                         unsigned int *ticket, double *out3);
+
+}  // namespace rsg

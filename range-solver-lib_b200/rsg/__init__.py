@@ -1,0 +1,313 @@
+"""Python host layer over librsg.so (the B200 sparse linear-solve library).
+
+Mirrors the reference's RMatrixSolver interface (include/rmatrixsolver.h):
+`Solver(conf).solve(A, b, x, preconditioner, block_size)` with the same
+argument meaning; the numerical work runs in the CUDA library through the C
+ABI declared in include/rsg.h.  Host arrays are numpy; device arrays may be
+passed as any object with `data_ptr()` (e.g. torch CUDA tensors).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import (BREAKDOWN, ERR_INVALID_ARG, ERR_SINGULAR, ERR_UNSUPPORTED, MEM_DEVICE, MEM_HOST, NOT_CONVERGED,
+                   OK, PREC_BLOCK_JACOBI, PREC_JACOBI, PREC_LEARNED, PREC_NONE, PRECISION_FP64, PRECISION_MIXED,
+                   SOLVER_CG, SOLVER_GMRES, STOP_REFERENCE, STOP_TRUE_RELRES, RsgError, SolverConf, Stats, Time)
+
+__all__ = ["Context", "Matrix", "Assembly", "make_conf", "RsgError", "SolverConf", "Stats", "Solver"]
+
+
+def _ptr(a) -> C.c_void_p:
+    if a is None:
+        return C.c_void_p(0)
+    if hasattr(a, "data_ptr"):
+        return C.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _is_device(a) -> bool:
+    return hasattr(a, "data_ptr") and getattr(a, "is_cuda", False)
+
+
+def make_conf(solver: str | int = "cg", n_outer: int = 1000, n_inner: int = 30, cvg: float = 1e-13,
+              eps: float = 1e-14, stop_rule: str | int = "reference", rtol: float = 1e-10,
+              precision: str | int = "fp64", scale_equations: bool = True, reliable_delta: float = 1e-2,
+              flexible: bool = False, use_graph: bool = True, check_interval: int = 16,
+              output_frequency: int = 0, output_file: str | None = None) -> SolverConf:
+    c = SolverConf()
+    _lib.load().rsg_conf_default(C.byref(c))
+    c.solver_type = solver if isinstance(solver, int) else {"cg": SOLVER_CG, "gmres": SOLVER_GMRES}[solver]
+    c.n_outer = n_outer
+    c.n_inner = n_inner
+    c.cvg = cvg
+    c.eps = eps
+    c.stop_rule = stop_rule if isinstance(stop_rule, int) else {"reference": STOP_REFERENCE,
+                                                                 "true": STOP_TRUE_RELRES}[stop_rule]
+    c.rtol = rtol
+    c.precision = precision if isinstance(precision, int) else {"fp64": PRECISION_FP64,
+                                                                 "mixed": PRECISION_MIXED}[precision]
+    c.scale_equations = 1 if scale_equations else 0
+    c.reliable_delta = reliable_delta
+    c.flexible = 1 if flexible else 0
+    c.use_graph = 1 if use_graph else 0
+    c.check_interval = check_interval
+    c.output_frequency = output_frequency
+    c.output_file = output_file.encode() if output_file else None
+    return c
+
+
+class Context:
+    """One GPU, one CUDA stream (rsg_context)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        s = self.lib.rsg_context_create(device, C.byref(h))
+        if s != OK:
+            raise RsgError(s, f"rsg_context_create({device}) failed: {self.lib.rsg_status_string(s).decode()}")
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if self.h:
+            self.lib.rsg_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def check(self, s: int, what: str, allow=(OK,)):
+        if s not in allow:
+            raise RsgError(s, f"{what}: {self.lib.rsg_status_string(s).decode()}: "
+                              f"{self.lib.rsg_last_error(self.h).decode()}")
+        return s
+
+    def sync(self):
+        self.check(self.lib.rsg_synchronize(self.h), "synchronize")
+
+    def set_stream(self, stream_ptr: int | None):
+        self.check(self.lib.rsg_context_set_stream(self.h, C.c_void_p(stream_ptr or 0)), "set_stream")
+
+    # ---- matrices ----
+    def matrix(self, rp, ci, val) -> "Matrix":
+        dev = _is_device(rp)
+        if not dev:
+            rp = np.ascontiguousarray(rp, np.uint32)
+            ci = np.ascontiguousarray(ci, np.uint32)
+            val = np.ascontiguousarray(val, np.float64)
+        n = int(rp.shape[0]) - 1
+        h = C.c_void_p()
+        self.check(self.lib.rsg_csr_create(self.h, n, _ptr(rp), _ptr(ci), _ptr(val), MEM_DEVICE if dev else MEM_HOST,
+                                           C.byref(h)), "csr_create")
+        return Matrix(self, h)
+
+    # ---- solve ----
+    def solve(self, A: "Matrix", b, x=None, conf: SolverConf | None = None, prec: int = PREC_JACOBI,
+              block_size: int = 1, allow=(OK, NOT_CONVERGED, BREAKDOWN)):
+        """RMatrixSolver::solve: returns (x, Stats).  Device arrays are updated in place."""
+        conf = conf or make_conf()
+        st = Stats()
+        if _is_device(b):
+            if x is None:
+                raise ValueError("device solve needs an x array")
+            s = self.lib.rsg_solve(self.h, A.h, C.byref(conf), prec, block_size, _ptr(b), _ptr(x), MEM_DEVICE,
+                                   C.byref(st))
+        else:
+            b = np.ascontiguousarray(b, np.float64)
+            x = np.zeros(A.n) if x is None else np.array(x, np.float64, copy=True)
+            s = self.lib.rsg_solve(self.h, A.h, C.byref(conf), prec, block_size, _ptr(b), _ptr(x), MEM_HOST,
+                                   C.byref(st))
+        self.check(s, "solve", allow)
+        return x, st
+
+    def spmv(self, A: "Matrix", x_dev, y_dev):
+        self.check(self.lib.rsg_spmv(self.h, A.h, _ptr(x_dev), _ptr(y_dev)), "spmv")
+
+    def spmv_f32(self, A: "Matrix", x_dev, y_dev):
+        self.check(self.lib.rsg_spmv_f32(self.h, A.h, _ptr(x_dev), _ptr(y_dev)), "spmv_f32")
+
+    def jacobi(self, A: "Matrix", d_dev):
+        self.check(self.lib.rsg_jacobi_build(self.h, A.h, _ptr(d_dev)), "jacobi_build")
+
+    def block_jacobi(self, A: "Matrix", block_size: int, blocks_dev) -> int:
+        w = C.c_uint32()
+        self.check(self.lib.rsg_block_jacobi_build(self.h, A.h, block_size, _ptr(blocks_dev), C.byref(w)),
+                   "block_jacobi_build")
+        return w.value
+
+    def true_relres(self, A: "Matrix", b_dev, x_dev) -> float:
+        r = C.c_double()
+        self.check(self.lib.rsg_true_relres(self.h, A.h, _ptr(b_dev), _ptr(x_dev), C.byref(r)), "true_relres")
+        return r.value
+
+
+class Matrix:
+    """Device CSR handle (rsg_csr)."""
+
+    def __init__(self, ctx: Context, h: C.c_void_p):
+        self.ctx = ctx
+        self.h = h
+        n = C.c_uint32()
+        nnz = C.c_uint64()
+        fro = C.c_double()
+        ctx.check(ctx.lib.rsg_csr_info(h, C.byref(n), C.byref(nnz), C.byref(fro)), "csr_info")
+        self.n, self.nnz, self.frobenius = n.value, nnz.value, fro.value
+
+    def update_values(self, val):
+        dev = _is_device(val)
+        if not dev:
+            val = np.ascontiguousarray(val, np.float64)
+        self.ctx.check(self.ctx.lib.rsg_csr_update_values(self.ctx.h, self.h, _ptr(val),
+                                                          MEM_DEVICE if dev else MEM_HOST), "csr_update_values")
+        self.refresh_info()
+
+    def refresh_info(self):
+        fro = C.c_double()
+        self.ctx.lib.rsg_csr_info(self.h, None, None, C.byref(fro))
+        self.frobenius = fro.value
+
+    def to_host(self):
+        """(row_ptr, col_idx, values) copied back to numpy."""
+        rp = np.empty(self.n + 1, np.uint32)
+        ci = np.empty(self.nnz, np.uint32)
+        val = np.empty(self.nnz, np.float64)
+        self.ctx.check(self.ctx.lib.rsg_csr_copy_to_host(self.ctx.h, self.h, _ptr(rp), _ptr(ci), _ptr(val)),
+                       "csr_copy_to_host")
+        return rp, ci, val
+
+    def device_arrays(self):
+        rp, ci, val = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        self.ctx.check(self.ctx.lib.rsg_csr_device_arrays(self.h, C.byref(rp), C.byref(ci), C.byref(val)),
+                       "csr_device_arrays")
+        return rp.value, ci.value, val.value
+
+    def close(self):
+        if self.h and self.ctx.h:
+            self.ctx.lib.rsg_csr_destroy(self.ctx.h, self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Solver:
+    """Mirror of RMatrixSolver (include/rmatrixsolver.h:9-52) over a Context."""
+
+    def __init__(self, ctx: Context, conf: SolverConf):
+        self.ctx = ctx
+        self.conf = conf
+        self._cache: dict[int, tuple[Matrix, tuple]] = {}
+
+    def solve(self, A_csr, b, x=None, prec: int = PREC_NONE, block_size: int = 1):
+        """A_csr: (row_ptr, col_idx, values) host arrays.  The matrix is cached by
+        identity of the row_ptr array; a same-pattern call only refreshes values
+        (the reference's findSparseMatrixCache, src/rmatrixsolver.cpp:99-109)."""
+        rp, ci, val = A_csr
+        key = id(rp)
+        hit = self._cache.get(key)
+        if hit is not None and hit[1] == (len(rp), len(ci)) and np.array_equal(hit[2], ci):
+            M = hit[0]
+            M.update_values(val)
+        else:
+            M = self.ctx.matrix(rp, ci, val)
+            self._cache[key] = (M, (len(rp), len(ci)), np.array(ci, copy=True))
+        return self.ctx.solve(M, b, x, self.conf, prec, block_size)
+
+
+class Assembly:
+    """Assembly plan (rsg_assembly): pattern + scatter map of one mesh and node book.
+
+    heat: RSolverHeat::prepare/assemblyMatrix (src/rsolverheat.cpp:361-455, :755-820);
+    stress: RSolverStress::prepare/assemblyMatrix (src/rsolverstress.cpp:384-715, :1654-1772).
+    """
+
+    def __init__(self, ctx: Context, h: C.c_void_p, kind: str):
+        self.ctx, self.h, self.kind = ctx, h, kind
+        n = C.c_uint32()
+        nnz = C.c_uint64()
+        ctx.check(ctx.lib.rsg_assembly_info(h, C.byref(n), C.byref(nnz)), "assembly_info")
+        self.n_free, self.nnz = n.value, nnz.value
+        self.A: Matrix | None = None
+
+    @classmethod
+    def heat(cls, ctx: Context, p) -> "Assembly":
+        m = p.mesh
+        xyz = np.ascontiguousarray(m.xyz, np.float64)
+        tets = np.ascontiguousarray(m.tets, np.uint32)
+        book = np.ascontiguousarray(p.book, np.uint32)
+        h = C.c_void_p()
+        ctx.check(ctx.lib.rsg_assembly_create_heat(ctx.h, m.n_nodes, _ptr(xyz), m.n_tets, _ptr(tets), _ptr(book),
+                                                   p.n_free, C.byref(h)), "assembly_create_heat")
+        return cls(ctx, h, "heat")
+
+    @classmethod
+    def stress(cls, ctx: Context, p) -> "Assembly":
+        m = p.mesh
+        xyz = np.ascontiguousarray(m.xyz, np.float64)
+        tets = np.ascontiguousarray(m.tets, np.uint32)
+        tris = np.ascontiguousarray(p.tris, np.uint32)
+        book = np.ascontiguousarray(p.book, np.uint32)
+        h = C.c_void_p()
+        ctx.check(ctx.lib.rsg_assembly_create_stress(ctx.h, m.n_nodes, _ptr(xyz), m.n_tets, _ptr(tets),
+                                                     tris.shape[0], _ptr(tris), _ptr(book), p.n_free, C.byref(h)),
+                  "assembly_create_stress")
+        return cls(ctx, h, "stress")
+
+    def _time(self, p) -> Time:
+        return Time(1 if p.transient else 0, p.alpha, p.dt)
+
+    def assemble(self, p, b_dev, inputs_on_device: dict | None = None) -> Matrix:
+        """Assemble problem p's values into the plan's matrix (created on first use) and b_dev (device)."""
+        hA = C.c_void_p(self.A.h.value if self.A is not None else 0)
+        tm = self._time(p)
+        if self.kind == "heat":
+            if inputs_on_device:
+                d = inputs_on_device
+                args = [d["k_e"], d["q_e"], d["rhoc_e"], d["node_t"]]
+                mem = MEM_DEVICE
+            else:
+                args = [np.ascontiguousarray(a, np.float64) for a in (p.k_e, p.q_e, p.rhoc_e, p.node_t)]
+                mem = MEM_HOST
+            s = self.ctx.lib.rsg_assemble_heat(self.ctx.h, self.h, *[_ptr(a) for a in args], C.byref(tm), mem,
+                                               C.byref(hA), _ptr(b_dev))
+        else:
+            args = [np.ascontiguousarray(a, np.float64) for a in (p.e_mod, p.nu, p.rho_e, p.gravity, p.texp_e,
+                                                                  p.dtemp_e, p.traction, p.node_u)]
+            s = self.ctx.lib.rsg_assemble_stress(self.ctx.h, self.h, *[_ptr(a) for a in args], C.byref(tm), MEM_HOST,
+                                                 C.byref(hA), _ptr(b_dev))
+        self.ctx.check(s, f"assemble_{self.kind}")
+        if self.A is None:
+            self.A = Matrix(self.ctx, hA)
+        else:
+            self.A.refresh_info()
+        return self.A
+
+    def close(self):
+        if self.A is not None:
+            self.A.close()
+            self.A = None
+        if self.h and self.ctx.h:
+            self.ctx.lib.rsg_assembly_destroy(self.ctx.h, self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,154 @@
+"""ctypes declarations of the C ABI in include/rsg.h (librsg.so).
+
+Loading fails loudly when the library has not been built; there is no CPU
+fallback anywhere in this package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(_HERE)
+REPO = os.path.dirname(PKG)
+LIB_PATH = os.path.join(PKG, "lib", "librsg.so")
+HEADER = os.path.join(REPO, "include", "rsg.h")
+
+# status codes
+OK = 0
+NOT_CONVERGED = 1
+BREAKDOWN = 2
+ERR_INVALID_ARG = -1
+ERR_CUDA = -2
+ERR_OUT_OF_MEMORY = -3
+ERR_UNSUPPORTED = -4
+ERR_SINGULAR = -5
+ERR_TIMEOUT = -6
+
+SOLVER_CG, SOLVER_GMRES = 0, 1
+PREC_NONE, PREC_JACOBI, PREC_BLOCK_JACOBI, PREC_LEARNED = 0, 1, 2, 3
+STOP_REFERENCE, STOP_TRUE_RELRES = 0, 1
+PRECISION_FP64, PRECISION_MIXED = 0, 1
+MEM_HOST, MEM_DEVICE = 0, 1
+
+
+class SolverConf(C.Structure):
+    _fields_ = [
+        ("solver_type", C.c_int32),
+        ("n_outer", C.c_uint32),
+        ("n_inner", C.c_uint32),
+        ("cvg", C.c_double),
+        ("output_frequency", C.c_uint32),
+        ("output_file", C.c_char_p),
+        ("eps", C.c_double),
+        ("stop_rule", C.c_int32),
+        ("rtol", C.c_double),
+        ("precision", C.c_int32),
+        ("scale_equations", C.c_int32),
+        ("reliable_delta", C.c_double),
+        ("flexible", C.c_int32),
+        ("use_graph", C.c_int32),
+        ("check_interval", C.c_uint32),
+        ("learned", C.c_void_p),
+        ("learned_initial_guess", C.c_int32),
+        ("reserved", C.c_int32 * 7),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_uint32),
+        ("outer", C.c_uint32),
+        ("error", C.c_double),
+        ("trend", C.c_double),
+        ("true_relres", C.c_double),
+        ("equation_scale", C.c_double),
+        ("norm_a", C.c_double),
+        ("norm_b", C.c_double),
+        ("seconds_setup", C.c_double),
+        ("seconds_solve", C.c_double),
+        ("converged", C.c_int32),
+        ("status", C.c_int32),
+        ("fallbacks", C.c_uint32),
+        ("reserved", C.c_uint32 * 5),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class Time(C.Structure):
+    _fields_ = [("transient", C.c_int32), ("alpha", C.c_double), ("dt", C.c_double)]
+
+
+_P = C.c_void_p
+_PP = C.POINTER(C.c_void_p)
+_U32P = C.POINTER(C.c_uint32)
+_U64P = C.POINTER(C.c_uint64)
+_DP = C.POINTER(C.c_double)
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "rsg_context_create": (C.c_int, [C.c_int, _PP]),
+    "rsg_context_destroy": (None, [_P]),
+    "rsg_status_string": (C.c_char_p, [C.c_int]),
+    "rsg_last_error": (C.c_char_p, [_P]),
+    "rsg_context_set_stream": (C.c_int, [_P, _P]),
+    "rsg_synchronize": (C.c_int, [_P]),
+    "rsg_conf_default": (None, [C.POINTER(SolverConf)]),
+    "rsg_csr_create": (C.c_int, [_P, C.c_uint32, _P, _P, _P, C.c_int32, _PP]),
+    "rsg_csr_update_values": (C.c_int, [_P, _P, _P, C.c_int32]),
+    "rsg_csr_destroy": (None, [_P, _P]),
+    "rsg_csr_info": (C.c_int, [_P, _U32P, _U64P, _DP]),
+    "rsg_csr_device_arrays": (C.c_int, [_P, _PP, _PP, _PP]),
+    "rsg_csr_copy_to_host": (C.c_int, [_P, _P, _P, _P, _P]),
+    "rsg_spmv": (C.c_int, [_P, _P, _P, _P]),
+    "rsg_spmv_f32": (C.c_int, [_P, _P, _P, _P]),
+    "rsg_jacobi_build": (C.c_int, [_P, _P, _P]),
+    "rsg_block_jacobi_build": (C.c_int, [_P, _P, C.c_uint32, _P, _U32P]),
+    "rsg_solve": (C.c_int, [_P, _P, C.POINTER(SolverConf), C.c_int32, C.c_uint32, _P, _P, C.c_int32,
+                            C.POINTER(Stats)]),
+    "rsg_true_relres": (C.c_int, [_P, _P, _P, _P, _DP]),
+    "rsg_assembly_create_heat": (C.c_int, [_P, C.c_uint32, _P, C.c_uint32, _P, _P, C.c_uint32, _PP]),
+    "rsg_assembly_create_stress": (C.c_int, [_P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32, _P, _P, C.c_uint32,
+                                             _PP]),
+    "rsg_assembly_destroy": (None, [_P, _P]),
+    "rsg_assembly_info": (C.c_int, [_P, _U32P, _U64P]),
+    "rsg_assemble_heat": (C.c_int, [_P, _P, _P, _P, _P, _P, C.POINTER(Time), C.c_int32, _PP, _P]),
+    "rsg_assemble_stress": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, C.POINTER(Time), C.c_int32, _PP,
+                                      _P]),
+}
+
+_lib = None
+
+
+def header_symbols() -> list[str]:
+    """Every function name declared with RSG_API in include/rsg.h."""
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"RSG_API\s+[^;(]*?\b(rsg_\w+)\s*\(", txt)))
+
+
+def load():
+    """Load librsg.so, declare every entry point; raise if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} not found: build it with `python range-solver-lib_b200/build.py` "
+                           "(the CUDA library is required; there is no CPU fallback)")
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name, None)
+        if fn is None:
+            continue
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class RsgError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"rsg status {status}: {message}")
+        self.status = status

@@ -1,0 +1,133 @@
+"""GPU assembly (rsg_assembly_* / rsg_assemble_*) against the CPU oracle.
+
+Bar: the sparsity pattern is identical; every assembled entry and RHS value
+matches the oracle within 1e-13 relative (absolute floor 1e-13 of the row's
+largest entry, for entries that cancel to rounding noise); repeated assemblies
+are bitwise identical.
+"""
+import numpy as np
+import pytest
+
+import rsg
+from oracle import oracle as O
+from rsg import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def device_csr(ctx, torch, M):
+    rp, ci, val = M.to_host()
+    return O.CSR(M.n, rp, ci, val)
+
+
+def compare(Ag, bg, Ao, bo, rtol=1e-13):
+    assert np.array_equal(Ag.rp, Ao.rp)
+    assert np.array_equal(Ag.ci, Ao.ci)
+    rowmax = np.maximum.reduceat(np.abs(Ao.val), Ao.rp[:-1].astype(np.int64))
+    scale = np.repeat(rowmax, np.diff(Ao.rp.astype(np.int64)))
+    diff = np.abs(Ag.val - Ao.val)
+    assert np.all(diff <= rtol * np.abs(Ao.val) + 1e-13 * scale), diff.max()
+    bscale = np.abs(bo).max() if bo.size else 1.0
+    assert np.all(np.abs(bg - bo) <= rtol * np.abs(bo) + 1e-13 * bscale)
+
+
+def run_heat(ctx, torch, p):
+    asm = rsg.Assembly.heat(ctx, p)
+    b = torch.empty(p.n_free, dtype=torch.float64, device="cuda")
+    M = asm.assemble(p, b)
+    ctx.sync()
+    return asm, M, b
+
+
+@pytest.mark.parametrize("transient,alpha", [(False, 1.0), (True, 1.0), (True, 0.5)])
+def test_heat_assembly_matches_oracle(ctx, torch_cuda, transient, alpha):
+    torch = torch_cuda
+    p = W.heat_cube(7, sigma=1.5, seed=4, source="random", transient=transient, dt=1e-3)
+    p.alpha = alpha
+    if transient:
+        p.node_t = W.uniform(4, 9, p.mesh.n_nodes)
+        p.node_t[p.mesh.xyz[:, 0] == 1.0] = 1.0
+        p.node_t[p.mesh.xyz[:, 0] == 0.0] = 0.0
+    asm, M, b = run_heat(ctx, torch, p)
+    Ao, bo = O.assemble_heat(p)
+    assert asm.n_free == Ao.n and asm.nnz == Ao.nnz
+    compare(device_csr(ctx, torch, M), b.cpu().numpy(), Ao, bo)
+    assert M.frobenius == pytest.approx(O.frobenius(Ao), rel=1e-13)
+
+
+def test_heat_assembly_deterministic_and_reassembly(ctx, torch_cuda):
+    torch = torch_cuda
+    p = W.heat_cube(9, sigma=1.0, seed=1, source="random")
+    asm, M, b = run_heat(ctx, torch, p)
+    v1 = device_csr(ctx, torch, M).val.copy()
+    b1 = b.clone()
+    asm.assemble(p, b)
+    ctx.sync()
+    assert np.array_equal(device_csr(ctx, torch, M).val, v1) and torch.equal(b, b1)
+    p2 = W.heat_cube(9, sigma=1.0, seed=2, source="random")
+    asm.assemble(p2, b)  # same pattern, new conductivities: written in place
+    ctx.sync()
+    Ao, bo = O.assemble_heat(p2)
+    compare(device_csr(ctx, torch, M), b.cpu().numpy(), Ao, bo)
+
+
+def test_heat_assembly_device_inputs(ctx, torch_cuda):
+    torch = torch_cuda
+    p = W.heat_cube(6, sigma=1.0, seed=3, source="random")
+    asm = rsg.Assembly.heat(ctx, p)
+    b = torch.empty(p.n_free, dtype=torch.float64, device="cuda")
+    d = {k: torch.tensor(getattr(p, k), device="cuda") for k in ("k_e", "q_e", "rhoc_e", "node_t")}
+    M = asm.assemble(p, b, inputs_on_device=d)
+    ctx.sync()
+    Ao, bo = O.assemble_heat(p)
+    compare(device_csr(ctx, torch, M), b.cpu().numpy(), Ao, bo)
+
+
+@pytest.mark.parametrize("variant", ["plain", "body_loads", "transient"])
+def test_stress_assembly_matches_oracle(ctx, torch_cuda, variant):
+    torch = torch_cuda
+    p = W.stress_beam(6, 3, 3)
+    if variant == "body_loads":
+        p.gravity = np.array([0.0, -9.81, 1.5])
+        p.texp_e = np.full(p.mesh.n_tets, 1.2e-5)
+        p.dtemp_e = W.uniform(3, 4, p.mesh.n_tets, -20.0, 40.0)
+        p.e_mod = W.lognormal(5, 6, p.mesh.n_tets, np.log(210e9), 0.3)
+    if variant == "transient":
+        p.transient, p.alpha, p.dt = True, 1.0, 1e-4
+        p.node_u = 1e-5 * W.normal(1, 2, 3 * p.mesh.n_nodes)
+        p.node_u[p.disabled] = 0.0
+    asm = rsg.Assembly.stress(ctx, p)
+    b = torch.empty(p.n_free, dtype=torch.float64, device="cuda")
+    M = asm.assemble(p, b)
+    ctx.sync()
+    Ao, bo = O.assemble_stress(p)
+    compare(device_csr(ctx, torch, M), b.cpu().numpy(), Ao, bo)
+
+
+def test_gpu_assembly_then_solve_patch_test(ctx, torch_cuda):
+    torch = torch_cuda
+    p = W.heat_cube(10, source="none")
+    asm, M, b = run_heat(ctx, torch, p)
+    x = torch.zeros_like(b)
+    _, st = ctx.solve(M, b, x, conf=rsg.make_conf(n_outer=10000, stop_rule="true", rtol=1e-13))
+    full = p.node_t.copy()
+    free = p.book != W.EOD
+    full[free] = x.cpu().numpy()[p.book[free]]
+    assert np.abs(full - p.mesh.xyz[:, 0]).max() < 1e-10
+
+
+def test_assembly_rejects_bad_inputs(ctx):
+    p = W.heat_cube(3)
+    bad = p.book.copy()
+    free = np.nonzero(bad != W.EOD)[0]
+    bad[free[0]], bad[free[1]] = bad[free[1]], bad[free[0]]  # not increasing
+    p2 = W.heat_cube(3)
+    p2.book = bad
+    with pytest.raises(rsg.RsgError) as e:
+        rsg.Assembly.heat(ctx, p2)
+    assert e.value.status == rsg.ERR_INVALID_ARG
+    p3 = W.heat_cube(3)
+    p3.mesh.tets = p3.mesh.tets.copy()
+    p3.mesh.tets[5, 2] = p3.mesh.n_nodes + 3
+    with pytest.raises(rsg.RsgError):
+        rsg.Assembly.heat(ctx, p3)

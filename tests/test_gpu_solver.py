@@ -1,0 +1,300 @@
+"""GPU parity of the solve path (rsg_solve / rsg_spmv / preconditioner builds)
+against the CPU oracle, through the C ABI.
+
+Tolerances: FP64 kernels match the oracle to rounding (SpMV 1e-13 of the row's
+absolute sum); solutions reach the FP64 true relative residual they were asked
+for (1e-10) and agree with the oracle's tight solution to ||x-x_ref||/||x_ref||
+<= 1e-8; reference-rule runs stop within two iterations of the oracle.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import rsg
+from oracle import oracle as O
+from rsg import workloads as W
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+_SYS = {}
+
+
+def heat(n, sigma=0.0, seed=0, source="unit"):
+    key = ("heat", n, sigma, seed, source)
+    if key not in _SYS:
+        _SYS[key] = O.assemble_heat(W.heat_cube(n, sigma=sigma, seed=seed, source=source))
+    return _SYS[key]
+
+
+def stress(nx, ny, nz):
+    key = ("stress", nx, ny, nz)
+    if key not in _SYS:
+        _SYS[key] = O.assemble_stress(W.stress_beam(nx, ny, nz))
+    return _SYS[key]
+
+
+def oracle_tight(A, b, prec=1, block=1):
+    x, st = O.solve(A, b, prec=prec, block_size=block, n_outer=200000, stop_rule="true", rtol=1e-12)
+    assert st.converged == 1
+    return x
+
+
+def ragged_csr(n=600, seed=0):
+    """Random square CSR with empty rows, short rows and rows longer than one warp chunk."""
+    rng = np.random.default_rng(seed)
+    lens = rng.integers(0, 20, n)
+    lens[::97] = 0
+    lens[5] = 700  # longer than the 512-product chunk buffer
+    lens[300:340] = 40
+    rp = np.zeros(n + 1, np.uint32)
+    rp[1:] = np.cumsum(lens)
+    ci = np.concatenate([np.sort(rng.choice(n, size=min(l, n), replace=False)) for l in lens]).astype(np.uint32)
+    rp[1:] = np.cumsum([min(l, n) for l in lens])
+    val = rng.standard_normal(ci.shape[0])
+    return O.CSR(n, rp, ci, val)
+
+
+def test_golden_vectors_gpu(ctx):
+    conf = rsg.make_conf(n_outer=1000, n_inner=1000, cvg=1e-13)
+    s = rsg.Solver(ctx, conf)
+    D = np.array([[4.0, 1.0], [1.0, 3.0]])
+    A = O.csr_from_dense(D)
+    x, st = s.solve((A.rp, A.ci, A.val), np.array([1.0, 2.0]))
+    assert abs(x[0] - 1 / 11) < 1e-6 and abs(x[1] - 7 / 11) < 1e-6
+    A = O.csr_from_dense(np.diag([2.0, 4.0, 5.0]))
+    x, st = s.solve((A.rp, A.ci, A.val), np.array([6.0, 8.0, 10.0]))
+    assert np.allclose(x, [3, 2, 2], atol=1e-6)
+
+
+@pytest.mark.parametrize("which", ["heat", "ragged", "stress"])
+def test_spmv_fp64_and_fp32_match_oracle(ctx, torch_cuda, which):
+    torch = torch_cuda
+    if which == "heat":
+        A, _ = heat(12, sigma=1.0, seed=1)
+    elif which == "ragged":
+        A = ragged_csr()
+    else:
+        A, _ = stress(6, 3, 3)
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    assert M.frobenius == pytest.approx(O.frobenius(A), rel=1e-13)
+    x = np.random.default_rng(2).standard_normal(A.n)
+    y_ref = O.spmv(A, x)
+    absrow = O.spmv(O.CSR(A.n, A.rp, A.ci, np.abs(A.val)), np.abs(x))
+    xd = torch.tensor(x, device="cuda")
+    yd = torch.empty_like(xd)
+    ctx.spmv(M, xd, yd)
+    ctx.sync()
+    assert np.all(np.abs(yd.cpu().numpy() - y_ref) <= 1e-13 * absrow + 1e-300)
+    x32 = torch.tensor(x, device="cuda", dtype=torch.float32)
+    y32 = torch.empty_like(x32)
+    ctx.spmv_f32(M, x32, y32)
+    ctx.sync()
+    assert np.all(np.abs(y32.cpu().numpy().astype(np.float64) - y_ref) <= 2e-6 * absrow + 1e-30)
+
+
+def test_preconditioner_builds_match_oracle(ctx, torch_cuda):
+    torch = torch_cuda
+    A, _ = stress(4, 2, 2)
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    d = torch.empty(A.n, dtype=torch.float64, device="cuda")
+    ctx.jacobi(M, d)
+    ctx.sync()
+    assert np.array_equal(d.cpu().numpy(), O.jacobi(A))
+    blocks = torch.empty(A.n * 3, dtype=torch.float64, device="cuda")
+    w = ctx.block_jacobi(M, 3, blocks)
+    B, w_ref = O.block_jacobi(A, 3)
+    assert w == w_ref == 3
+    assert np.allclose(blocks.cpu().numpy().reshape(A.n, 3), B, rtol=1e-12, atol=1e-16 * np.abs(B).max())
+
+
+def test_cg_reference_rule_parity_small_heat(ctx):
+    # the reference's small configuration: 20^3 hexes, k=1, unit source, Jacobi-PCG, cvg 1e-10
+    A, b = heat(20)
+    conf = rsg.make_conf(n_outer=5000, cvg=1e-10)
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    x, st = ctx.solve(M, b, conf=conf, prec=rsg.PREC_JACOBI)
+    xo, sto = O.solve(A, b, prec=1, n_outer=5000, cvg=1e-10)
+    assert st.status == rsg.OK and st.converged == 1
+    assert abs(int(st.iterations) - int(sto.iterations)) <= 2
+    assert st.error < 1e-10
+    assert rel_err(x, xo) < 1e-8
+    assert st.true_relres == pytest.approx(sto.true_relres, rel=0.2)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_cg_true_residual_lognormal(ctx, precision, use_graph):
+    A, b = heat(20, sigma=1.5, seed=0, source="random")
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    conf = rsg.make_conf(n_outer=20000, stop_rule="true", rtol=1e-10, precision=precision, use_graph=use_graph)
+    x, st = ctx.solve(M, b, conf=conf, prec=rsg.PREC_JACOBI)
+    assert st.status == rsg.OK and st.converged == 1
+    assert st.true_relres <= 1e-10
+    assert O.true_relres(A, b, x) <= 1.0e-10
+    err = rel_err(x, oracle_tight(A, b))
+    print(f"{precision} graph={use_graph}: iters={st.iterations} updates={st.outer} relres={st.true_relres:.3e} "
+          f"err={err:.3e}")
+    assert err <= 1e-8
+    _, sto = O.solve(A, b, prec=1, n_outer=20000, stop_rule="true", rtol=1e-10)
+    assert st.iterations <= 1.3 * sto.iterations + 5
+
+
+def test_graph_and_host_loop_are_bitwise_identical(ctx):
+    A, b = heat(14, sigma=1.0, seed=5, source="random")
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    xs = []
+    for g in (True, False, True):
+        conf = rsg.make_conf(n_outer=20000, stop_rule="true", rtol=1e-10, use_graph=g)
+        x, st = ctx.solve(M, b, conf=conf)
+        xs.append(x)
+    assert np.array_equal(xs[0], xs[1]) and np.array_equal(xs[0], xs[2])
+
+
+@pytest.mark.parametrize("stop", ["reference", "true"])
+def test_gmres_parity(ctx, stop):
+    A, b = heat(10, sigma=1.0, seed=2, source="random")
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    kw = dict(solver="gmres", n_outer=500, n_inner=30, cvg=1e-11, stop_rule=stop, rtol=1e-10)
+    x, st = ctx.solve(M, b, conf=rsg.make_conf(**kw), prec=rsg.PREC_JACOBI)
+    xo, sto = O.solve(A, b, prec=1, **kw)
+    assert st.converged == 1
+    assert abs(int(st.outer) - int(sto.outer)) <= 1
+    assert abs(int(st.iterations) - int(sto.iterations)) <= 3
+    assert rel_err(x, xo) < 1e-7
+    if stop == "true":
+        assert st.true_relres <= 1e-10
+
+
+def test_gmres_nonsymmetric_block_jacobi(ctx):
+    rng = np.random.default_rng(7)
+    n = 60
+    D = np.diag(4.0 + rng.random(n)) + 0.3 * rng.standard_normal((n, n)) * (rng.random((n, n)) < 0.1)
+    A = O.csr_from_dense(D)
+    b = rng.standard_normal(n)
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    kw = dict(solver="gmres", n_outer=100, n_inner=10, stop_rule="true", rtol=1e-11)
+    x, st = ctx.solve(M, b, conf=rsg.make_conf(**kw), prec=rsg.PREC_BLOCK_JACOBI, block_size=3)
+    assert rel_err(x, np.linalg.solve(D, b)) < 1e-9
+
+
+@pytest.mark.parametrize("prec,block", [(rsg.PREC_JACOBI, 1), (rsg.PREC_BLOCK_JACOBI, 3), (rsg.PREC_NONE, 1)])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_stress_cg_preconditioners(ctx, prec, block, precision):
+    A, b = stress(8, 4, 4)
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    conf = rsg.make_conf(n_outer=50000, stop_rule="true", rtol=1e-10, precision=precision)
+    x, st = ctx.solve(M, b, conf=conf, prec=prec, block_size=block)
+    assert st.status == rsg.OK
+    assert st.true_relres <= 1e-10
+    assert rel_err(x, oracle_tight(A, b, prec=max(prec, 1), block=block)) <= 1e-8
+
+
+def test_deterministic_repeat_and_device_arrays(ctx, torch_cuda):
+    torch = torch_cuda
+    A, b = heat(12, sigma=1.5, seed=9, source="random")
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    conf = rsg.make_conf(n_outer=20000, stop_rule="true", rtol=1e-10)
+    x1, _ = ctx.solve(M, b, conf=conf)
+    x2, _ = ctx.solve(M, b, conf=conf)
+    assert np.array_equal(x1, x2)
+    bd = torch.tensor(b, device="cuda")
+    xd = torch.zeros_like(bd)
+    _, st = ctx.solve(M, bd, xd, conf=conf)
+    assert np.array_equal(xd.cpu().numpy(), x1)
+
+
+def test_update_values_same_pattern(ctx):
+    A, b = heat(10)
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    conf = rsg.make_conf(n_outer=20000, stop_rule="true", rtol=1e-11)
+    x1, _ = ctx.solve(M, b, conf=conf)
+    M.update_values(2.0 * A.val)
+    assert M.frobenius == pytest.approx(2.0 * O.frobenius(A), rel=1e-13)
+    x2, _ = ctx.solve(M, b, conf=conf)
+    assert rel_err(2.0 * x2, x1) < 1e-9
+
+
+def test_solver_cache_mirrors_reference(ctx):
+    A, b = heat(8)
+    s = rsg.Solver(ctx, rsg.make_conf(n_outer=5000, stop_rule="true", rtol=1e-11))
+    rp, ci, val = A.rp, A.ci, A.val.copy()
+    x1, _ = s.solve((rp, ci, val), b, prec=rsg.PREC_JACOBI)
+    val *= 4.0
+    x2, _ = s.solve((rp, ci, val), b, prec=rsg.PREC_JACOBI)
+    assert len(s._cache) == 1
+    assert rel_err(4.0 * x2, x1) < 1e-9
+
+
+# ---------------- edge cases and failure reporting ----------------
+
+def test_zero_rhs_returns_zero(ctx):
+    A, _ = heat(6)
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    for stop in ("reference", "true"):
+        x, st = ctx.solve(M, np.zeros(A.n), conf=rsg.make_conf(stop_rule=stop))
+        assert np.all(x == 0.0)
+
+
+def test_iteration_cap_reports_not_converged(ctx):
+    A, b = heat(12, sigma=1.5, seed=1, source="random")
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    for precision in ("fp64", "mixed"):
+        x, st = ctx.solve(M, b, conf=rsg.make_conf(n_outer=7, stop_rule="true", precision=precision))
+        assert st.status == rsg.NOT_CONVERGED and st.iterations == 7 and st.converged == 0
+
+
+def test_nan_rhs_reports_breakdown(ctx):
+    A, b = heat(6)
+    b = b.copy()
+    b[3] = np.nan
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    for stop in ("reference", "true"):
+        x, st = ctx.solve(M, b, conf=rsg.make_conf(stop_rule=stop))
+        assert st.status == rsg.BREAKDOWN
+
+
+def test_invalid_inputs_are_rejected(ctx):
+    A, b = heat(4)
+    bad = A.ci.copy()
+    bad[7] = A.n + 5
+    with pytest.raises(rsg.RsgError) as e:
+        ctx.matrix(A.rp, bad, A.val)
+    assert e.value.status == rsg.ERR_INVALID_ARG
+    rp = A.rp.copy()
+    rp[3], rp[4] = rp[4], rp[3]
+    with pytest.raises(rsg.RsgError):
+        ctx.matrix(rp, A.ci, A.val)
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    c = rsg.make_conf()
+    c.solver_type = 7
+    with pytest.raises(rsg.RsgError) as e:
+        ctx.solve(M, b, conf=c)
+    assert e.value.status == rsg.ERR_INVALID_ARG
+    with pytest.raises(rsg.RsgError):
+        ctx.solve(M, b, prec=9)
+    with pytest.raises(rsg.RsgError):
+        ctx.solve(M, b, conf=rsg.make_conf(precision="mixed", stop_rule="reference"))
+
+
+def test_singular_block_is_reported(ctx):
+    D = np.eye(6)
+    D[0:3, 0:3] = [[1, 2, 3], [2, 4, 6], [1, 1, 1]]
+    A = O.csr_from_dense(D)
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    with pytest.raises(rsg.RsgError) as e:
+        ctx.solve(M, np.ones(6), prec=rsg.PREC_BLOCK_JACOBI, block_size=3)
+    assert e.value.status == rsg.ERR_SINGULAR
+
+
+def test_convergence_log_file(ctx, tmp_path):
+    A, b = heat(6)
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    f = tmp_path / "cvg.txt"
+    conf = rsg.make_conf(n_outer=5000, cvg=1e-10, output_frequency=5, output_file=str(f))
+    x, st = ctx.solve(M, b, conf=conf)
+    lines = f.read_text().splitlines()
+    assert lines[0] == "Iteration number|Solver residual|Solver convergence"
+    its = [int(l.split("|")[0]) for l in lines[1:]]
+    assert its[0] == 1 and its[-1] == st.iterations and all(i % 5 == 1 for i in its[:-1])
