@@ -1,0 +1,346 @@
+"""Benchmark: time-to-solve of the heterogeneous-heat system on B200.
+
+Workload ("heat_lognormal_100"): unit cube, 100^3 hexes -> 6,000,000 linear
+tets, 1,030,301 nodes (1,009,899 free DOFs), per-tet conductivity
+lognormal(0, 1.5), per-node source U(0,1) averaged per tet, T=0 / T=1 on
+x=0 / x=1; target FP64 true relative residual 1e-10.  Inputs are generated
+from seeds (synthetic data of the stated shape; no dataset is involved).
+
+One step = one solve of that system to 1e-10 with the library's fastest
+solver (mixed-precision Jacobi-PCG with reliable updates), matrix and
+right-hand side resident in HBM, x zeroed in the step.  The plain FP64
+Jacobi-PCG drop-in is timed the same way and reported beside it.  Steps are
+timed with CUDA events on the library's stream, L2 is flushed (256 MB write)
+between steps, and the max over ranks is taken.  With --gpus N each rank
+solves its own replica (different seed): the path does not shard, so this is
+weak scaling of independent replicas, no collective on the data path.
+
+`--impl reference` times the reference algorithm's CPU implementation (the
+OpenMP oracle, a restatement of RMatrixSolver::solveCG + Jacobi) on all host
+cores on the same system, one full solve per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "range-solver-lib_b200"))
+sys.path.insert(0, REPO)
+
+METRIC = "time-to-solve (s) at FP64 rel. residual 1e-10: learned/mixed vs plain GPU PCG"
+UNIT = "s"
+N_HEX = int(os.environ.get("RSG_BENCH_N", "100"))
+SIGMA = 1.5
+RTOL = 1e-10
+
+
+def load_peaks() -> tuple[float, str]:
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        rows = [r.split(",") for r in getattr(self, "out", "").strip().splitlines() if r.count(",") >= 8]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i] and "Not" not in r[5 + i]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def build_problem(seed: int):
+    from rsg import workloads as W
+    return W.heat_cube(N_HEX, sigma=SIGMA, seed=seed, source="random")
+
+
+def spmv_bytes(n: int, nnz: int, val_bytes: int, idx_bytes: int, vec_bytes: int) -> int:
+    """Algorithmic bytes of the fused CG direction kernel: matrix values + column
+    indexes + row pointer, gathered z and p_old read once, p_new and q written once."""
+    return nnz * (val_bytes + idx_bytes) + 4 * (n + 1) + 4 * n * vec_bytes
+
+
+def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
+    import torch
+    import rsg
+
+    torch.cuda.set_device(local_rank)
+    ctx = rsg.Context(local_rank)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)  # torch ops and the library share one stream
+    ctx.set_stream(stream.cuda_stream)
+    p = build_problem(seed=rank)
+    asm = rsg.Assembly.heat(ctx, p)
+    n = asm.n_free
+    b = torch.empty(n, dtype=torch.float64, device="cuda")
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    A = asm.assemble(p, b)
+    # assembly timing (numeric phase, plan already built)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    asm_ms = []
+    for _ in range(3):
+        ev[0].record(stream)
+        asm.assemble(p, b)
+        ev[1].record(stream)
+        ev[1].synchronize()
+        asm_ms.append(ev[0].elapsed_time(ev[1]))
+
+    conf_mixed = rsg.make_conf(n_outer=50000, stop_rule="true", rtol=RTOL, precision="mixed",
+                               reliable_delta=args.delta)
+    conf_fp64 = rsg.make_conf(n_outer=50000, stop_rule="true", rtol=RTOL, precision="fp64")
+
+    def step(conf):
+        flush.fill_(1)  # evict L2 between steps (not timed)
+        x.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _, st = ctx.solve(A, b, x, conf=conf)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3, st
+
+    for _ in range(args.warmup):
+        step(conf_mixed)
+    step(conf_fp64)
+
+    def timed(conf, k):
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+        tot, stats = 0.0, None
+        for _ in range(k):
+            t, stats = step(conf)
+            tot += t
+        torch.cuda.synchronize()
+        if world > 1:
+            import torch.distributed as dist
+            tt = torch.tensor([tot], dtype=torch.float64, device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            tot = float(tt.item())
+        return tot / k, stats
+
+    sampler = ClockSampler(local_rank)
+    with sampler:
+        t_mixed, st_m = timed(conf_mixed, args.steps)
+    t_fp64, st_f = timed(conf_fp64, max(1, args.steps))
+    x_mixed_ok = st_m.true_relres <= RTOL
+
+    # accuracy of the mixed solution against the FP64 one (both at 1e-10)
+    _, st_m = ctx.solve(A, b, x.zero_(), conf=conf_mixed)
+    x_m = x.clone()
+    _, st_f = ctx.solve(A, b, x.zero_(), conf=conf_fp64)
+    err_vs_fp64 = float(torch.linalg.norm(x_m - x) / torch.linalg.norm(x))
+
+    # dominant kernels, timed live (HBM-bound: L2 flushed before each launch)
+    kd = {}
+    for name, kid in (("cg_dir_fp64", 0), ("cg_dir_mixed", 1), ("cg_update_fp64", 2),
+                      ("cg_update_mixed", 3)):
+        kd[name] = {"cold_s": ctx.profile_kernel(A, kid, reps=10, flush_l2=True),
+                    "warm_s": ctx.profile_kernel(A, kid, reps=20, flush_l2=False)}
+    nnz = A.nnz
+    peak, peak_kind = load_peaks()
+    by64 = spmv_bytes(n, nnz, 8, 2, 8)
+    by32 = spmv_bytes(n, nnz, 4, 2, 4)
+    achieved64 = by64 / kd["cg_dir_fp64"]["cold_s"] / 1e9
+    achieved32 = by32 / kd["cg_dir_mixed"]["cold_s"] / 1e9
+    traffic = None
+    tf = os.path.join(REPO, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        try:
+            traffic = json.load(open(tf)).get("cg_dir_mixed_bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    # launches per solve: setup (norm, 2 scalings, Jacobi, FP32 copy, init residual + z, fold,
+    # unscale, true residual) + per 2-iteration graph body (3 kernels per iteration + tail)
+    def launches(st, mixed):
+        bodies = (st.iterations + 1) // 2
+        return 10 + bodies * 7 + (1 if mixed else 0)
+
+    # end to end through the reference-facing API with pinned host buffers
+    rp_h, ci_h, val_h = A.to_host()
+    val_pin = torch.from_numpy(val_h).pin_memory().numpy()
+    b_pin = torch.empty(n, dtype=torch.float64).pin_memory()
+    b_pin.copy_(b.cpu())
+    b_pin = b_pin.numpy()
+    x_pin = torch.zeros(n, dtype=torch.float64).pin_memory().numpy()
+    e2e = []
+    for i in range(max(2, min(args.steps, 5))):
+        x_pin[:] = 0.0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        A.update_values(val_pin)  # the reference re-reads A's values on every solve (src/rmatrixsolver.cpp:56-97)
+        xs, st_e = ctx.solve(A, b_pin, x_pin, conf=conf_mixed)
+        t1 = time.perf_counter()
+        if i > 0:
+            e2e.append(t1 - t0)
+    e2e_s = float(np.mean(e2e))
+
+    out = {
+        "t_mixed": t_mixed, "t_fp64": t_fp64, "st_m": st_m, "st_f": st_f, "ok": x_mixed_ok,
+        "err_vs_fp64": err_vs_fp64, "kd": kd, "achieved64": achieved64, "achieved32": achieved32, "peak": peak,
+        "peak_kind": peak_kind, "by64": by64, "by32": by32, "traffic": traffic, "n": n, "nnz": nnz,
+        "asm_ms": float(np.median(asm_ms)), "clocks": sampler.summary(), "e2e_s": e2e_s,
+        "h2d": int(nnz * 8 + 2 * n * 8), "d2h": int(n * 8), "launches": launches(st_m, True),
+        "launches_fp64": launches(st_f, False), "ctx": ctx, "A": A, "b": b, "rp": rp_h, "ci": ci_h, "val": val_h,
+    }
+    return out
+
+
+def cpu_baseline(rp, ci, val, b, threads: int) -> dict:
+    from oracle import oracle as O
+    Ah = O.CSR(len(rp) - 1, rp, ci, val)
+    x, st = O.solve(Ah, b, prec=1, n_outer=50000, stop_rule="true", rtol=RTOL, threads=threads)
+    return {"value": st.seconds, "iterations": st.iterations, "relres": st.true_relres}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--delta", type=float, default=1e-2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    threads = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from oracle import oracle as O
+        p = build_problem(seed=0)
+        t0 = time.perf_counter()
+        Ah, bh = O.assemble_heat(p)
+        t_asm = time.perf_counter() - t0
+        times = []
+        st = None
+        for i in range(args.warmup + args.steps):
+            x, st = O.solve(Ah, bh, prec=1, n_outer=50000, stop_rule="true", rtol=RTOL, threads=threads)
+            if i >= args.warmup:
+                times.append(st.seconds)
+        v = float(np.mean(times))
+        print(json.dumps({
+            "metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"heat_lognormal_{N_HEX}", "n_free": Ah.n, "nnz": Ah.nnz, "sigma": SIGMA,
+                       "rtol": RTOL, "solver": "Jacobi-PCG FP64 (OpenMP oracle restating RMatrixSolver::solveCG)",
+                       "iterations": st.iterations, "true_relres": st.true_relres, "assembly_s_serial": t_asm},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": "one full Jacobi-PCG solve of the 100^3 system per step"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }), flush=True)
+        return
+
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+
+    r = run_ours(args, rank, world, local_rank)
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(r["rp"], r["ci"], r["val"], r["b"].cpu().numpy(), threads)
+    st_m, st_f = r["st_m"], r["st_f"]
+    kd = r["kd"]
+    line = {
+        "metric": METRIC, "value": r["t_mixed"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["t_mixed"] * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32-inner/f64-outer", "data": "synthetic (seeded lognormal heat, 100^3 hexes)",
+        "config": {"workload": f"heat_lognormal_{N_HEX}", "n_free": r["n"], "nnz": r["nnz"], "sigma": SIGMA,
+                   "rtol": RTOL, "solver": "mixed-precision Jacobi-PCG, reliable updates",
+                   "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}",
+                   "iterations": st_m.iterations, "residual_refreshes": st_m.outer,
+                   "true_relres": st_m.true_relres, "err_vs_fp64_solution": r["err_vs_fp64"],
+                   "plain_fp64_pcg_s": r["t_fp64"], "plain_fp64_iterations": st_f.iterations,
+                   "plain_fp64_true_relres": st_f.true_relres,
+                   "speedup_vs_plain_fp64": r["t_fp64"] / r["t_mixed"],
+                   "assembly_numeric_s": r["asm_ms"] / 1e3,
+                   "fp64_ms_per_iteration": r["t_fp64"] / max(st_f.iterations, 1) * 1e3,
+                   "mixed_ms_per_iteration": r["t_mixed"] / max(st_m.iterations, 1) * 1e3},
+        "roofline": {"bound": "hbm", "kernel": "k_mx_dir (fused FP32 CG direction + SpMV)",
+                     "achieved": r["achieved32"], "peak": r["peak"], "unit": "GB/s",
+                     "frac": r["achieved32"] / r["peak"], "traffic": r["traffic"],
+                     "algorithmic_bytes": r["by32"], "avg_launch_s": kd["cg_dir_mixed"]["cold_s"],
+                     "peak_source": r["peak_kind"]},
+        "roofline_fp64": {"bound": "hbm", "kernel": "k_cg_dir (fused FP64 CG direction + SpMV)",
+                          "achieved": r["achieved64"], "peak": r["peak"], "unit": "GB/s",
+                          "frac": r["achieved64"] / r["peak"], "algorithmic_bytes": r["by64"],
+                          "avg_launch_s": kd["cg_dir_fp64"]["cold_s"], "peak_source": r["peak_kind"]},
+        "kernels": kd,
+        "e2e": {"value": r["e2e_s"], "unit": UNIT, "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"],
+                "api": "rsg_csr_update_values + rsg_solve with pinned host buffers"},
+        "gpu_launches": r["launches"] * args.steps,
+        "clocks": r["clocks"],
+    }
+    if cpu:
+        line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": "one full FP64 Jacobi-PCG solve (OpenMP oracle) of the same system",
+                                "iterations": cpu["iterations"], "true_relres": cpu["relres"]}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -84,7 +84,8 @@ typedef struct {
     uint32_t check_interval;    /* host-driven loop: iterations per convergence poll */
     const void *learned;        /* rsg_learned* for RSG_PREC_LEARNED / learned initial guess */
     int32_t  learned_initial_guess;
-    int32_t  reserved[7];
+    int32_t  l2_resident_f32;   /* mixed: stream the FP32 matrix with L2 evict_last (it fits in L2 up to ~1.3M rows) */
+    int32_t  reserved[6];
 } rsg_solver_conf;
 
 typedef struct {
@@ -157,6 +158,22 @@ RSG_API rsg_status rsg_block_jacobi_build(rsg_context *ctx, const rsg_csr *A, ui
  * device arrays of n_rows doubles according to `memory`. */
 RSG_API rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_conf *conf, int32_t prec_type,
                              uint32_t block_size, const double *b, double *x, int32_t memory, rsg_stats *stats);
+
+/* Diagnostic (no reference counterpart): average device time in seconds of one
+ * of the solver's kernels on matrix A over `reps` launches on the context
+ * stream, measured with CUDA events.  flush_l2 != 0 writes a buffer larger
+ * than L2 before every launch (excluded from the timing), giving the
+ * HBM-bound time; 0 measures back-to-back launches as inside a solve. */
+typedef enum {
+    RSG_KERNEL_CG_DIR_FP64 = 0,    /* p = z + beta p, q = A p, p^T q   (FP64 CSR) */
+    RSG_KERNEL_CG_DIR_MIXED = 1,   /* same with FP32 values and 16-bit column offsets */
+    RSG_KERNEL_CG_UPDATE_FP64 = 2, /* x, r update + Jacobi + dots */
+    RSG_KERNEL_CG_UPDATE_MIXED = 3,
+    RSG_KERNEL_SPMV_FP64 = 4,
+    RSG_KERNEL_SPMV_FP32 = 5
+} rsg_kernel_id;
+RSG_API rsg_status rsg_profile_kernel(rsg_context *ctx, const rsg_csr *A, int32_t kernel, uint32_t reps,
+                                      int32_t flush_l2, double *seconds);
 
 /* FP64 true relative residual ||b - A x|| / ||b|| (device pointers). */
 RSG_API rsg_status rsg_true_relres(rsg_context *ctx, const rsg_csr *A, const double *b, const double *x,

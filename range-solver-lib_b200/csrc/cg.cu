@@ -28,6 +28,7 @@
 #include "krylov.cuh"
 
 #include <cmath>
+#include <cstring>
 
 namespace rsg {
 
@@ -156,12 +157,11 @@ __device__ __forceinline__ double clamp_pq(double pq, double eps)
 // ---------------- FP64 kernels ----------------
 
 template <int RPW>
-__global__ void __launch_bounds__(kBlock) k_cg_init_res(Csr<double> M, const double *__restrict__ b,
+__global__ void __launch_bounds__(kBlock) k_cg_init_res(Csr<double> M, Sell<double> S, int use_sell, const double *__restrict__ b,
                                                         const double *__restrict__ x, double *__restrict__ r,
                                                         double *partials, CgState *st)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *prod = reinterpret_cast<double *>(smem_raw);
     __shared__ double sh[64];
     double acc[2] = {0.0, 0.0};
     auto gx = [&](uint32_t c) { return x[c]; };
@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(kBlock) k_cg_init_res(Csr<double> M, const dou
         acc[0] += ri * ri;
         acc[1] += b[row] * b[row];
     };
-    for_rows<double, double, RPW>(M, gx, epi, prod);
+    for_rows_any<double, RPW>(M, S, use_sell != 0, gx, epi, smem_raw, &st->ticket[7], true);
     double tot[2];
     if (grid_sum<2>(acc, partials, &st->ticket[3], sh, tot) && threadIdx.x == 0) {
         st->rn = sqrt(tot[0]);
@@ -233,12 +233,11 @@ __global__ void __launch_bounds__(kBlock) k_cg_prec(uint32_t n, uint32_t w, cons
 }
 
 template <int RPW>
-__global__ void __launch_bounds__(kBlock) k_cg_dir(Csr<double> M, const double *__restrict__ z,
+__global__ void __launch_bounds__(kBlock) k_cg_dir(Csr<double> M, Sell<double> S, int use_sell, const double *__restrict__ z,
                                                    const double *__restrict__ p_old, double *__restrict__ p_new,
                                                    double *__restrict__ q, double *partials, CgState *st)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *prod = reinterpret_cast<double *>(smem_raw);
     __shared__ double sh[32];
     if (st->done) return;
     const double beta = st->beta;
@@ -250,7 +249,7 @@ __global__ void __launch_bounds__(kBlock) k_cg_dir(Csr<double> M, const double *
         q[row] = v;
         acc[0] += p * v;
     };
-    for_rows<double, double, RPW>(M, gx, epi, prod);
+    for_rows_any<double, RPW>(M, S, use_sell != 0, gx, epi, smem_raw, &st->ticket[7], true);
     double tot[1];
     if (grid_sum<1>(acc, partials, &st->ticket[0], sh, tot) && threadIdx.x == 0) {
         const double pq = clamp_pq(tot[0], st->eps);
@@ -269,21 +268,62 @@ __global__ void __launch_bounds__(kBlock) k_cg_update(uint32_t n, uint32_t w, co
     __shared__ double sh[96];
     if (st->done) return;
     const double alpha = st->alpha;
-    const uint32_t G = PK == 2 ? w : 1, ng = n / G;
     double acc[3] = {0.0, 0.0, 0.0};
-    double rl[kMaxBlock];
-    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
-        for (uint32_t k = 0; k < G; k++) {
-            const size_t i = size_t(g) * G + k;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    if (PK < 2) {
+        // two rows per thread with 16-byte loads (vectors are 256-byte aligned)
+        const uint32_t npair = n / 2;
+        auto row2 = [&](double2 pv, double2 qv, double2 xv, double2 rv, double2 dv, uint32_t i2) {
+            double2 xo, ro, zo;
+            xo.x = fma(alpha, pv.x, xv.x);
+            xo.y = fma(alpha, pv.y, xv.y);
+            ro.x = fma(-alpha, qv.x, rv.x);
+            ro.y = fma(-alpha, qv.y, rv.y);
+            zo.x = PK == 1 ? dv.x * ro.x : ro.x;
+            zo.y = PK == 1 ? dv.y * ro.y : ro.y;
+            reinterpret_cast<double2 *>(x)[i2] = xo;
+            reinterpret_cast<double2 *>(r)[i2] = ro;
+            reinterpret_cast<double2 *>(z)[i2] = zo;
+            acc[0] += ro.x * zo.x + ro.y * zo.y;
+            acc[1] += ro.x * ro.x + ro.y * ro.y;
+            acc[2] += xo.x * xo.x + xo.y * xo.y;
+        };
+        for (uint32_t i2 = tid; i2 < npair; i2 += stride) {
+            const double2 pv = reinterpret_cast<const double2 *>(p)[i2];
+            const double2 qv = reinterpret_cast<const double2 *>(q)[i2];
+            const double2 xv = reinterpret_cast<const double2 *>(x)[i2];
+            const double2 rv = reinterpret_cast<const double2 *>(r)[i2];
+            const double2 dv = PK == 1 ? reinterpret_cast<const double2 *>(d)[i2] : make_double2(1.0, 1.0);
+            row2(pv, qv, xv, rv, dv, i2);
+        }
+        if ((n & 1u) && tid == 0) {
+            const uint32_t i = n - 1;
             const double xi = fma(alpha, p[i], x[i]);
             const double ri = fma(-alpha, q[i], r[i]);
+            const double zi = PK == 1 ? d[i] * ri : ri;
             x[i] = xi;
             r[i] = ri;
+            z[i] = zi;
+            acc[0] += ri * zi;
             acc[1] += ri * ri;
             acc[2] += xi * xi;
-            rl[k] = ri;
         }
-        acc[0] += prec_group64<PK>(g, w, d, rl, z);
+    } else {
+        const uint32_t G = w, ng = n / G;
+        double rl[kMaxBlock];
+        for (uint32_t g = tid; g < ng; g += stride) {
+            for (uint32_t k = 0; k < G; k++) {
+                const size_t i = size_t(g) * G + k;
+                const double xi = fma(alpha, p[i], x[i]);
+                const double ri = fma(-alpha, q[i], r[i]);
+                x[i] = xi;
+                r[i] = ri;
+                acc[1] += ri * ri;
+                acc[2] += xi * xi;
+                rl[k] = ri;
+            }
+            acc[0] += prec_group64<PK>(g, w, d, rl, z);
+        }
     }
     double tot[3];
     if (grid_sum<3>(acc, partials, &st->ticket[1], sh, tot) && threadIdx.x == 0)
@@ -291,13 +331,12 @@ __global__ void __launch_bounds__(kBlock) k_cg_update(uint32_t n, uint32_t w, co
 }
 
 template <int RPW, int PK>
-__global__ void __launch_bounds__(kBlock) k_cg_check(Csr<double> M, const double *__restrict__ d,
+__global__ void __launch_bounds__(kBlock) k_cg_check(Csr<double> M, Sell<double> S, int use_sell, const double *__restrict__ d,
                                                      const double *__restrict__ b, const double *__restrict__ x,
                                                      double *__restrict__ r, double *__restrict__ z,
                                                      double *partials, CgState *st)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *prod = reinterpret_cast<double *>(smem_raw);
     __shared__ double sh[64];
     if (st->done || !st->need_check) return;
     double acc[2] = {0.0, 0.0};
@@ -315,7 +354,7 @@ __global__ void __launch_bounds__(kBlock) k_cg_check(Csr<double> M, const double
             acc[0] += ri * zi;
         }
     };
-    for_rows<double, double, RPW>(M, gx, epi, prod);
+    for_rows_any<double, RPW>(M, S, use_sell != 0, gx, epi, smem_raw, &st->ticket[7], true);
     double tot[2];
     if (grid_sum<2>(acc, partials, &st->ticket[2], sh, tot) && threadIdx.x == 0) {
         if (PK == 2) st->check_rn = sqrt(tot[1]);
@@ -383,13 +422,12 @@ __global__ void __launch_bounds__(kBlock) k_mx_prec(uint32_t n, uint32_t w, cons
 }
 
 template <int RPW>
-__global__ void __launch_bounds__(kBlock) k_mx_dir(Csr<float> M, const float *__restrict__ z,
+__global__ void __launch_bounds__(kBlock) k_mx_dir(Csr<float> M, Sell<float> S, int use_sell, const float *__restrict__ z,
                                                    const float *__restrict__ p_old, float *__restrict__ p_new,
                                                    float *__restrict__ q, double *__restrict__ x,
                                                    float *__restrict__ y, double *partials, CgState *st)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    float *prod = reinterpret_cast<float *>(smem_raw);
     __shared__ double sh[32];
     if (st->done) return;
     const float beta = float(st->beta);
@@ -407,7 +445,7 @@ __global__ void __launch_bounds__(kBlock) k_mx_dir(Csr<float> M, const float *__
             y[row] = 0.f;
         }
     };
-    for_rows<float, float, RPW>(M, gx, epi, prod);
+    for_rows_any<float, RPW>(M, S, use_sell != 0, gx, epi, smem_raw, &st->ticket[7], st->evict_first32 != 0);
     double acc[1] = {pq.value()};
     double tot[1];
     if (grid_sum<1>(acc, partials, &st->ticket[0], sh, tot) && threadIdx.x == 0) {
@@ -429,19 +467,65 @@ __global__ void __launch_bounds__(kBlock) k_mx_update(uint32_t n, uint32_t w, co
     __shared__ double sh[64];
     if (st->done) return;
     const float alpha = float(st->alpha);
-    const uint32_t G = PK == 2 ? w : 1, ng = n / G;
     Dot2 rz, rr;
-    float rl[kMaxBlock];
-    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
-        for (uint32_t k = 0; k < G; k++) {
-            const size_t i = size_t(g) * G + k;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    if (PK < 2) {
+        // four rows per thread with 16-byte loads (vectors are 256-byte aligned)
+        const uint32_t nq = n / 4;
+        for (uint32_t i4 = tid; i4 < nq; i4 += stride) {
+            const float4 pv = reinterpret_cast<const float4 *>(p)[i4];
+            const float4 qv = reinterpret_cast<const float4 *>(q)[i4];
+            float4 yv = reinterpret_cast<const float4 *>(y)[i4];
+            float4 rv = reinterpret_cast<const float4 *>(r)[i4];
+            const float4 dv = PK == 1 ? reinterpret_cast<const float4 *>(d)[i4] : make_float4(1.f, 1.f, 1.f, 1.f);
+            float4 zv;
+            yv.x = fmaf(alpha, pv.x, yv.x);
+            yv.y = fmaf(alpha, pv.y, yv.y);
+            yv.z = fmaf(alpha, pv.z, yv.z);
+            yv.w = fmaf(alpha, pv.w, yv.w);
+            rv.x = fmaf(-alpha, qv.x, rv.x);
+            rv.y = fmaf(-alpha, qv.y, rv.y);
+            rv.z = fmaf(-alpha, qv.z, rv.z);
+            rv.w = fmaf(-alpha, qv.w, rv.w);
+            zv.x = PK == 1 ? dv.x * rv.x : rv.x;
+            zv.y = PK == 1 ? dv.y * rv.y : rv.y;
+            zv.z = PK == 1 ? dv.z * rv.z : rv.z;
+            zv.w = PK == 1 ? dv.w * rv.w : rv.w;
+            reinterpret_cast<float4 *>(y)[i4] = yv;
+            reinterpret_cast<float4 *>(r)[i4] = rv;
+            reinterpret_cast<float4 *>(z)[i4] = zv;
+            rz.add_prod(rv.x, zv.x);
+            rz.add_prod(rv.y, zv.y);
+            rz.add_prod(rv.z, zv.z);
+            rz.add_prod(rv.w, zv.w);
+            rr.add_prod(rv.x, rv.x);
+            rr.add_prod(rv.y, rv.y);
+            rr.add_prod(rv.z, rv.z);
+            rr.add_prod(rv.w, rv.w);
+        }
+        for (uint32_t i = nq * 4 + tid; i < n; i += stride) {
             y[i] = fmaf(alpha, p[i], y[i]);
             const float ri = fmaf(-alpha, q[i], r[i]);
+            const float zi = PK == 1 ? d[i] * ri : ri;
             r[i] = ri;
+            z[i] = zi;
+            rz.add_prod(ri, zi);
             rr.add_prod(ri, ri);
-            rl[k] = ri;
         }
-        prec_group32<PK>(g, w, d, rl, z, rz);
+    } else {
+        const uint32_t G = w, ng = n / G;
+        float rl[kMaxBlock];
+        for (uint32_t g = tid; g < ng; g += stride) {
+            for (uint32_t k = 0; k < G; k++) {
+                const size_t i = size_t(g) * G + k;
+                y[i] = fmaf(alpha, p[i], y[i]);
+                const float ri = fmaf(-alpha, q[i], r[i]);
+                r[i] = ri;
+                rr.add_prod(ri, ri);
+                rl[k] = ri;
+            }
+            prec_group32<PK>(g, w, d, rl, z, rz);
+        }
     }
     double acc[2] = {rz.value(), rr.value()};
     double tot[2];
@@ -450,13 +534,12 @@ __global__ void __launch_bounds__(kBlock) k_mx_update(uint32_t n, uint32_t w, co
 }
 
 template <int RPW, int PK>
-__global__ void __launch_bounds__(kBlock) k_mx_check(Csr<double> M, const float *__restrict__ d,
+__global__ void __launch_bounds__(kBlock) k_mx_check(Csr<double> M, Sell<double> S, int use_sell, const float *__restrict__ d,
                                                      const double *__restrict__ b, const double *__restrict__ x,
                                                      const float *__restrict__ y, float *__restrict__ r32,
                                                      float *__restrict__ z, double *partials, CgState *st)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *prod = reinterpret_cast<double *>(smem_raw);
     __shared__ double sh[64];
     if (st->done || !st->need_check) return;
     const double sigma = st->sigma, inv_sigma = 1.0 / sigma;
@@ -477,7 +560,7 @@ __global__ void __launch_bounds__(kBlock) k_mx_check(Csr<double> M, const float 
             rz.add_prod(rf, zf);
         }
     };
-    for_rows<double, double, RPW>(M, gx, epi, prod);
+    for_rows_any<double, RPW>(M, S, use_sell != 0, gx, epi, smem_raw, &st->ticket[7], true);
     double acc[2] = {rz.value(), rr[0]};
     double tot[2];
     if (grid_sum<2>(acc, partials, &st->ticket[2], sh, tot) && threadIdx.x == 0) {
@@ -526,7 +609,9 @@ template <int RPW, int PK>
 void launch_init(rsg_context *ctx, const CgArgs &a, const Launch &L)
 {
     const Csr<double> M64 = view<double>(a.A, true);
-    k_cg_init_res<RPW><<<L.g_spmv64, kBlock, L.s64, ctx->stream>>>(M64, a.b, a.x, a.r, a.partials, a.st);
+    const Sell<double> S64 = sell_view<double>(a.A);
+    const int us = a.A->use_sell;
+    k_cg_init_res<RPW><<<L.g_spmv64, kBlock, L.s64, ctx->stream>>>(M64, S64, us, a.b, a.x, a.r, a.partials, a.st);
     if (!a.mixed)
         k_cg_prec<PK><<<L.g_vec, kBlock, 0, ctx->stream>>>(a.A->n, a.P.w, a.P.d, a.r, a.z, a.partials, a.st, 0);
     else
@@ -539,14 +624,18 @@ void launch_body(rsg_context *ctx, const CgArgs &a, const Launch &L, cudaGraphCo
 {
     const uint32_t n = a.A->n;
     const Csr<double> M64 = view<double>(a.A, true);
+    const Sell<double> S64 = sell_view<double>(a.A);
+    const Sell<float> S32 = sell_view<float>(a.A);
+    const int us = a.A->use_sell;
     if (!a.mixed) {
         for (int half = 0; half < 2; half++) {
             double *po = half ? a.p1 : a.p0, *pn = half ? a.p0 : a.p1;
-            k_cg_dir<RPW><<<L.g_spmv64, kBlock, L.s64, ctx->stream>>>(M64, a.z, po, pn, a.q, a.partials, a.st);
+            k_cg_dir<RPW><<<L.g_spmv64, kBlock, L.s64, ctx->stream>>>(M64, S64, us, a.z, po, pn, a.q, a.partials,
+                                                                      a.st);
             k_cg_update<PK><<<L.g_vec, kBlock, 0, ctx->stream>>>(n, a.P.w, a.P.d, pn, a.q, a.x, a.r, a.z, a.partials,
                                                                 a.st);
-            k_cg_check<RPW, PK><<<L.g_spmv64, kBlock, L.s64, ctx->stream>>>(M64, a.P.d, a.b, a.x, a.r, a.z,
-                                                                            a.partials, a.st);
+            k_cg_check<RPW, PK><<<L.g_spmv64, kBlock, L.s64, ctx->stream>>>(M64, S64, us, a.P.d, a.b, a.x, a.r,
+                                                                            a.z, a.partials, a.st);
             if (PK == 2)
                 k_cg_prec<PK><<<L.g_vec, kBlock, 0, ctx->stream>>>(n, a.P.w, a.P.d, a.r, a.z, a.partials, a.st, 1);
         }
@@ -554,12 +643,12 @@ void launch_body(rsg_context *ctx, const CgArgs &a, const Launch &L, cudaGraphCo
         const Csr<float> M32 = view<float>(a.A, true);
         for (int half = 0; half < 2; half++) {
             float *po = half ? a.p32b : a.p32a, *pn = half ? a.p32a : a.p32b;
-            k_mx_dir<RPW><<<L.g_spmv32, kBlock, L.s32, ctx->stream>>>(M32, a.z32, po, pn, a.q32, a.x, a.y32,
-                                                                      a.partials, a.st);
+            k_mx_dir<RPW><<<L.g_spmv32, kBlock, L.s32, ctx->stream>>>(M32, S32, us, a.z32, po, pn, a.q32, a.x,
+                                                                      a.y32, a.partials, a.st);
             k_mx_update<PK><<<L.g_vec, kBlock, 0, ctx->stream>>>(n, a.P.w, a.P.d32, pn, a.q32, a.y32, a.r32, a.z32,
                                                                 a.partials, a.st);
-            k_mx_check<RPW, PK><<<L.g_spmv64, kBlock, L.s64, ctx->stream>>>(M64, a.P.d32, a.b, a.x, a.y32, a.r32,
-                                                                            a.z32, a.partials, a.st);
+            k_mx_check<RPW, PK><<<L.g_spmv64, kBlock, L.s64, ctx->stream>>>(M64, S64, us, a.P.d32, a.b, a.x,
+                                                                            a.y32, a.r32, a.z32, a.partials, a.st);
             if (PK == 2)
                 k_mx_prec<PK><<<L.g_vec, kBlock, 0, ctx->stream>>>(n, a.P.w, a.P.d32, nullptr, a.r32, a.z32,
                                                                   a.partials, a.st, 1);
@@ -572,13 +661,13 @@ template <int RPW, int PK>
 rsg_status run_typed(rsg_context *ctx, const CgArgs &a, double *seconds)
 {
     Launch L;
-    L.s64 = prod_smem<double>();
-    L.s32 = prod_smem<float>();
-    set_smem(k_cg_init_res<RPW>, L.s64);
-    set_smem(k_cg_dir<RPW>, L.s64);
-    set_smem(k_cg_check<RPW, PK>, L.s64);
-    set_smem(k_mx_dir<RPW>, L.s32);
-    set_smem(k_mx_check<RPW, PK>, L.s64);
+    L.s64 = a.A->use_sell ? 0 : tma_smem<double>();
+    L.s32 = a.A->use_sell ? 0 : tma_smem<float>();
+    set_smem(k_cg_init_res<RPW>, tma_smem<double>());
+    set_smem(k_cg_dir<RPW>, tma_smem<double>());
+    set_smem(k_cg_check<RPW, PK>, tma_smem<double>());
+    set_smem(k_mx_dir<RPW>, tma_smem<float>());
+    set_smem(k_mx_check<RPW, PK>, tma_smem<double>());
     const long long chunk_threads = (long long)a.A->n * 32 / RPW;
     L.g_spmv64 = std::min(grid_for(ctx, (const void *)k_cg_dir<RPW>, kBlock, L.s64, chunk_threads), kMaxGrid);
     L.g_spmv32 = std::min(grid_for(ctx, (const void *)k_mx_dir<RPW>, kBlock, L.s32, chunk_threads), kMaxGrid);
@@ -663,6 +752,114 @@ rsg_status run_typed(rsg_context *ctx, const CgArgs &a, double *seconds)
 
 }  // namespace
 
+namespace {
+
+__global__ void k_flush(uint4 *buf, size_t n16, unsigned int salt)
+{
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n16; i += size_t(gridDim.x) * blockDim.x)
+        buf[i] = make_uint4(salt, salt, salt, salt);
+}
+
+template <int RPW>
+rsg_status profile_typed(rsg_context *ctx, const rsg_csr *A, int kernel, uint32_t reps, int flush, double *seconds)
+{
+    const uint32_t n = A->n;
+    const size_t flush_bytes = flush ? (size_t(256) << 20) : 0;
+    size_t bytes = 8 * arena_bytes(n, sizeof(double)) + arena_bytes(size_t(4) * kMaxGrid, sizeof(double)) +
+                   arena_bytes(1, sizeof(CgState)) + flush_bytes + 4096;
+    RSG_TRY(arena_reserve(ctx, bytes));
+    double *v64[5];
+    for (auto &p : v64) p = arena_take<double>(ctx, n);
+    float *v32[6];
+    for (auto &p : v32) p = arena_take<float>(ctx, n);
+    double *partials = arena_take<double>(ctx, size_t(4) * kMaxGrid);
+    CgState *st = arena_take<CgState>(ctx, 1);
+    uint4 *fbuf = flush ? reinterpret_cast<uint4 *>(arena_take<char>(ctx, flush_bytes)) : nullptr;
+    for (auto p : v64) RSG_CHECK_CUDA(ctx, cudaMemsetAsync(p, 0, size_t(n) * sizeof(double), ctx->stream));
+    for (auto p : v32) RSG_CHECK_CUDA(ctx, cudaMemsetAsync(p, 0, size_t(n) * sizeof(float), ctx->stream));
+    CgState h;
+    std::memset(&h, 0, sizeof(h));
+    h.beta = 0.5;
+    h.alpha = 0.25;
+    h.rho = h.rho_new = 1.0;
+    h.sigma = 1.0;
+    h.eps = 1e-300;
+    h.max_it = 0xffffffffu;
+    h.stop_rule = RSG_STOP_TRUE_RELRES;
+    h.rtol = 0.0;
+    h.delta = 0.0;
+    h.bn = 1.0;
+    RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(st, &h, sizeof(h), cudaMemcpyHostToDevice, ctx->stream));
+    const size_t s64 = A->use_sell ? 0 : tma_smem<double>(), s32 = A->use_sell ? 0 : tma_smem<float>();
+    set_smem(k_cg_dir<RPW>, tma_smem<double>());
+    set_smem(k_mx_dir<RPW>, tma_smem<float>());
+    const Sell<double> S64 = sell_view<double>(A);
+    const Sell<float> S32 = sell_view<float>(A);
+    const int us = A->use_sell;
+    const long long ct = (long long)n * 32 / RPW;
+    const int g64 = std::min(grid_for(ctx, (const void *)k_cg_dir<RPW>, kBlock, s64, ct), kMaxGrid);
+    const int g32 = std::min(grid_for(ctx, (const void *)k_mx_dir<RPW>, kBlock, s32, ct), kMaxGrid);
+    const int gv = std::min(grid_for(ctx, (const void *)k_cg_update<1>, kBlock, 0, n), kMaxGrid);
+    const Csr<double> M64 = view<double>(A, true);
+    const Csr<float> M32 = view<float>(A, true);
+    auto launch = [&]() {
+        switch (kernel) {
+        case RSG_KERNEL_CG_DIR_FP64:
+            k_cg_dir<RPW><<<g64, kBlock, s64, ctx->stream>>>(M64, S64, us, v64[0], v64[1], v64[2], v64[3], partials,
+                                                             st);
+            break;
+        case RSG_KERNEL_CG_DIR_MIXED:
+            k_mx_dir<RPW><<<g32, kBlock, s32, ctx->stream>>>(M32, S32, us, v32[0], v32[1], v32[2], v32[3], v64[0],
+                                                             v32[4], partials, st);
+            break;
+        case RSG_KERNEL_CG_UPDATE_FP64:
+            k_cg_update<1><<<gv, kBlock, 0, ctx->stream>>>(n, 1, v64[4], v64[0], v64[1], v64[2], v64[3], v64[4],
+                                                          partials, st);
+            break;
+        case RSG_KERNEL_CG_UPDATE_MIXED:
+            k_mx_update<1><<<gv, kBlock, 0, ctx->stream>>>(n, 1, v32[5], v32[0], v32[1], v32[2], v32[3], v32[4],
+                                                          partials, st);
+            break;
+        case RSG_KERNEL_SPMV_FP64:
+            spmv64(ctx, A, v64[0], v64[1], true);
+            break;
+        default:
+            spmv32(ctx, A, v32[0], v32[1], true);
+            break;
+        }
+    };
+    launch();  // warm-up
+    double total = 0.0;
+    cudaEvent_t e0 = ctx->ev[2], e1 = ctx->ev[3];
+    if (!flush) RSG_CHECK_CUDA(ctx, cudaEventRecord(e0, ctx->stream));
+    for (uint32_t r = 0; r < reps; r++) {
+        if (flush) {
+            k_flush<<<ctx->num_sms * 8, kBlock, 0, ctx->stream>>>(fbuf, flush_bytes / 16, r);
+            RSG_CHECK_CUDA(ctx, cudaEventRecord(e0, ctx->stream));
+        }
+        launch();
+        if (flush) {
+            RSG_CHECK_CUDA(ctx, cudaEventRecord(e1, ctx->stream));
+            RSG_CHECK_CUDA(ctx, cudaEventSynchronize(e1));
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            total += ms;
+        }
+    }
+    if (!flush) {
+        RSG_CHECK_CUDA(ctx, cudaEventRecord(e1, ctx->stream));
+        RSG_CHECK_CUDA(ctx, cudaEventSynchronize(e1));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        total = ms;
+    }
+    RSG_CHECK_CUDA(ctx, cudaGetLastError());
+    *seconds = total * 1e-3 / std::max<uint32_t>(reps, 1);
+    return RSG_OK;
+}
+
+}  // namespace
+
 rsg_status cg_run(rsg_context *ctx, const CgArgs &a, double *seconds)
 {
     const int rpw = pick_rpw(a.A);
@@ -675,3 +872,15 @@ rsg_status cg_run(rsg_context *ctx, const CgArgs &a, double *seconds)
 }
 
 }  // namespace rsg
+
+using namespace rsg;
+
+extern "C" rsg_status rsg_profile_kernel(rsg_context *ctx, const rsg_csr *A, int32_t kernel, uint32_t reps,
+                                         int32_t flush_l2, double *seconds)
+{
+    if (!ctx || !A || !seconds || kernel < 0 || kernel > RSG_KERNEL_SPMV_FP32)
+        return set_error(ctx, RSG_ERR_INVALID_ARG, "profile_kernel: bad arguments");
+    RSG_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
+    RSG_RPW_DISPATCH(pick_rpw(A), return profile_typed<RPW>(ctx, A, kernel, reps, flush_l2, seconds));
+    return RSG_ERR_UNSUPPORTED;
+}

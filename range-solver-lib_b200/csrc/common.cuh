@@ -35,6 +35,7 @@ struct rsg_context {
     std::string last_error;
     rsg::Arena ws;                    // per-solve workspace
     double *pinned = nullptr;         // small pinned host buffer for readbacks (64 doubles)
+    unsigned int *errw = nullptr;     // device word: set when a kernel's bounded wait ran out
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
@@ -50,6 +51,17 @@ struct rsg_csr {
     uint32_t max_row = 0;             // longest row
     uint32_t max_warp_nnz = 0;        // longest 32-row chunk
     bool has_off16 = false;
+    // SELL-32 copy (slice = 32 rows = one warp; element k of lane l at
+    // slice_ptr[s] + (k/4)*128 + 4l + k%4, rows padded to a multiple of 4)
+    bool use_sell = false;
+    uint32_t n_slices = 0;
+    uint64_t sell_elems = 0;
+    uint32_t *slice_ptr = nullptr;    // n_slices + 1
+    uint32_t *slice_len4 = nullptr;   // padded row length / 4 per slice
+    double *sval = nullptr;
+    float *sval32 = nullptr;
+    int16_t *soff = nullptr;          // col - (row & ~31), when every offset fits
+    uint32_t *scol = nullptr;         // otherwise uint32 columns
 };
 
 namespace rsg {

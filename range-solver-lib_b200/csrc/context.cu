@@ -71,6 +71,10 @@ rsg_status rsg_context_create(int device, rsg_context **out)
         return RSG_ERR_CUDA;
     }
     for (auto &e : ctx->ev) cudaEventCreate(&e);
+    if (cudaMalloc(&ctx->errw, 256) != cudaSuccess || cudaMemset(ctx->errw, 0, 256) != cudaSuccess) {
+        rsg_context_destroy(ctx);
+        return RSG_ERR_CUDA;
+    }
     *out = ctx;
     return RSG_OK;
 }
@@ -82,6 +86,7 @@ void rsg_context_destroy(rsg_context *ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->ws.base) cudaFree(ctx->ws.base);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    if (ctx->errw) cudaFree(ctx->errw);
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -128,6 +133,12 @@ rsg_status rsg_synchronize(rsg_context *ctx)
 {
     if (!ctx) return RSG_ERR_INVALID_ARG;
     RSG_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    unsigned int e = 0;
+    RSG_CHECK_CUDA(ctx, cudaMemcpy(&e, ctx->errw, sizeof(e), cudaMemcpyDeviceToHost));
+    if (e) {
+        cudaMemset(ctx->errw, 0, sizeof(e));
+        return rsg::set_error(ctx, RSG_ERR_TIMEOUT, "a kernel's bounded wait for its copies ran out");
+    }
     return RSG_OK;
 }
 

@@ -6,6 +6,7 @@
 #include "csr.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 
 namespace rsg {
 
@@ -60,14 +61,14 @@ __global__ void k_csr_analyze(uint32_t n, uint64_t nnz, const uint32_t *__restri
     if (grid_sum<1>(nrm, partials, &out->ticket, sh, tot) && threadIdx.x == 0) out->norm = sqrt(tot[0]);
 }
 
-template <typename V, typename A, int RPW>
-__global__ void __launch_bounds__(kBlock) k_spmv(Csr<V> M, const V *__restrict__ x, V *__restrict__ y)
+template <typename V, int RPW>
+__global__ void __launch_bounds__(kBlock) k_spmv(Csr<V> M, Sell<V> S, int use_sell, const V *__restrict__ x,
+                                                 V *__restrict__ y, unsigned int *err)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    A *prod = reinterpret_cast<A *>(smem_raw);
     auto gx = [&](uint32_t c) { return x[c]; };
-    auto epi = [&](uint32_t row, A acc) { y[row] = V(acc); };
-    for_rows<V, A, RPW>(M, gx, epi, prod);
+    auto epi = [&](uint32_t row, V acc) { y[row] = acc; };
+    for_rows_any<V, RPW>(M, S, use_sell != 0, gx, epi, smem_raw, err, true);
 }
 
 __global__ void k_jacobi(uint32_t n, const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ci,
@@ -144,12 +145,11 @@ __global__ void k_block_jacobi(uint32_t n, uint32_t w, const uint32_t *__restric
 }
 
 template <int RPW>
-__global__ void __launch_bounds__(kBlock) k_true_res(Csr<double> M, const double *__restrict__ b,
+__global__ void __launch_bounds__(kBlock) k_true_res(Csr<double> M, Sell<double> S, int use_sell, const double *__restrict__ b,
                                                      const double *__restrict__ x, double *partials,
-                                                     unsigned int *ticket, double *out)
+                                                     unsigned int *ticket, double *out, unsigned int *err)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *prod = reinterpret_cast<double *>(smem_raw);
     __shared__ double sh[64];
     double acc[2] = {0.0, 0.0};
     auto gx = [&](uint32_t c) { return x[c]; };
@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(kBlock) k_true_res(Csr<double> M, const double
         acc[0] += r * r;
         acc[1] += b[row] * b[row];
     };
-    for_rows<double, double, RPW>(M, gx, epi, prod);
+    for_rows_any<double, RPW>(M, S, use_sell != 0, gx, epi, smem_raw, err, true);
     double tot[2];
     if (grid_sum<2>(acc, partials, ticket, sh, tot) && threadIdx.x == 0) {
         out[0] = sqrt(tot[0]);
@@ -167,17 +167,129 @@ __global__ void __launch_bounds__(kBlock) k_true_res(Csr<double> M, const double
     }
 }
 
+__global__ void k_sell_len(uint32_t n, uint32_t n_slices, const uint32_t *__restrict__ rp, uint32_t *len4)
+{
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n_slices; s += gridDim.x * blockDim.x) {
+        uint32_t m = 0;
+        const uint32_t r1 = min(n, s * 32u + 32u);
+        for (uint32_t r = s * 32u; r < r1; r++) m = max(m, rp[r + 1] - rp[r]);
+        len4[s] = (m + 3u) / 4u;
+    }
+}
+
+// Scatter CSR entries into the SELL-32 layout (thread per row).
+__global__ void k_sell_fill(uint32_t n, const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ci,
+                            const double *__restrict__ val, const int16_t *__restrict__ off16,
+                            const uint32_t *__restrict__ slice_ptr, double *__restrict__ sval,
+                            float *__restrict__ sval32, int16_t *__restrict__ soff, uint32_t *__restrict__ scol,
+                            int values_only)
+{
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const size_t base = size_t(slice_ptr[r >> 5]) + 4u * (r & 31u);
+        const uint32_t s = rp[r], e = rp[r + 1];
+        for (uint32_t j = s; j < e; j++) {
+            const uint32_t k = j - s;
+            const size_t pos = base + size_t(k >> 2) * 128u + (k & 3u);
+            sval[pos] = val[j];
+            sval32[pos] = __double2float_rn(val[j]);
+            if (!values_only) {
+                if (soff) soff[pos] = off16[j];
+                else scol[pos] = ci[j];
+            }
+        }
+    }
+}
+
 // ---------------- host helpers ----------------
+
+static void free_sell(rsg_csr *A)
+{
+    cudaFree(A->slice_ptr);
+    cudaFree(A->slice_len4);
+    cudaFree(A->sval);
+    cudaFree(A->sval32);
+    cudaFree(A->soff);
+    cudaFree(A->scol);
+    A->slice_ptr = A->slice_len4 = A->scol = nullptr;
+    A->sval = nullptr;
+    A->sval32 = nullptr;
+    A->soff = nullptr;
+    A->use_sell = false;
+}
 
 static void free_csr(rsg_csr *A)
 {
     if (!A) return;
+    free_sell(A);
     cudaFree(A->rp);
     cudaFree(A->ci);
     cudaFree(A->val);
     cudaFree(A->val32);
     cudaFree(A->off16);
     delete A;
+}
+
+// Build the SELL-32 copy when its padding costs at most 25% over the CSR.
+static rsg_status build_sell(rsg_context *ctx, rsg_csr *A)
+{
+    A->n_slices = (A->n + 31u) / 32u;
+    if (cudaMalloc(&A->slice_len4, size_t(A->n_slices) * sizeof(uint32_t)) != cudaSuccess)
+        return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "SELL slice lengths");
+    const int g = grid_for(ctx, (const void *)k_sell_len, kBlock, 0, A->n_slices);
+    k_sell_len<<<g, kBlock, 0, ctx->stream>>>(A->n, A->n_slices, A->rp, A->slice_len4);
+    std::vector<uint32_t> len4(A->n_slices);
+    std::vector<uint32_t> ptr(size_t(A->n_slices) + 1, 0);
+    RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(len4.data(), A->slice_len4, len4.size() * sizeof(uint32_t),
+                                        cudaMemcpyDeviceToHost, ctx->stream));
+    RSG_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    uint64_t total = 0;
+    for (uint32_t s2 = 0; s2 < A->n_slices; s2++) {
+        ptr[s2] = uint32_t(total);
+        total += uint64_t(len4[s2]) * 128u;
+        if (total > 0xfffffff0ull) {
+            free_sell(A);
+            return RSG_OK;  // too large for 32-bit slice offsets: keep the CSR path
+        }
+    }
+    ptr[A->n_slices] = uint32_t(total);
+    if (A->nnz == 0 || double(total) > 1.25 * double(A->nnz)) {
+        free_sell(A);
+        return RSG_OK;
+    }
+    A->sell_elems = total;
+    const size_t t = std::max<uint64_t>(total, 1);
+    if (cudaMalloc(&A->slice_ptr, ptr.size() * sizeof(uint32_t)) != cudaSuccess ||
+        cudaMalloc(&A->sval, t * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&A->sval32, t * sizeof(float)) != cudaSuccess ||
+        (A->has_off16 ? cudaMalloc(&A->soff, t * sizeof(int16_t)) : cudaMalloc(&A->scol, t * sizeof(uint32_t))) !=
+            cudaSuccess) {
+        free_sell(A);
+        cudaGetLastError();
+        return RSG_OK;  // not enough memory for the copy: keep the CSR path
+    }
+    RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(A->slice_ptr, ptr.data(), ptr.size() * sizeof(uint32_t),
+                                        cudaMemcpyHostToDevice, ctx->stream));
+    RSG_CHECK_CUDA(ctx, cudaMemsetAsync(A->sval, 0, t * sizeof(double), ctx->stream));
+    RSG_CHECK_CUDA(ctx, cudaMemsetAsync(A->sval32, 0, t * sizeof(float), ctx->stream));
+    if (A->soff) RSG_CHECK_CUDA(ctx, cudaMemsetAsync(A->soff, 0, t * sizeof(int16_t), ctx->stream));
+    else RSG_CHECK_CUDA(ctx, cudaMemsetAsync(A->scol, 0, t * sizeof(uint32_t), ctx->stream));
+    const int gf = grid_for(ctx, (const void *)k_sell_fill, kBlock, 0, A->n);
+    k_sell_fill<<<gf, kBlock, 0, ctx->stream>>>(A->n, A->rp, A->ci, A->val, A->off16, A->slice_ptr, A->sval,
+                                               A->sval32, A->soff, A->scol, 0);
+    RSG_CHECK_CUDA(ctx, cudaGetLastError());
+    RSG_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    A->use_sell = true;
+    return RSG_OK;
+}
+
+static rsg_status refill_sell_values(rsg_context *ctx, rsg_csr *A)
+{
+    if (!A->use_sell) return RSG_OK;
+    const int gf = grid_for(ctx, (const void *)k_sell_fill, kBlock, 0, A->n);
+    k_sell_fill<<<gf, kBlock, 0, ctx->stream>>>(A->n, A->rp, A->ci, A->val, A->off16, A->slice_ptr, A->sval,
+                                               A->sval32, A->soff, A->scol, 1);
+    RSG_CHECK_CUDA(ctx, cudaGetLastError());
+    return RSG_OK;
 }
 
 static rsg_status analyze(rsg_context *ctx, rsg_csr *A, bool values_only)
@@ -205,17 +317,21 @@ static rsg_status analyze(rsg_context *ctx, rsg_csr *A, bool values_only)
     return RSG_OK;
 }
 
-rsg_status csr_refresh(rsg_context *ctx, rsg_csr *A) { return analyze(ctx, A, true); }
+rsg_status csr_refresh(rsg_context *ctx, rsg_csr *A)
+{
+    RSG_TRY(analyze(ctx, A, true));
+    return refill_sell_values(ctx, A);
+}
 
 rsg_status spmv64(rsg_context *ctx, const rsg_csr *A, const double *x, double *y, bool off16)
 {
     const Csr<double> M = view<double>(A, off16);
-    const size_t smem = prod_smem<double>();
+    const size_t smem = A->use_sell ? 0 : tma_smem<double>();
     RSG_RPW_DISPATCH(pick_rpw(A), {
-        auto k = k_spmv<double, double, RPW>;
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        auto k = k_spmv<double, RPW>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tma_smem<double>()));
         const int grid = grid_for(ctx, (const void *)k, kBlock, smem, (long long)A->n * 32 / RPW);
-        k<<<grid, kBlock, smem, ctx->stream>>>(M, x, y);
+        k<<<grid, kBlock, smem, ctx->stream>>>(M, sell_view<double>(A), A->use_sell, x, y, ctx->errw);
     });
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
     return RSG_OK;
@@ -224,12 +340,12 @@ rsg_status spmv64(rsg_context *ctx, const rsg_csr *A, const double *x, double *y
 rsg_status spmv32(rsg_context *ctx, const rsg_csr *A, const float *x, float *y, bool off16)
 {
     const Csr<float> M = view<float>(A, off16);
-    const size_t smem = prod_smem<float>();
+    const size_t smem = A->use_sell ? 0 : tma_smem<float>();
     RSG_RPW_DISPATCH(pick_rpw(A), {
-        auto k = k_spmv<float, float, RPW>;
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        auto k = k_spmv<float, RPW>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tma_smem<float>()));
         const int grid = grid_for(ctx, (const void *)k, kBlock, smem, (long long)A->n * 32 / RPW);
-        k<<<grid, kBlock, smem, ctx->stream>>>(M, x, y);
+        k<<<grid, kBlock, smem, ctx->stream>>>(M, sell_view<float>(A), A->use_sell, x, y, ctx->errw);
     });
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
     return RSG_OK;
@@ -262,13 +378,14 @@ rsg_status true_residual(rsg_context *ctx, const rsg_csr *A, const double *b, co
                          unsigned int *ticket, double *out3)
 {
     const Csr<double> M = view<double>(A, true);
-    const size_t smem = prod_smem<double>();
+    const size_t smem = A->use_sell ? 0 : tma_smem<double>();
     RSG_RPW_DISPATCH(pick_rpw(A), {
         auto k = k_true_res<RPW>;
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tma_smem<double>()));
         const int grid = std::min(grid_for(ctx, (const void *)k, kBlock, smem, (long long)A->n * 32 / RPW),
                                   kMaxGrid);
-        k<<<grid, kBlock, smem, ctx->stream>>>(M, b, x, partials, ticket, out3);
+        k<<<grid, kBlock, smem, ctx->stream>>>(M, sell_view<double>(A), A->use_sell, b, x, partials, ticket, out3,
+                                               ctx->errw);
     });
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
     return RSG_OK;
@@ -318,6 +435,7 @@ rsg_status rsg_csr_create(rsg_context *ctx, uint32_t n, const uint32_t *rp, cons
         (nnz32 && cudaMemcpyAsync(A->val, val, size_t(nnz32) * sizeof(double), kind, ctx->stream) != cudaSuccess))
         return fail(set_error(ctx, RSG_ERR_CUDA, "csr_create: upload failed"));
     rsg_status s = analyze(ctx, A, false);
+    if (s == RSG_OK && std::getenv("RSG_NO_SELL") == nullptr) s = build_sell(ctx, A);
     if (s != RSG_OK) return fail(s);
     *out = A;
     return RSG_OK;
@@ -330,7 +448,7 @@ rsg_status rsg_csr_update_values(rsg_context *ctx, rsg_csr *A, const double *val
     const cudaMemcpyKind kind = memory == RSG_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
     if (A->nnz && val != A->val)
         RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(A->val, val, A->nnz * sizeof(double), kind, ctx->stream));
-    return analyze(ctx, A, true);
+    return csr_refresh(ctx, A);
 }
 
 void rsg_csr_destroy(rsg_context *ctx, rsg_csr *A)

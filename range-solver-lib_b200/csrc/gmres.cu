@@ -19,13 +19,12 @@
 namespace rsg {
 
 template <int RPW>
-__global__ void __launch_bounds__(kBlock) k_gm_residual(Csr<double> M, const double *__restrict__ b,
+__global__ void __launch_bounds__(kBlock) k_gm_residual(Csr<double> M, Sell<double> S, int use_sell, const double *__restrict__ b,
                                                         const double *__restrict__ x, double *__restrict__ ro,
                                                         double *__restrict__ H, double *__restrict__ g,
                                                         double *partials, GmresState *st)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *prod = reinterpret_cast<double *>(smem_raw);
     __shared__ double sh[96];
     if (st->done) return;
     double acc[3] = {0.0, 0.0, 0.0};
@@ -37,7 +36,7 @@ __global__ void __launch_bounds__(kBlock) k_gm_residual(Csr<double> M, const dou
         acc[1] += r * r;
         acc[2] += b[row] * b[row];
     };
-    for_rows<double, double, RPW>(M, gx, epi, prod);
+    for_rows_any<double, RPW>(M, S, use_sell != 0, gx, epi, smem_raw, &st->ticket[7], true);
     double tot[3];
     if (grid_sum<3>(acc, partials, &st->ticket[0], sh, tot)) {
         const uint32_t m = st->m;
@@ -117,16 +116,15 @@ __global__ void __launch_bounds__(kBlock) k_gm_vz(uint32_t n, uint32_t w_, const
 }
 
 template <int RPW>
-__global__ void __launch_bounds__(kBlock) k_gm_spmv(Csr<double> M, const double *__restrict__ Z,
-                                                    double *__restrict__ wv, const GmresState *st, uint32_t k)
+__global__ void __launch_bounds__(kBlock) k_gm_spmv(Csr<double> M, Sell<double> S, int use_sell, const double *__restrict__ Z,
+                                                    double *__restrict__ wv, GmresState *st, uint32_t k)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *prod = reinterpret_cast<double *>(smem_raw);
     if (st->done || st->inner_done) return;
     const double *z = Z + size_t(k) * M.n;
     auto gx = [&](uint32_t c) { return z[c]; };
     auto epi = [&](uint32_t row, double v) { wv[row] = v; };
-    for_rows<double, double, RPW>(M, gx, epi, prod);
+    for_rows_any<double, RPW>(M, S, use_sell != 0, gx, epi, smem_raw, &st->ticket[7], true);
 }
 
 // h_i = v_i^T w for i <= k: blockIdx.y = i.  Last block of the 2-D grid stores column k of H.
@@ -289,9 +287,11 @@ rsg_status run_typed(rsg_context *ctx, const GmresArgs &a, double *seconds)
 {
     const uint32_t n = a.A->n, m = a.m;
     const Csr<double> M = view<double>(a.A, true);
-    const size_t s64 = prod_smem<double>();
-    cudaFuncSetAttribute(k_gm_residual<RPW>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(s64));
-    cudaFuncSetAttribute(k_gm_spmv<RPW>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(s64));
+    const size_t s64 = a.A->use_sell ? 0 : tma_smem<double>();
+    cudaFuncSetAttribute(k_gm_residual<RPW>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tma_smem<double>()));
+    cudaFuncSetAttribute(k_gm_spmv<RPW>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tma_smem<double>()));
+    const Sell<double> S = sell_view<double>(a.A);
+    const int us = a.A->use_sell;
     const long long ct = (long long)n * 32 / RPW;
     const int g_sp = std::min(grid_for(ctx, (const void *)k_gm_spmv<RPW>, kBlock, s64, ct), kMaxGrid);
     const int g_res = std::min(grid_for(ctx, (const void *)k_gm_residual<RPW>, kBlock, s64, ct), kMaxGrid);
@@ -301,10 +301,10 @@ rsg_status run_typed(rsg_context *ctx, const GmresArgs &a, double *seconds)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     RSG_CHECK_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    k_gm_residual<RPW><<<g_res, kBlock, s64, ctx->stream>>>(M, a.b, a.x, a.ro, a.H, a.g, a.partials, a.st);
+    k_gm_residual<RPW><<<g_res, kBlock, s64, ctx->stream>>>(M, S, us, a.b, a.x, a.ro, a.H, a.g, a.partials, a.st);
     for (uint32_t k = 0; k < m; k++) {
         k_gm_vz<PK><<<g_vec, kBlock, 0, ctx->stream>>>(n, a.P.w, a.P.d, a.ro, a.w, a.wnorm, a.V, a.Z, a.st, k);
-        k_gm_spmv<RPW><<<g_sp, kBlock, s64, ctx->stream>>>(M, a.Z, a.w, a.st, k);
+        k_gm_spmv<RPW><<<g_sp, kBlock, s64, ctx->stream>>>(M, S, us, a.Z, a.w, a.st, k);
         k_gm_dots<<<dim3(g_dot, k + 1), kBlock, 0, ctx->stream>>>(n, a.V, a.w, a.H, a.hv, a.partials, a.st, k);
         k_gm_correct<<<g_vec, kBlock, 0, ctx->stream>>>(n, a.V, a.w, a.hv, a.H, a.cs, a.sn, a.g, a.wnorm,
                                                        a.partials, a.st, k);

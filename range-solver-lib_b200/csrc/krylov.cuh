@@ -30,8 +30,8 @@ struct CgState {
     uint32_t n_updates;
     uint32_t body_count;
     uint32_t body_limit;
-    uint32_t pad;
-    unsigned int ticket[8];
+    int32_t evict_first32;  // L2 policy of the FP32 matrix stream (1 evict_first, 0 evict_last)
+    unsigned int ticket[8];  // [7] = bounded-wait error word
     double *history;   // error per iteration (may be null)
     double *trend_hist;
 };

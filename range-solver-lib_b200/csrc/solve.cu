@@ -216,6 +216,7 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
         h.body_limit = max_it / 2 + 16;
         h.history = hist;
         h.trend_hist = thist;
+        h.evict_first32 = c.l2_resident_f32 ? 0 : 1;
         RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(cst, &h, sizeof(h), cudaMemcpyHostToDevice, ctx->stream));
         RSG_TRY(cg_run(ctx, a, &solve_seconds));
         RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(&h, cst, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
@@ -225,7 +226,7 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
         st_out.error = h.error;
         st_out.trend = h.trend;
         st_out.converged = h.converged;
-        solve_status = rsg_status(h.status);
+        solve_status = h.ticket[7] ? RSG_ERR_TIMEOUT : rsg_status(h.status);
         if (want_hist) {
             std::vector<double> e(h.it), t(h.it);
             cudaMemcpy(e.data(), hist, h.it * sizeof(double), cudaMemcpyDeviceToHost);
@@ -264,7 +265,7 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
         st_out.error = h.error;
         st_out.trend = h.trend;
         st_out.converged = h.converged;
-        solve_status = rsg_status(h.status);
+        solve_status = h.ticket[7] ? RSG_ERR_TIMEOUT : rsg_status(h.status);
         if (want_hist) {
             std::vector<double> e(h.outer_logged), t(h.outer_logged);
             cudaMemcpy(e.data(), hist, h.outer_logged * sizeof(double), cudaMemcpyDeviceToHost);
@@ -290,6 +291,7 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
         std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count() - solve_seconds;
     st_out.status = solve_status;
     if (stats) *stats = st_out;
-    if (solve_status == RSG_ERR_TIMEOUT) return set_error(ctx, RSG_ERR_TIMEOUT, "solve loop hit its hard limit");
+    if (solve_status == RSG_ERR_TIMEOUT)
+        return set_error(ctx, RSG_ERR_TIMEOUT, "solve loop hit its hard limit or a bounded copy wait ran out");
     return solve_status;
 }

@@ -19,6 +19,8 @@
 
 #include "common.cuh"
 
+#include <type_traits>
+
 namespace rsg {
 
 constexpr uint32_t kCap = 512;  // products per warp held in shared memory
@@ -32,6 +34,43 @@ struct Csr {
     uint32_t n;
 };
 
+// Streaming loads of the matrix: read-only path, not allocated in L1 (the
+// matrix is used once per product; L1 is kept for the x gathers).
+__device__ __forceinline__ double2 ld_stream(const double2 *p)
+{
+    double2 v;
+    asm("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ float4 ld_stream(const float4 *p)
+{
+    float4 v;
+    asm("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "l"(p));
+    return v;
+}
+__device__ __forceinline__ uint2 ld_stream(const uint2 *p)
+{
+    uint2 v;
+    asm("ld.global.nc.L1::no_allocate.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ uint4 ld_stream(const uint4 *p)
+{
+    uint4 v;
+    asm("ld.global.nc.L1::no_allocate.v4.u32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(p));
+    return v;
+}
+__device__ __forceinline__ uint32_t ld_stream(const uint32_t *p)
+{
+    uint32_t v;
+    asm("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+
 template <typename V>
 struct VecLoad;
 template <>
@@ -39,21 +78,21 @@ struct VecLoad<double> {
     static constexpr int W = 2;
     __device__ __forceinline__ static void vals(const double *p, double (&v)[2])
     {
-        double2 t = __ldg(reinterpret_cast<const double2 *>(p));
+        double2 t = ld_stream(reinterpret_cast<const double2 *>(p));
         v[0] = t.x;
         v[1] = t.y;
     }
     __device__ __forceinline__ static void cols(const uint32_t *p, uint32_t (&c)[2])
     {
-        uint2 t = __ldg(reinterpret_cast<const uint2 *>(p));
+        uint2 t = ld_stream(reinterpret_cast<const uint2 *>(p));
         c[0] = t.x;
         c[1] = t.y;
     }
     __device__ __forceinline__ static void offs(const int16_t *p, int (&c)[2])
     {
-        short2 t = __ldg(reinterpret_cast<const short2 *>(p));
-        c[0] = t.x;
-        c[1] = t.y;
+        uint32_t t = ld_stream(reinterpret_cast<const uint32_t *>(p));
+        c[0] = int(int16_t(t & 0xffffu));
+        c[1] = int(int16_t(t >> 16));
     }
 };
 template <>
@@ -61,7 +100,7 @@ struct VecLoad<float> {
     static constexpr int W = 4;
     __device__ __forceinline__ static void vals(const float *p, float (&v)[4])
     {
-        float4 t = __ldg(reinterpret_cast<const float4 *>(p));
+        float4 t = ld_stream(reinterpret_cast<const float4 *>(p));
         v[0] = t.x;
         v[1] = t.y;
         v[2] = t.z;
@@ -69,7 +108,7 @@ struct VecLoad<float> {
     }
     __device__ __forceinline__ static void cols(const uint32_t *p, uint32_t (&c)[4])
     {
-        uint4 t = __ldg(reinterpret_cast<const uint4 *>(p));
+        uint4 t = ld_stream(reinterpret_cast<const uint4 *>(p));
         c[0] = t.x;
         c[1] = t.y;
         c[2] = t.z;
@@ -77,11 +116,11 @@ struct VecLoad<float> {
     }
     __device__ __forceinline__ static void offs(const int16_t *p, int (&c)[4])
     {
-        short4 t = __ldg(reinterpret_cast<const short4 *>(p));
-        c[0] = t.x;
-        c[1] = t.y;
-        c[2] = t.z;
-        c[3] = t.w;
+        uint2 t = ld_stream(reinterpret_cast<const uint2 *>(p));
+        c[0] = int(int16_t(t.x & 0xffffu));
+        c[1] = int(int16_t(t.x >> 16));
+        c[2] = int(int16_t(t.y & 0xffffu));
+        c[3] = int(int16_t(t.y >> 16));
     }
 };
 
@@ -117,23 +156,34 @@ __device__ __forceinline__ void warp_chunk(const Csr<V> &M, uint32_t row0, GX &g
     const int base = int(row0 & ~31u);
 
     if (end - start <= kCap) {
+        // Issue every matrix load of the chunk first, then every gather, so that
+        // a warp keeps up to kCap/(32 W) + 1 independent 16-byte loads in flight.
+        constexpr int MAXIT = int(kCap) / (32 * W) + 1;
         const uint32_t g = start & ~uint32_t(W - 1);
-        for (uint32_t j0 = g + uint32_t(lane) * W; j0 < end; j0 += 32u * W) {
-            V v[W];
-            VecLoad<V>::vals(M.val + j0, v);
-            uint32_t c[W];
-            if (M.off) {
-                int o[W];
-                VecLoad<V>::offs(M.off + j0, o);
+        V v[MAXIT][W];
+        uint32_t c[MAXIT][W];
 #pragma unroll
-                for (int k = 0; k < W; k++) c[k] = uint32_t(base + o[k]);
-            } else {
-                VecLoad<V>::cols(M.ci + j0, c);
+        for (int it = 0; it < MAXIT; it++) {
+            const uint32_t j0 = g + (uint32_t(it) * 32u + uint32_t(lane)) * W;
+            if (j0 < end) {
+                VecLoad<V>::vals(M.val + j0, v[it]);
+                if (M.off) {
+                    int o[W];
+                    VecLoad<V>::offs(M.off + j0, o);
+#pragma unroll
+                    for (int k = 0; k < W; k++) c[it][k] = uint32_t(base + o[k]);
+                } else {
+                    VecLoad<V>::cols(M.ci + j0, c[it]);
+                }
             }
+        }
+#pragma unroll
+        for (int it = 0; it < MAXIT; it++) {
+            const uint32_t j0 = g + (uint32_t(it) * 32u + uint32_t(lane)) * W;
 #pragma unroll
             for (int k = 0; k < W; k++) {
-                uint32_t j = j0 + k;
-                if (j >= start && j < end) prod[j - start] = A(v[k]) * A(gx(c[k]));
+                const uint32_t j = j0 + k;
+                if (j0 < end && j >= start && j < end) prod[j - start] = A(v[it][k]) * A(gx(c[it][k]));
             }
         }
         __syncwarp();
@@ -166,6 +216,315 @@ __device__ __forceinline__ void for_rows(const Csr<V> &M, GX &gx, EPI &epi, A *s
     const uint32_t warps_total = gridDim.x * (blockDim.x >> 5);
     for (uint32_t c = blockIdx.x * (blockDim.x >> 5) + warp; c < n_chunks; c += warps_total)
         warp_chunk<V, A, RPW>(M, c * RPW, gx, epi, prod, lane);
+}
+
+// ---------------------------------------------------------------------------
+// TMA-staged pipeline.  Each warp streams its row chunks through NS shared-
+// memory stages: one lane issues bulk copies (cp.async.bulk, the TMA unit) of
+// the chunk's values and column indexes and arms the stage's mbarrier with the
+// byte count; the warp computes the previous chunk meanwhile.  Products are
+// formed in place in the stage, summed per row, and the stage is re-armed
+// with the chunk NS positions ahead.  The matrix stream therefore never
+// occupies registers, and every warp keeps one chunk in flight while it
+// computes another.  Waits are bounded: past kWaitLimit polls the kernel
+// records an error, drains its own copies (again bounded) and stops taking
+// chunks, so a stuck copy cannot hang the GPU.
+// ---------------------------------------------------------------------------
+constexpr int kStages = 2;
+constexpr uint32_t kStageElems = kCap + 16;  // chunk nonzeros plus alignment slack
+constexpr uint32_t kWaitLimit = 1u << 20;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arm(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar, uint64_t policy)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;"
+        ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
+        : "memory");
+}
+__device__ __forceinline__ uint64_t policy_evict_first()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_last()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// bounded wait; returns false (and flags *err) when the limit is reached
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, unsigned int *err)
+{
+    for (uint32_t t = 0; t < kWaitLimit; t++)
+        if (mbar_try_wait(bar, parity)) return true;
+    if (err) atomicOr(err, 1u);
+    return false;
+}
+
+template <typename V>
+struct Stage {
+    // index slots are sized for uint32 columns; 16-bit offsets use the first half
+    static constexpr uint32_t kValBytes = kStageElems * sizeof(V);
+    static constexpr uint32_t kIdxBytes = kStageElems * sizeof(uint32_t);
+    static constexpr uint32_t kBytes = kValBytes + kIdxBytes;
+    // per warp: kStages stages + kStages mbarriers (16-byte padded)
+    static constexpr uint32_t kWarpBytes = kStages * kBytes + 16 * kStages;
+};
+
+template <typename V>
+constexpr size_t tma_smem() { return size_t(kWarpsPerBlock) * Stage<V>::kWarpBytes; }
+
+// Grid-stride over row chunks with the TMA pipeline.  Every thread of the block
+// calls it; returns normally even on a wait timeout (the caller's grid
+// reduction still runs).  `evict_first` selects the L2 policy of the stream.
+template <typename V, int RPW, class GX, class EPI>
+__device__ __forceinline__ void for_rows_tma(const Csr<V> &M, GX &gx, EPI &epi, unsigned char *smem,
+                                             unsigned int *err, bool evict_first)
+{
+    using S = Stage<V>;
+    constexpr int L = 32 / RPW;
+    const bool off = M.off != nullptr;
+    const uint32_t isz = off ? 2u : 4u;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned char *wbase = smem + size_t(warp) * S::kWarpBytes;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(wbase + kStages * S::kBytes);
+    const uint32_t n_chunks = (M.n + RPW - 1) / RPW;
+    const uint32_t warps_total = gridDim.x * (blockDim.x >> 5);
+    const uint32_t first = blockIdx.x * (blockDim.x >> 5) + warp;
+    const unsigned char *idx_g = off ? reinterpret_cast<const unsigned char *>(M.off)
+                                     : reinterpret_cast<const unsigned char *>(M.ci);
+    const uint64_t pol = evict_first ? policy_evict_first() : policy_evict_last();
+
+    if (lane == 0) {
+        for (int s = 0; s < kStages; s++) mbar_init(&bar[s], 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+
+    // issue chunk c into stage s (lane 0); returns whether a copy is in flight
+    auto issue = [&](uint32_t c, int s) -> bool {
+        if (c >= n_chunks) return false;
+        const uint32_t row0 = c * RPW;
+        const uint32_t nrows = min(uint32_t(RPW), M.n - row0);
+        const uint32_t start = __ldg(&M.rp[row0]), end = __ldg(&M.rp[row0 + nrows]);
+        if (end - start > kCap) return false;  // long rows: handled without staging
+        const uint32_t a0 = start & ~7u, a1 = (end + 7u) & ~7u;
+        if (a1 == a0) return false;
+        if (lane == 0) {
+            unsigned char *st = wbase + s * S::kBytes;
+            const uint32_t vb = (a1 - a0) * sizeof(V), ib = (a1 - a0) * isz;
+            mbar_arm(&bar[s], vb + ib);
+            bulk_load(st, M.val + a0, vb, &bar[s], pol);
+            bulk_load(st + S::kValBytes, idx_g + size_t(a0) * isz, ib, &bar[s], pol);
+        }
+        return true;
+    };
+
+    bool inflight[kStages];
+    uint32_t phase[kStages];
+#pragma unroll
+    for (int s = 0; s < kStages; s++) {
+        phase[s] = 0;
+        inflight[s] = issue(first + s * warps_total, s);
+    }
+    bool failed = false;
+    int s = 0;
+    for (uint32_t c = first; c < n_chunks; c += warps_total) {
+        const uint32_t row0 = c * RPW;
+        const uint32_t nrows = min(uint32_t(RPW), M.n - row0);
+        const uint32_t end = __ldg(&M.rp[row0 + nrows]);
+        const uint32_t my_rp = (lane < int(nrows)) ? __ldg(&M.rp[row0 + lane]) : end;
+        const uint32_t start = __shfl_sync(0xffffffffu, my_rp, 0);
+        const int base = int(row0 & ~31u);
+        if (inflight[s]) {
+            if (!mbar_wait(&bar[s], phase[s], err)) {
+                failed = true;
+                break;
+            }
+            phase[s] ^= 1u;
+            inflight[s] = false;
+            unsigned char *st = wbase + s * S::kBytes;
+            V *sv = reinterpret_cast<V *>(st);
+            const int16_t *so = reinterpret_cast<const int16_t *>(st + S::kValBytes);
+            const uint32_t *sc = reinterpret_cast<const uint32_t *>(st + S::kValBytes);
+            const uint32_t a0 = start & ~7u;
+            if (off) {
+#pragma unroll 4
+                for (uint32_t j = start + lane; j < end; j += 32) {
+                    const uint32_t k = j - a0;
+                    sv[k] = sv[k] * V(gx(uint32_t(base + int(so[k]))));
+                }
+            } else {
+#pragma unroll 4
+                for (uint32_t j = start + lane; j < end; j += 32) {
+                    const uint32_t k = j - a0;
+                    sv[k] = sv[k] * V(gx(sc[k]));
+                }
+            }
+            __syncwarp();
+            const int r = lane / L, sub = lane % L;
+            const uint32_t rs = __shfl_sync(0xffffffffu, my_rp, r) - a0;
+            const uint32_t nx = __shfl_sync(0xffffffffu, my_rp, min(r + 1, 31));
+            const uint32_t re = ((r + 1 < int(nrows)) ? nx : end) - a0;
+            V acc = V(0);
+            if (r < int(nrows))
+                for (uint32_t k = rs + sub; k < re; k += L) acc += sv[k];
+#pragma unroll
+            for (int o = L / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (sub == 0 && r < int(nrows)) epi(row0 + r, acc);
+            __syncwarp();
+            fence_async_shared();  // generic writes to the stage precede the next async copy into it
+            __syncwarp();
+        } else if (end - start > 0) {
+            // long rows (or a chunk that was not staged): whole warp per row from global memory
+            for (uint32_t rr = 0; rr < nrows; rr++) {
+                V acc = warp_row<V, V>(M, row0 + rr, gx, lane);
+                if (lane == 0) epi(row0 + rr, acc);
+            }
+        } else {
+            if (lane < int(nrows)) epi(row0 + lane, V(0));
+        }
+        inflight[s] = issue(c + kStages * warps_total, s);
+        s = (s + 1 == kStages) ? 0 : s + 1;
+    }
+    if (failed) {
+        // drain every copy this warp still has in flight before the shared memory is released
+#pragma unroll
+        for (int t = 0; t < kStages; t++)
+            if (inflight[t]) mbar_wait(&bar[t], phase[t], nullptr);
+    }
+    __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// SELL-32 path (preferred when padding is small).  One warp per 32-row slice,
+// one thread per row; every lane reads 4 consecutive elements of its row per
+// 16-byte load (two for FP64 values), so a warp load instruction moves 512 B
+// (FP32) / 1 KB (FP64) of contiguous matrix data, and all of a row's loads are
+// independent.  Each row is summed by one thread in CSR column order with no
+// fused multiply-add, which is the reference's multiplyRow arithmetic
+// (src/rmatrixsolver.cpp:111-119) step for step.
+// ---------------------------------------------------------------------------
+template <typename V>
+struct Sell {
+    const uint32_t *rp;
+    const uint32_t *slice_ptr;
+    const uint32_t *slice_len4;
+    const V *val;
+    const int16_t *off;
+    const uint32_t *col;
+    uint32_t n, n_slices;
+};
+
+// FP64: separate multiply and add (no contraction), as the reference's loop;
+// FP32 (inner solver only): fused multiply-add.
+__device__ __forceinline__ double row_acc(double acc, double v, double x) { return __dadd_rn(acc, __dmul_rn(v, x)); }
+__device__ __forceinline__ float row_acc(float acc, float v, float x) { return fmaf(v, x, acc); }
+
+__device__ __forceinline__ void ld4(const double *p, double (&v)[4])
+{
+    const double2 a = __ldcs(reinterpret_cast<const double2 *>(p));
+    const double2 b = __ldcs(reinterpret_cast<const double2 *>(p) + 1);
+    v[0] = a.x;
+    v[1] = a.y;
+    v[2] = b.x;
+    v[3] = b.y;
+}
+__device__ __forceinline__ void ld4(const float *p, float (&v)[4])
+{
+    const float4 a = __ldcs(reinterpret_cast<const float4 *>(p));
+    v[0] = a.x;
+    v[1] = a.y;
+    v[2] = a.z;
+    v[3] = a.w;
+}
+
+template <typename V, class GX, class EPI>
+__device__ __forceinline__ void for_rows_sell(const Sell<V> &M, GX &gx, EPI &epi)
+{
+    const int lane = threadIdx.x & 31;
+    const uint32_t warps_total = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); s < M.n_slices; s += warps_total) {
+        const uint32_t row0 = s * 32u, row = row0 + lane;
+        const bool valid = row < M.n;
+        const uint32_t len = valid ? __ldg(&M.rp[row + 1]) - __ldg(&M.rp[row]) : 0u;
+        const uint32_t g4 = __ldg(&M.slice_len4[s]);
+        const size_t base = size_t(__ldg(&M.slice_ptr[s])) + 4u * lane;
+        V acc = V(0);
+#pragma unroll 2
+        for (uint32_t g = 0; g < g4; g++) {
+            const size_t e = base + size_t(g) * 128u;
+            V v[4];
+            ld4(M.val + e, v);
+            uint32_t c[4];
+            if (M.off) {
+                const short4 o = __ldcs(reinterpret_cast<const short4 *>(M.off + e));
+                c[0] = uint32_t(int(row0) + o.x);
+                c[1] = uint32_t(int(row0) + o.y);
+                c[2] = uint32_t(int(row0) + o.z);
+                c[3] = uint32_t(int(row0) + o.w);
+            } else {
+                const uint4 o = __ldcs(reinterpret_cast<const uint4 *>(M.col + e));
+                c[0] = o.x;
+                c[1] = o.y;
+                c[2] = o.z;
+                c[3] = o.w;
+            }
+#pragma unroll
+            for (int t = 0; t < 4; t++)
+                if (4u * g + t < len) acc = row_acc(acc, v[t], V(gx(c[t])));
+        }
+        if (valid) epi(row, acc);
+    }
+}
+
+template <typename V>
+inline Sell<V> sell_view(const rsg_csr *A);
+template <>
+inline Sell<double> sell_view<double>(const rsg_csr *A)
+{
+    return Sell<double>{A->rp, A->slice_ptr, A->slice_len4, A->sval, A->soff, A->scol, A->n, A->n_slices};
+}
+template <>
+inline Sell<float> sell_view<float>(const rsg_csr *A)
+{
+    return Sell<float>{A->rp, A->slice_ptr, A->slice_len4, A->sval32, A->soff, A->scol, A->n, A->n_slices};
+}
+
+// Runs the SELL path when the matrix has it, else the TMA-staged CSR stream.
+template <typename V, int RPW, class GX, class EPI>
+__device__ __forceinline__ void for_rows_any(const Csr<V> &M, const Sell<V> &S, bool use_sell, GX &gx, EPI &epi,
+                                             unsigned char *smem, unsigned int *err, bool evict_first)
+{
+    if (use_sell) for_rows_sell<V>(S, gx, epi);
+    else for_rows_tma<V, RPW>(M, gx, epi, smem, err, evict_first);
 }
 
 template <typename V>

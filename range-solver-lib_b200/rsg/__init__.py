@@ -37,7 +37,8 @@ def make_conf(solver: str | int = "cg", n_outer: int = 1000, n_inner: int = 30, 
               eps: float = 1e-14, stop_rule: str | int = "reference", rtol: float = 1e-10,
               precision: str | int = "fp64", scale_equations: bool = True, reliable_delta: float = 1e-2,
               flexible: bool = False, use_graph: bool = True, check_interval: int = 16,
-              output_frequency: int = 0, output_file: str | None = None) -> SolverConf:
+              output_frequency: int = 0, output_file: str | None = None,
+              l2_resident_f32: bool = False) -> SolverConf:
     c = SolverConf()
     _lib.load().rsg_conf_default(C.byref(c))
     c.solver_type = solver if isinstance(solver, int) else {"cg": SOLVER_CG, "gmres": SOLVER_GMRES}[solver]
@@ -57,6 +58,7 @@ def make_conf(solver: str | int = "cg", n_outer: int = 1000, n_inner: int = 30, 
     c.check_interval = check_interval
     c.output_frequency = output_frequency
     c.output_file = output_file.encode() if output_file else None
+    c.l2_resident_f32 = 1 if l2_resident_f32 else 0
     return c
 
 
@@ -147,6 +149,13 @@ class Context:
         self.check(self.lib.rsg_block_jacobi_build(self.h, A.h, block_size, _ptr(blocks_dev), C.byref(w)),
                    "block_jacobi_build")
         return w.value
+
+    def profile_kernel(self, A: "Matrix", kernel: int, reps: int = 20, flush_l2: bool = True) -> float:
+        """Average device seconds of one solver kernel (rsg_kernel_id) on A."""
+        t = C.c_double()
+        self.check(self.lib.rsg_profile_kernel(self.h, A.h, kernel, reps, 1 if flush_l2 else 0, C.byref(t)),
+                   "profile_kernel")
+        return t.value
 
     def true_relres(self, A: "Matrix", b_dev, x_dev) -> float:
         r = C.c_double()

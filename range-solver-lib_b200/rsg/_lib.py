@@ -52,7 +52,8 @@ class SolverConf(C.Structure):
         ("check_interval", C.c_uint32),
         ("learned", C.c_void_p),
         ("learned_initial_guess", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("l2_resident_f32", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
 
@@ -110,6 +111,7 @@ SIGNATURES = {
     "rsg_solve": (C.c_int, [_P, _P, C.POINTER(SolverConf), C.c_int32, C.c_uint32, _P, _P, C.c_int32,
                             C.POINTER(Stats)]),
     "rsg_true_relres": (C.c_int, [_P, _P, _P, _P, _DP]),
+    "rsg_profile_kernel": (C.c_int, [_P, _P, C.c_int32, C.c_uint32, C.c_int32, _DP]),
     "rsg_assembly_create_heat": (C.c_int, [_P, C.c_uint32, _P, C.c_uint32, _P, _P, C.c_uint32, _PP]),
     "rsg_assembly_create_stress": (C.c_int, [_P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32, _P, _P, C.c_uint32,
                                              _PP]),

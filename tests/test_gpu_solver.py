@@ -298,3 +298,20 @@ def test_convergence_log_file(ctx, tmp_path):
     assert lines[0] == "Iteration number|Solver residual|Solver convergence"
     its = [int(l.split("|")[0]) for l in lines[1:]]
     assert its[0] == 1 and its[-1] == st.iterations and all(i % 5 == 1 for i in its[:-1])
+
+
+def test_csr_stream_path_agrees_with_sell_path(ctx, monkeypatch):
+    """The TMA-staged CSR-stream SpMV (used when SELL-32 padding would cost
+    more than 25%) and the SELL-32 path give the same solution."""
+    A, b = heat(14, sigma=1.5, seed=3, source="random")
+    conf = rsg.make_conf(n_outer=20000, stop_rule="true", rtol=1e-11)
+    M_sell = ctx.matrix(A.rp, A.ci, A.val)
+    monkeypatch.setenv("RSG_NO_SELL", "1")
+    M_csr = ctx.matrix(A.rp, A.ci, A.val)
+    monkeypatch.delenv("RSG_NO_SELL")
+    for precision in ("fp64", "mixed"):
+        conf = rsg.make_conf(n_outer=20000, stop_rule="true", rtol=1e-11, precision=precision)
+        x1, s1 = ctx.solve(M_sell, b, conf=conf)
+        x2, s2 = ctx.solve(M_csr, b, conf=conf)
+        assert s1.true_relres <= 1e-11 and s2.true_relres <= 1e-11
+        assert rel_err(x1, x2) < 1e-9
