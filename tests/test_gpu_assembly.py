@@ -77,6 +77,7 @@ def test_heat_assembly_device_inputs(ctx, torch_cuda):
     asm = rsg.Assembly.heat(ctx, p)
     b = torch.empty(p.n_free, dtype=torch.float64, device="cuda")
     d = {k: torch.tensor(getattr(p, k), device="cuda") for k in ("k_e", "q_e", "rhoc_e", "node_t")}
+    torch.cuda.synchronize()  # the library runs on its own stream
     M = asm.assemble(p, b, inputs_on_device=d)
     ctx.sync()
     Ao, bo = O.assemble_heat(p)
@@ -109,6 +110,7 @@ def test_gpu_assembly_then_solve_patch_test(ctx, torch_cuda):
     p = W.heat_cube(10, source="none")
     asm, M, b = run_heat(ctx, torch, p)
     x = torch.zeros_like(b)
+    torch.cuda.synchronize()
     _, st = ctx.solve(M, b, x, conf=rsg.make_conf(n_outer=10000, stop_rule="true", rtol=1e-13))
     full = p.node_t.copy()
     free = p.book != W.EOD

@@ -84,11 +84,13 @@ def test_spmv_fp64_and_fp32_match_oracle(ctx, torch_cuda, which):
     absrow = O.spmv(O.CSR(A.n, A.rp, A.ci, np.abs(A.val)), np.abs(x))
     xd = torch.tensor(x, device="cuda")
     yd = torch.empty_like(xd)
+    torch.cuda.synchronize()  # the library runs on its own stream
     ctx.spmv(M, xd, yd)
     ctx.sync()
     assert np.all(np.abs(yd.cpu().numpy() - y_ref) <= 1e-13 * absrow + 1e-300)
     x32 = torch.tensor(x, device="cuda", dtype=torch.float32)
     y32 = torch.empty_like(x32)
+    torch.cuda.synchronize()
     ctx.spmv_f32(M, x32, y32)
     ctx.sync()
     assert np.all(np.abs(y32.cpu().numpy().astype(np.float64) - y_ref) <= 2e-6 * absrow + 1e-30)
@@ -201,6 +203,7 @@ def test_deterministic_repeat_and_device_arrays(ctx, torch_cuda):
     assert np.array_equal(x1, x2)
     bd = torch.tensor(b, device="cuda")
     xd = torch.zeros_like(bd)
+    torch.cuda.synchronize()
     _, st = ctx.solve(M, bd, xd, conf=conf)
     assert np.array_equal(xd.cpu().numpy(), x1)
 
