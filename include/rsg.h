@@ -179,6 +179,26 @@ RSG_API rsg_status rsg_profile_kernel(rsg_context *ctx, const rsg_csr *A, int32_
 RSG_API rsg_status rsg_true_relres(rsg_context *ctx, const rsg_csr *A, const double *b, const double *x,
                                    double *relres);
 
+/* No counterpart in the reference.  The FP64 true relative residual of
+ * rsg_true_relres for callers that cannot allocate device memory -- host
+ * applications that give all device memory to their own pool allocator, or
+ * that cannot accept the device-wide synchronisation of cudaMalloc/cudaFree
+ * inside their loop.  It creates no context or handle and allocates nothing:
+ * row_ptr (n_rows+1), col_idx, values, b, x and out3 are caller-owned device
+ * arrays, out3 receives {||b - A x||, ||b||, ||b - A x|| / ||b||}, and the
+ * kernel runs on `stream` (NULL = legacy default stream) without waiting for it.
+ * Its scratch is a fixed 1 MiB array inside the library, held by every GPU that
+ * loads the library until the process exits; n_rows above
+ * RSG_NOALLOC_MAX_ROWS is rejected with RSG_ERR_INVALID_ARG.  Calls share that
+ * array: calls whose kernels overlap on the GPU race and give wrong results,
+ * so order them on one stream.  The first call on a device looks up the
+ * array's address with that device current; make it before any stream
+ * capture.  A column index >= n_rows is not read and makes the result NaN. */
+#define RSG_NOALLOC_MAX_ROWS 2097152u
+RSG_API rsg_status rsg_true_relres_noalloc(uint32_t n_rows, const uint32_t *row_ptr, const uint32_t *col_idx,
+                                           const double *values, const double *b, const double *x, double *out3,
+                                           void *stream);
+
 /* ---- assembly (RSolverHeat / RSolverStress prepare + assemblyMatrix) ----
  * A plan is the sparsity pattern of the free-DOF system plus the
  * element-to-nonzero scatter map (the reference precedent is

@@ -31,6 +31,7 @@ PREC_NONE, PREC_JACOBI, PREC_BLOCK_JACOBI, PREC_LEARNED = 0, 1, 2, 3
 STOP_REFERENCE, STOP_TRUE_RELRES = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 MEM_HOST, MEM_DEVICE = 0, 1
+NOALLOC_MAX_ROWS = 2097152
 
 
 class SolverConf(C.Structure):
@@ -112,6 +113,7 @@ SIGNATURES = {
                             C.POINTER(Stats)]),
     "rsg_true_relres": (C.c_int, [_P, _P, _P, _P, _DP]),
     "rsg_profile_kernel": (C.c_int, [_P, _P, C.c_int32, C.c_uint32, C.c_int32, _DP]),
+    "rsg_true_relres_noalloc": (C.c_int, [C.c_uint32, _P, _P, _P, _P, _P, _P, _P]),
     "rsg_assembly_create_heat": (C.c_int, [_P, C.c_uint32, _P, C.c_uint32, _P, _P, C.c_uint32, _PP]),
     "rsg_assembly_create_stress": (C.c_int, [_P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32, _P, _P, C.c_uint32,
                                              _PP]),
