@@ -128,8 +128,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         asm_ms.append(ev[0].elapsed_time(ev[1]))
 
     conf_mixed = rsg.make_conf(n_outer=50000, stop_rule="true", rtol=RTOL, precision="mixed",
-                               reliable_delta=args.delta)
-    conf_fp64 = rsg.make_conf(n_outer=50000, stop_rule="true", rtol=RTOL, precision="fp64")
+                               reliable_delta=args.delta, use_graph=not args.host_loop)
+    conf_fp64 = rsg.make_conf(n_outer=50000, stop_rule="true", rtol=RTOL, precision="fp64",
+                              use_graph=not args.host_loop)
 
     def step(conf):
         flush.fill_(1)  # evict L2 between steps (not timed)
@@ -186,13 +187,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     by32 = spmv_bytes(n, nnz, 4, 2, 4)
     achieved64 = by64 / kd["cg_dir_fp64"]["cold_s"] / 1e9
     achieved32 = by32 / kd["cg_dir_mixed"]["cold_s"] / 1e9
-    traffic = None
-    tf = os.path.join(REPO, "profiles", "traffic.json")
-    if os.path.exists(tf):
-        try:
-            traffic = json.load(open(tf)).get("cg_dir_mixed_bytes_per_launch")
-        except Exception:
-            traffic = None
+    # DRAM bytes (read + write) of one k_mx_dir launch on this workload, from the ncu capture
+    # summarised in profiles/k_mx_dir_heat_lognormal_100.md
+    traffic = 113.0e6 if N_HEX == 100 else None
 
     # launches per solve: setup (norm, 2 scalings, Jacobi, FP32 copy, init residual + z, fold,
     # unscale, true residual) + per 2-iteration graph body (3 kernels per iteration + tail)
@@ -245,6 +242,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--delta", type=float, default=1e-2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--host-loop", action="store_true",
+                    help="drive the CG loop from the host (same kernels, launched one by one) so that "
+                         "profilers which cannot see kernels inside conditional CUDA graphs list them")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 

@@ -669,8 +669,9 @@ rsg_status run_typed(rsg_context *ctx, const CgArgs &a, double *seconds)
     set_smem(k_mx_dir<RPW>, tma_smem<float>());
     set_smem(k_mx_check<RPW, PK>, tma_smem<double>());
     const long long chunk_threads = (long long)a.A->n * 32 / RPW;
-    L.g_spmv64 = std::min(grid_for(ctx, (const void *)k_cg_dir<RPW>, kBlock, L.s64, chunk_threads), kMaxGrid);
-    L.g_spmv32 = std::min(grid_for(ctx, (const void *)k_mx_dir<RPW>, kBlock, L.s32, chunk_threads), kMaxGrid);
+    (void)chunk_threads;
+    L.g_spmv64 = spmv_grid(ctx, a.A, (const void *)k_cg_dir<RPW>, L.s64, RPW);
+    L.g_spmv32 = spmv_grid(ctx, a.A, (const void *)k_mx_dir<RPW>, L.s32, RPW);
     L.g_vec = std::min(grid_for(ctx, (const void *)k_cg_update<PK>, kBlock, 0, a.A->n), kMaxGrid);
 
     RSG_CHECK_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
@@ -797,8 +798,9 @@ rsg_status profile_typed(rsg_context *ctx, const rsg_csr *A, int kernel, uint32_
     const Sell<float> S32 = sell_view<float>(A);
     const int us = A->use_sell;
     const long long ct = (long long)n * 32 / RPW;
-    const int g64 = std::min(grid_for(ctx, (const void *)k_cg_dir<RPW>, kBlock, s64, ct), kMaxGrid);
-    const int g32 = std::min(grid_for(ctx, (const void *)k_mx_dir<RPW>, kBlock, s32, ct), kMaxGrid);
+    (void)ct;
+    const int g64 = spmv_grid(ctx, A, (const void *)k_cg_dir<RPW>, s64, RPW);
+    const int g32 = spmv_grid(ctx, A, (const void *)k_mx_dir<RPW>, s32, RPW);
     const int gv = std::min(grid_for(ctx, (const void *)k_cg_update<1>, kBlock, 0, n), kMaxGrid);
     const Csr<double> M64 = view<double>(A, true);
     const Csr<float> M32 = view<float>(A, true);

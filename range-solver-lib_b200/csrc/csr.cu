@@ -330,7 +330,7 @@ rsg_status spmv64(rsg_context *ctx, const rsg_csr *A, const double *x, double *y
     RSG_RPW_DISPATCH(pick_rpw(A), {
         auto k = k_spmv<double, RPW>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tma_smem<double>()));
-        const int grid = grid_for(ctx, (const void *)k, kBlock, smem, (long long)A->n * 32 / RPW);
+        const int grid = spmv_grid(ctx, A, (const void *)k, smem, RPW);
         k<<<grid, kBlock, smem, ctx->stream>>>(M, sell_view<double>(A), A->use_sell, x, y, ctx->errw);
     });
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
@@ -344,7 +344,7 @@ rsg_status spmv32(rsg_context *ctx, const rsg_csr *A, const float *x, float *y, 
     RSG_RPW_DISPATCH(pick_rpw(A), {
         auto k = k_spmv<float, RPW>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tma_smem<float>()));
-        const int grid = grid_for(ctx, (const void *)k, kBlock, smem, (long long)A->n * 32 / RPW);
+        const int grid = spmv_grid(ctx, A, (const void *)k, smem, RPW);
         k<<<grid, kBlock, smem, ctx->stream>>>(M, sell_view<float>(A), A->use_sell, x, y, ctx->errw);
     });
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
@@ -382,8 +382,7 @@ rsg_status true_residual(rsg_context *ctx, const rsg_csr *A, const double *b, co
     RSG_RPW_DISPATCH(pick_rpw(A), {
         auto k = k_true_res<RPW>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tma_smem<double>()));
-        const int grid = std::min(grid_for(ctx, (const void *)k, kBlock, smem, (long long)A->n * 32 / RPW),
-                                  kMaxGrid);
+        const int grid = spmv_grid(ctx, A, (const void *)k, smem, RPW);
         k<<<grid, kBlock, smem, ctx->stream>>>(M, sell_view<double>(A), A->use_sell, b, x, partials, ticket, out3,
                                                ctx->errw);
     });

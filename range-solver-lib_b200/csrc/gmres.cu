@@ -293,8 +293,9 @@ rsg_status run_typed(rsg_context *ctx, const GmresArgs &a, double *seconds)
     const Sell<double> S = sell_view<double>(a.A);
     const int us = a.A->use_sell;
     const long long ct = (long long)n * 32 / RPW;
-    const int g_sp = std::min(grid_for(ctx, (const void *)k_gm_spmv<RPW>, kBlock, s64, ct), kMaxGrid);
-    const int g_res = std::min(grid_for(ctx, (const void *)k_gm_residual<RPW>, kBlock, s64, ct), kMaxGrid);
+    (void)ct;
+    const int g_sp = spmv_grid(ctx, a.A, (const void *)k_gm_spmv<RPW>, s64, RPW);
+    const int g_res = spmv_grid(ctx, a.A, (const void *)k_gm_residual<RPW>, s64, RPW);
     const int g_vec = std::min(grid_for(ctx, (const void *)k_gm_correct, kBlock, 0, n), kMaxGrid);
     const int g_dot = std::min(std::min(grid_for(ctx, (const void *)k_gm_dots, kBlock, 0, n), 512), kMaxGrid);
 

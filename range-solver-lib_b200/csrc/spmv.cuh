@@ -478,7 +478,7 @@ __device__ __forceinline__ void for_rows_sell(const Sell<V> &M, GX &gx, EPI &epi
         const uint32_t g4 = __ldg(&M.slice_len4[s]);
         const size_t base = size_t(__ldg(&M.slice_ptr[s])) + 4u * lane;
         V acc = V(0);
-#pragma unroll 2
+#pragma unroll 4
         for (uint32_t g = 0; g < g4; g++) {
             const size_t e = base + size_t(g) * 128u;
             V v[4];
