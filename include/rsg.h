@@ -199,6 +199,28 @@ RSG_API rsg_status rsg_true_relres_noalloc(uint32_t n_rows, const uint32_t *row_
                                            const double *values, const double *b, const double *x, double *out3,
                                            void *stream);
 
+/* ---- batched solves ----
+ * Many independent systems of uneven size solved together (the reference
+ * solves one system per RMatrixSolver::solve call, src/rmatrixsolver.cpp:158-201,
+ * e.g. once per load case or per mesh).  The caller passes the systems as one
+ * block-diagonal CSR (host arrays): system s owns rows and columns
+ * [sys_row_begin[s], sys_row_begin[s+1]).  Each system is solved with CG (NONE
+ * or JACOBI) to the FP64 true relative residual conf->rtol (stop_rule must be
+ * RSG_STOP_TRUE_RELRES), in FP64 or mixed precision, with its own iteration
+ * count and convergence; the whole batch is one device-driven loop. */
+typedef struct rsg_batch rsg_batch;
+RSG_API rsg_status rsg_batch_create(rsg_context *ctx, uint32_t n_systems, const uint32_t *sys_row_begin,
+                                    const uint32_t *row_ptr, const uint32_t *col_idx, const double *values,
+                                    rsg_batch **out);
+RSG_API void       rsg_batch_destroy(rsg_context *ctx, rsg_batch *batch);
+RSG_API rsg_status rsg_batch_info(const rsg_batch *batch, uint32_t *n_systems, uint32_t *rows,
+                                  uint32_t *padded_rows, uint64_t *nnz);
+/* b and x: concatenated per system (rows of sys_row_begin), host or device per `memory`; x is in/out.
+ * per_system (n_systems entries) and summary may be NULL. */
+RSG_API rsg_status rsg_batch_solve(rsg_context *ctx, rsg_batch *batch, const rsg_solver_conf *conf, int32_t prec_type,
+                                   const double *b, double *x, int32_t memory, rsg_stats *per_system,
+                                   rsg_stats *summary);
+
 /* ---- assembly (RSolverHeat / RSolverStress prepare + assemblyMatrix) ----
  * A plan is the sparsity pattern of the free-DOF system plus the
  * element-to-nonzero scatter map (the reference precedent is

@@ -32,128 +32,6 @@
 
 namespace rsg {
 
-// ---------------- state transitions (thread 0 of the last block) ----------------
-
-__device__ void finalize_update64(CgState *st, double rz, double rr, double xx)
-{
-    st->rho_new = rz;
-    st->beta = rz / st->rho;
-    const double rn = sqrt(rr), xn = sqrt(xx);
-    st->rn = rn;
-    st->xn = xn;
-    double norm = st->an * xn + st->bn;
-    if (fabs(norm) < st->eps) norm = st->eps;
-    const double err = rn / norm;
-    st->trend = err - st->error;
-    st->error = err;
-    const uint32_t it = ++st->it;
-    if (st->history) {
-        st->history[it - 1] = err;
-        st->trend_hist[it - 1] = st->trend;
-    }
-    if (st->stop_rule == RSG_STOP_REFERENCE) {
-        // RIterationInfo::hasConverged, src/riterationinfo.cpp:90-109
-        const bool conv = !dev_isnormal(err) || !dev_isnormal(st->trend) || err < st->cvg ||
-                          fabs(st->trend) < st->eps * st->eps;
-        if (conv) {
-            st->done = 1;
-            st->converged = 1;
-            st->status = isfinite(err) ? RSG_OK : RSG_BREAKDOWN;
-        } else if (it >= st->max_it) {
-            st->done = 1;
-            st->status = RSG_NOT_CONVERGED;
-        }
-    } else {
-        if (!isfinite(rn)) {
-            st->done = 1;
-            st->status = RSG_BREAKDOWN;
-        } else if (rn <= st->rtol * st->bn) {
-            st->need_check = 1;
-        } else if (it >= st->max_it) {
-            st->done = 1;
-            st->status = RSG_NOT_CONVERGED;
-        }
-    }
-}
-
-__device__ void finalize_check64(CgState *st, double rz, double rn)
-{
-    st->n_updates++;
-    st->rn = rn;
-    if (!isfinite(rn)) {
-        st->done = 1;
-        st->status = RSG_BREAKDOWN;
-    } else if (rn <= st->rtol * st->bn) {
-        st->done = 1;
-        st->converged = 1;
-        st->status = RSG_OK;
-    } else {
-        // the recurrence drifted from the true residual: restart the direction
-        // (p = z) so that a tolerance below the attainable accuracy stagnates
-        // instead of diverging
-        st->rho_new = rz;
-        st->beta = 0.0;
-        st->need_check = 0;
-        if (st->it >= st->max_it) {
-            st->done = 1;
-            st->status = RSG_NOT_CONVERGED;
-        }
-    }
-}
-
-__device__ void finalize_update_mixed(CgState *st, double rz, double rr)
-{
-    st->rho_new = rz;
-    st->beta = rz / st->rho;
-    const double rn = sqrt(rr) / st->sigma;
-    st->rn = rn;
-    const uint32_t it = ++st->it;
-    const double rel = st->bn > 0.0 ? rn / st->bn : rn;
-    st->trend = rel - st->error;
-    st->error = rel;
-    if (st->history) {
-        st->history[it - 1] = rel;
-        st->trend_hist[it - 1] = st->trend;
-    }
-    if (!isfinite(rn) || rn <= st->rtol * st->bn || rn <= st->delta * st->max_r) st->need_check = 1;
-    else if (it >= st->max_it) {
-        st->done = 1;
-        st->status = RSG_NOT_CONVERGED;
-    }
-}
-
-__device__ void finalize_check_mixed(CgState *st, double rz, double rn)
-{
-    st->n_updates++;
-    st->fold = 1;
-    st->rn = rn;
-    if (!isfinite(rn)) {
-        st->done = 1;
-        st->status = RSG_BREAKDOWN;
-    } else if (rn <= st->rtol * st->bn) {
-        st->done = 1;
-        st->converged = 1;
-        st->status = RSG_OK;
-    } else {
-        st->max_r = rn;
-        st->rho_new = rz;
-        st->beta = rz / st->rho;
-        st->need_check = 0;
-        if (st->it >= st->max_it) {
-            st->done = 1;
-            st->status = RSG_NOT_CONVERGED;
-        }
-    }
-}
-
-__device__ __forceinline__ double clamp_pq(double pq, double eps)
-{
-    // src/rmatrixsolver.cpp:304-315
-    if (pq > 0.0) return fmax(pq, eps);
-    if (pq < 0.0) return fmin(pq, -eps);
-    return eps;
-}
-
 // ---------------- FP64 kernels ----------------
 
 template <int RPW>

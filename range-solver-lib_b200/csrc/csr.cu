@@ -229,8 +229,8 @@ static void free_csr(rsg_csr *A)
     delete A;
 }
 
-// Build the SELL-32 copy when its padding costs at most 25% over the CSR.
-static rsg_status build_sell(rsg_context *ctx, rsg_csr *A)
+// Build the SELL-32 copy when its padding costs at most 25% over the CSR (or always when forced).
+static rsg_status build_sell(rsg_context *ctx, rsg_csr *A, bool force)
 {
     A->n_slices = (A->n + 31u) / 32u;
     if (cudaMalloc(&A->slice_len4, size_t(A->n_slices) * sizeof(uint32_t)) != cudaSuccess)
@@ -252,7 +252,7 @@ static rsg_status build_sell(rsg_context *ctx, rsg_csr *A)
         }
     }
     ptr[A->n_slices] = uint32_t(total);
-    if (A->nnz == 0 || double(total) > 1.25 * double(A->nnz)) {
+    if (A->nnz == 0 || (!force && double(total) > 1.25 * double(A->nnz))) {
         free_sell(A);
         return RSG_OK;
     }
@@ -399,6 +399,14 @@ extern "C" {
 rsg_status rsg_csr_create(rsg_context *ctx, uint32_t n, const uint32_t *rp, const uint32_t *ci, const double *val,
                           int32_t memory, rsg_csr **out)
 {
+    return csr_create_ex(ctx, n, rp, ci, val, memory, std::getenv("RSG_NO_SELL") ? -1 : 0, out);
+}
+
+}  // extern "C"
+
+rsg_status rsg::csr_create_ex(rsg_context *ctx, uint32_t n, const uint32_t *rp, const uint32_t *ci, const double *val,
+                              int32_t memory, int sell_mode, rsg_csr **out)
+{
     if (!ctx || !out || !rp || n == 0) return set_error(ctx, RSG_ERR_INVALID_ARG, "csr_create: bad arguments");
     *out = nullptr;
     RSG_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
@@ -434,11 +442,13 @@ rsg_status rsg_csr_create(rsg_context *ctx, uint32_t n, const uint32_t *rp, cons
         (nnz32 && cudaMemcpyAsync(A->val, val, size_t(nnz32) * sizeof(double), kind, ctx->stream) != cudaSuccess))
         return fail(set_error(ctx, RSG_ERR_CUDA, "csr_create: upload failed"));
     rsg_status s = analyze(ctx, A, false);
-    if (s == RSG_OK && std::getenv("RSG_NO_SELL") == nullptr) s = build_sell(ctx, A);
+    if (s == RSG_OK && sell_mode >= 0) s = build_sell(ctx, A, sell_mode > 0);
     if (s != RSG_OK) return fail(s);
     *out = A;
     return RSG_OK;
 }
+
+extern "C" {
 
 rsg_status rsg_csr_update_values(rsg_context *ctx, rsg_csr *A, const double *val, int32_t memory)
 {

@@ -43,6 +43,9 @@ inline int spmv_grid(rsg_context *ctx, const rsg_csr *A, const void *kernel, siz
 
 rsg_status spmv64(rsg_context *ctx, const rsg_csr *A, const double *x, double *y, bool off16);
 rsg_status spmv32(rsg_context *ctx, const rsg_csr *A, const float *x, float *y, bool off16);
+// rsg_csr_create with an explicit SELL-32 choice: 0 = when padding costs <= 25%, 1 = always, -1 = never.
+rsg_status csr_create_ex(rsg_context *ctx, uint32_t n, const uint32_t *rp, const uint32_t *ci, const double *val,
+                         int32_t memory, int sell_mode, rsg_csr **out);
 // Recompute ||A||_F and the FP32 copy after the values were rewritten in place.
 rsg_status csr_refresh(rsg_context *ctx, rsg_csr *A);
 rsg_status jacobi_build(rsg_context *ctx, const rsg_csr *A, double *d);

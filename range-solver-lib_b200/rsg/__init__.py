@@ -18,7 +18,7 @@ from ._lib import (BREAKDOWN, ERR_INVALID_ARG, ERR_SINGULAR, ERR_UNSUPPORTED, ME
                    OK, PREC_BLOCK_JACOBI, PREC_JACOBI, PREC_LEARNED, PREC_NONE, PRECISION_FP64, PRECISION_MIXED,
                    SOLVER_CG, SOLVER_GMRES, STOP_REFERENCE, STOP_TRUE_RELRES, RsgError, SolverConf, Stats, Time)
 
-__all__ = ["Context", "Matrix", "Assembly", "make_conf", "RsgError", "SolverConf", "Stats", "Solver"]
+__all__ = ["Context", "Matrix", "Assembly", "Batch", "make_conf", "RsgError", "SolverConf", "Stats", "Solver"]
 
 
 def _ptr(a) -> C.c_void_p:
@@ -313,6 +313,69 @@ class Assembly:
             self.A = None
         if self.h and self.ctx.h:
             self.ctx.lib.rsg_assembly_destroy(self.ctx.h, self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Independent systems of uneven size solved together (rsg_batch).
+
+    systems: list of (row_ptr, col_idx, values) host CSR arrays, one per system.
+    """
+
+    def __init__(self, ctx: Context, systems):
+        self.ctx = ctx
+        sizes = [len(rp) - 1 for rp, _, _ in systems]
+        self.row_begin = np.zeros(len(systems) + 1, np.uint32)
+        self.row_begin[1:] = np.cumsum(sizes)
+        rps, cis, vals = [], [], []
+        nnz_off = 0
+        for (rp, ci, val), r0 in zip(systems, self.row_begin[:-1]):
+            rp = np.asarray(rp, np.int64)
+            rps.append(rp[:-1] + nnz_off)
+            cis.append(np.asarray(ci, np.int64) + int(r0))
+            vals.append(np.asarray(val, np.float64))
+            nnz_off += int(rp[-1])
+        self.rp = np.ascontiguousarray(np.concatenate(rps + [np.array([nnz_off])]).astype(np.uint32))
+        self.ci = np.ascontiguousarray(np.concatenate(cis).astype(np.uint32))
+        self.val = np.ascontiguousarray(np.concatenate(vals))
+        self.sizes = sizes
+        h = C.c_void_p()
+        ctx.check(ctx.lib.rsg_batch_create(ctx.h, len(systems), _ptr(self.row_begin), _ptr(self.rp), _ptr(self.ci),
+                                           _ptr(self.val), C.byref(h)), "batch_create")
+        self.h = h
+        ns, rows, prow, nnz = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint64()
+        ctx.lib.rsg_batch_info(h, C.byref(ns), C.byref(rows), C.byref(prow), C.byref(nnz))
+        self.n_systems, self.rows, self.padded_rows, self.nnz = ns.value, rows.value, prow.value, nnz.value
+
+    def split(self, v):
+        return [v[self.row_begin[i]:self.row_begin[i + 1]] for i in range(self.n_systems)]
+
+    def solve(self, b, x=None, conf: SolverConf | None = None, prec: int = PREC_JACOBI,
+              allow=(OK, NOT_CONVERGED, BREAKDOWN)):
+        """Returns (x, per-system Stats list, summary Stats)."""
+        conf = conf or make_conf(stop_rule="true")
+        per = (Stats * self.n_systems)()
+        summ = Stats()
+        if _is_device(b):
+            s = self.ctx.lib.rsg_batch_solve(self.ctx.h, self.h, C.byref(conf), prec, _ptr(b), _ptr(x), MEM_DEVICE,
+                                             per, C.byref(summ))
+        else:
+            b = np.ascontiguousarray(b, np.float64)
+            x = np.zeros(self.rows) if x is None else np.array(x, np.float64, copy=True)
+            s = self.ctx.lib.rsg_batch_solve(self.ctx.h, self.h, C.byref(conf), prec, _ptr(b), _ptr(x), MEM_HOST,
+                                             per, C.byref(summ))
+        self.ctx.check(s, "batch_solve", allow)
+        return x, list(per), summ
+
+    def close(self):
+        if self.h and self.ctx.h:
+            self.ctx.lib.rsg_batch_destroy(self.ctx.h, self.h)
         self.h = None
 
     def __del__(self):

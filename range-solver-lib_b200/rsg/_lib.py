@@ -114,6 +114,10 @@ SIGNATURES = {
     "rsg_true_relres": (C.c_int, [_P, _P, _P, _P, _DP]),
     "rsg_profile_kernel": (C.c_int, [_P, _P, C.c_int32, C.c_uint32, C.c_int32, _DP]),
     "rsg_true_relres_noalloc": (C.c_int, [C.c_uint32, _P, _P, _P, _P, _P, _P, _P]),
+    "rsg_batch_create": (C.c_int, [_P, C.c_uint32, _P, _P, _P, _P, _PP]),
+    "rsg_batch_destroy": (None, [_P, _P]),
+    "rsg_batch_info": (C.c_int, [_P, _U32P, _U32P, _U32P, _U64P]),
+    "rsg_batch_solve": (C.c_int, [_P, _P, C.POINTER(SolverConf), C.c_int32, _P, _P, C.c_int32, _P, _P]),
     "rsg_assembly_create_heat": (C.c_int, [_P, C.c_uint32, _P, C.c_uint32, _P, _P, C.c_uint32, _PP]),
     "rsg_assembly_create_stress": (C.c_int, [_P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32, _P, _P, C.c_uint32,
                                              _PP]),
