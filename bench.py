@@ -242,6 +242,10 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--delta", type=float, default=1e-2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="heat100", choices=["heat100", "stress", "batch256", "transient40"],
+                    help="heat100 (default, the headline); stress: 64x32x32 elasticity beam; batch256: 256 "
+                         "independent heat cubes with 8..60 hexes per side; transient40: 64 backward-Euler steps "
+                         "on a 40^3 mesh")
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the CG loop from the host (same kernels, launched one by one) so that "
                          "profilers which cannot see kernels inside conditional CUDA graphs list them")
@@ -252,6 +256,9 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     threads = os.cpu_count() or 1
+
+    if args.workload != "heat100":
+        return run_other(args, rank, world, local_rank, threads)
 
     if args.impl == "reference":
         if rank != 0:
@@ -336,6 +343,143 @@ def main():
                                 "sample": "one full FP64 Jacobi-PCG solve (OpenMP oracle) of the same system",
                                 "iterations": cpu["iterations"], "true_relres": cpu["relres"]}
     print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _events_time(fn, stream):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    out = fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / 1e3, out
+
+
+def run_other(args, rank, world, local_rank, threads):
+    """Secondary workloads (one JSON line each); the driver's default is heat100."""
+    import torch
+    import rsg
+    from rsg import workloads as W
+    from oracle import oracle as O
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=900))
+    torch.cuda.set_device(local_rank)
+    ctx = rsg.Context(local_rank)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    line = {"n_gpus": world, "steps": args.steps, "warmup": args.warmup, "vs_baseline": None, "data": "synthetic",
+            "scaling": "weak"}
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        import torch.distributed as dist
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    if args.workload == "stress":
+        p = W.stress_beam(64, 32, 32)
+        asm = rsg.Assembly.stress(ctx, p)
+        b = torch.empty(asm.n_free, dtype=torch.float64, device="cuda")
+        x = torch.zeros_like(b)
+        A = asm.assemble(p, b)
+        res = {}
+        for name, prec, blk, precision in (("jacobi_fp64", rsg.PREC_JACOBI, 1, "fp64"),
+                                           ("jacobi_mixed", rsg.PREC_JACOBI, 1, "mixed"),
+                                           ("block3_fp64", rsg.PREC_BLOCK_JACOBI, 3, "fp64"),
+                                           ("block3_mixed", rsg.PREC_BLOCK_JACOBI, 3, "mixed")):
+            conf = rsg.make_conf(n_outer=100000, stop_rule="true", rtol=RTOL, precision=precision)
+            for _ in range(args.warmup):
+                x.zero_()
+                ctx.solve(A, b, x, conf=conf, prec=prec, block_size=blk)
+            tot = 0.0
+            for _ in range(args.steps):
+                flush.fill_(1)
+                x.zero_()
+                t, (_, st) = _events_time(lambda: ctx.solve(A, b, x, conf=conf, prec=prec, block_size=blk), stream)
+                tot += t
+            res[name] = {"s": max_over_ranks(tot / args.steps), "iterations": st.iterations,
+                         "true_relres": st.true_relres}
+        best = min(res, key=lambda k: res[k]["s"])
+        line.update({"metric": "time-to-solve (s) at FP64 rel. residual 1e-10, 64x32x32 elasticity beam",
+                     "value": res[best]["s"], "unit": "s", "ms_per_step": res[best]["s"] * 1e3,
+                     "higher_is_better": False, "dtype": "f64 / f32-inner",
+                     "config": {"workload": "stress_beam_64x32x32", "n_free": A.n, "nnz": A.nnz, "best": best,
+                                "variants": res}})
+        if world == 1 and not args.no_cpu_baseline:
+            rp, ci, val = A.to_host()
+            xo, sto = O.solve(O.CSR(A.n, rp, ci, val), b.cpu().numpy(), prec=1, n_outer=100000, stop_rule="true",
+                              rtol=RTOL, threads=threads)
+            line["cpu_baseline"] = {"value": sto.seconds, "unit": "s", "cores": threads, "kind": "port",
+                                    "sample": "one full FP64 Jacobi-PCG solve of the same system",
+                                    "iterations": sto.iterations}
+    elif args.workload == "batch256":
+        rng = np.random.default_rng(1000 + rank)
+        sizes = rng.integers(8, 61, 256)
+        systems, rhs = [], []
+        for i, n in enumerate(sizes):
+            p = W.heat_cube(int(n), sigma=1.0, seed=10000 * rank + i, source="random")
+            asm = rsg.Assembly.heat(ctx, p)
+            bb = torch.empty(asm.n_free, dtype=torch.float64, device="cuda")
+            A = asm.assemble(p, bb)
+            systems.append(A.to_host())
+            rhs.append(bb.cpu().numpy())
+            asm.close()
+        batch = rsg.Batch(ctx, systems)
+        b_all = torch.from_numpy(np.concatenate(rhs)).cuda()
+        x_all = torch.zeros_like(b_all)
+        res = {}
+        for precision in ("fp64", "mixed"):
+            conf = rsg.make_conf(n_outer=100000, stop_rule="true", rtol=RTOL, precision=precision,
+                                 use_graph=not args.host_loop)
+            for _ in range(args.warmup):
+                x_all.zero_()
+                batch.solve(b_all, x_all, conf=conf)
+            tot = 0.0
+            for _ in range(args.steps):
+                flush.fill_(1)
+                x_all.zero_()
+                t, (_, per, summ) = _events_time(lambda: batch.solve(b_all, x_all, conf=conf), stream)
+                tot += t
+            res[precision] = {"s": max_over_ranks(tot / args.steps), "max_iterations": summ.iterations,
+                              "worst_true_relres": summ.true_relres}
+        t_best = min(r["s"] for r in res.values())
+        line.update({"metric": "systems solved per second to FP64 rel. residual 1e-10 (256 uneven heat systems per GPU)",
+                     "value": 256 * world / t_best, "unit": "systems/s", "ms_per_step": t_best * 1e3,
+                     "higher_is_better": True, "dtype": "f64 / f32-inner",
+                     "config": {"workload": "batch256_heat_8to60", "rows": batch.rows, "nnz": batch.nnz,
+                                "parallelism": f"independent shards x{world}", "variants": res}})
+        if world == 1 and not args.no_cpu_baseline:
+            t0 = time.perf_counter()
+            for (rp, ci, val), bb in list(zip(systems, rhs))[:16]:
+                O.solve(O.CSR(len(rp) - 1, rp, ci, val), bb, prec=1, n_outer=100000, stop_rule="true", rtol=RTOL,
+                        threads=threads)
+            t16 = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": 16 / t16, "unit": "systems/s", "cores": threads, "kind": "port",
+                                    "sample": "the first 16 systems of the batch, solved one after another"}
+    else:  # transient40
+        p = W.heat_cube(40, sigma=1.0, seed=rank, source="random", transient=True, dt=1e-3)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        steps = rsg.transient_heat(ctx, p, 64)
+        t = max_over_ranks((time.perf_counter() - t0) / 64)
+        line.update({"metric": "seconds per backward-Euler step (GPU re-assembly + solve to 1e-10), 40^3 heat",
+                     "value": t, "unit": "s", "ms_per_step": t * 1e3, "higher_is_better": False, "dtype": "f64",
+                     "config": {"workload": "transient_heat_40_64steps", "steps": 64,
+                                "iterations_per_step": [int(st.iterations) for _, st in steps[:8]],
+                                "note": "wall clock per step including the host read-back of T"}})
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()

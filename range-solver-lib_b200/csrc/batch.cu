@@ -47,6 +47,14 @@ struct BView {
     uint32_t n_slices, n_sys;
 };
 
+// Systems a kernel visits: ids and the exclusive prefix of their slice counts.
+struct Active {
+    uint32_t n_sys;      // number of listed systems
+    uint32_t n_slices;   // their slices in total
+    uint32_t *sys;       // [capacity]
+    uint32_t *prefix;    // [capacity + 1]
+};
+
 // SELL row product of this lane's row in slice s.
 template <typename V, class GX>
 __device__ __forceinline__ V sell_row(const Sell<V> &M, uint32_t s, int lane, GX &gx)
@@ -82,232 +90,268 @@ __device__ __forceinline__ V sell_row(const Sell<V> &M, uint32_t s, int lane, GX
     return acc;
 }
 
-// Record this slice's partial sums; the warp that completes the system's last
-// slice returns true with the system totals (slice order) in every lane.
-template <int NV>
-__device__ __forceinline__ bool slice_done(double (&v)[NV], uint32_t s, uint32_t sys, const BView &B, double *part,
-                                           unsigned int *ticket, double (&tot)[NV])
+// Warp loop over a contiguous block of the listed systems' slices (so warps share
+// the active work evenly).  Systems that `skip(st)` rejects are jumped over as a
+// whole.  For every visited slice, `body(s, st, v)` fills this lane's
+// contributions; the warp sums them and lane 0 stores the slice's partials.
+// No atomics: the per-system totals are formed by bk_reduce.
+template <int NV, class SKIP, class BODY>
+__device__ __forceinline__ void batch_loop(const BView &B, const Active *L, CgState *S, double *part, SKIP skip,
+                                           BODY body)
 {
     const int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int k = 0; k < NV; k++) v[k] = warp_sum(v[k]);
-    const uint32_t b0 = B.sys_slice[sys], b1 = B.sys_slice[sys + 1];
-    int last = 0;
-    if (lane == 0) {
-#pragma unroll
-        for (int k = 0; k < NV; k++) part[size_t(s) * NV + k] = v[k];
-        __threadfence();
-        last = (atomicAdd(ticket, 1u) == (b1 - b0) - 1u);
+    const uint32_t W = gridDim.x * (blockDim.x >> 5);
+    const uint32_t w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const uint32_t total = L->n_slices, n_list = L->n_sys;
+    const uint32_t per = (total + W - 1) / W;
+    const uint32_t a_begin = min(total, w * per), a_end = min(total, a_begin + per);
+    if (a_begin >= a_end) return;
+    uint32_t lo = 0, hi = n_list;  // last k with prefix[k] <= a_begin
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) / 2;
+        if (L->prefix[mid] <= a_begin) lo = mid;
+        else hi = mid;
     }
-    last = __shfl_sync(0xffffffffu, last, 0);
-    if (!last) return false;
-    __threadfence();
+    uint32_t k = lo;
+    uint32_t a = a_begin;
+    while (a < a_end) {
+        const uint32_t sys = L->sys[k], k_end = L->prefix[k + 1];
+        CgState *st = &S[sys];
+        if (skip(st)) {
+            a = k_end;
+            k++;
+            continue;
+        }
+        const uint32_t base = B.sys_slice[sys] - L->prefix[k];
+        const uint32_t stop = min(a_end, k_end);
+        for (; a < stop; a++) {
+            const uint32_t s = base + a;
+            double v[NV];
+            body(s, st, v);
 #pragma unroll
-    for (int k = 0; k < NV; k++) tot[k] = 0.0;
-    for (uint32_t q = b0 + lane; q < b1; q += 32)
+            for (int q = 0; q < NV; q++) v[q] = warp_sum(v[q]);
+            if (lane == 0)
 #pragma unroll
-        for (int k = 0; k < NV; k++) tot[k] += __ldcg(&part[size_t(q) * NV + k]);
-#pragma unroll
-    for (int k = 0; k < NV; k++) tot[k] = warp_sum(tot[k]);
-    if (lane == 0) *ticket = 0u;
-    return true;
+                for (int q = 0; q < NV; q++) part[size_t(s) * NV + q] = v[q];
+        }
+        k++;
+    }
 }
 
-#define BATCH_SLICE_LOOP                                                                                     \
+// One block per listed system: adds the system's slice partials in a fixed order
+// and applies the state transition `kind` (the same transitions as the
+// single-system solver).
+enum RedKind { RED_INIT_RES = 0, RED_INIT_Z, RED_DIR64, RED_DIR32, RED_UPD64, RED_UPD32, RED_CHK64, RED_CHK32, RED_TRUE };
+
+template <int NV, int KIND>
+__global__ void __launch_bounds__(kBlock) bk_reduce(BView B, const Active *L, CgState *S, const double *part,
+                                                    double *relres)
+{
+    __shared__ double sh[NV * 32];
+    if (blockIdx.x >= L->n_sys) return;
+    const uint32_t sys = L->sys[blockIdx.x];
+    CgState *st = &S[sys];
+    const bool skip = (KIND == RED_INIT_RES || KIND == RED_TRUE) ? false
+                      : (KIND == RED_CHK64 || KIND == RED_CHK32) ? (st->done || !st->need_check)
+                                                                 : st->done != 0;
+    if (skip) return;
+    const uint32_t b0 = B.sys_slice[sys], b1 = B.sys_slice[sys + 1];
+    double acc[NV];
+#pragma unroll
+    for (int q = 0; q < NV; q++) acc[q] = 0.0;
+    for (uint32_t s = b0 + threadIdx.x; s < b1; s += blockDim.x)
+#pragma unroll
+        for (int q = 0; q < NV; q++) acc[q] += part[size_t(s) * NV + q];
+    block_sum<NV>(acc, sh);
+    if (threadIdx.x != 0) return;
+    if (KIND == RED_INIT_RES) {
+        st->rn = sqrt(acc[0]);
+        st->bn = sqrt(acc[1]);
+        st->max_r = st->rn;
+        st->sigma = st->bn > 0.0 ? 1.0 / st->bn : 1.0;
+        if (!(st->rn > st->rtol * st->bn)) {
+            st->done = 1;
+            st->converged = 1;
+            st->status = isfinite(st->rn) ? RSG_OK : RSG_BREAKDOWN;
+        }
+    } else if (KIND == RED_INIT_Z) {
+        st->rho = st->rho_new = acc[0];
+        st->beta = 0.0;
+    } else if (KIND == RED_DIR64 || KIND == RED_DIR32) {
+        double pq = acc[0];
+        if (KIND == RED_DIR32) {
+            if (pq == 0.0) pq = 1e-300;
+        } else {
+            pq = clamp_pq(pq, st->eps);
+        }
+        st->pq = pq;
+        st->rho = st->rho_new;
+        st->alpha = st->rho / pq;
+        st->fold = 0;
+    } else if (KIND == RED_UPD64) {
+        finalize_update64(st, acc[0], acc[1], acc[2]);
+    } else if (KIND == RED_UPD32) {
+        finalize_update_mixed(st, acc[0], acc[1]);
+    } else if (KIND == RED_CHK64) {
+        finalize_check64(st, acc[0], sqrt(acc[1]));
+    } else if (KIND == RED_CHK32) {
+        finalize_check_mixed(st, acc[0], sqrt(acc[1]));
+    } else {
+        relres[sys] = acc[1] > 0.0 ? sqrt(acc[0] / acc[1]) : sqrt(acc[0]);
+    }
+}
+
+#define BATCH_ROWS_LOOP                                                                                      \
     const int lane = threadIdx.x & 31;                                                                      \
     const uint32_t warps_total = gridDim.x * (blockDim.x >> 5);                                             \
     for (uint32_t s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); s < B.n_slices; s += warps_total)
 
-__global__ void __launch_bounds__(kBlock) bk_init_res(Sell<double> M, BView B, const double *__restrict__ b,
+__global__ void __launch_bounds__(kBlock) bk_init_res(Sell<double> M, BView B, const Active *L, const double *__restrict__ b,
                                                       const double *__restrict__ x, double *__restrict__ r,
                                                       double *part, CgState *S)
 {
-    BATCH_SLICE_LOOP
-    {
-        const uint32_t sys = B.slice_sys[s];
-        CgState *st = &S[sys];
-        auto gx = [&](uint32_t c) { return x[c]; };
-        const double ax = sell_row<double>(M, s, lane, gx);
-        const uint32_t row = s * 32u + lane;
-        double v[2] = {0.0, 0.0};
-        if (row < M.n) {
-            const double ri = b[row] - ax;
-            r[row] = ri;
-            v[0] = ri * ri;
-            v[1] = b[row] * b[row];
-        }
-        double tot[2];
-        if (slice_done<2>(v, s, sys, B, part, &st->ticket[3], tot) && lane == 0) {
-            st->rn = sqrt(tot[0]);
-            st->bn = sqrt(tot[1]);
-            st->max_r = st->rn;
-            st->sigma = st->bn > 0.0 ? 1.0 / st->bn : 1.0;
-            if (!(st->rn > st->rtol * st->bn)) {
-                st->done = 1;
-                st->converged = 1;
-                st->status = isfinite(st->rn) ? RSG_OK : RSG_BREAKDOWN;
+    const int lane = threadIdx.x & 31;
+    auto gx = [&](uint32_t c) { return x[c]; };
+    batch_loop<2>(
+        B, L, S, part, [](const CgState *) { return false; },
+        [&](uint32_t s, CgState *, double(&v)[2]) {
+            const double ax = sell_row<double>(M, s, lane, gx);
+            const uint32_t row = s * 32u + lane;
+            v[0] = v[1] = 0.0;
+            if (row < M.n) {
+                const double ri = b[row] - ax;
+                r[row] = ri;
+                v[0] = ri * ri;
+                v[1] = b[row] * b[row];
             }
-        }
-    }
+        });
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(kBlock) bk_init_z(BView B, uint32_t n, const double *__restrict__ d,
+__global__ void __launch_bounds__(kBlock) bk_init_z(BView B, const Active *L, uint32_t n, const double *__restrict__ d,
                                                     const float *__restrict__ d32, const double *__restrict__ r,
                                                     double *__restrict__ z, float *__restrict__ r32,
                                                     float *__restrict__ z32, double *part, CgState *S)
 {
-    BATCH_SLICE_LOOP
-    {
-        const uint32_t sys = B.slice_sys[s];
-        CgState *st = &S[sys];
-        if (st->done) continue;
-        const uint32_t row = s * 32u + lane;
-        double v[1] = {0.0};
-        if (row < n) {
-            if (MIXED) {
-                const float rf = float(r[row] * st->sigma);
-                const float zf = d32 ? d32[row] * rf : rf;
-                r32[row] = rf;
-                z32[row] = zf;
-                v[0] = double(rf) * double(zf);
-            } else {
-                const double zi = d ? d[row] * r[row] : r[row];
-                z[row] = zi;
-                v[0] = r[row] * zi;
+    const int lane = threadIdx.x & 31;
+    batch_loop<1>(
+        B, L, S, part, [](const CgState *st) { return st->done != 0; },
+        [&](uint32_t s, CgState *st, double(&v)[1]) {
+            const uint32_t row = s * 32u + lane;
+            v[0] = 0.0;
+            if (row < n) {
+                if (MIXED) {
+                    const float rf = float(r[row] * st->sigma);
+                    const float zf = d32 ? d32[row] * rf : rf;
+                    r32[row] = rf;
+                    z32[row] = zf;
+                    v[0] = double(rf) * double(zf);
+                } else {
+                    const double zi = d ? d[row] * r[row] : r[row];
+                    z[row] = zi;
+                    v[0] = r[row] * zi;
+                }
             }
-        }
-        double tot[1];
-        if (slice_done<1>(v, s, sys, B, part, &st->ticket[4], tot) && lane == 0) {
-            st->rho = st->rho_new = tot[0];
-            st->beta = 0.0;
-        }
-    }
+        });
 }
 
 template <typename V, bool MIXED>
-__global__ void __launch_bounds__(kBlock) bk_dir(Sell<V> M, BView B, const V *__restrict__ z,
+__global__ void __launch_bounds__(kBlock) bk_dir(Sell<V> M, BView B, const Active *L, const V *__restrict__ z,
                                                  const V *__restrict__ p_old, V *__restrict__ p_new,
                                                  V *__restrict__ q, double *__restrict__ x, float *__restrict__ y,
                                                  double *part, CgState *S)
 {
-    BATCH_SLICE_LOOP
-    {
-        const uint32_t sys = B.slice_sys[s];
-        CgState *st = &S[sys];
-        if (st->done) continue;
-        const V beta = V(st->beta);
-        auto gx = [&](uint32_t c) { return MIXED ? V(fmaf(float(beta), float(p_old[c]), float(z[c])))
-                                                 : V(fma(double(beta), double(p_old[c]), double(z[c]))); };
-        const V ax = sell_row<V>(M, s, lane, gx);
-        const uint32_t row = s * 32u + lane;
-        double v[1] = {0.0};
-        if (row < M.n) {
-            const V p = gx(row);
-            p_new[row] = p;
-            q[row] = ax;
-            v[0] = double(p) * double(ax);
-            if (MIXED && st->fold) {
-                x[row] = fma(double(y[row]), 1.0 / st->sigma, x[row]);
-                y[row] = 0.f;
+    const int lane = threadIdx.x & 31;
+    batch_loop<1>(
+        B, L, S, part, [](const CgState *st) { return st->done != 0; },
+        [&](uint32_t s, CgState *st, double(&v)[1]) {
+            const V beta = V(st->beta);
+            auto gx = [&](uint32_t c) { return MIXED ? V(fmaf(float(beta), float(p_old[c]), float(z[c])))
+                                                     : V(fma(double(beta), double(p_old[c]), double(z[c]))); };
+            const V ax = sell_row<V>(M, s, lane, gx);
+            const uint32_t row = s * 32u + lane;
+            v[0] = 0.0;
+            if (row < M.n) {
+                const V p = gx(row);
+                p_new[row] = p;
+                q[row] = ax;
+                v[0] = double(p) * double(ax);
+                if (MIXED && st->fold) {
+                    x[row] = fma(double(y[row]), 1.0 / st->sigma, x[row]);
+                    y[row] = 0.f;
+                }
             }
-        }
-        double tot[1];
-        if (slice_done<1>(v, s, sys, B, part, &st->ticket[0], tot) && lane == 0) {
-            double pq = tot[0];
-            if (MIXED) {
-                if (pq == 0.0) pq = 1e-300;
-            } else {
-                pq = clamp_pq(pq, st->eps);
-            }
-            st->pq = pq;
-            st->rho = st->rho_new;
-            st->alpha = st->rho / pq;
-            st->fold = 0;
-        }
-    }
+        });
 }
 
 template <typename V, bool MIXED>
-__global__ void __launch_bounds__(kBlock) bk_update(BView B, uint32_t n, const V *__restrict__ d,
+__global__ void __launch_bounds__(kBlock) bk_update(BView B, const Active *L, uint32_t n, const V *__restrict__ d,
                                                     const V *__restrict__ p, const V *__restrict__ q,
                                                     V *__restrict__ xy, V *__restrict__ r, V *__restrict__ z,
                                                     double *part, CgState *S)
 {
-    BATCH_SLICE_LOOP
-    {
-        const uint32_t sys = B.slice_sys[s];
-        CgState *st = &S[sys];
-        if (st->done) continue;
-        const V alpha = V(st->alpha);
-        const uint32_t row = s * 32u + lane;
-        double v[3] = {0.0, 0.0, 0.0};
-        if (row < n) {
-            const V xi = MIXED ? V(fmaf(float(alpha), float(p[row]), float(xy[row])))
-                               : V(fma(double(alpha), double(p[row]), double(xy[row])));
-            const V ri = MIXED ? V(fmaf(-float(alpha), float(q[row]), float(r[row])))
-                               : V(fma(-double(alpha), double(q[row]), double(r[row])));
-            const V zi = d ? d[row] * ri : ri;
-            xy[row] = xi;
-            r[row] = ri;
-            z[row] = zi;
-            v[0] = double(ri) * double(zi);
-            v[1] = double(ri) * double(ri);
-            v[2] = double(xi) * double(xi);
-        }
-        double tot[3];
-        if (slice_done<3>(v, s, sys, B, part, &st->ticket[1], tot) && lane == 0) {
-            if (MIXED) finalize_update_mixed(st, tot[0], tot[1]);
-            else finalize_update64(st, tot[0], tot[1], tot[2]);
-        }
-    }
+    const int lane = threadIdx.x & 31;
+    batch_loop<3>(
+        B, L, S, part, [](const CgState *st) { return st->done != 0; },
+        [&](uint32_t s, CgState *st, double(&v)[3]) {
+            const V alpha = V(st->alpha);
+            const uint32_t row = s * 32u + lane;
+            v[0] = v[1] = v[2] = 0.0;
+            if (row < n) {
+                const V xi = MIXED ? V(fmaf(float(alpha), float(p[row]), float(xy[row])))
+                                   : V(fma(double(alpha), double(p[row]), double(xy[row])));
+                const V ri = MIXED ? V(fmaf(-float(alpha), float(q[row]), float(r[row])))
+                                   : V(fma(-double(alpha), double(q[row]), double(r[row])));
+                const V zi = d ? d[row] * ri : ri;
+                xy[row] = xi;
+                r[row] = ri;
+                z[row] = zi;
+                v[0] = double(ri) * double(zi);
+                v[1] = double(ri) * double(ri);
+                v[2] = double(xi) * double(xi);
+            }
+        });
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(kBlock) bk_check(Sell<double> M, BView B, const double *__restrict__ d,
+__global__ void __launch_bounds__(kBlock) bk_check(Sell<double> M, BView B, const Active *L, const double *__restrict__ d,
                                                    const float *__restrict__ d32, const double *__restrict__ b,
                                                    const double *__restrict__ x, const float *__restrict__ y,
                                                    double *__restrict__ r, double *__restrict__ z,
                                                    float *__restrict__ r32, float *__restrict__ z32, double *part,
                                                    CgState *S)
 {
-    BATCH_SLICE_LOOP
-    {
-        const uint32_t sys = B.slice_sys[s];
-        CgState *st = &S[sys];
-        if (st->done || !st->need_check) continue;
-        const double sigma = st->sigma, inv_sigma = 1.0 / sigma;
-        auto gx = [&](uint32_t c) { return MIXED ? fma(double(y[c]), inv_sigma, x[c]) : x[c]; };
-        const double ax = sell_row<double>(M, s, lane, gx);
-        const uint32_t row = s * 32u + lane;
-        double v[2] = {0.0, 0.0};
-        if (row < M.n) {
-            const double ri = b[row] - ax;
-            v[1] = ri * ri;
-            if (MIXED) {
-                const float rf = float(ri * sigma);
-                const float zf = d32 ? d32[row] * rf : rf;
-                r32[row] = rf;
-                z32[row] = zf;
-                v[0] = double(rf) * double(zf);
-            } else {
-                const double zi = d ? d[row] * ri : ri;
-                r[row] = ri;
-                z[row] = zi;
-                v[0] = ri * zi;
+    const int lane = threadIdx.x & 31;
+    batch_loop<2>(
+        B, L, S, part, [](const CgState *st) { return st->done != 0 || st->need_check == 0; },
+        [&](uint32_t s, CgState *st, double(&v)[2]) {
+            const double sigma = st->sigma, inv_sigma = 1.0 / sigma;
+            auto gx = [&](uint32_t c) { return MIXED ? fma(double(y[c]), inv_sigma, x[c]) : x[c]; };
+            const double ax = sell_row<double>(M, s, lane, gx);
+            const uint32_t row = s * 32u + lane;
+            v[0] = v[1] = 0.0;
+            if (row < M.n) {
+                const double ri = b[row] - ax;
+                v[1] = ri * ri;
+                if (MIXED) {
+                    const float rf = float(ri * sigma);
+                    const float zf = d32 ? d32[row] * rf : rf;
+                    r32[row] = rf;
+                    z32[row] = zf;
+                    v[0] = double(rf) * double(zf);
+                } else {
+                    const double zi = d ? d[row] * ri : ri;
+                    r[row] = ri;
+                    z[row] = zi;
+                    v[0] = ri * zi;
+                }
             }
-        }
-        double tot[2];
-        if (slice_done<2>(v, s, sys, B, part, &st->ticket[2], tot) && lane == 0) {
-            if (MIXED) finalize_check_mixed(st, tot[0], sqrt(tot[1]));
-            else finalize_check64(st, tot[0], sqrt(tot[1]));
-        }
-    }
+        });
 }
 
 __global__ void bk_fold(BView B, uint32_t n, double *__restrict__ x, float *__restrict__ y, const CgState *S)
 {
-    BATCH_SLICE_LOOP
+    BATCH_ROWS_LOOP
     {
         const uint32_t row = s * 32u + lane;
         if (row < n) {
@@ -317,40 +361,69 @@ __global__ void bk_fold(BView B, uint32_t n, double *__restrict__ x, float *__re
     }
 }
 
-__global__ void bk_true_res(Sell<double> M, BView B, const double *__restrict__ b, const double *__restrict__ x,
+__global__ void bk_true_res(Sell<double> M, BView B, const Active *L, const double *__restrict__ b, const double *__restrict__ x,
                             double *part, CgState *S, double *relres)
 {
-    BATCH_SLICE_LOOP
-    {
-        const uint32_t sys = B.slice_sys[s];
-        auto gx = [&](uint32_t c) { return x[c]; };
-        const double ax = sell_row<double>(M, s, lane, gx);
-        const uint32_t row = s * 32u + lane;
-        double v[2] = {0.0, 0.0};
-        if (row < M.n) {
-            const double ri = b[row] - ax;
-            v[0] = ri * ri;
-            v[1] = b[row] * b[row];
-        }
-        double tot[2];
-        if (slice_done<2>(v, s, sys, B, part, &S[sys].ticket[5], tot) && lane == 0)
-            relres[sys] = tot[1] > 0.0 ? sqrt(tot[0] / tot[1]) : sqrt(tot[0]);
-    }
+    const int lane = threadIdx.x & 31;
+    auto gx = [&](uint32_t c) { return x[c]; };
+    batch_loop<2>(
+        B, L, S, part, [](const CgState *) { return false; },
+        [&](uint32_t s, CgState *, double(&v)[2]) {
+            const double ax = sell_row<double>(M, s, lane, gx);
+            const uint32_t row = s * 32u + lane;
+            v[0] = v[1] = 0.0;
+            if (row < M.n) {
+                const double ri = b[row] - ax;
+                v[0] = ri * ri;
+                v[1] = b[row] * b[row];
+            }
+        });
 }
 
-// Loop control: keeps the graph's while node running while any system is active.
-__global__ void bk_tail(const CgState *S, uint32_t n_sys, BatchCtl *ctl, cudaGraphConditionalHandle h, int use_cond)
+// Loop control: rebuilds the list of active systems (block-wide scan), keeps the
+// graph's while node running while any system is active, enforces the hard limit.
+__global__ void __launch_bounds__(kBlock) bk_tail(const CgState *S, const uint32_t *sys_slice, uint32_t n_sys,
+                                                  Active *L, BatchCtl *ctl, cudaGraphConditionalHandle h,
+                                                  int use_cond)
 {
-    __shared__ int active;
-    if (threadIdx.x == 0) active = 0;
+    __shared__ uint32_t cnt_sys[kBlock], cnt_sl[kBlock];
+    const uint32_t t = threadIdx.x, per = (n_sys + blockDim.x - 1) / blockDim.x;
+    const uint32_t i0 = min(n_sys, t * per), i1 = min(n_sys, i0 + per);
+    uint32_t ns = 0, nsl = 0;
+    for (uint32_t i = i0; i < i1; i++)
+        if (!S[i].done) {
+            ns++;
+            nsl += sys_slice[i + 1] - sys_slice[i];
+        }
+    cnt_sys[t] = ns;
+    cnt_sl[t] = nsl;
     __syncthreads();
-    int a = 0;
-    for (uint32_t i = threadIdx.x; i < n_sys; i += blockDim.x) a |= (S[i].done == 0);
-    if (a) active = 1;
+    if (t == 0) {  // exclusive scan (blockDim entries)
+        uint32_t a = 0, b = 0;
+        for (uint32_t k = 0; k < blockDim.x; k++) {
+            const uint32_t x = cnt_sys[k], y = cnt_sl[k];
+            cnt_sys[k] = a;
+            cnt_sl[k] = b;
+            a += x;
+            b += y;
+        }
+        L->n_sys = a;
+        L->n_slices = b;
+    }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    uint32_t o = cnt_sys[t], pre = cnt_sl[t];
+    for (uint32_t i = i0; i < i1; i++)
+        if (!S[i].done) {
+            L->sys[o] = i;
+            L->prefix[o] = pre;
+            pre += sys_slice[i + 1] - sys_slice[i];
+            o++;
+        }
+    __syncthreads();
+    if (t == 0) {
+        L->prefix[L->n_sys] = L->n_slices;
         const uint32_t bc = ++ctl->body_count;
-        int keep = active;
+        int keep = L->n_sys > 0;
         if (keep && bc >= ctl->body_limit) {
             ctl->timeout = 1;
             keep = 0;
@@ -512,6 +585,7 @@ rsg_status rsg_batch_solve(rsg_context *ctx, rsg_batch *B, const rsg_solver_conf
     const uint32_t max_it = std::max<uint32_t>(conf->n_outer, 1);
     const size_t vn = arena_bytes(n, sizeof(double)), vf = arena_bytes(n, sizeof(float));
     size_t bytes = 8 * vn + arena_bytes(size_t(nsl) * 3, sizeof(double)) + arena_bytes(ns, sizeof(CgState)) +
+                   2 * arena_bytes(1, sizeof(Active)) + 4 * arena_bytes(size_t(ns) + 1, sizeof(uint32_t)) +
                    arena_bytes(ns, sizeof(double)) + arena_bytes(1, sizeof(BatchCtl)) + 2 * arena_bytes(B->user_rows, 8);
     if (mixed) bytes += 7 * vf;
     RSG_TRY(arena_reserve(ctx, bytes));
@@ -522,6 +596,9 @@ rsg_status rsg_batch_solve(rsg_context *ctx, rsg_batch *B, const rsg_solver_conf
     CgState *S = arena_take<CgState>(ctx, ns);
     double *relres = arena_take<double>(ctx, ns);
     BatchCtl *ctl = arena_take<BatchCtl>(ctx, 1);
+    Active *L_all = arena_take<Active>(ctx, 1), *L_act = arena_take<Active>(ctx, 1);
+    uint32_t *la_sys = arena_take<uint32_t>(ctx, size_t(ns) + 1), *la_pre = arena_take<uint32_t>(ctx, size_t(ns) + 1);
+    uint32_t *lb_sys = arena_take<uint32_t>(ctx, size_t(ns) + 1), *lb_pre = arena_take<uint32_t>(ctx, size_t(ns) + 1);
     double *bu = memory == RSG_MEM_HOST ? arena_take<double>(ctx, B->user_rows) : const_cast<double *>(b);
     double *xu = memory == RSG_MEM_HOST ? arena_take<double>(ctx, B->user_rows) : x;
     float *r32 = nullptr, *z32 = nullptr, *pa = nullptr, *pb = nullptr, *q32 = nullptr, *y32 = nullptr, *d32 = nullptr;
@@ -577,6 +654,20 @@ rsg_status rsg_batch_solve(rsg_context *ctx, rsg_batch *B, const rsg_solver_conf
         RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(S, hs.data(), ns * sizeof(CgState), cudaMemcpyHostToDevice, sm));
         BatchCtl c = {0, max_it / 2 + 16, 0, 1};
         RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(ctl, &c, sizeof(c), cudaMemcpyHostToDevice, sm));
+        // both lists start with every system
+        std::vector<uint32_t> ids(ns), pre(size_t(ns) + 1);
+        for (uint32_t i = 0; i < ns; i++) {
+            ids[i] = i;
+            pre[i] = B->pad_begin[i] / 32;
+        }
+        pre[ns] = nsl;
+        Active la = {ns, nsl, la_sys, la_pre}, lb = {ns, nsl, lb_sys, lb_pre};
+        RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(la_sys, ids.data(), ns * 4, cudaMemcpyHostToDevice, sm));
+        RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(la_pre, pre.data(), (size_t(ns) + 1) * 4, cudaMemcpyHostToDevice, sm));
+        RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(lb_sys, ids.data(), ns * 4, cudaMemcpyHostToDevice, sm));
+        RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(lb_pre, pre.data(), (size_t(ns) + 1) * 4, cudaMemcpyHostToDevice, sm));
+        RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(L_all, &la, sizeof(Active), cudaMemcpyHostToDevice, sm));
+        RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(L_act, &lb, sizeof(Active), cudaMemcpyHostToDevice, sm));
         RSG_CHECK_CUDA(ctx, cudaStreamSynchronize(sm));
     }
     const BView V{B->d_slice_sys, B->d_sys_slice, nsl, ns};
@@ -584,32 +675,41 @@ rsg_status rsg_batch_solve(rsg_context *ctx, rsg_batch *B, const rsg_solver_conf
     const Sell<float> M32 = sell_view<float>(B->A);
     const int g = std::min(grid_for(ctx, (const void *)bk_dir<double, false>, kBlock, 0, (long long)nsl * 32), kMaxGrid);
     cudaEventRecord(ctx->ev[0], sm);
-    bk_init_res<<<g, kBlock, 0, sm>>>(M64, V, bp, xp, r, part, S);
+    const int gr = int(ns);  // reduce kernels: one block per listed system
+    bk_init_res<<<g, kBlock, 0, sm>>>(M64, V, L_all, bp, xp, r, part, S);
+    bk_reduce<2, RED_INIT_RES><<<gr, kBlock, 0, sm>>>(V, L_all, S, part, nullptr);
     if (mixed) {
-        bk_init_z<true><<<g, kBlock, 0, sm>>>(V, n, jac ? d : nullptr, jac ? d32 : nullptr, r, z, r32, z32, part, S);
+        bk_init_z<true><<<g, kBlock, 0, sm>>>(V, L_all, n, jac ? d : nullptr, jac ? d32 : nullptr, r, z, r32, z32, part, S);
     } else {
-        bk_init_z<false><<<g, kBlock, 0, sm>>>(V, n, jac ? d : nullptr, nullptr, r, z, r32, z32, part, S);
+        bk_init_z<false><<<g, kBlock, 0, sm>>>(V, L_all, n, jac ? d : nullptr, nullptr, r, z, r32, z32, part, S);
     }
+    bk_reduce<1, RED_INIT_Z><<<gr, kBlock, 0, sm>>>(V, L_all, S, part, nullptr);
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
 
     auto body = [&](cudaGraphConditionalHandle h, int use_cond) {
         for (int half = 0; half < 2; half++) {
             if (!mixed) {
                 double *po = half ? p1 : p0, *pn = half ? p0 : p1;
-                bk_dir<double, false><<<g, kBlock, 0, sm>>>(M64, V, z, po, pn, q, xp, nullptr, part, S);
-                bk_update<double, false><<<g, kBlock, 0, sm>>>(V, n, jac ? d : nullptr, pn, q, xp, r, z, part, S);
-                bk_check<false><<<g, kBlock, 0, sm>>>(M64, V, jac ? d : nullptr, nullptr, bp, xp, nullptr, r, z,
+                bk_dir<double, false><<<g, kBlock, 0, sm>>>(M64, V, L_act, z, po, pn, q, xp, nullptr, part, S);
+                bk_reduce<1, RED_DIR64><<<gr, kBlock, 0, sm>>>(V, L_act, S, part, nullptr);
+                bk_update<double, false><<<g, kBlock, 0, sm>>>(V, L_act, n, jac ? d : nullptr, pn, q, xp, r, z, part, S);
+                bk_reduce<3, RED_UPD64><<<gr, kBlock, 0, sm>>>(V, L_act, S, part, nullptr);
+                bk_check<false><<<g, kBlock, 0, sm>>>(M64, V, L_act, jac ? d : nullptr, nullptr, bp, xp, nullptr, r, z,
                                                      nullptr, nullptr, part, S);
+                bk_reduce<2, RED_CHK64><<<gr, kBlock, 0, sm>>>(V, L_act, S, part, nullptr);
             } else {
                 float *po = half ? pb : pa, *pn = half ? pa : pb;
-                bk_dir<float, true><<<g, kBlock, 0, sm>>>(M32, V, z32, po, pn, q32, xp, y32, part, S);
-                bk_update<float, true><<<g, kBlock, 0, sm>>>(V, n, jac ? d32 : nullptr, pn, q32, y32, r32, z32, part,
+                bk_dir<float, true><<<g, kBlock, 0, sm>>>(M32, V, L_act, z32, po, pn, q32, xp, y32, part, S);
+                bk_reduce<1, RED_DIR32><<<gr, kBlock, 0, sm>>>(V, L_act, S, part, nullptr);
+                bk_update<float, true><<<g, kBlock, 0, sm>>>(V, L_act, n, jac ? d32 : nullptr, pn, q32, y32, r32, z32, part,
                                                             S);
-                bk_check<true><<<g, kBlock, 0, sm>>>(M64, V, nullptr, jac ? d32 : nullptr, bp, xp, y32, r, z, r32,
+                bk_reduce<3, RED_UPD32><<<gr, kBlock, 0, sm>>>(V, L_act, S, part, nullptr);
+                bk_check<true><<<g, kBlock, 0, sm>>>(M64, V, L_act, nullptr, jac ? d32 : nullptr, bp, xp, y32, r, z, r32,
                                                     z32, part, S);
+                bk_reduce<2, RED_CHK32><<<gr, kBlock, 0, sm>>>(V, L_act, S, part, nullptr);
             }
         }
-        bk_tail<<<1, kBlock, 0, sm>>>(S, ns, ctl, h, use_cond);
+        bk_tail<<<1, kBlock, 0, sm>>>(S, B->d_sys_slice, ns, L_act, ctl, h, use_cond);
     };
 
     rsg_status status = RSG_OK;
@@ -660,7 +760,8 @@ rsg_status rsg_batch_solve(rsg_context *ctx, rsg_batch *B, const rsg_solver_conf
         }
     }
     if (mixed) bk_fold<<<g, kBlock, 0, sm>>>(V, n, xp, y32, S);
-    bk_true_res<<<g, kBlock, 0, sm>>>(M64, V, bp, xp, part, S, relres);
+    bk_true_res<<<g, kBlock, 0, sm>>>(M64, V, L_all, bp, xp, part, S, relres);
+    bk_reduce<2, RED_TRUE><<<gr, kBlock, 0, sm>>>(V, L_all, S, part, relres);
     cudaEventRecord(ctx->ev[1], sm);
     bk_gather<<<gu, kBlock, 0, sm>>>(B->user_rows, B->d_user2pad, xp, xu);
     if (memory == RSG_MEM_HOST)

@@ -383,3 +383,40 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def transient_heat(ctx: Context, problem, n_steps: int, conf: SolverConf | None = None, precision: str = "fp64",
+                   stream_sync=None):
+    """Backward-Euler (theta) time stepping of a heat problem on the GPU.
+
+    The reference's time loop (src/rsolver.cpp:106-144) calls RSolverHeat::prepare
+    every step, which rebuilds A and b from scratch (A.clear(), src/rsolverheat.cpp:85)
+    with the theta scheme of assemblyMatrix (:768-779), then solves with x = 0 as
+    the initial guess.  Here the assembly plan (pattern + scatter map) is built
+    once and each step re-assembles values and RHS on the GPU into the same
+    matrix; the previous step's temperatures are the initial guess.
+    Returns the list of nodal temperature arrays after each step (host numpy).
+    """
+    import copy
+    p = copy.copy(problem)
+    p.transient = True
+    p.node_t = np.array(problem.node_t, np.float64, copy=True)
+    asm = Assembly.heat(ctx, p)
+    import torch  # device buffers for b and x
+    b = torch.empty(asm.n_free, dtype=torch.float64, device=f"cuda:{ctx.device}")
+    x = torch.zeros_like(b)
+    conf = conf or make_conf(n_outer=50000, stop_rule="true", rtol=1e-10, precision=precision)
+    free = p.book != 0xFFFFFFFF
+    idx = p.book[free].astype(np.int64)
+    out = []
+    for _ in range(n_steps):
+        A = asm.assemble(p, b)
+        torch.cuda.synchronize()
+        x.copy_(torch.from_numpy(p.node_t[free][np.argsort(idx)]).to(b.device))
+        torch.cuda.synchronize()
+        _, st = ctx.solve(A, b, x, conf=conf)
+        xs = x.cpu().numpy()
+        p.node_t[free] = xs[idx]
+        out.append((p.node_t.copy(), st))
+    asm.close()
+    return out
