@@ -221,6 +221,34 @@ RSG_API rsg_status rsg_batch_solve(rsg_context *ctx, rsg_batch *batch, const rsg
                                    const double *b, double *x, int32_t memory, rsg_stats *per_system,
                                    rsg_stats *summary);
 
+/* ---- learned preconditioner ----
+ * No counterpart in the reference (its preconditioners are NONE / JACOBI /
+ * BLOCK_JACOBI, src/rmatrixpreconditioner.cpp).  A message-passing network over
+ * the matrix graph maps a residual r to z = M(r) ~ A^{-1} r: node features are
+ * the Jacobi-scaled residual, the diagonal, the row-sum ratio (non-zero next to
+ * Dirichlet boundaries) and optional node coordinates; edge weights are the
+ * normalised off-diagonals.  It is used as RSG_PREC_LEARNED (flexible CG, or
+ * GMRES with flexible = 1) with Jacobi as fallback, and as an initial guess
+ * (conf.learned_initial_guess).  All device arrays; xyz (3 per row) may be NULL.
+ * Training minimises ||r - A M(r)||^2 / ||r||^2 with Adam on the GPU. */
+RSG_API rsg_status rsg_learned_create(rsg_context *ctx, uint32_t layers, uint64_t seed, rsg_learned **out);
+RSG_API void       rsg_learned_destroy(rsg_context *ctx, rsg_learned *model);
+RSG_API rsg_status rsg_learned_info(const rsg_learned *model, uint32_t *layers, uint32_t *hidden, uint64_t *n_params,
+                                    uint64_t *step);
+/* which: 0 = parameters, 1 = last gradient, 2 = Adam first moment, 3 = Adam second moment (n_params floats) */
+RSG_API rsg_status rsg_learned_get_params(rsg_context *ctx, const rsg_learned *model, float *host, int32_t which);
+RSG_API rsg_status rsg_learned_set_params(rsg_context *ctx, rsg_learned *model, const float *host, int32_t which);
+RSG_API rsg_status rsg_learned_set_step(rsg_learned *model, uint64_t step);
+/* z = M(r); tensor_cores != 0 runs the dense layers as BF16 MMA with FP32 accumulation, else FP32 */
+RSG_API rsg_status rsg_learned_apply(rsg_context *ctx, rsg_learned *model, const rsg_csr *A, const double *r,
+                                     double *z, const double *xyz, int32_t tensor_cores);
+/* loss and gradient (into the model's gradient buffer) for one residual, no update */
+RSG_API rsg_status rsg_learned_loss_grad(rsg_context *ctx, rsg_learned *model, const rsg_csr *A, const double *r,
+                                         const double *xyz, int32_t tensor_cores, double *loss);
+/* forward (tensor cores) + backward + one Adam step with learning rate lr */
+RSG_API rsg_status rsg_learned_train_step(rsg_context *ctx, rsg_learned *model, const rsg_csr *A, const double *r,
+                                          const double *xyz, float lr, double *loss);
+
 /* ---- assembly (RSolverHeat / RSolverStress prepare + assemblyMatrix) ----
  * A plan is the sparsity pattern of the free-DOF system plus the
  * element-to-nonzero scatter map (the reference precedent is

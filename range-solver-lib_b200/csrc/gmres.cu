@@ -13,6 +13,7 @@
 // Each cycle is one captured CUDA graph; the host polls the device state once
 // per cycle.
 #include "gmres.cuh"
+#include "gnn.cuh"
 
 #include <cmath>
 
@@ -282,6 +283,8 @@ rsg_status gmres_carve(rsg_context *ctx, GmresArgs &a, uint32_t n, uint32_t m)
 
 namespace {
 
+constexpr double kLearnedMinDrop = 0.1;
+
 template <int RPW, int PK>
 rsg_status run_typed(rsg_context *ctx, const GmresArgs &a, double *seconds)
 {
@@ -299,48 +302,88 @@ rsg_status run_typed(rsg_context *ctx, const GmresArgs &a, double *seconds)
     const int g_vec = std::min(grid_for(ctx, (const void *)k_gm_correct, kBlock, 0, n), kMaxGrid);
     const int g_dot = std::min(std::min(grid_for(ctx, (const void *)k_gm_dots, kBlock, 0, n), 512), kMaxGrid);
 
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    RSG_CHECK_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    k_gm_residual<RPW><<<g_res, kBlock, s64, ctx->stream>>>(M, S, us, a.b, a.x, a.ro, a.H, a.g, a.partials, a.st);
-    for (uint32_t k = 0; k < m; k++) {
-        k_gm_vz<PK><<<g_vec, kBlock, 0, ctx->stream>>>(n, a.P.w, a.P.d, a.ro, a.w, a.wnorm, a.V, a.Z, a.st, k);
-        k_gm_spmv<RPW><<<g_sp, kBlock, s64, ctx->stream>>>(M, S, us, a.Z, a.w, a.st, k);
-        k_gm_dots<<<dim3(g_dot, k + 1), kBlock, 0, ctx->stream>>>(n, a.V, a.w, a.H, a.hv, a.partials, a.st, k);
-        k_gm_correct<<<g_vec, kBlock, 0, ctx->stream>>>(n, a.V, a.w, a.hv, a.H, a.cs, a.sn, a.g, a.wnorm,
-                                                       a.partials, a.st, k);
+    // One captured graph per cycle; with the learned preconditioner a second graph
+    // (Jacobi z_k) is captured as the fallback.
+    auto capture = [&](rsg_learned *G, cudaGraph_t *graph, cudaGraphExec_t *exec) -> rsg_status {
+        if (G) RSG_TRY(gnn_prepare(ctx, G, a.A, false));  // no allocation inside the capture
+        RSG_CHECK_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        k_gm_residual<RPW><<<g_res, kBlock, s64, ctx->stream>>>(M, S, us, a.b, a.x, a.ro, a.H, a.g, a.partials,
+                                                               a.st);
+        for (uint32_t k = 0; k < m; k++) {
+            k_gm_vz<PK><<<g_vec, kBlock, 0, ctx->stream>>>(n, a.P.w, a.P.d, a.ro, a.w, a.wnorm, a.V, a.Z, a.st, k);
+            if (G) {  // flexible GMRES: z_k = M(v_k) from the network (Z is stored, src/rmatrixsolver.cpp:446)
+                const rsg_status gs =
+                    gnn_forward(ctx, G, a.A, a.V + size_t(k) * n, a.Z + size_t(k) * n, nullptr, false, true);
+                if (gs != RSG_OK) {
+                    cudaGraph_t dummy = nullptr;
+                    cudaStreamEndCapture(ctx->stream, &dummy);
+                    if (dummy) cudaGraphDestroy(dummy);
+                    return gs;
+                }
+            }
+            k_gm_spmv<RPW><<<g_sp, kBlock, s64, ctx->stream>>>(M, S, us, a.Z, a.w, a.st, k);
+            k_gm_dots<<<dim3(g_dot, k + 1), kBlock, 0, ctx->stream>>>(n, a.V, a.w, a.H, a.hv, a.partials, a.st, k);
+            k_gm_correct<<<g_vec, kBlock, 0, ctx->stream>>>(n, a.V, a.w, a.hv, a.H, a.cs, a.sn, a.g, a.wnorm,
+                                                           a.partials, a.st, k);
+        }
+        k_gm_backsub<<<1, 32, 0, ctx->stream>>>(a.H, a.g, a.y, a.st);
+        k_gm_update<<<g_vec, kBlock, 0, ctx->stream>>>(n, a.Z, a.y, a.x, a.st);
+        k_gm_cycle_end<<<1, 32, 0, ctx->stream>>>(a.st);
+        cudaError_t e = cudaStreamEndCapture(ctx->stream, graph);
+        if (e != cudaSuccess) return set_error(ctx, RSG_ERR_CUDA, "GMRES capture: %s", cudaGetErrorString(e));
+        e = cudaGraphInstantiate(exec, *graph, 0);
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(*graph);
+            *graph = nullptr;
+            return set_error(ctx, RSG_ERR_CUDA, "GMRES instantiate: %s", cudaGetErrorString(e));
+        }
+        return RSG_OK;
+    };
+    cudaGraph_t graph = nullptr, graph_j = nullptr;
+    cudaGraphExec_t exec = nullptr, exec_j = nullptr;
+    rsg_status s = capture(a.G, &graph, &exec);
+    if (s == RSG_OK && a.G) s = capture(nullptr, &graph_j, &exec_j);
+    if (s != RSG_OK) {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        return s;
     }
-    k_gm_backsub<<<1, 32, 0, ctx->stream>>>(a.H, a.g, a.y, a.st);
-    k_gm_update<<<g_vec, kBlock, 0, ctx->stream>>>(n, a.Z, a.y, a.x, a.st);
-    k_gm_cycle_end<<<1, 32, 0, ctx->stream>>>(a.st);
-    cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
-    if (e != cudaSuccess) return set_error(ctx, RSG_ERR_CUDA, "GMRES capture: %s", cudaGetErrorString(e));
-    e = cudaGraphInstantiate(&exec, graph, 0);
-    if (e != cudaSuccess) {
-        cudaGraphDestroy(graph);
-        return set_error(ctx, RSG_ERR_CUDA, "GMRES instantiate: %s", cudaGetErrorString(e));
-    }
-    rsg_status s = RSG_OK;
+    cudaError_t e = cudaSuccess;
     cudaEventRecord(ctx->ev[0], ctx->stream);
     int32_t *done_h = reinterpret_cast<int32_t *>(ctx->pinned);
+    double *beta_h = ctx->pinned + 1;
+    bool learned = a.G != nullptr;
+    double beta_prev = 0.0;
+    if (a.fallbacks) *a.fallbacks = 0;
     // k_gm_cycle_end marks the state done after max_outer cycles; the host bound is a backstop
     const uint64_t max_cycles = uint64_t(a.st_max_outer) + 2;
     for (uint64_t cycle = 0; cycle < max_cycles; cycle++) {
-        e = cudaGraphLaunch(exec, ctx->stream);
+        e = cudaGraphLaunch(learned ? exec : (exec_j ? exec_j : exec), ctx->stream);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(done_h, &a.st->done, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess && a.G)
+            e = cudaMemcpyAsync(beta_h, &a.st->beta, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) {
             s = set_error(ctx, RSG_ERR_CUDA, "GMRES cycle: %s", cudaGetErrorString(e));
             break;
         }
         if (*done_h) break;
+        // beta of this cycle is the residual left by the previous one: a learned cycle
+        // that removed less than kLearnedMinDrop of it hands over to Jacobi for good
+        if (learned && cycle > 0 && !(*beta_h < (1.0 - kLearnedMinDrop) * beta_prev)) {
+            learned = false;
+            if (a.fallbacks) (*a.fallbacks)++;
+        }
+        beta_prev = *beta_h;
     }
     cudaEventRecord(ctx->ev[1], ctx->stream);
     cudaStreamSynchronize(ctx->stream);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
     *seconds = ms * 1e-3;
+    if (exec_j) cudaGraphExecDestroy(exec_j);
+    if (graph_j) cudaGraphDestroy(graph_j);
     cudaGraphExecDestroy(exec);
     cudaGraphDestroy(graph);
     return s;

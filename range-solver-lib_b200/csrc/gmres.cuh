@@ -36,6 +36,8 @@ struct GmresArgs {
     // carved buffers
     double *V, *Z, *w, *ro, *H, *cs, *sn, *g, *y, *hv, *wnorm;
     uint32_t st_max_outer;
+    rsg_learned *G = nullptr;   // learned (variable) preconditioner: z_k = M(v_k)
+    uint32_t *fallbacks = nullptr;  // out: cycles handed over to Jacobi
 };
 
 size_t gmres_workspace_bytes(uint32_t n, uint32_t m, bool flexible);

@@ -1,0 +1,50 @@
+// Internal interface of the learned (message-passing) preconditioner.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include <vector>
+
+#include "csr.cuh"
+
+namespace rsg {
+constexpr int kGnnHidden = 64;
+constexpr int kGnnFeatures = 8;
+constexpr int kGnnGradBlocks = 256;
+}  // namespace rsg
+
+struct rsg_learned {
+    int L = 6;
+    size_t n_params = 0;
+    uint64_t step = 0;
+    float *params = nullptr, *grad = nullptr, *adam_m = nullptr, *adam_v = nullptr;
+    // per-matrix caches and activations (grow-only)
+    const rsg_csr *cached = nullptr;
+    uint64_t cached_nnz = 0;
+    double cached_norm = 0.0;
+    uint32_t cap = 0;
+    bool train_bufs = false;
+    std::vector<float *> h, m;
+    float *s = nullptr, *logd = nullptr, *rsum = nullptr, *feat = nullptr, *pre0 = nullptr;
+    float *gh = nullptr, *gh2 = nullptr, *gm = nullptr, *dz = nullptr, *blk = nullptr, *scal32 = nullptr;
+    double *dbuf = nullptr;
+};
+
+namespace rsg {
+void gnn_free_buffers(rsg_learned *G);
+rsg_status gnn_prepare(rsg_context *ctx, rsg_learned *G, const rsg_csr *A, bool train);
+rsg_status gnn_forward(rsg_context *ctx, rsg_learned *G, const rsg_csr *A, const double *r, double *z,
+                       const double *xyz, bool train, bool tensor_cores);
+rsg_status gnn_loss_grad(rsg_context *ctx, rsg_learned *G, const rsg_csr *A, const double *r, const double *xyz,
+                         bool tensor_cores, double *loss);
+void rsg_axpy_f32(rsg_context *ctx, size_t n, float a, const float *x, float *y);
+
+struct FcgResult {
+    uint32_t iterations, fallbacks, checks;
+    int32_t status;
+    double rn, bn, seconds;
+};
+size_t fcg_workspace_bytes(uint32_t n);
+rsg_status fcg_run(rsg_context *ctx, const rsg_csr *A, rsg_learned *G, const double *d, const double *b, double *x,
+                   double *partials, uint32_t max_it, double rtol, FcgResult *res);
+}  // namespace rsg

@@ -8,6 +8,7 @@
 // on the GPU and reported, and the per-iteration errors are printed / written
 // in RIterationInfo's formats (src/riterationinfo.cpp:111-193) when asked.
 #include "gmres.cuh"
+#include "gnn.cuh"
 #include "krylov.cuh"
 
 #include <chrono>
@@ -83,9 +84,17 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
     std::memset(&st_out, 0, sizeof(st_out));
     if (c.solver_type != RSG_SOLVER_CG && c.solver_type != RSG_SOLVER_GMRES)
         return set_error(ctx, RSG_ERR_INVALID_ARG, "Unknown matrix solver type '%d'", c.solver_type);
-    if (prec_type < RSG_PREC_NONE || prec_type > RSG_PREC_BLOCK_JACOBI)
-        return set_error(ctx, prec_type == RSG_PREC_LEARNED ? RSG_ERR_UNSUPPORTED : RSG_ERR_INVALID_ARG,
-                         "Invalid matrix preconditioner type '%d'", prec_type);
+    if (prec_type < RSG_PREC_NONE || prec_type > RSG_PREC_LEARNED)
+        return set_error(ctx, RSG_ERR_INVALID_ARG, "Invalid matrix preconditioner type '%d'", prec_type);
+    rsg_learned *G = static_cast<rsg_learned *>(const_cast<void *>(c.learned));
+    if ((prec_type == RSG_PREC_LEARNED || c.learned_initial_guess) && !G)
+        return set_error(ctx, RSG_ERR_INVALID_ARG, "learned preconditioner requested without conf.learned");
+    if (prec_type == RSG_PREC_LEARNED && c.solver_type == RSG_SOLVER_CG && c.stop_rule != RSG_STOP_TRUE_RELRES)
+        return set_error(ctx, RSG_ERR_INVALID_ARG, "flexible CG with the learned preconditioner needs TRUE_RELRES");
+    if (prec_type == RSG_PREC_LEARNED && c.precision != RSG_PRECISION_FP64)
+        return set_error(ctx, RSG_ERR_UNSUPPORTED, "the learned preconditioner runs with FP64 Krylov vectors");
+    const bool learned = prec_type == RSG_PREC_LEARNED;
+    if (learned) c.flexible = 1;
     if (c.precision == RSG_PRECISION_MIXED && c.stop_rule != RSG_STOP_TRUE_RELRES)
         return set_error(ctx, RSG_ERR_INVALID_ARG, "mixed precision requires stop_rule TRUE_RELRES");
     if (c.precision == RSG_PRECISION_MIXED && c.solver_type != RSG_SOLVER_CG)
@@ -109,7 +118,9 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
     bytes += arena_bytes(1, sizeof(CgState)) + arena_bytes(1, sizeof(GmresState));
     bytes += arena_bytes(64, sizeof(double));
     if (want_hist) bytes += 2 * arena_bytes(hist_len, sizeof(double));
-    if (!gmres) {
+    if (learned && !gmres) {
+        bytes += fcg_workspace_bytes(n);
+    } else if (!gmres) {
         bytes += 5 * vn;                               // r z p0 p1 q
         if (mixed) bytes += 6 * vf + arena_bytes(size_t(n) * w, sizeof(float));
     } else {
@@ -136,9 +147,9 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
 
     // ---- preconditioner ----
     Precond P;
-    P.kind = prec_type;
+    P.kind = learned ? RSG_PREC_JACOBI : prec_type;
     P.w = w;
-    if (prec_type == RSG_PREC_JACOBI) {
+    if (prec_type == RSG_PREC_JACOBI || learned) {
         RSG_TRY(jacobi_build(ctx, A, d));
     } else if (prec_type == RSG_PREC_BLOCK_JACOBI) {
         unsigned int *flag = ticket + 8;
@@ -169,9 +180,25 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
     if (scale != 1.0) k_scale<<<gv, kBlock, 0, ctx->stream>>>(n, x_dev, x_dev, scale);
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
 
+    if (c.learned_initial_guess) {
+        // x0 = M(b): the network's estimate of A^{-1} b (M is positively homogeneous,
+        // so the equation scaling carries over)
+        RSG_TRY(gnn_forward(ctx, G, A, y, x_dev, nullptr, false, true));
+    }
+
     double solve_seconds = 0.0;
     rsg_status solve_status = RSG_OK;
-    if (!gmres) {
+    if (learned && !gmres) {
+        FcgResult fr;
+        RSG_TRY(fcg_run(ctx, A, G, d, y, x_dev, partials, max_it, c.rtol, &fr));
+        st_out.iterations = fr.iterations;
+        st_out.outer = fr.checks;
+        st_out.fallbacks = fr.fallbacks;
+        st_out.converged = fr.status == RSG_OK;
+        st_out.error = fr.bn > 0.0 ? fr.rn / fr.bn : fr.rn;
+        solve_seconds = fr.seconds;
+        solve_status = rsg_status(fr.status);
+    } else if (!gmres) {
         CgArgs a = {};
         a.A = A;
         a.b = y;
@@ -243,6 +270,9 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
         a.st = gst;
         a.m = m;
         a.flexible = c.flexible != 0;
+        a.G = learned ? G : nullptr;
+        uint32_t gm_fallbacks = 0;
+        a.fallbacks = &gm_fallbacks;
         a.st_max_outer = max_it;
         RSG_TRY(gmres_carve(ctx, a, n, m));
         GmresState h;
@@ -258,6 +288,7 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
         h.trend_hist = thist;
         RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(gst, &h, sizeof(h), cudaMemcpyHostToDevice, ctx->stream));
         RSG_TRY(gmres_run(ctx, a, &solve_seconds));
+        st_out.fallbacks = gm_fallbacks;
         RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(&h, gst, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
         RSG_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         st_out.iterations = h.total_inner;

@@ -118,6 +118,15 @@ SIGNATURES = {
     "rsg_batch_destroy": (None, [_P, _P]),
     "rsg_batch_info": (C.c_int, [_P, _U32P, _U32P, _U32P, _U64P]),
     "rsg_batch_solve": (C.c_int, [_P, _P, C.POINTER(SolverConf), C.c_int32, _P, _P, C.c_int32, _P, _P]),
+    "rsg_learned_create": (C.c_int, [_P, C.c_uint32, C.c_uint64, _PP]),
+    "rsg_learned_destroy": (None, [_P, _P]),
+    "rsg_learned_info": (C.c_int, [_P, _U32P, _U32P, _U64P, _U64P]),
+    "rsg_learned_get_params": (C.c_int, [_P, _P, _P, C.c_int32]),
+    "rsg_learned_set_params": (C.c_int, [_P, _P, _P, C.c_int32]),
+    "rsg_learned_set_step": (C.c_int, [_P, C.c_uint64]),
+    "rsg_learned_apply": (C.c_int, [_P, _P, _P, _P, _P, _P, C.c_int32]),
+    "rsg_learned_loss_grad": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, _DP]),
+    "rsg_learned_train_step": (C.c_int, [_P, _P, _P, _P, _P, C.c_float, _DP]),
     "rsg_assembly_create_heat": (C.c_int, [_P, C.c_uint32, _P, C.c_uint32, _P, _P, C.c_uint32, _PP]),
     "rsg_assembly_create_stress": (C.c_int, [_P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32, _P, _P, C.c_uint32,
                                              _PP]),
