@@ -2,10 +2,13 @@
 //
 // The reference's CG (src/rmatrixsolver.cpp:208-355) assumes a fixed
 // preconditioner.  With a variable one (the network's output is a non-linear
-// function of r) this is flexible CG with one stored direction (Notay's FCG(1)):
-//     p_k = z_k - (z_k^T A p_{k-1} / p_{k-1}^T A p_{k-1}) p_{k-1},
+// function of r) this is truncated flexible CG, FCG(m) (Notay, SIAM J. Sci.
+// Comput. 22, 2000): the new direction is A-orthogonalised against the last m
+// stored directions,
+//     p_k = z_k - sum_j (z_k^T A p_j / p_j^T A p_j) p_j,   j = k-m .. k-1,
 //     alpha_k = p_k^T r_k / p_k^T A p_k,
-// which equals the reference's recurrences for a fixed SPD preconditioner.
+// which for a fixed SPD preconditioner reproduces the reference's recurrences
+// (the extra coefficients vanish in exact arithmetic).  m = min(n_inner, 16).
 // The learned step is abandoned for Jacobi (the reference's preconditioner)
 // as soon as it fails: z not a descent direction (r^T z <= 0), p^T A p <= 0,
 // or no new lowest residual norm for kStall iterations.  Stopping: FP64 true
@@ -18,23 +21,34 @@
 namespace rsg {
 namespace {
 
-constexpr uint32_t kStall = 10;
+constexpr uint32_t kStall = 25;
+constexpr int kDotsNV = kFcgMaxDirs + 1;
 
-// r^T z and z^T q_old (q_old = A p_{k-1})
-__global__ void k_fcg_dots(uint32_t n, const double *__restrict__ r, const double *__restrict__ z,
-                           const double *__restrict__ q, double *partials, unsigned int *ticket, double *out)
+struct DirCoef {
+    double c[kFcgMaxDirs];
+    int slot[kFcgMaxDirs];
+    int cnt;
+};
+
+// out[0] = r^T z, out[1 + j] = z^T Q[slot j] (j < cnt)
+__global__ void k_fcg_mdots(uint32_t n, const double *__restrict__ r, const double *__restrict__ z,
+                            const double *__restrict__ Q, DirCoef dc, double *partials, unsigned int *ticket,
+                            double *out)
 {
-    __shared__ double sh[64];
-    double acc[2] = {0.0, 0.0};
+    __shared__ double sh[32 * kDotsNV];
+    double acc[kDotsNV];
+#pragma unroll
+    for (int k = 0; k < kDotsNV; k++) acc[k] = 0.0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        acc[0] += r[i] * z[i];
-        acc[1] += z[i] * q[i];
+        const double zi = z[i];
+        acc[0] += r[i] * zi;
+#pragma unroll
+        for (int j = 0; j < kFcgMaxDirs; j++)
+            if (j < dc.cnt) acc[1 + j] += zi * Q[size_t(dc.slot[j]) * n + i];
     }
-    double tot[2];
-    if (grid_sum<2>(acc, partials, ticket, sh, tot) && threadIdx.x == 0) {
-        out[0] = tot[0];
-        out[1] = tot[1];
-    }
+    double tot[kDotsNV];
+    if (grid_sum<kDotsNV>(acc, partials, ticket, sh, tot) && threadIdx.x == 0)
+        for (int k = 0; k < kDotsNV; k++) out[k] = tot[k];
 }
 
 __global__ void k_fcg_jacobi(uint32_t n, const double *__restrict__ d, const double *__restrict__ r,
@@ -44,10 +58,17 @@ __global__ void k_fcg_jacobi(uint32_t n, const double *__restrict__ d, const dou
         z[i] = d ? d[i] * r[i] : r[i];
 }
 
-__global__ void k_fcg_dir(uint32_t n, const double *__restrict__ z, double beta, double *__restrict__ p)
+// p = z - sum_j c_j P[slot j]
+__global__ void k_fcg_newdir(uint32_t n, const double *__restrict__ z, const double *__restrict__ P, DirCoef dc,
+                             double *__restrict__ p)
 {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        p[i] = fma(beta, p[i], z[i]);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double v = z[i];
+#pragma unroll
+        for (int j = 0; j < kFcgMaxDirs; j++)
+            if (j < dc.cnt) v = fma(-dc.c[j], P[size_t(dc.slot[j]) * n + i], v);
+        p[i] = v;
+    }
 }
 
 // p^T q and p^T r
@@ -103,22 +124,28 @@ __global__ void k_fcg_resid(uint32_t n, const double *__restrict__ b, const doub
 
 }  // namespace
 
-size_t fcg_workspace_bytes(uint32_t n) { return 4 * arena_bytes(n, sizeof(double)) + arena_bytes(64, 8); }
+uint32_t fcg_dirs(uint32_t n_inner) { return std::max<uint32_t>(1, std::min<uint32_t>(n_inner, kFcgMaxDirs)); }
+
+size_t fcg_workspace_bytes(uint32_t n, uint32_t m)
+{
+    return 2 * arena_bytes(n, sizeof(double)) + 2 * arena_bytes(size_t(m + 1) * n, sizeof(double)) +
+           arena_bytes(64, 8);
+}
 
 rsg_status fcg_run(rsg_context *ctx, const rsg_csr *A, rsg_learned *G, const double *d, const double *b, double *x,
-                   double *partials, uint32_t max_it, double rtol, FcgResult *res)
+                   double *partials, uint32_t max_it, double rtol, uint32_t m, FcgResult *res)
 {
     const uint32_t n = A->n;
     cudaStream_t sm = ctx->stream;
-    double *r = arena_take<double>(ctx, n), *z = arena_take<double>(ctx, n), *p = arena_take<double>(ctx, n),
-           *q = arena_take<double>(ctx, n);
+    const uint32_t slots = m + 1;  // m stored directions + the one being built
+    double *r = arena_take<double>(ctx, n), *z = arena_take<double>(ctx, n);
+    double *P = arena_take<double>(ctx, size_t(slots) * n), *Q = arena_take<double>(ctx, size_t(slots) * n);
     double *sc = arena_take<double>(ctx, 64);
     if (!sc) return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "fcg workspace");
     unsigned int *ticket = reinterpret_cast<unsigned int *>(sc + 32);
     double *out = sc;
     double *h = ctx->pinned;
     RSG_CHECK_CUDA(ctx, cudaMemsetAsync(sc, 0, 64 * 8, sm));
-    RSG_CHECK_CUDA(ctx, cudaMemsetAsync(p, 0, size_t(n) * 8, sm));
     const int g = std::min(grid_for(ctx, (const void *)k_fcg_update, kBlock, 0, n), kMaxGrid);
     auto fetch = [&](int count) -> rsg_status {
         RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(h, out, count * sizeof(double), cudaMemcpyDeviceToHost, sm));
@@ -127,43 +154,49 @@ rsg_status fcg_run(rsg_context *ctx, const rsg_csr *A, rsg_learned *G, const dou
     };
     if (G) RSG_TRY(gnn_prepare(ctx, G, A, false));
     cudaEventRecord(ctx->ev[0], sm);
-    // r = b - A x
-    RSG_TRY(spmv64(ctx, A, x, q, true));
-    k_fcg_resid<<<g, kBlock, 0, sm>>>(n, b, q, r, partials, ticket, out);
+    // r = b - A x (Q slot 0 as scratch)
+    RSG_TRY(spmv64(ctx, A, x, Q, true));
+    k_fcg_resid<<<g, kBlock, 0, sm>>>(n, b, Q, r, partials, ticket, out);
     RSG_TRY(fetch(2));
     const double bn = std::sqrt(h[1]);
     double rn = std::sqrt(h[0]);
     bool learned = G != nullptr;
-    double pq_old = 0.0, best = rn;
+    double best = rn;
     uint32_t since_best = 0;
+    // stored directions, oldest first: slot index and p^T A p
+    int ring_slot[kFcgMaxDirs];
+    double ring_pq[kFcgMaxDirs];
+    uint32_t cnt = 0, next_slot = 0;
     res->iterations = 0;
     res->fallbacks = 0;
     res->checks = 0;
     res->status = RSG_NOT_CONVERGED;
-    bool restart = true;
     auto fall_back = [&]() {
         learned = false;
         res->fallbacks++;
-        restart = true;
+        cnt = 0;
     };
     if (!(rn > rtol * bn)) {
         res->status = RSG_OK;
         max_it = 0;
     }
     for (uint32_t it = 0; it < max_it; it++) {
+        DirCoef dc;
+        dc.cnt = int(cnt);
+        for (uint32_t j = 0; j < cnt; j++) dc.slot[j] = ring_slot[j];
         if (learned) RSG_TRY(gnn_forward(ctx, G, A, r, z, nullptr, false, true));
         else k_fcg_jacobi<<<g, kBlock, 0, sm>>>(n, d, r, z);
-        k_fcg_dots<<<g, kBlock, 0, sm>>>(n, r, z, q, partials, ticket, out);
-        RSG_TRY(fetch(2));
+        k_fcg_mdots<<<g, kBlock, 0, sm>>>(n, r, z, Q, dc, partials, ticket, out);
+        RSG_TRY(fetch(1 + int(cnt)));
         if (learned && !(h[0] > 0.0)) {  // not a descent direction
             fall_back();
+            dc.cnt = 0;
             k_fcg_jacobi<<<g, kBlock, 0, sm>>>(n, d, r, z);
-            k_fcg_dots<<<g, kBlock, 0, sm>>>(n, r, z, q, partials, ticket, out);
-            RSG_TRY(fetch(2));
         }
-        const double beta = restart || !(pq_old > 0.0) ? 0.0 : -h[1] / pq_old;
-        restart = false;
-        k_fcg_dir<<<g, kBlock, 0, sm>>>(n, z, beta, p);
+        for (int j = 0; j < dc.cnt; j++) dc.c[j] = h[1 + j] / ring_pq[j];
+        const int slot = int(next_slot);
+        double *p = P + size_t(slot) * n, *q = Q + size_t(slot) * n;
+        k_fcg_newdir<<<g, kBlock, 0, sm>>>(n, z, P, dc, p);
         RSG_TRY(spmv64(ctx, A, p, q, true));
         k_fcg_pdots<<<g, kBlock, 0, sm>>>(n, p, q, r, partials, ticket, out);
         RSG_TRY(fetch(2));
@@ -171,14 +204,32 @@ rsg_status fcg_run(rsg_context *ctx, const rsg_csr *A, rsg_learned *G, const dou
         if (!(pq > 0.0) || !std::isfinite(pq)) {
             if (learned) {
                 fall_back();
-                pq_old = 0.0;
                 continue;
             }
             res->status = RSG_BREAKDOWN;
             break;
         }
+        // keep p_k: drop the oldest stored direction when m are held
+        if (cnt == m) {
+            for (uint32_t j = 1; j < cnt; j++) {
+                ring_slot[j - 1] = ring_slot[j];
+                ring_pq[j - 1] = ring_pq[j];
+            }
+            cnt--;
+        }
+        ring_slot[cnt] = slot;
+        ring_pq[cnt] = pq;
+        cnt++;
+        // the next free slot is the one no stored direction uses
+        for (uint32_t s = 0; s < slots; s++) {
+            bool used = false;
+            for (uint32_t j = 0; j < cnt; j++) used |= ring_slot[j] == int(s);
+            if (!used) {
+                next_slot = s;
+                break;
+            }
+        }
         const double alpha = pr / pq;
-        pq_old = pq;
         k_fcg_update<<<g, kBlock, 0, sm>>>(n, alpha, p, q, x, r, partials, ticket, out);
         RSG_TRY(fetch(1));
         rn = std::sqrt(h[0]);
@@ -195,16 +246,16 @@ rsg_status fcg_run(rsg_context *ctx, const rsg_csr *A, rsg_learned *G, const dou
         }
         if (rn <= rtol * bn) {  // recompute the true residual before stopping
             res->checks++;
-            RSG_TRY(spmv64(ctx, A, x, q, true));
-            k_fcg_resid<<<g, kBlock, 0, sm>>>(n, b, q, r, partials, ticket, out);
+            double *ax = Q + size_t(next_slot) * n;  // free slot as scratch
+            RSG_TRY(spmv64(ctx, A, x, ax, true));
+            k_fcg_resid<<<g, kBlock, 0, sm>>>(n, b, ax, r, partials, ticket, out);
             RSG_TRY(fetch(2));
             rn = std::sqrt(h[0]);
             if (rn <= rtol * bn) {
                 res->status = RSG_OK;
                 break;
             }
-            restart = true;
-            pq_old = 0.0;
+            cnt = 0;  // restart the directions on the recomputed residual
         }
     }
     cudaEventRecord(ctx->ev[1], sm);

@@ -58,6 +58,19 @@ __global__ void k_gnn_prep(uint32_t n, const uint32_t *__restrict__ rp, const ui
     if (grid_sum<1>(acc, partials, ticket, sh, tot) && threadIdx.x == 0) *mean_logd = float(tot[0] / double(n));
 }
 
+// normalised edge weights of the message passing, one per stored nonzero
+__global__ void k_gnn_edges(uint32_t n, const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ci,
+                            const double *__restrict__ val, const float *__restrict__ s, float *__restrict__ ew)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float si = s[i];
+        for (uint32_t j = rp[i]; j < rp[i + 1]; j++) {
+            const uint32_t c = ci[j];
+            ew[j] = c == i ? 0.f : -float(val[j]) * si * s[c];
+        }
+    }
+}
+
 // ||D^{-1/2} r||^2 -> rms
 __global__ void k_gnn_rms(uint32_t n, const double *__restrict__ r, const float *__restrict__ s, double *partials,
                           unsigned int *ticket, float *rms)
@@ -107,21 +120,18 @@ __global__ void k_gnn_input(uint32_t n, const double *__restrict__ r, const floa
     }
 }
 
-// m = W h with W_ij = -a_ij s_i s_j (j != i): warp per row, 2 features per lane.
+// m = W h with W_ij = -a_ij s_i s_j (j != i), from the per-nonzero edge weights
+// (0 on the diagonal): warp per row, 2 features per lane.
 __global__ void k_gnn_spmm(uint32_t n, const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ci,
-                           const double *__restrict__ val, const float *__restrict__ s, const float *__restrict__ h,
-                           float *__restrict__ m)
+                           const float *__restrict__ ew, const float *__restrict__ h, float *__restrict__ m)
 {
     const int lane = threadIdx.x & 31;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     for (uint32_t i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
         float2 acc = make_float2(0.f, 0.f);
-        const float si = s[i];
         for (uint32_t j = rp[i]; j < rp[i + 1]; j++) {
-            const uint32_t c = ci[j];
-            if (c == i) continue;
-            const float wgt = -float(val[j]) * si * s[c];
-            const float2 hv = reinterpret_cast<const float2 *>(h + size_t(c) * H)[lane];
+            const float wgt = ew[j];
+            const float2 hv = reinterpret_cast<const float2 *>(h + size_t(ci[j]) * H)[lane];
             acc.x = fmaf(wgt, hv.x, acc.x);
             acc.y = fmaf(wgt, hv.y, acc.y);
         }
@@ -436,6 +446,13 @@ void gnn_free_buffers(rsg_learned *G)
     }
     cudaFree(G->dbuf);
     G->dbuf = nullptr;
+    cudaFree(G->ew);
+    G->ew = nullptr;
+    G->ew_cap = 0;
+    for (auto &b : G->hb) {
+        cudaFree(b);
+        b = nullptr;
+    }
     G->cap = 0;
     G->cached = nullptr;
 }
@@ -458,6 +475,7 @@ rsg_status gnn_prepare(rsg_context *ctx, rsg_learned *G, const rsg_csr *A, bool 
         G->rsum = dev_alloc<float>(n);
         G->scal32 = dev_alloc<float>(64);
         G->dbuf = dev_alloc<double>(size_t(4) * n + size_t(4) * kMaxGrid + 64);
+        for (auto &b : G->hb) b = dev_alloc<__nv_bfloat16>(size_t(n) * H);
         if (train) {
             G->feat = dev_alloc<float>(size_t(n) * F);
             G->pre0 = dev_alloc<float>(size_t(n) * H);
@@ -471,9 +489,18 @@ rsg_status gnn_prepare(rsg_context *ctx, rsg_learned *G, const rsg_csr *A, bool 
             if (!p) return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "learned: activations");
         for (float *p : G->m)
             if (!p) return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "learned: activations");
-        if (!G->s || !G->logd || !G->rsum || !G->dbuf || !G->scal32 ||
+        if (!G->s || !G->logd || !G->rsum || !G->dbuf || !G->scal32 || !G->hb[0] || !G->hb[1] ||
             (train && (!G->feat || !G->pre0 || !G->gh || !G->gh2 || !G->gm || !G->dz || !G->blk)))
             return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "learned: buffers");
+    }
+    int umma_grid = 0;
+    if (!gnn_umma_setup(ctx, &umma_grid)) return set_error(ctx, RSG_ERR_CUDA, "learned: tensor-core layer set-up");
+    if (A->nnz > G->ew_cap) {
+        cudaFree(G->ew);
+        G->ew = dev_alloc<float>(A->nnz);
+        G->ew_cap = G->ew ? A->nnz : 0;
+        if (!G->ew) return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "learned: edge weights");
+        G->cached = nullptr;
     }
     if (G->cached != A || realloc || G->cached_nnz != A->nnz || G->cached_norm != A->norm) {
         double *partials = G->dbuf + size_t(4) * n;
@@ -482,6 +509,7 @@ rsg_status gnn_prepare(rsg_context *ctx, rsg_learned *G, const rsg_csr *A, bool 
         const int g = std::min(grid_for(ctx, (const void *)k_gnn_prep, kBlock, 0, n), kMaxGrid);
         k_gnn_prep<<<g, kBlock, 0, ctx->stream>>>(n, A->rp, A->ci, A->val, G->s, G->logd, G->rsum, partials, ticket,
                                                   G->scal32);
+        k_gnn_edges<<<g, kBlock, 0, ctx->stream>>>(n, A->rp, A->ci, A->val, G->s, G->ew);
         RSG_CHECK_CUDA(ctx, cudaGetLastError());
         G->cached = A;
         G->cached_nnz = A->nnz;
@@ -502,6 +530,7 @@ rsg_status gnn_forward(rsg_context *ctx, rsg_learned *G, const rsg_csr *A, const
     float *rms = G->scal32 + 1;
     const int gv = std::min(grid_for(ctx, (const void *)k_gnn_rms, kBlock, 0, n), kMaxGrid);
     k_gnn_rms<<<gv, kBlock, 0, sm>>>(n, r, G->s, partials, ticket, rms);
+    if (!train && tensor_cores) return gnn_forward_umma(ctx, G, A, r, z, xyz, rms);
     const int gi = std::min(grid_for(ctx, (const void *)k_gnn_input, kBlock, 0, n), kMaxGrid);
     float *h0 = G->h[0];
     k_gnn_input<<<gi, kBlock, 0, sm>>>(n, r, G->s, G->logd, G->rsum, G->scal32, rms, xyz, G->params,
@@ -514,7 +543,7 @@ rsg_status gnn_forward(rsg_context *ctx, rsg_learned *G, const rsg_csr *A, const
         float *hout = train ? G->h[l + 1] : G->h[(l + 1) & 1];
         float *m = train ? G->m[l] : G->m[0];
         const float *W = G->params + off_layer(l), *b = W + size_t(K2) * H;
-        k_gnn_spmm<<<gs, kBlock, 0, sm>>>(n, A->rp, A->ci, A->val, G->s, hin, m);
+        k_gnn_spmm<<<gs, kBlock, 0, sm>>>(n, A->rp, A->ci, G->ew, hin, m);
         if (tensor_cores) k_gnn_dense_tc<<<gt, 32 * kTcWarps, 0, sm>>>(n, hin, m, W, b, hout);
         else k_gnn_dense_f32<<<gf, kBlock, 0, sm>>>(n, hin, m, W, b, hout);
     }
@@ -558,7 +587,7 @@ rsg_status gnn_loss_grad(rsg_context *ctx, rsg_learned *G, const rsg_csr *A, con
         k_gnn_layer_wgrad<<<nb, kBlock, 0, sm>>>(n, G->h[l], G->m[l], G->dz, G->blk);
         k_gnn_sum_blocks<<<32, kBlock, 0, sm>>>(G->blk, nb, K2 * H + H, G->grad + off_layer(l));
         // g_prev += W^T-graph gm (the graph weights are symmetric): reuse the SpMM into gm, then add
-        k_gnn_spmm<<<gs, kBlock, 0, sm>>>(n, A->rp, A->ci, A->val, G->s, G->gm, G->dz);
+        k_gnn_spmm<<<gs, kBlock, 0, sm>>>(n, A->rp, A->ci, G->ew, G->gm, G->dz);
         // g_prev = g2 + dz
         auto *a = g2;
         const size_t cnt = size_t(n) * H;

@@ -28,6 +28,9 @@ struct rsg_learned {
     float *s = nullptr, *logd = nullptr, *rsum = nullptr, *feat = nullptr, *pre0 = nullptr;
     float *gh = nullptr, *gh2 = nullptr, *gm = nullptr, *dz = nullptr, *blk = nullptr, *scal32 = nullptr;
     double *dbuf = nullptr;
+    __nv_bfloat16 *hb[2] = {nullptr, nullptr};  // BF16 activations of the tensor-core inference path
+    float *ew = nullptr;                         // edge weights -a_ij s_i s_j (0 on the diagonal), per nonzero
+    uint64_t ew_cap = 0;
 };
 
 namespace rsg {
@@ -37,6 +40,9 @@ rsg_status gnn_forward(rsg_context *ctx, rsg_learned *G, const rsg_csr *A, const
                        const double *xyz, bool train, bool tensor_cores);
 rsg_status gnn_loss_grad(rsg_context *ctx, rsg_learned *G, const rsg_csr *A, const double *r, const double *xyz,
                          bool tensor_cores, double *loss);
+rsg_status gnn_forward_umma(rsg_context *ctx, rsg_learned *G, const rsg_csr *A, const double *r, double *z,
+                            const double *xyz, const float *rms);
+bool gnn_umma_setup(rsg_context *ctx, int *grid);
 void rsg_axpy_f32(rsg_context *ctx, size_t n, float a, const float *x, float *y);
 
 struct FcgResult {
@@ -44,7 +50,9 @@ struct FcgResult {
     int32_t status;
     double rn, bn, seconds;
 };
-size_t fcg_workspace_bytes(uint32_t n);
+constexpr int kFcgMaxDirs = 16;
+uint32_t fcg_dirs(uint32_t n_inner);
+size_t fcg_workspace_bytes(uint32_t n, uint32_t m);
 rsg_status fcg_run(rsg_context *ctx, const rsg_csr *A, rsg_learned *G, const double *d, const double *b, double *x,
-                   double *partials, uint32_t max_it, double rtol, FcgResult *res);
+                   double *partials, uint32_t max_it, double rtol, uint32_t m, FcgResult *res);
 }  // namespace rsg

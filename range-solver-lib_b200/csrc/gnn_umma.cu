@@ -1,0 +1,363 @@
+// Inference path of the learned preconditioner on the 5th-generation tensor
+// cores: one fused kernel per message-passing layer,
+//     h_out = h + relu([h, G h] W_l + b_l),   G_ij = -a_ij s_i s_j (i != j),
+// with h stored as BF16 (128 B per row).  A CTA owns a tile of 128 rows:
+//   1. its 8 warps gather m = G h for the tile (8 lanes per row, 16-byte loads
+//      of the neighbours' BF16 rows, FP32 accumulation) and write [h | m] into
+//      shared memory in the canonical K-major layout (8x16-byte core matrices);
+//   2. one thread issues 8 tcgen05.mma (M=128, N=64, K=16 each, BF16 in, FP32
+//      accumulate) into a 64-column TMEM accumulator and commits to an mbarrier;
+//   3. all warps read the accumulator back with tcgen05.ld and apply bias, ReLU
+//      and the residual connection; the last layer also applies the output
+//      layer and writes z = M(r) in FP64.
+// W_l^T lives in shared memory as BF16 for the CTA's lifetime (persistent CTAs).
+// Waits on the mbarrier are bounded: past kWaitLimit polls the kernel flags the
+// context's error word, waits (bounded) for its MMAs, frees its TMEM and returns.
+#include "gnn.cuh"
+#include "spmv.cuh"
+
+namespace rsg {
+namespace {
+
+constexpr int H = kGnnHidden;   // 64
+constexpr int F = kGnnFeatures; // 8
+constexpr int K2 = 2 * H;       // 128
+constexpr int kTileRows = 128;
+constexpr int kThreads = 256;
+constexpr uint32_t kTmemCols = 64;
+constexpr uint32_t kATileBytes = kTileRows * K2 * 2;  // 32 KB
+constexpr uint32_t kBTileBytes = H * K2 * 2;          // 16 KB
+constexpr uint32_t kLBO = 128;                        // K-adjacent core matrices
+constexpr uint32_t kSBO = (K2 / 8) * 128;             // 8-row groups: 16 core matrices of 128 B
+constexpr uint32_t kOffB = kATileBytes;
+constexpr uint32_t kOffBias = kOffB + kBTileBytes;
+constexpr uint32_t kOffWout = kOffBias + H * 4;
+constexpr uint32_t kOffPart = kOffWout + H * 4;
+constexpr uint32_t kOffBar = kOffPart + kTileRows * 4;
+constexpr uint32_t kOffTmem = kOffBar + 16;
+constexpr uint32_t kLayerSmem = kOffTmem + 16;
+
+// Instruction descriptor of tcgen05.mma kind::f16: FP32 accumulator (bits 4-5 = 1),
+// A and B BF16 (bits 7-9 and 10-12 = 1), both K-major, N>>3 at bits 17-22, M>>4 at 24-28.
+constexpr uint32_t kIdesc =
+    (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(H >> 3) << 17) | (uint32_t(kTileRows >> 4) << 24);
+
+// byte offset of BF16 element (row, k) in a K-major tile without swizzle
+__device__ __forceinline__ uint32_t tile_off(uint32_t row, uint32_t k)
+{
+    return (row >> 3) * kSBO + (k >> 3) * kLBO + (row & 7) * 16 + (k & 7) * 2;
+}
+
+// shared-memory matrix descriptor: start address, LBO, SBO (all >> 4), version 1, no swizzle
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr)
+{
+    return uint64_t((saddr & 0x3FFFFu) >> 4) | (uint64_t(kLBO >> 4) << 16) | (uint64_t(kSBO >> 4) << 32) |
+           (uint64_t(1) << 46);
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+        "tcgen05.wait::ld.sync.aligned;\n"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr)
+        : "memory");
+}
+
+__device__ __forceinline__ void unpack8(const uint4 &u, float (&f)[8])
+{
+    const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+        f[2 * t] = __uint_as_float(w[t] << 16);
+        f[2 * t + 1] = __uint_as_float(w[t] & 0xffff0000u);
+    }
+}
+
+__device__ __forceinline__ uint32_t pack2(float lo, float hi)
+{
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t *>(&v);
+}
+
+// features and input layer, BF16 output: h0 = relu(f W_in + b_in)
+__global__ void k_gnn_input_bf16(uint32_t n, const double *__restrict__ r, const float *__restrict__ s,
+                                 const float *__restrict__ logd, const float *__restrict__ rsum,
+                                 const float *__restrict__ mean_logd, const float *__restrict__ rms,
+                                 const double *__restrict__ xyz, const float *__restrict__ P,
+                                 __nv_bfloat16 *__restrict__ h0)
+{
+    __shared__ float w[F * H + H];
+    for (int k = threadIdx.x; k < F * H + H; k += blockDim.x) w[k] = P[k];
+    __syncthreads();
+    const float inv = 1.0f / *rms, ml = *mean_logd;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float f[F];
+        f[0] = float(r[i] * double(s[i])) * inv;
+        f[1] = logd[i] - ml;
+        f[2] = rsum[i];
+        f[3] = xyz ? float(xyz[3 * size_t(i)]) : 0.f;
+        f[4] = xyz ? float(xyz[3 * size_t(i) + 1]) : 0.f;
+        f[5] = xyz ? float(xyz[3 * size_t(i) + 2]) : 0.f;
+        f[6] = 1.f;
+        f[7] = 0.f;
+        uint4 *dst = reinterpret_cast<uint4 *>(h0 + size_t(i) * H);
+#pragma unroll 1
+        for (int c8 = 0; c8 < H / 8; c8++) {
+            float o[8];
+#pragma unroll
+            for (int t = 0; t < 8; t++) {
+                const int c = c8 * 8 + t;
+                float z = w[F * H + c];
+#pragma unroll
+                for (int k = 0; k < F; k++) z = fmaf(f[k], w[k * H + c], z);
+                o[t] = fmaxf(z, 0.f);
+            }
+            dst[c8] = make_uint4(pack2(o[0], o[1]), pack2(o[2], o[3]), pack2(o[4], o[5]), pack2(o[6], o[7]));
+        }
+    }
+}
+
+template <bool LAST>
+__global__ void __launch_bounds__(kThreads) k_gnn_layer_umma(
+    uint32_t n, const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ci, const float *__restrict__ ew,
+    const float *__restrict__ s, const __nv_bfloat16 *__restrict__ h, const float *__restrict__ W,
+    const float *__restrict__ bias, const float *__restrict__ pout, const float *__restrict__ rms,
+    __nv_bfloat16 *__restrict__ h_out, double *__restrict__ z, unsigned int *err)
+{
+    extern __shared__ __align__(1024) unsigned char sm[];
+    unsigned char *At = sm;
+    unsigned char *Bt = sm + kOffB;
+    float *bs = reinterpret_cast<float *>(sm + kOffBias);
+    float *wo = reinterpret_cast<float *>(sm + kOffWout);
+    float *part = reinterpret_cast<float *>(sm + kOffPart);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + kOffBar);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + kOffTmem);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+    // B = W^T (N = 64 output columns x K = 128), BF16, K-major
+    for (int e = tid; e < K2 * H; e += kThreads) {
+        const int k = e / H, c = e % H;
+        *reinterpret_cast<__nv_bfloat16 *>(Bt + tile_off(c, k)) = __float2bfloat16_rn(W[e]);
+    }
+    if (tid < H) {
+        bs[tid] = bias[tid];
+        wo[tid] = LAST ? pout[tid] : 0.f;
+    }
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_async_shared();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const float b_out = LAST ? pout[H] : 0.f;
+    const float sc = LAST ? *rms : 0.f;
+    const uint32_t tiles = (n + kTileRows - 1) / kTileRows;
+    const int q = lane >> 3, kc = lane & 7;  // gather: 4 rows per warp pass, 8 lanes x 16 B per row
+    const int quarter = warp & 3, half = warp >> 2;
+    uint32_t phase = 0;
+    bool in_flight = false, failed = false;
+
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const uint32_t r0 = tile * kTileRows;
+        // 1. gather m = G h and stage [h | m] (BF16) in the A tile.  The 8 lanes of a row
+        //    fetch 8 of its (column, weight) pairs at once and then 8 neighbour rows
+        //    back to back, so each lane keeps 8 independent 16-byte loads in flight.
+#pragma unroll 1
+        for (int pass = 0; pass < 4; pass++) {
+            const uint32_t trow = uint32_t(warp * 16 + pass * 4 + q);
+            const uint32_t row = r0 + trow;
+            float acc[8];
+#pragma unroll
+            for (int t = 0; t < 8; t++) acc[t] = 0.f;
+            uint4 hown = make_uint4(0u, 0u, 0u, 0u);
+            uint32_t jb = 0, je = 0;
+            if (row < n) {
+                hown = *reinterpret_cast<const uint4 *>(h + size_t(row) * H + kc * 8);
+                jb = rp[row];
+                je = rp[row + 1];
+            }
+            const uint32_t trips = __reduce_max_sync(0xffffffffu, (je - jb + 7) / 8);
+            const uint32_t rown = row < n ? row : 0u;
+            for (uint32_t it = 0; it < trips; it++) {
+                const uint32_t jj = jb + it * 8 + uint32_t(kc);
+                uint32_t c_mine = rown;
+                float w_mine = 0.f;
+                if (jj < je) {  // the diagonal's weight is 0
+                    c_mine = ci[jj];
+                    w_mine = ew[jj];
+                }
+                uint4 hv[8];
+                float wt[8];
+#pragma unroll
+                for (int t = 0; t < 8; t++) {
+                    const uint32_t ct = __shfl_sync(0xffffffffu, c_mine, (lane & ~7) + t);
+                    wt[t] = __shfl_sync(0xffffffffu, w_mine, (lane & ~7) + t);
+                    hv[t] = *reinterpret_cast<const uint4 *>(h + size_t(ct) * H + kc * 8);
+                }
+#pragma unroll
+                for (int t = 0; t < 8; t++) {
+                    float f[8];
+                    unpack8(hv[t], f);
+#pragma unroll
+                    for (int u = 0; u < 8; u++) acc[u] = fmaf(wt[t], f[u], acc[u]);
+                }
+            }
+            *reinterpret_cast<uint4 *>(At + tile_off(trow, kc * 8)) = hown;
+            *reinterpret_cast<uint4 *>(At + tile_off(trow, H + kc * 8)) =
+                make_uint4(pack2(acc[0], acc[1]), pack2(acc[2], acc[3]), pack2(acc[4], acc[5]),
+                           pack2(acc[6], acc[7]));
+        }
+        fence_async_shared();  // generic-proxy smem writes -> visible to the tensor core
+        __syncthreads();
+        // 2. one thread issues the MMAs: D[128 x 64] = A[128 x 128] B^T
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(At), b0 = smem_u32(Bt);
+#pragma unroll
+            for (int ks = 0; ks < K2 / 16; ks++)
+                umma_bf16(tmem, smem_desc(a0 + ks * 2 * kLBO), smem_desc(b0 + ks * 2 * kLBO), ks > 0 ? 1u : 0u);
+            umma_commit(bar);
+        }
+        in_flight = true;
+        const bool ok = mbar_wait(bar, phase, err);
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        in_flight = false;
+        phase ^= 1u;
+        tc_fence_after();
+        // 3. epilogue: warp (quarter, half) reads TMEM lanes 32*quarter.., columns 32*half..
+        const uint32_t trow = uint32_t(quarter * 32 + lane), row = r0 + trow;
+        uint32_t v[32];
+        tmem_ld32(tmem + (uint32_t(quarter * 32) << 16) + uint32_t(half * 32), v);
+        float o[32];
+        float dot = 0.f;
+#pragma unroll
+        for (int c8 = 0; c8 < 4; c8++) {
+            const int cb = half * 32 + c8 * 8;
+            float hp[8];
+            unpack8(*reinterpret_cast<const uint4 *>(At + tile_off(trow, cb)), hp);
+#pragma unroll
+            for (int t = 0; t < 8; t++) {
+                const int c = cb + t;
+                const float val_o = hp[t] + fmaxf(__uint_as_float(v[c8 * 8 + t]) + bs[c], 0.f);
+                o[c8 * 8 + t] = val_o;
+                dot = fmaf(val_o, wo[c], dot);
+            }
+        }
+        if constexpr (!LAST) {
+            if (row < n) {
+                uint4 *dst = reinterpret_cast<uint4 *>(h_out + size_t(row) * H + half * 32);
+#pragma unroll
+                for (int c8 = 0; c8 < 4; c8++)
+                    dst[c8] = make_uint4(pack2(o[c8 * 8], o[c8 * 8 + 1]), pack2(o[c8 * 8 + 2], o[c8 * 8 + 3]),
+                                         pack2(o[c8 * 8 + 4], o[c8 * 8 + 5]), pack2(o[c8 * 8 + 6], o[c8 * 8 + 7]));
+            }
+        } else {
+            if (half == 1) part[trow] = dot;
+            __syncthreads();
+            if (half == 0 && row < n) z[row] = double(dot + part[trow] + b_out) * double(sc) * double(s[row]);
+        }
+        tc_fence_before();
+        __syncthreads();  // A tile, TMEM and part[] free for the next tile
+    }
+    if (failed && in_flight && tid == 0) mbar_wait(bar, phase, nullptr);  // let the MMAs drain (bounded)
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    }
+}
+
+__host__ __device__ inline size_t off_layer(int l) { return size_t(F) * H + H + size_t(l) * (size_t(K2) * H + H); }
+
+}  // namespace
+
+bool gnn_umma_setup(rsg_context *ctx, int *grid)
+{
+    static bool attr = false;
+    if (!attr) {
+        for (const void *f : {(const void *)k_gnn_layer_umma<false>, (const void *)k_gnn_layer_umma<true>}) {
+            if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kLayerSmem)) != cudaSuccess ||
+                cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess)
+                return false;
+        }
+        attr = true;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gnn_layer_umma<false>, kThreads, kLayerSmem) !=
+            cudaSuccess ||
+        per_sm < 1)
+        return false;
+    // Four CTAs fit an SM by shared memory and registers; CTAs beyond the resident
+    // ones wait for a slot, so a larger grid never over-commits the 512 TMEM columns
+    // (each resident CTA holds kTmemCols of them).
+    per_sm = std::min(std::max(per_sm, 4), int(512 / kTmemCols));
+    *grid = per_sm * ctx->num_sms;
+    return true;
+}
+
+// z = M(r) through the BF16 tensor-core layers; h buffers hb[0], hb[1] (n x 64 BF16 each).
+rsg_status gnn_forward_umma(rsg_context *ctx, rsg_learned *G, const rsg_csr *A, const double *r, double *z,
+                            const double *xyz, const float *rms)
+{
+    const uint32_t n = A->n;
+    cudaStream_t sm = ctx->stream;
+    int gl = 0;
+    if (!gnn_umma_setup(ctx, &gl)) return set_error(ctx, RSG_ERR_CUDA, "learned: tensor-core layer set-up");
+    const uint32_t tiles = (n + kTileRows - 1) / kTileRows;
+    gl = int(std::min<uint32_t>(uint32_t(gl), std::max<uint32_t>(tiles, 1)));
+    const int gi = std::min(grid_for(ctx, (const void *)k_gnn_input_bf16, kBlock, 0, n), kMaxGrid);
+    k_gnn_input_bf16<<<gi, kBlock, 0, sm>>>(n, r, G->s, G->logd, G->rsum, G->scal32, rms, xyz, G->params, G->hb[0]);
+    for (int l = 0; l < G->L; l++) {
+        const float *W = G->params + off_layer(l), *b = W + size_t(K2) * H;
+        const float *pout = G->params + off_layer(G->L);
+        const __nv_bfloat16 *hin = G->hb[l & 1];
+        __nv_bfloat16 *hout = G->hb[(l + 1) & 1];
+        if (l + 1 < G->L)
+            k_gnn_layer_umma<false><<<gl, kThreads, kLayerSmem, sm>>>(n, A->rp, A->ci, G->ew, G->s, hin, W, b, pout,
+                                                                     rms, hout, z, ctx->errw);
+        else
+            k_gnn_layer_umma<true><<<gl, kThreads, kLayerSmem, sm>>>(n, A->rp, A->ci, G->ew, G->s, hin, W, b, pout,
+                                                                    rms, hout, z, ctx->errw);
+    }
+    RSG_CHECK_CUDA(ctx, cudaGetLastError());
+    return RSG_OK;
+}
+
+}  // namespace rsg

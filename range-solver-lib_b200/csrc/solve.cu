@@ -119,7 +119,7 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
     bytes += arena_bytes(64, sizeof(double));
     if (want_hist) bytes += 2 * arena_bytes(hist_len, sizeof(double));
     if (learned && !gmres) {
-        bytes += fcg_workspace_bytes(n);
+        bytes += fcg_workspace_bytes(n, fcg_dirs(c.n_inner));
     } else if (!gmres) {
         bytes += 5 * vn;                               // r z p0 p1 q
         if (mixed) bytes += 6 * vf + arena_bytes(size_t(n) * w, sizeof(float));
@@ -190,7 +190,7 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
     rsg_status solve_status = RSG_OK;
     if (learned && !gmres) {
         FcgResult fr;
-        RSG_TRY(fcg_run(ctx, A, G, d, y, x_dev, partials, max_it, c.rtol, &fr));
+        RSG_TRY(fcg_run(ctx, A, G, d, y, x_dev, partials, max_it, c.rtol, fcg_dirs(c.n_inner), &fr));
         st_out.iterations = fr.iterations;
         st_out.outer = fr.checks;
         st_out.fallbacks = fr.fallbacks;

@@ -156,6 +156,83 @@ def train(ctx, model: Learned, samples, steps: int, lr: float = 1e-3, seed: int 
     return losses
 
 
+def family_sigma(seed: int, lo: float = 0.5, hi: float = 2.0) -> float:
+    """Per-seed conductivity spread sigma ~ U(lo, hi) of the learned-preconditioner heat family."""
+    from . import workloads as W
+    return float(lo + (hi - lo) * W.uniform(seed, 3, 1)[0])
+
+
+def train_heat_family(ctx, model: Learned, n_hex: int, seeds, lr: float = 1e-3, lr_final: float = 1e-4,
+                      checkpoints=(0, 1, 2, 4, 8, 16, 32, 64, 128, 256), n_random: int = 1, log_every: int = 0,
+                      base=None):
+    """Online training over seeded lognormal heat problems on one n_hex^3 mesh: for each seed
+    the GPU assembles the system (one plan, new values), the plain Jacobi-PCG trajectory
+    gives residuals, and each residual is one Adam step.  Returns per-step losses."""
+    import torch
+    from . import Assembly
+    from . import workloads as W
+    base = base or W.heat_cube(n_hex, sigma=1.0, seed=0, source="random")
+    asm = Assembly.heat(ctx, base)
+    b = torch.empty(asm.n_free, dtype=torch.float64, device=f"cuda:{ctx.device}")
+    seeds = list(seeds)
+    per = len(checkpoints) * (1 + n_random)
+    total = max(len(seeds) * per, 1)
+    rng = np.random.default_rng(12345)
+    losses, t = [], 0
+    for seed in seeds:
+        p = W.reseed_heat(base, sigma=family_sigma(seed), seed=seed)
+        A = asm.assemble(p, b)
+        ctx.sync()
+        rs = trajectory_residuals(ctx, A, b, checkpoints, n_random, seed)
+        for i in rng.permutation(len(rs)):
+            cur = lr_final + 0.5 * (lr - lr_final) * (1.0 + np.cos(np.pi * min(t, total - 1) / max(total - 1, 1)))
+            losses.append(model.train_step(A, rs[i], float(cur)))
+            t += 1
+        if log_every and (len(losses) // per) % log_every == 0:
+            print(f"seed {seed}  steps {t}  loss {np.mean(losses[-per:]):.4f}", flush=True)
+    asm.close()
+    return losses
+
+
+def evaluate_heat_family(ctx, model: Learned, n_hex: int, seeds, rtol: float = 1e-10, base=None,
+                         methods=("pcg", "fcg", "gmres", "fgmres"), max_it: int = 100000):
+    """Solve each held-out seed with plain Jacobi-PCG / GMRES(30) and their learned (flexible)
+    counterparts; returns one dict per seed with iterations, device seconds, true residual."""
+    import torch
+    from . import Assembly, make_conf, PREC_LEARNED
+    from . import workloads as W
+    base = base or W.heat_cube(n_hex, sigma=1.0, seed=0, source="random")
+    asm = Assembly.heat(ctx, base)
+    b = torch.empty(asm.n_free, dtype=torch.float64, device=f"cuda:{ctx.device}")
+    x = torch.zeros_like(b)
+    confs = {
+        "pcg": (PREC_JACOBI, make_conf(n_outer=max_it, stop_rule="true", rtol=rtol)),
+        "fcg": (PREC_LEARNED, learned_conf(model, make_conf(n_outer=max_it, stop_rule="true", rtol=rtol))),
+        "gmres": (PREC_JACOBI, make_conf(solver="gmres", n_outer=max_it, n_inner=30, stop_rule="true", rtol=rtol)),
+        "fgmres": (PREC_LEARNED, learned_conf(model, make_conf(solver="gmres", n_outer=max_it, n_inner=30,
+                                                               stop_rule="true", rtol=rtol))),
+        "pcg_x0": (PREC_JACOBI, learned_conf(model, make_conf(n_outer=max_it, stop_rule="true", rtol=rtol),
+                                             initial_guess=True)),
+    }
+    out = []
+    for seed in seeds:
+        p = W.reseed_heat(base, sigma=family_sigma(seed), seed=seed)
+        A = asm.assemble(p, b)
+        ctx.sync()
+        row = {"seed": int(seed), "sigma": family_sigma(seed)}
+        for name in methods:
+            prec, conf = confs[name]
+            x.zero_()
+            torch.cuda.synchronize()
+            _, st = ctx.solve(A, b, x, conf=conf, prec=prec)
+            row[name] = {"iterations": int(st.iterations), "seconds": float(st.seconds_solve),
+                         "true_relres": float(st.true_relres), "fallbacks": int(st.fallbacks),
+                         "converged": int(st.converged)}
+        out.append(row)
+    asm.close()
+    return out
+
+
 def learned_conf(model: Learned, base: SolverConf | None = None, initial_guess: bool = False) -> SolverConf:
     """A copy of base (default: TRUE_RELRES CG) that points at model."""
     from . import make_conf
@@ -165,4 +242,5 @@ def learned_conf(model: Learned, base: SolverConf | None = None, initial_guess: 
     return c
 
 
-__all__ = ["Learned", "trajectory_residuals", "train", "learned_conf", "PARAMS", "GRAD", "ADAM_M", "ADAM_V", "OK"]
+__all__ = ["Learned", "trajectory_residuals", "train", "learned_conf", "train_heat_family", "evaluate_heat_family",
+           "family_sigma", "PARAMS", "GRAD", "ADAM_M", "ADAM_V", "OK"]

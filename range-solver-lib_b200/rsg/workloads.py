@@ -176,6 +176,18 @@ def heat_cube(n: int, *, sigma: float = 0.0, seed: int = 0, source: str = "unit"
                        name=f"heat_cube_{n}", meta=dict(n=n, sigma=sigma, seed=seed, source=source))
 
 
+def reseed_heat(p: HeatProblem, *, sigma: float, seed: int, mu: float = 0.0) -> HeatProblem:
+    """p with a new lognormal(mu, sigma) conductivity field and random source drawn from seed
+    (same mesh, node book and boundary values; the streams heat_cube uses for that seed)."""
+    import copy
+    q = copy.copy(p)
+    m = p.mesh
+    q.k_e = lognormal(seed, 1, m.n_tets, mu, sigma)
+    q.q_e = uniform(seed, 2, m.n_nodes)[m.tets].mean(axis=1)
+    q.meta = dict(p.meta, sigma=sigma, seed=seed, source="random")
+    return q
+
+
 @dataclass
 class StressProblem:
     """Linear elasticity on a tet mesh (RSolverStress inputs), 3 dofs per node interleaved."""
