@@ -242,10 +242,15 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--delta", type=float, default=1e-2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="heat100", choices=["heat100", "stress", "batch256", "transient40"],
+    ap.add_argument("--workload", default="heat100",
+                    choices=["heat100", "stress", "batch256", "transient40", "learned"],
                     help="heat100 (default, the headline); stress: 64x32x32 elasticity beam; batch256: 256 "
                          "independent heat cubes with 8..60 hexes per side; transient40: 64 backward-Euler steps "
-                         "on a 40^3 mesh")
+                         "on a 40^3 mesh; learned: train the learned preconditioner on the GPU on seeded "
+                         "60^3 lognormal heat problems, evaluate on held-out seeds and on the 100^3 system")
+    ap.add_argument("--train-seeds", type=int, default=100, help="learned: training problems (seeds)")
+    ap.add_argument("--eval-seeds", type=int, default=8, help="learned: held-out evaluation seeds")
+    ap.add_argument("--learned-hex", type=int, default=60, help="learned: hexes per side of the family mesh")
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the CG loop from the host (same kernels, launched one by one) so that "
                          "profilers which cannot see kernels inside conditional CUDA graphs list them")
@@ -467,6 +472,71 @@ def run_other(args, rank, world, local_rank, threads):
             t16 = time.perf_counter() - t0
             line["cpu_baseline"] = {"value": 16 / t16, "unit": "systems/s", "cores": threads, "kind": "port",
                                     "sample": "the first 16 systems of the batch, solved one after another"}
+    elif args.workload == "learned":
+        from rsg import learned as RL
+        model = RL.Learned(ctx, layers=6, seed=1 + rank)
+        base = W.heat_cube(args.learned_hex, sigma=1.0, seed=0, source="random")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        losses = RL.train_heat_family(ctx, model, args.learned_hex, range(100000, 100000 + args.train_seeds),
+                                      base=base)
+        torch.cuda.synchronize()
+        t_train = time.perf_counter() - t0
+        methods = ("pcg", "fcg", "gmres", "fgmres", "pcg_x0")
+        ev = RL.evaluate_heat_family(ctx, model, args.learned_hex, range(args.eval_seeds), rtol=RTOL, base=base,
+                                     methods=methods)
+
+        def mean(meth, key):
+            return float(np.mean([row[meth][key] for row in ev]))
+        summary = {m: {"iterations": mean(m, "iterations"), "seconds": mean(m, "seconds"),
+                       "worst_true_relres": max(row[m]["true_relres"] for row in ev),
+                       "fallbacks": int(sum(row[m]["fallbacks"] for row in ev)),
+                       "converged": int(sum(row[m]["converged"] for row in ev))} for m in methods}
+        # the 100^3 headline system with the same model
+        p100 = W.heat_cube(N_HEX, sigma=SIGMA, seed=0, source="random")
+        asm = rsg.Assembly.heat(ctx, p100)
+        b = torch.empty(asm.n_free, dtype=torch.float64, device="cuda")
+        x = torch.zeros_like(b)
+        A = asm.assemble(p100, b)
+        big = {}
+        for name, prec, conf in (
+                ("pcg", rsg.PREC_JACOBI, rsg.make_conf(n_outer=100000, stop_rule="true", rtol=RTOL)),
+                ("fcg", rsg.PREC_LEARNED, RL.learned_conf(model, rsg.make_conf(n_outer=100000, stop_rule="true",
+                                                                                rtol=RTOL))),
+                ("gmres", rsg.PREC_JACOBI, rsg.make_conf(solver="gmres", n_outer=100000, n_inner=30,
+                                                         stop_rule="true", rtol=RTOL)),
+                ("fgmres", rsg.PREC_LEARNED, RL.learned_conf(model, rsg.make_conf(
+                    solver="gmres", n_outer=100000, n_inner=30, stop_rule="true", rtol=RTOL)))):
+            x.zero_()
+            torch.cuda.synchronize()
+            _, st = ctx.solve(A, b, x, conf=conf, prec=prec)
+            big[name] = {"iterations": st.iterations, "seconds": st.seconds_solve, "true_relres": st.true_relres,
+                         "fallbacks": st.fallbacks}
+        r_apply = b.clone()
+        z = torch.empty_like(b)
+        model.apply(A, r_apply, z)
+        ctx.sync()
+        t_apply, _ = _events_time(lambda: [model.apply(A, r_apply, z) for _ in range(10)], stream)
+        asm.close()
+        line.update({
+            "metric": f"time-to-solve (s) at FP64 rel. residual 1e-10, learned-preconditioned FCG(16), "
+                      f"held-out {args.learned_hex}^3 lognormal heat seeds",
+            "value": max_over_ranks(summary["fcg"]["seconds"]), "unit": "s",
+            "ms_per_step": summary["fcg"]["seconds"] * 1e3, "higher_is_better": False,
+            "dtype": "f64 Krylov / bf16 network (fp32 accumulate)",
+            "config": {"workload": f"learned_heat_{args.learned_hex}", "train_seeds": args.train_seeds,
+                       "train_steps": len(losses), "train_seconds": t_train,
+                       "train_loss_first100": float(np.mean(losses[:100])),
+                       "train_loss_last100": float(np.mean(losses[-100:])),
+                       "eval_seeds": args.eval_seeds, "summary": summary,
+                       "iteration_ratio_pcg_over_fcg": summary["pcg"]["iterations"] / summary["fcg"]["iterations"],
+                       "iteration_ratio_gmres_over_fgmres":
+                           summary["gmres"]["iterations"] / summary["fgmres"]["iterations"],
+                       "time_ratio_fcg_over_pcg": summary["fcg"]["seconds"] / summary["pcg"]["seconds"],
+                       "time_ratio_fgmres_over_gmres": summary["fgmres"]["seconds"] / summary["gmres"]["seconds"],
+                       f"heat_lognormal_{N_HEX}": big,
+                       f"network_apply_s_{N_HEX}": t_apply / 10,
+                       "network": "6 message-passing layers, 64 wide, BF16 tcgen05 MMA with FP32 accumulation"}})
     else:  # transient40
         p = W.heat_cube(40, sigma=1.0, seed=rank, source="random", transient=True, dt=1e-3)
         torch.cuda.synchronize()
