@@ -84,8 +84,11 @@ typedef struct {
     uint32_t check_interval;    /* host-driven loop: iterations per convergence poll */
     const void *learned;        /* rsg_learned* for RSG_PREC_LEARNED / learned initial guess */
     int32_t  learned_initial_guess;
-    int32_t  l2_resident_f32;   /* mixed: stream the FP32 matrix with L2 evict_last (it fits in L2 up to ~1.3M rows) */
-    int32_t  reserved[6];
+    int32_t  l2_resident_f32;   /* mixed, CSR-stream layout only: FP32 matrix loads with L2 evict_last
+                                   (slower than evict_first on SELL-32 in measurements, so not applied there) */
+    int32_t  autotune;          /* 1: autotune A's launch shapes on its first solve (rsg_autotune, with the
+                                   cache file named by the RSG_TUNE_CACHE environment variable if set) */
+    int32_t  reserved[5];
 } rsg_solver_conf;
 
 typedef struct {
@@ -174,6 +177,29 @@ typedef enum {
 } rsg_kernel_id;
 RSG_API rsg_status rsg_profile_kernel(rsg_context *ctx, const rsg_csr *A, int32_t kernel, uint32_t reps,
                                       int32_t flush_l2, double *seconds);
+
+/* Autotuner (no counterpart in the reference, whose loops are OpenMP).  Picks
+ * A's layout (SELL-32, or the CSR stream with a rows-per-warp chunk) and the
+ * grid sizes of the CG loop's two kernels per iteration (fused direction +
+ * SpMV, and update) by timing short fixed-length Jacobi-PCG solves of A itself
+ * in FP64 and mixed precision for each candidate; the built-in defaults are a
+ * candidate too.  The choice stays with A for every later solve.  cache_path
+ * (may be NULL): a text file keyed by device, matrix shape and layout; a
+ * matching line is used without timing, a new result is appended.  Tuning
+ * allocates two n-vectors for the duration of the call. */
+typedef struct rsg_tune_info {
+    int32_t  tuned;                  /* 1 when A carries autotuned shapes */
+    int32_t  from_cache;
+    int32_t  format;                 /* 1 SELL-32, 0 CSR stream */
+    uint32_t rows_per_warp;          /* CSR stream chunk (32 for SELL-32) */
+    uint32_t grid_dir_fp64, grid_dir_fp32, grid_update_fp64, grid_update_fp32;  /* 0 = built-in default */
+    double   seconds_iter_fp64, seconds_iter_fp32;                   /* per CG iteration, chosen shapes */
+    double   seconds_iter_fp64_default, seconds_iter_fp32_default;   /* per CG iteration, built-in shapes */
+    uint32_t candidates;             /* timed solves */
+    int32_t  reserved[3];
+} rsg_tune_info;
+RSG_API rsg_status rsg_autotune(rsg_context *ctx, rsg_csr *A, const char *cache_path, rsg_tune_info *out);
+RSG_API rsg_status rsg_tune_get(const rsg_csr *A, rsg_tune_info *out);
 
 /* FP64 true relative residual ||b - A x|| / ||b|| (device pointers). */
 RSG_API rsg_status rsg_true_relres(rsg_context *ctx, const rsg_csr *A, const double *b, const double *x,

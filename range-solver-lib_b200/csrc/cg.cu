@@ -480,6 +480,7 @@ void set_smem(K k, size_t smem)
 
 struct Launch {
     int g_spmv64, g_spmv32, g_vec;
+    int g_dir64, g_dir32, g_upd64, g_upd32;  // the loop's kernels: autotuned shapes or the defaults
     size_t s64, s32;
 };
 
@@ -508,9 +509,9 @@ void launch_body(rsg_context *ctx, const CgArgs &a, const Launch &L, cudaGraphCo
     if (!a.mixed) {
         for (int half = 0; half < 2; half++) {
             double *po = half ? a.p1 : a.p0, *pn = half ? a.p0 : a.p1;
-            k_cg_dir<RPW><<<L.g_spmv64, kBlock, L.s64, ctx->stream>>>(M64, S64, us, a.z, po, pn, a.q, a.partials,
+            k_cg_dir<RPW><<<L.g_dir64, kBlock, L.s64, ctx->stream>>>(M64, S64, us, a.z, po, pn, a.q, a.partials,
                                                                       a.st);
-            k_cg_update<PK><<<L.g_vec, kBlock, 0, ctx->stream>>>(n, a.P.w, a.P.d, pn, a.q, a.x, a.r, a.z, a.partials,
+            k_cg_update<PK><<<L.g_upd64, kBlock, 0, ctx->stream>>>(n, a.P.w, a.P.d, pn, a.q, a.x, a.r, a.z, a.partials,
                                                                 a.st);
             k_cg_check<RPW, PK><<<L.g_spmv64, kBlock, L.s64, ctx->stream>>>(M64, S64, us, a.P.d, a.b, a.x, a.r,
                                                                             a.z, a.partials, a.st);
@@ -521,9 +522,9 @@ void launch_body(rsg_context *ctx, const CgArgs &a, const Launch &L, cudaGraphCo
         const Csr<float> M32 = view<float>(a.A, true);
         for (int half = 0; half < 2; half++) {
             float *po = half ? a.p32b : a.p32a, *pn = half ? a.p32a : a.p32b;
-            k_mx_dir<RPW><<<L.g_spmv32, kBlock, L.s32, ctx->stream>>>(M32, S32, us, a.z32, po, pn, a.q32, a.x,
+            k_mx_dir<RPW><<<L.g_dir32, kBlock, L.s32, ctx->stream>>>(M32, S32, us, a.z32, po, pn, a.q32, a.x,
                                                                       a.y32, a.partials, a.st);
-            k_mx_update<PK><<<L.g_vec, kBlock, 0, ctx->stream>>>(n, a.P.w, a.P.d32, pn, a.q32, a.y32, a.r32, a.z32,
+            k_mx_update<PK><<<L.g_upd32, kBlock, 0, ctx->stream>>>(n, a.P.w, a.P.d32, pn, a.q32, a.y32, a.r32, a.z32,
                                                                 a.partials, a.st);
             k_mx_check<RPW, PK><<<L.g_spmv64, kBlock, L.s64, ctx->stream>>>(M64, S64, us, a.P.d32, a.b, a.x,
                                                                             a.y32, a.r32, a.z32, a.partials, a.st);
@@ -551,6 +552,11 @@ rsg_status run_typed(rsg_context *ctx, const CgArgs &a, double *seconds)
     L.g_spmv64 = spmv_grid(ctx, a.A, (const void *)k_cg_dir<RPW>, L.s64, RPW);
     L.g_spmv32 = spmv_grid(ctx, a.A, (const void *)k_mx_dir<RPW>, L.s32, RPW);
     L.g_vec = std::min(grid_for(ctx, (const void *)k_cg_update<PK>, kBlock, 0, a.A->n), kMaxGrid);
+    const rsg_csr::Tune &T = a.A->tune;
+    L.g_dir64 = T.valid && T.g_dir64 > 0 ? T.g_dir64 : L.g_spmv64;
+    L.g_dir32 = T.valid && T.g_dir32 > 0 ? T.g_dir32 : L.g_spmv32;
+    L.g_upd64 = T.valid && T.g_upd64 > 0 ? T.g_upd64 : L.g_vec;
+    L.g_upd32 = T.valid && T.g_upd32 > 0 ? T.g_upd32 : L.g_vec;
 
     RSG_CHECK_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
     launch_init<RPW, PK>(ctx, a, L);

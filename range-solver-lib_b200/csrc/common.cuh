@@ -62,6 +62,16 @@ struct rsg_csr {
     float *sval32 = nullptr;
     int16_t *soff = nullptr;          // col - (row & ~31), when every offset fits
     uint32_t *scol = nullptr;         // otherwise uint32 columns
+    // launch shapes chosen by the autotuner (0 = the built-in default)
+    struct Tune {
+        bool valid = false;
+        bool from_cache = false;
+        int32_t rpw = 0;              // CSR-stream rows per warp chunk (<= the largest that fits)
+        int32_t g_dir64 = 0, g_dir32 = 0, g_upd64 = 0, g_upd32 = 0;
+        double it64 = 0, it32 = 0;    // seconds per CG iteration with these shapes
+        double it64_default = 0, it32_default = 0;
+        uint32_t candidates = 0;
+    } tune;
 };
 
 namespace rsg {

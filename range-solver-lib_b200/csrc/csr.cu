@@ -284,7 +284,7 @@ static rsg_status build_sell(rsg_context *ctx, rsg_csr *A, bool force)
 
 static rsg_status refill_sell_values(rsg_context *ctx, rsg_csr *A)
 {
-    if (!A->use_sell) return RSG_OK;
+    if (!A->sval) return RSG_OK;  // refreshed whenever built: the autotuner may switch layouts later
     const int gf = grid_for(ctx, (const void *)k_sell_fill, kBlock, 0, A->n);
     k_sell_fill<<<gf, kBlock, 0, ctx->stream>>>(A->n, A->rp, A->ci, A->val, A->off16, A->slice_ptr, A->sval,
                                                A->sval32, A->soff, A->scol, 1);

@@ -59,6 +59,7 @@ struct CgArgs {
     uint32_t check_interval;
 };
 
+rsg_status autotune_run(rsg_context *ctx, rsg_csr *A, const char *cache_path);
 rsg_status cg_run(rsg_context *ctx, const CgArgs &a, double *seconds);
 
 // ---------------- state transitions (thread 0 of the last block) ----------------

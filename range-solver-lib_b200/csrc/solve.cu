@@ -7,6 +7,8 @@
 // Afterwards the FP64 true relative residual of the returned x is recomputed
 // on the GPU and reported, and the per-iteration errors are printed / written
 // in RIterationInfo's formats (src/riterationinfo.cpp:111-193) when asked.
+#include <cstdlib>
+
 #include "gmres.cuh"
 #include "gnn.cuh"
 #include "krylov.cuh"
@@ -95,6 +97,7 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
         return set_error(ctx, RSG_ERR_UNSUPPORTED, "the learned preconditioner runs with FP64 Krylov vectors");
     const bool learned = prec_type == RSG_PREC_LEARNED;
     if (learned) c.flexible = 1;
+    if (c.autotune && !A->tune.valid) RSG_TRY(autotune_run(ctx, A, std::getenv("RSG_TUNE_CACHE")));
     if (c.precision == RSG_PRECISION_MIXED && c.stop_rule != RSG_STOP_TRUE_RELRES)
         return set_error(ctx, RSG_ERR_INVALID_ARG, "mixed precision requires stop_rule TRUE_RELRES");
     if (c.precision == RSG_PRECISION_MIXED && c.solver_type != RSG_SOLVER_CG)

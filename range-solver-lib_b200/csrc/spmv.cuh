@@ -542,12 +542,19 @@ inline Csr<float> view<float>(const rsg_csr *A, bool use_off16)
 
 // Rows per warp chosen from the longest 32-row chunk: smaller chunks keep the
 // stream phase inside kCap for wider stencils (elasticity: up to 81 per row).
-inline int pick_rpw(const rsg_csr *A)
+// Largest rows-per-warp chunk of the CSR stream whose products fit the staging buffer.
+inline int natural_rpw(const rsg_csr *A)
 {
     if (A->max_warp_nnz <= kCap) return 32;
     if (A->max_warp_nnz <= 2 * kCap) return 16;
     if (A->max_warp_nnz <= 4 * kCap) return 8;
     return 4;
+}
+// The autotuner may pick a smaller chunk (always valid: fewer rows, fewer products).
+inline int pick_rpw(const rsg_csr *A)
+{
+    const int nat = natural_rpw(A);
+    return A->tune.rpw > 0 && A->tune.rpw < nat ? A->tune.rpw : nat;
 }
 
 template <typename A>

@@ -38,7 +38,7 @@ def make_conf(solver: str | int = "cg", n_outer: int = 1000, n_inner: int = 30, 
               precision: str | int = "fp64", scale_equations: bool = True, reliable_delta: float = 1e-2,
               flexible: bool = False, use_graph: bool = True, check_interval: int = 16,
               output_frequency: int = 0, output_file: str | None = None,
-              l2_resident_f32: bool = False) -> SolverConf:
+              l2_resident_f32: bool = False, autotune: bool = False) -> SolverConf:
     c = SolverConf()
     _lib.load().rsg_conf_default(C.byref(c))
     c.solver_type = solver if isinstance(solver, int) else {"cg": SOLVER_CG, "gmres": SOLVER_GMRES}[solver]
@@ -59,6 +59,7 @@ def make_conf(solver: str | int = "cg", n_outer: int = 1000, n_inner: int = 30, 
     c.output_frequency = output_frequency
     c.output_file = output_file.encode() if output_file else None
     c.l2_resident_f32 = 1 if l2_resident_f32 else 0
+    c.autotune = 1 if autotune else 0
     return c
 
 
@@ -156,6 +157,18 @@ class Context:
         self.check(self.lib.rsg_profile_kernel(self.h, A.h, kernel, reps, 1 if flush_l2 else 0, C.byref(t)),
                    "profile_kernel")
         return t.value
+
+    def autotune(self, A: "Matrix", cache_path: str | None = None) -> dict:
+        """Pick A's layout and launch shapes by timing short solves of A (rsg_autotune)."""
+        info = _lib.TuneInfo()
+        self.check(self.lib.rsg_autotune(self.h, A.h, cache_path.encode() if cache_path else None, C.byref(info)),
+                   "autotune")
+        return info.as_dict()
+
+    def tune_info(self, A: "Matrix") -> dict:
+        info = _lib.TuneInfo()
+        self.check(self.lib.rsg_tune_get(A.h, C.byref(info)), "tune_get")
+        return info.as_dict()
 
     def true_relres(self, A: "Matrix", b_dev, x_dev) -> float:
         r = C.c_double()

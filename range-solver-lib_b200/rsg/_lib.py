@@ -54,7 +54,8 @@ class SolverConf(C.Structure):
         ("learned", C.c_void_p),
         ("learned_initial_guess", C.c_int32),
         ("l2_resident_f32", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("autotune", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 
@@ -74,6 +75,28 @@ class Stats(C.Structure):
         ("status", C.c_int32),
         ("fallbacks", C.c_uint32),
         ("reserved", C.c_uint32 * 5),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class TuneInfo(C.Structure):
+    _fields_ = [
+        ("tuned", C.c_int32),
+        ("from_cache", C.c_int32),
+        ("format", C.c_int32),
+        ("rows_per_warp", C.c_uint32),
+        ("grid_dir_fp64", C.c_uint32),
+        ("grid_dir_fp32", C.c_uint32),
+        ("grid_update_fp64", C.c_uint32),
+        ("grid_update_fp32", C.c_uint32),
+        ("seconds_iter_fp64", C.c_double),
+        ("seconds_iter_fp32", C.c_double),
+        ("seconds_iter_fp64_default", C.c_double),
+        ("seconds_iter_fp32_default", C.c_double),
+        ("candidates", C.c_uint32),
+        ("reserved", C.c_int32 * 3),
     ]
 
     def as_dict(self) -> dict:
@@ -112,6 +135,8 @@ SIGNATURES = {
     "rsg_solve": (C.c_int, [_P, _P, C.POINTER(SolverConf), C.c_int32, C.c_uint32, _P, _P, C.c_int32,
                             C.POINTER(Stats)]),
     "rsg_true_relres": (C.c_int, [_P, _P, _P, _P, _DP]),
+    "rsg_autotune": (C.c_int, [_P, _P, C.c_char_p, C.POINTER(TuneInfo)]),
+    "rsg_tune_get": (C.c_int, [_P, C.POINTER(TuneInfo)]),
     "rsg_profile_kernel": (C.c_int, [_P, _P, C.c_int32, C.c_uint32, C.c_int32, _DP]),
     "rsg_true_relres_noalloc": (C.c_int, [C.c_uint32, _P, _P, _P, _P, _P, _P, _P]),
     "rsg_batch_create": (C.c_int, [_P, C.c_uint32, _P, _P, _P, _P, _PP]),

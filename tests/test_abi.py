@@ -54,3 +54,25 @@ def test_rsg_package_fails_loudly_without_library(tmp_path, monkeypatch):
     monkeypatch.setattr(_lib, "_lib", None)
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         _lib.load()
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """The ctypes mirrors of the public structs have the C compiler's size and field offsets."""
+    structs = {"rsg_solver_conf": _lib.SolverConf, "rsg_stats": _lib.Stats, "rsg_time": _lib.Time,
+               "rsg_tune_info": _lib.TuneInfo}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "rsg.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'printf("{cname}.{f} %zu\\n", offsetof({cname}, {f}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(_lib.REPO, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    got = dict(line.rsplit(" ", 1) for line in out.splitlines() if line)
+    for cname, py in structs.items():
+        assert int(got[cname]) == C.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert int(got[f"{cname}.{f}"]) == getattr(py, f).offset, f"{cname}.{f}"
