@@ -127,6 +127,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         ev[1].synchronize()
         asm_ms.append(ev[0].elapsed_time(ev[1]))
 
+    # launch shapes of the CG loop picked by the library's autotuner (set-up, not timed)
+    tune = ctx.autotune(A) if not args.no_autotune else ctx.tune_info(A)
     conf_mixed = rsg.make_conf(n_outer=50000, stop_rule="true", rtol=RTOL, precision="mixed",
                                reliable_delta=args.delta, use_graph=not args.host_loop)
     conf_fp64 = rsg.make_conf(n_outer=50000, stop_rule="true", rtol=RTOL, precision="fp64",
@@ -220,7 +222,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         "t_mixed": t_mixed, "t_fp64": t_fp64, "st_m": st_m, "st_f": st_f, "ok": x_mixed_ok,
         "err_vs_fp64": err_vs_fp64, "kd": kd, "achieved64": achieved64, "achieved32": achieved32, "peak": peak,
         "peak_kind": peak_kind, "by64": by64, "by32": by32, "traffic": traffic, "n": n, "nnz": nnz,
-        "asm_ms": float(np.median(asm_ms)), "clocks": sampler.summary(), "e2e_s": e2e_s,
+        "asm_ms": float(np.median(asm_ms)), "clocks": sampler.summary(), "e2e_s": e2e_s, "tune": tune,
         "h2d": int(nnz * 8 + 2 * n * 8), "d2h": int(n * 8), "launches": launches(st_m, True),
         "launches_fp64": launches(st_f, False), "ctx": ctx, "A": A, "b": b, "rp": rp_h, "ci": ci_h, "val": val_h,
     }
@@ -242,6 +244,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--delta", type=float, default=1e-2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="heat100: keep the built-in launch shapes")
     ap.add_argument("--workload", default="heat100",
                     choices=["heat100", "stress", "batch256", "transient40", "learned"],
                     help="heat100 (default, the headline); stress: 64x32x32 elasticity beam; batch256: 256 "
@@ -327,7 +330,8 @@ def main():
                    "speedup_vs_plain_fp64": r["t_fp64"] / r["t_mixed"],
                    "assembly_numeric_s": r["asm_ms"] / 1e3,
                    "fp64_ms_per_iteration": r["t_fp64"] / max(st_f.iterations, 1) * 1e3,
-                   "mixed_ms_per_iteration": r["t_mixed"] / max(st_m.iterations, 1) * 1e3},
+                   "mixed_ms_per_iteration": r["t_mixed"] / max(st_m.iterations, 1) * 1e3,
+                   "autotune": r["tune"]},
         "roofline": {"bound": "hbm", "kernel": "k_mx_dir (fused FP32 CG direction + SpMV)",
                      "achieved": r["achieved32"], "peak": r["peak"], "unit": "GB/s",
                      "frac": r["achieved32"] / r["peak"], "traffic": r["traffic"],
