@@ -178,6 +178,20 @@ typedef enum {
 RSG_API rsg_status rsg_profile_kernel(rsg_context *ctx, const rsg_csr *A, int32_t kernel, uint32_t reps,
                                       int32_t flush_l2, double *seconds);
 
+/* Several right-hand sides of one matrix (replaces k RMatrixSolver::solve calls
+ * with the same A, src/rmatrixsolver.cpp:158-201, e.g. load cases or
+ * REigenValueSolver's repeated solves, src/reigenvaluesolver.cpp:119-392):
+ * FP64 CG with JACOBI or NONE, every column with its own recurrences and the
+ * RSG_STOP_TRUE_RELRES rule (conf->stop_rule must be TRUE_RELRES, precision
+ * FP64; no equation scaling is applied -- the true-residual rule does not
+ * depend on it).  One pass over the matrix per iteration serves all columns.
+ * B and X hold k columns of n values each (column j at offset j*n), X is
+ * in/out (initial guesses), host or device memory as `memory` says; 1 <= k <= 16.
+ * per_rhs (k entries) and summary (worst case over the columns) may be NULL. */
+RSG_API rsg_status rsg_solve_multi(rsg_context *ctx, rsg_csr *A, const rsg_solver_conf *conf, int32_t prec_type,
+                                   uint32_t k, const double *B, double *X, int32_t memory, rsg_stats *per_rhs,
+                                   rsg_stats *summary);
+
 /* Autotuner (no counterpart in the reference, whose loops are OpenMP).  Picks
  * A's layout (SELL-32, or the CSR stream with a rows-per-warp chunk) and the
  * grid sizes of the CG loop's two kernels per iteration (fused direction +

@@ -136,6 +136,28 @@ class Context:
         self.check(s, "solve", allow)
         return x, st
 
+    def solve_multi(self, A: "Matrix", B, X=None, conf: SolverConf | None = None, prec: int = PREC_JACOBI,
+                    allow=(OK, NOT_CONVERGED, BREAKDOWN)):
+        """k right-hand sides of one matrix (rsg_solve_multi).  B: (k, n) array, one
+        right-hand side per row (numpy, or a contiguous CUDA tensor; then X must be one
+        too and is updated in place).  Returns (X, [Stats per column], summary Stats)."""
+        conf = conf or make_conf(stop_rule="true")
+        k = int(B.shape[0])
+        per = (Stats * k)()
+        summ = Stats()
+        if _is_device(B):
+            if X is None:
+                raise ValueError("device solve_multi needs an X array")
+            s = self.lib.rsg_solve_multi(self.h, A.h, C.byref(conf), prec, k, _ptr(B), _ptr(X), MEM_DEVICE, per,
+                                         C.byref(summ))
+        else:
+            B = np.ascontiguousarray(B, np.float64)
+            X = np.zeros_like(B) if X is None else np.array(X, np.float64, copy=True)
+            s = self.lib.rsg_solve_multi(self.h, A.h, C.byref(conf), prec, k, _ptr(B), _ptr(X), MEM_HOST, per,
+                                         C.byref(summ))
+        self.check(s, "solve_multi", allow)
+        return X, list(per), summ
+
     def spmv(self, A: "Matrix", x_dev, y_dev):
         self.check(self.lib.rsg_spmv(self.h, A.h, _ptr(x_dev), _ptr(y_dev)), "spmv")
 
