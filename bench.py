@@ -63,7 +63,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
@@ -166,9 +166,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         return tot / k, stats
 
     sampler = ClockSampler(local_rank)
-    with sampler:
+    with sampler:  # clocks over both timed regions
         t_mixed, st_m = timed(conf_mixed, args.steps)
-    t_fp64, st_f = timed(conf_fp64, max(1, args.steps))
+        t_fp64, st_f = timed(conf_fp64, max(1, args.steps))
     x_mixed_ok = st_m.true_relres <= RTOL
 
     # accuracy of the mixed solution against the FP64 one (both at 1e-10)
@@ -239,7 +239,7 @@ def cpu_baseline(rp, ci, val, b, threads: int) -> dict:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--delta", type=float, default=1e-2)
