@@ -17,6 +17,8 @@
 #include "assembly_plan.h"
 #include "csr.cuh"
 
+#include <algorithm>
+#include <cstdlib>
 #include <cstring>
 
 struct rsg_assembly {
@@ -34,6 +36,7 @@ struct rsg_assembly {
     uint8_t *node_mask = nullptr;
     double *stage = nullptr;   // host inputs staged on the device
     size_t stage_cap = 0;
+    uint32_t max_row = 0;      // longest row of the pattern (the thread-local kernels take short rows)
 };
 
 namespace rsg {
@@ -67,6 +70,43 @@ __device__ __forceinline__ uint32_t node_of(const uint4 t, int k)
     return k == 0 ? t.x : k == 1 ? t.y : k == 2 ? t.z : t.w;
 }
 
+// Contribution of one (row node, adjacent tet) pair to the row: Ar[n] for the tet's
+// 4 nodes (theta scheme applied when transient) and the right-hand side part be
+// (source, transient history, Dirichlet lifting).
+__device__ __forceinline__ void heat_adj(uint32_t t, const uint32_t *__restrict__ adj_elem,
+                                         const uint8_t *__restrict__ adj_loc, const double *__restrict__ xyz,
+                                         const uint4 *__restrict__ tets, const uint32_t *__restrict__ book,
+                                         const double *__restrict__ k_e, const double *__restrict__ q_e,
+                                         const double *__restrict__ rhoc_e, const double *__restrict__ node_t,
+                                         int transient, double alpha, double dt, double (&Ar)[4], double &be)
+{
+    const uint32_t e = adj_elem[t];
+    const int m = adj_loc[t];
+    const uint4 tv = tets[e];
+    double G[4][3];
+    const double V = tet_geometry(xyz, tv, G);
+    const double k = k_e[e];
+    for (int n = 0; n < 4; n++) Ar[n] = (G[m][0] * G[n][0] + G[m][1] * G[n][1] + G[m][2] * G[n][2]) * k * V;
+    const double fe = q_e[e] * V / 4.0;
+    if (transient) {
+        const double rc = rhoc_e[e];
+        be = dt * fe;
+        for (int n = 0; n < 4; n++) {
+            const double Me = rc * V * (m == n ? 2.0 : 1.0) / 20.0;
+            const double Ke = Ar[n];
+            Ar[n] = Me + alpha * dt * Ke;
+            be += (Me - (1.0 - alpha) * dt * Ke) * node_t[node_of(tv, n)];
+        }
+    } else {
+        be = fe;
+    }
+    for (int n = 0; n < 4; n++) {
+        const uint32_t nd = node_of(tv, n);
+        if (book[nd] == RSG_EOD) be -= Ar[n] * node_t[nd];
+    }
+}
+
+// Rows accumulated in global memory (any row length).
 __global__ void __launch_bounds__(kBlock) k_asm_heat(
     uint32_t n_free, const uint32_t *__restrict__ row_node, const uint32_t *__restrict__ rp,
     const uint32_t *__restrict__ adj_ptr, const uint32_t *__restrict__ adj_elem, const uint8_t *__restrict__ adj_loc,
@@ -80,38 +120,47 @@ __global__ void __launch_bounds__(kBlock) k_asm_heat(
         for (uint32_t j = start; j < end; j++) val[j] = 0.0;
         double bs = 0.0;
         for (uint32_t t = adj_ptr[a]; t < adj_ptr[a + 1]; t++) {
-            const uint32_t e = adj_elem[t];
-            const int m = adj_loc[t];
+            double Ar[4], be;
+            heat_adj(t, adj_elem, adj_loc, xyz, tets, book, k_e, q_e, rhoc_e, node_t, transient, alpha, dt, Ar, be);
             const ushort4 off4 = adj_off[t];
             const uint16_t off[4] = {off4.x, off4.y, off4.z, off4.w};
-            const uint4 tv = tets[e];
-            double G[4][3];
-            const double V = tet_geometry(xyz, tv, G);
-            const double k = k_e[e];
-            double Ar[4];
-            for (int n = 0; n < 4; n++) Ar[n] = (G[m][0] * G[n][0] + G[m][1] * G[n][1] + G[m][2] * G[n][2]) * k * V;
-            const double fe = q_e[e] * V / 4.0;
-            double be;
-            if (transient) {
-                const double rc = rhoc_e[e];
-                be = dt * fe;
-                for (int n = 0; n < 4; n++) {
-                    const double Me = rc * V * (m == n ? 2.0 : 1.0) / 20.0;
-                    const double Ke = Ar[n];
-                    Ar[n] = Me + alpha * dt * Ke;
-                    be += (Me - (1.0 - alpha) * dt * Ke) * node_t[node_of(tv, n)];
-                }
-            } else {
-                be = fe;
-            }
-            for (int n = 0; n < 4; n++) {
-                const uint32_t nd = node_of(tv, n);
-                if (book[nd] == RSG_EOD) be -= Ar[n] * node_t[nd];
-            }
             bs += be;
             for (int n = 0; n < 4; n++)
                 if (off[n] != 0xffffu) val[start + off[n]] += Ar[n];
         }
+        b[r] = bs;
+    }
+}
+
+// One thread per row with the row accumulated in a thread-local array (rows of up to
+// kLocalRowMax entries): the same per-entry order as k_asm_heat without the
+// read-modify-write round trips through global memory.
+constexpr uint32_t kLocalRowMax = 32;
+
+__global__ void __launch_bounds__(kBlock) k_asm_heat_local(
+    uint32_t n_free, const uint32_t *__restrict__ row_node, const uint32_t *__restrict__ rp,
+    const uint32_t *__restrict__ adj_ptr, const uint32_t *__restrict__ adj_elem, const uint8_t *__restrict__ adj_loc,
+    const ushort4 *__restrict__ adj_off, const double *__restrict__ xyz, const uint4 *__restrict__ tets,
+    const uint32_t *__restrict__ book, const double *__restrict__ k_e, const double *__restrict__ q_e,
+    const double *__restrict__ rhoc_e, const double *__restrict__ node_t, int transient, double alpha, double dt,
+    double *__restrict__ val, double *__restrict__ b)
+{
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n_free; r += gridDim.x * blockDim.x) {
+        const uint32_t a = row_node[r], start = rp[r], len = rp[r + 1] - start;
+        double acc[kLocalRowMax];
+#pragma unroll
+        for (uint32_t j = 0; j < kLocalRowMax; j++) acc[j] = 0.0;
+        double bs = 0.0;
+        for (uint32_t t = adj_ptr[a]; t < adj_ptr[a + 1]; t++) {
+            double Ar[4], be;
+            heat_adj(t, adj_elem, adj_loc, xyz, tets, book, k_e, q_e, rhoc_e, node_t, transient, alpha, dt, Ar, be);
+            const ushort4 off4 = adj_off[t];
+            const uint16_t off[4] = {off4.x, off4.y, off4.z, off4.w};
+            bs += be;
+            for (int n = 0; n < 4; n++)
+                if (off[n] < kLocalRowMax) acc[off[n]] += Ar[n];
+        }
+        for (uint32_t j = 0; j < len; j++) val[start + j] = acc[j];
         b[r] = bs;
     }
 }
@@ -135,6 +184,88 @@ __device__ __forceinline__ void be_row(const double g[3], int j, double out[6])
     }
 }
 
+// Right-hand side of one traction triangle for component i (thickness 0: no stiffness).
+__device__ __forceinline__ double traction_fe(uint32_t f, int i, const double *__restrict__ xyz,
+                                              const uint32_t *__restrict__ tris, const double *__restrict__ traction,
+                                              int transient, double dt)
+{
+    const uint32_t v0 = tris[3 * size_t(f)], v1 = tris[3 * size_t(f) + 1], v2 = tris[3 * size_t(f) + 2];
+    double p[3], q[3];
+    for (int k = 0; k < 3; k++) {
+        p[k] = xyz[3 * size_t(v1) + k] - xyz[3 * size_t(v0) + k];
+        q[k] = xyz[3 * size_t(v2) + k] - xyz[3 * size_t(v0) + k];
+    }
+    const double cr[3] = {p[1] * q[2] - p[2] * q[1], p[2] * q[0] - p[0] * q[2], p[0] * q[1] - p[1] * q[0]};
+    const double area = 0.5 * sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+    const double fe = traction[3 * size_t(f) + i] * area / 3.0;
+    return transient ? dt * fe : fe;
+}
+
+// Contribution of one (row node a, component i, adjacent tet) triple: Ar[3n+j] for the
+// tet's 4 nodes x 3 components (theta scheme applied when transient) and its be.
+__device__ __forceinline__ void stress_adj(uint32_t t, int i, const uint32_t *__restrict__ adj_elem,
+                                           const uint8_t *__restrict__ adj_loc, const double *__restrict__ xyz,
+                                           const uint4 *__restrict__ tets, const uint32_t *__restrict__ book,
+                                           const double *__restrict__ e_mod, const double *__restrict__ nu,
+                                           const double *__restrict__ rho_e, const double *__restrict__ gravity,
+                                           const double *__restrict__ texp_e, const double *__restrict__ dtemp_e,
+                                           const double *__restrict__ node_u, int transient, double alpha, double dt,
+                                           double (&Ar)[12], double &be, uint4 &tv)
+{
+    const uint32_t e = adj_elem[t];
+    const int m = adj_loc[t];
+    tv = tets[e];
+    double G[4][3];
+    const double V = tet_geometry(xyz, tv, G);
+    const double E = e_mod[e], v = nu[e];
+    const double f = E / ((1.0 + v) * (1.0 - 2.0 * v));
+    double De[6][6];
+    for (int p = 0; p < 6; p++)
+        for (int q = 0; q < 6; q++) De[p][q] = 0.0;
+    De[0][0] = 1.0 - v; De[0][1] = v;       De[0][2] = v;
+    De[1][0] = v;       De[1][1] = 1.0 - v; De[1][2] = v;
+    De[2][0] = v;       De[2][1] = v;       De[2][2] = 1.0 - v;
+    De[3][3] = De[4][4] = De[5][5] = (1.0 - 2.0 * v) / 2.0;
+    for (int p = 0; p < 6; p++)
+        for (int q = 0; q < 6; q++) De[p][q] *= f;
+    double Bm[6], BD[6];
+    be_row(G[m], i, Bm);
+    for (int q = 0; q < 6; q++) {
+        double s = 0.0;
+        for (int k = 0; k < 6; k++) s += Bm[k] * De[k][q];
+        BD[q] = s;
+    }
+    for (int n = 0; n < 4; n++)
+        for (int j = 0; j < 3; j++) {
+            double Bn[6];
+            be_row(G[n], j, Bn);
+            double s = 0.0;
+            for (int k = 0; k < 6; k++) s += BD[k] * Bn[k];
+            Ar[3 * n + j] = s * V;
+        }
+    double fe = gravity[i] * rho_e[e] * V / 4.0;
+    for (int k = 0; k < 3; k++) fe += texp_e[e] * dtemp_e[e] * BD[k] * V;
+    if (transient) {
+        be = dt * fe;
+        const double mv = rho_e[e] * V;
+        for (int n = 0; n < 4; n++)
+            for (int j = 0; j < 3; j++) {
+                const double Me = (j == i) ? mv * (m == n ? 2.0 : 1.0) / 20.0 : 0.0;
+                const double Ke = Ar[3 * n + j];
+                Ar[3 * n + j] = Me + alpha * dt * Ke;
+                be += (Me - (1.0 - alpha) * dt * Ke) * node_u[3 * size_t(node_of(tv, n)) + j];
+            }
+    } else {
+        be = fe;
+    }
+    for (int n = 0; n < 4; n++) {
+        const uint32_t nd = node_of(tv, n);
+        for (int j = 0; j < 3; j++)
+            if (book[3 * size_t(nd) + j] == RSG_EOD) be -= Ar[3 * n + j] * node_u[3 * size_t(nd) + j];
+    }
+}
+
+// Rows accumulated in global memory (any row length).
 __global__ void __launch_bounds__(128) k_asm_stress(
     uint32_t n_free, const uint32_t *__restrict__ row_node, const uint8_t *__restrict__ row_comp,
     const uint32_t *__restrict__ rp, const uint32_t *__restrict__ adj_ptr, const uint32_t *__restrict__ adj_elem,
@@ -151,77 +282,16 @@ __global__ void __launch_bounds__(128) k_asm_stress(
         const int i = row_comp[r];
         for (uint32_t j = start; j < end; j++) val[j] = 0.0;
         double bs = 0.0;
-        // traction triangles (thickness 0: right-hand side only)
-        for (uint32_t t = tadj_ptr[a]; t < tadj_ptr[a + 1]; t++) {
-            const uint32_t f = tadj_tri[t];
-            const uint32_t v0 = tris[3 * size_t(f)], v1 = tris[3 * size_t(f) + 1], v2 = tris[3 * size_t(f) + 2];
-            double p[3], q[3];
-            for (int k = 0; k < 3; k++) {
-                p[k] = xyz[3 * size_t(v1) + k] - xyz[3 * size_t(v0) + k];
-                q[k] = xyz[3 * size_t(v2) + k] - xyz[3 * size_t(v0) + k];
-            }
-            const double cr[3] = {p[1] * q[2] - p[2] * q[1], p[2] * q[0] - p[0] * q[2], p[0] * q[1] - p[1] * q[0]};
-            const double area = 0.5 * sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
-            const double fe = traction[3 * size_t(f) + i] * area / 3.0;
-            bs += transient ? dt * fe : fe;
-        }
+        for (uint32_t t = tadj_ptr[a]; t < tadj_ptr[a + 1]; t++)
+            bs += traction_fe(tadj_tri[t], i, xyz, tris, traction, transient, dt);
         for (uint32_t t = adj_ptr[a]; t < adj_ptr[a + 1]; t++) {
-            const uint32_t e = adj_elem[t];
-            const int m = adj_loc[t];
+            double Ar[12], be;
+            uint4 tv;
+            stress_adj(t, i, adj_elem, adj_loc, xyz, tets, book, e_mod, nu, rho_e, gravity, texp_e, dtemp_e, node_u,
+                       transient, alpha, dt, Ar, be, tv);
+            bs += be;
             const ushort4 off4 = adj_off[t];
             const uint16_t off[4] = {off4.x, off4.y, off4.z, off4.w};
-            const uint4 tv = tets[e];
-            double G[4][3];
-            const double V = tet_geometry(xyz, tv, G);
-            const double E = e_mod[e], v = nu[e];
-            const double f = E / ((1.0 + v) * (1.0 - 2.0 * v));
-            double De[6][6];
-            for (int p = 0; p < 6; p++)
-                for (int q = 0; q < 6; q++) De[p][q] = 0.0;
-            De[0][0] = 1.0 - v; De[0][1] = v;       De[0][2] = v;
-            De[1][0] = v;       De[1][1] = 1.0 - v; De[1][2] = v;
-            De[2][0] = v;       De[2][1] = v;       De[2][2] = 1.0 - v;
-            De[3][3] = De[4][4] = De[5][5] = (1.0 - 2.0 * v) / 2.0;
-            for (int p = 0; p < 6; p++)
-                for (int q = 0; q < 6; q++) De[p][q] *= f;
-            double Bm[6], BD[6];
-            be_row(G[m], i, Bm);
-            for (int q = 0; q < 6; q++) {
-                double s = 0.0;
-                for (int k = 0; k < 6; k++) s += Bm[k] * De[k][q];
-                BD[q] = s;
-            }
-            double Ar[12];
-            for (int n = 0; n < 4; n++)
-                for (int j = 0; j < 3; j++) {
-                    double Bn[6];
-                    be_row(G[n], j, Bn);
-                    double s = 0.0;
-                    for (int k = 0; k < 6; k++) s += BD[k] * Bn[k];
-                    Ar[3 * n + j] = s * V;
-                }
-            double fe = gravity[i] * rho_e[e] * V / 4.0;
-            for (int k = 0; k < 3; k++) fe += texp_e[e] * dtemp_e[e] * BD[k] * V;
-            double be;
-            if (transient) {
-                be = dt * fe;
-                const double mv = rho_e[e] * V;
-                for (int n = 0; n < 4; n++)
-                    for (int j = 0; j < 3; j++) {
-                        const double Me = (j == i) ? mv * (m == n ? 2.0 : 1.0) / 20.0 : 0.0;
-                        const double Ke = Ar[3 * n + j];
-                        Ar[3 * n + j] = Me + alpha * dt * Ke;
-                        be += (Me - (1.0 - alpha) * dt * Ke) * node_u[3 * size_t(node_of(tv, n)) + j];
-                    }
-            } else {
-                be = fe;
-            }
-            for (int n = 0; n < 4; n++) {
-                const uint32_t nd = node_of(tv, n);
-                for (int j = 0; j < 3; j++)
-                    if (book[3 * size_t(nd) + j] == RSG_EOD) be -= Ar[3 * n + j] * node_u[3 * size_t(nd) + j];
-            }
-            bs += be;
             for (int n = 0; n < 4; n++) {
                 if (off[n] == 0xffffu) continue;
                 const uint8_t mask = node_mask[node_of(tv, n)];
@@ -232,6 +302,60 @@ __global__ void __launch_bounds__(128) k_asm_stress(
         }
         b[r] = bs;
     }
+}
+
+// One thread per row with the row accumulated in a thread-local array (rows of up to
+// kLocalStressRowMax entries), as k_asm_heat_local.
+constexpr uint32_t kLocalStressRowMax = 96;
+
+__global__ void __launch_bounds__(128) k_asm_stress_local(
+    uint32_t n_free, const uint32_t *__restrict__ row_node, const uint8_t *__restrict__ row_comp,
+    const uint32_t *__restrict__ rp, const uint32_t *__restrict__ adj_ptr, const uint32_t *__restrict__ adj_elem,
+    const uint8_t *__restrict__ adj_loc, const ushort4 *__restrict__ adj_off, const uint32_t *__restrict__ tadj_ptr,
+    const uint32_t *__restrict__ tadj_tri, const uint8_t *__restrict__ node_mask, const double *__restrict__ xyz,
+    const uint4 *__restrict__ tets, const uint32_t *__restrict__ tris, const uint32_t *__restrict__ book,
+    const double *__restrict__ e_mod, const double *__restrict__ nu, const double *__restrict__ rho_e,
+    const double *__restrict__ gravity, const double *__restrict__ texp_e, const double *__restrict__ dtemp_e,
+    const double *__restrict__ traction, const double *__restrict__ node_u, int transient, double alpha, double dt,
+    double *__restrict__ val, double *__restrict__ b)
+{
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n_free; r += gridDim.x * blockDim.x) {
+        const uint32_t a = row_node[r], start = rp[r], len = rp[r + 1] - start;
+        const int i = row_comp[r];
+        double acc[kLocalStressRowMax];
+        for (uint32_t j = 0; j < len; j++) acc[j] = 0.0;
+        double bs = 0.0;
+        for (uint32_t t = tadj_ptr[a]; t < tadj_ptr[a + 1]; t++)
+            bs += traction_fe(tadj_tri[t], i, xyz, tris, traction, transient, dt);
+        for (uint32_t t = adj_ptr[a]; t < adj_ptr[a + 1]; t++) {
+            double Ar[12], be;
+            uint4 tv;
+            stress_adj(t, i, adj_elem, adj_loc, xyz, tets, book, e_mod, nu, rho_e, gravity, texp_e, dtemp_e, node_u,
+                       transient, alpha, dt, Ar, be, tv);
+            bs += be;
+            const ushort4 off4 = adj_off[t];
+            const uint16_t off[4] = {off4.x, off4.y, off4.z, off4.w};
+            for (int n = 0; n < 4; n++) {
+                if (off[n] == 0xffffu) continue;
+                const uint8_t mask = node_mask[node_of(tv, n)];
+                uint32_t rank = 0;
+                for (int j = 0; j < 3; j++)
+                    if (mask & (1u << j)) {
+                        const uint32_t pos = off[n] + rank++;
+                        if (pos < kLocalStressRowMax) acc[pos] += Ar[3 * n + j];
+                    }
+            }
+        }
+        for (uint32_t j = 0; j < len; j++) val[start + j] = acc[j];
+        b[r] = bs;
+    }
+}
+
+// RSG_ASM_ROW_THREADS=1 selects the kernels that accumulate in global memory (tests compare the two)
+bool row_threads_forced()
+{
+    const char *v = std::getenv("RSG_ASM_ROW_THREADS");
+    return v && v[0] == '1';
 }
 
 template <typename T>
@@ -273,6 +397,7 @@ rsg_status create_plan(rsg_context *ctx, uint32_t n_nodes, const double *xyz, ui
     p->dofs = dofs;
     p->n_free = n_free;
     p->nnz = H.ci.size();
+    for (size_t r = 0; r + 1 < H.rp.size(); r++) p->max_row = std::max(p->max_row, H.rp[r + 1] - H.rp[r]);
     rsg_status s = RSG_OK;
     auto chk = [&](rsg_status r) {
         if (s == RSG_OK) s = r;
@@ -412,13 +537,14 @@ rsg_status rsg_assemble_heat(rsg_context *ctx, rsg_assembly *p, const double *k_
     const double *d[4];
     RSG_TRY(stage_inputs(ctx, p, memory, {p->n_tets, p->n_tets, p->n_tets, p->n_nodes},
                          {k_e, q_e, transient ? rhoc_e : nullptr, node_t}, d));
-    const int grid = std::min(grid_for(ctx, (const void *)k_asm_heat, kBlock, 0, p->n_free), kMaxGrid * 4);
     const double alpha = time ? time->alpha : 1.0, dt = time ? time->dt : 0.0;
+    auto kern = p->max_row <= kLocalRowMax && !row_threads_forced() ? k_asm_heat_local : k_asm_heat;
+    const int grid = std::min(grid_for(ctx, (const void *)kern, kBlock, 0, p->n_free), kMaxGrid * 4);
     return assemble_into(ctx, p, A, [&](double *val) {
-        k_asm_heat<<<grid, kBlock, 0, ctx->stream>>>(p->n_free, p->row_node, p->rp, p->adj_ptr, p->adj_elem,
-                                                    p->adj_loc, reinterpret_cast<const ushort4 *>(p->adj_off), p->xyz,
-                                                    reinterpret_cast<const uint4 *>(p->tets), p->book, d[0], d[1],
-                                                    d[2], d[3], transient ? 1 : 0, alpha, dt, val, b_device);
+        kern<<<grid, kBlock, 0, ctx->stream>>>(p->n_free, p->row_node, p->rp, p->adj_ptr, p->adj_elem, p->adj_loc,
+                                              reinterpret_cast<const ushort4 *>(p->adj_off), p->xyz,
+                                              reinterpret_cast<const uint4 *>(p->tets), p->book, d[0], d[1], d[2],
+                                              d[3], transient ? 1 : 0, alpha, dt, val, b_device);
     });
 }
 
@@ -437,10 +563,12 @@ rsg_status rsg_assemble_stress(rsg_context *ctx, rsg_assembly *p, const double *
                          {p->n_tets, p->n_tets, p->n_tets, 3, p->n_tets, p->n_tets, size_t(p->n_tris) * 3,
                           size_t(p->n_nodes) * 3},
                          {e_mod, nu, rho_e, gravity, texp_e, dtemp_e, p->n_tris ? traction : nullptr, node_u}, d));
-    const int grid = std::min(grid_for(ctx, (const void *)k_asm_stress, 128, 0, p->n_free), kMaxGrid * 4);
     const double alpha = time ? time->alpha : 1.0, dt = time ? time->dt : 0.0;
+    auto kern = p->max_row <= kLocalStressRowMax && !row_threads_forced() ? k_asm_stress_local : k_asm_stress;
+    const int block = 128;
+    const int grid = std::min(grid_for(ctx, (const void *)kern, block, 0, p->n_free), kMaxGrid * 4);
     return assemble_into(ctx, p, A, [&](double *val) {
-        k_asm_stress<<<grid, 128, 0, ctx->stream>>>(
+        kern<<<grid, block, 0, ctx->stream>>>(
             p->n_free, p->row_node, p->row_comp, p->rp, p->adj_ptr, p->adj_elem, p->adj_loc,
             reinterpret_cast<const ushort4 *>(p->adj_off), p->tadj_ptr, p->tadj_tri, p->node_mask, p->xyz,
             reinterpret_cast<const uint4 *>(p->tets), p->tris, p->book, d[0], d[1], d[2], d[3], d[4], d[5], d[6],

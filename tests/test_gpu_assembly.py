@@ -133,3 +133,30 @@ def test_assembly_rejects_bad_inputs(ctx):
     p3.mesh.tets[5, 2] = p3.mesh.n_nodes + 3
     with pytest.raises(rsg.RsgError):
         rsg.Assembly.heat(ctx, p3)
+
+
+@pytest.mark.parametrize("kind", ["heat", "heat_transient", "stress", "stress_transient"])
+def test_warp_and_thread_row_kernels_bitwise_equal(ctx, torch_cuda, monkeypatch, kind):
+    """The warp-per-row kernels apply every element contribution to an entry in the
+    same order as the one-thread-per-row kernels: identical bits."""
+    torch = torch_cuda
+    if kind.startswith("heat"):
+        p = W.heat_cube(8, sigma=1.2, seed=6, source="random", transient=kind.endswith("transient"), dt=1e-3)
+        if p.transient:
+            p.node_t = W.uniform(6, 9, p.mesh.n_nodes)
+    else:
+        p = W.stress_beam(6, 4, 4)
+        if kind.endswith("transient"):
+            p.transient, p.dt, p.alpha = True, 1e-4, 0.5
+            p.node_u = W.uniform(2, 3, 3 * p.mesh.n_nodes) * 1e-4
+    out = []
+    for forced in ("0", "1"):
+        monkeypatch.setenv("RSG_ASM_ROW_THREADS", forced)
+        asm = rsg.Assembly.heat(ctx, p) if kind.startswith("heat") else rsg.Assembly.stress(ctx, p)
+        b = torch.empty(asm.n_free, dtype=torch.float64, device="cuda")
+        M = asm.assemble(p, b)
+        ctx.sync()
+        out.append((M.to_host()[2], b.cpu().numpy()))
+        asm.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
