@@ -189,7 +189,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     # dominant kernels, timed live (HBM-bound: L2 flushed before each launch)
     kd = {}
     for name, kid in (("cg_dir_fp64", 0), ("cg_dir_mixed", 1), ("cg_update_fp64", 2),
-                      ("cg_update_mixed", 3)):
+                      ("cg_update_mixed", 3), ("spmv_fp64", 4), ("spmv_fp32", 5)):
         kd[name] = {"cold_s": ctx.profile_kernel(A, kid, reps=10, flush_l2=True),
                     "warm_s": ctx.profile_kernel(A, kid, reps=20, flush_l2=False)}
     nnz = A.nnz
@@ -230,7 +230,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     out = {
         "t_mixed": t_mixed, "t_fp64": t_fp64, "st_m": st_m, "st_f": st_f, "ok": x_mixed_ok,
         "err_vs_fp64": err_vs_fp64, "kd": kd, "achieved64": achieved64, "achieved32": achieved32, "peak": peak,
-        "peak_kind": peak_kind, "by64": by64, "by32": by32, "traffic": traffic, "n": n, "nnz": nnz,
+        "peak_kind": peak_kind, "by64": by64, "by32": by32,
+        "by_spmv64": nnz * 10 + 4 * (n + 1) + 2 * n * 8, "traffic": traffic, "n": n, "nnz": nnz,
         "asm_ms": float(np.median(asm_ms[1:])), "asm_host_ms": float(np.median(asm_host_ms[1:])),
         "clocks": sampler.summary(), "e2e_s": e2e_s, "tune": tune,
         "h2d": int(nnz * 8 + 2 * n * 8), "d2h": int(n * 8), "launches": launches(st_m, True),
@@ -354,6 +355,12 @@ def main():
                           "achieved": r["achieved64"], "peak": r["peak"], "unit": "GB/s",
                           "frac": r["achieved64"] / r["peak"], "algorithmic_bytes": r["by64"],
                           "avg_launch_s": kd["cg_dir_fp64"]["cold_s"], "peak_source": r["peak_kind"]},
+        "roofline_spmv_fp64": {"bound": "hbm", "kernel": "k_spmv (FP64 SpMV alone, rsg_spmv)",
+                               "achieved": r["by_spmv64"] / kd["spmv_fp64"]["cold_s"] / 1e9, "peak": r["peak"],
+                               "unit": "GB/s", "frac": r["by_spmv64"] / kd["spmv_fp64"]["cold_s"] / 1e9 / r["peak"],
+                               "algorithmic_bytes": r["by_spmv64"], "avg_launch_s": kd["spmv_fp64"]["cold_s"],
+                               "peak_source": r["peak_kind"],
+                               "bytes": "nnz*(8+2) + 4*(n+1) + 2*n*8 (values, 16-bit offsets, row pointers, x, y)"},
         "kernels": kd,
         "e2e": {"value": r["e2e_s"], "unit": UNIT, "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"],
                 "api": "rsg_csr_update_values + rsg_solve with pinned host buffers"},
