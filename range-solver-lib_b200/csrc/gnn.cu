@@ -293,71 +293,216 @@ __global__ void k_gnn_output_bwd(uint32_t n, const double *__restrict__ gz, cons
     }
 }
 
-// Layer backward, part 1 (thread per row): recompute z from h_prev, m and W (FP32);
-// dz = g * [z > 0]; gx = dz W^T -> g_prev = g + gx[:H], gm = gx[H:].
-// The weight gradient is accumulated by k_gnn_layer_wgrad.
-__global__ void k_gnn_layer_bwd(uint32_t n, const float *__restrict__ hp, const float *__restrict__ m,
-                                const float *__restrict__ W, const float *__restrict__ bias,
-                                const float *__restrict__ g, float *__restrict__ dz_out, float *__restrict__ gprev,
-                                float *__restrict__ gm)
+// Layer backward, part 1, for tiles of 64 rows with W and W^T in shared memory and
+// register tiles (4 rows x 4 columns of z, 4 rows x 8 features of gx per thread):
+// recompute z = [h_prev, m] W + b (FP32, k in order), dz = g * [z > 0], gx = dz W^T
+// (c in order) -> g_prev = g + gx[:H], gm = gx[H:].  Every output is accumulated in the
+// order of a sequential loop over its row.  The weight gradient is k_gnn_layer_wgrad.
+constexpr int kBwdRows = 64;
+constexpr int kXsStride = K2 + 4;
+constexpr int kDsStride = H + 4;
+constexpr size_t kBwdSmem =
+    sizeof(float) * (size_t(K2) * H + size_t(H) * K2 + size_t(kBwdRows) * kXsStride + size_t(kBwdRows) * kDsStride + H);
+
+__global__ void __launch_bounds__(256) k_gnn_layer_bwd(uint32_t n, const float *__restrict__ hp,
+                                                       const float *__restrict__ m, const float *__restrict__ W,
+                                                       const float *__restrict__ bias, const float *__restrict__ g,
+                                                       float *__restrict__ dz_out, float *__restrict__ gprev,
+                                                       float *__restrict__ gm)
 {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        float dz[H];
-        for (int c = 0; c < H; c++) {
-            float z = bias[c];
-            for (int k = 0; k < H; k++) z = fmaf(hp[size_t(i) * H + k], W[size_t(k) * H + c], z);
-            for (int k = 0; k < H; k++) z = fmaf(m[size_t(i) * H + k], W[size_t(H + k) * H + c], z);
-            dz[c] = z > 0.f ? g[size_t(i) * H + c] : 0.f;
-            dz_out[size_t(i) * H + c] = dz[c];
+    extern __shared__ __align__(16) float sb[];
+    float *Ws = sb;                               // [K2][H]
+    float *WT = Ws + K2 * H;                      // [H][K2]
+    float *Xs = WT + H * K2;                      // [kBwdRows][kXsStride]
+    float *Ds = Xs + kBwdRows * kXsStride;        // [kBwdRows][kDsStride]
+    float *bs = Ds + kBwdRows * kDsStride;        // [H]
+    const int tid = threadIdx.x;
+    for (int e = tid; e < K2 * H; e += blockDim.x) {
+        const float w = W[e];
+        Ws[e] = w;
+        WT[(e % H) * K2 + e / H] = w;
+    }
+    for (int c = tid; c < H; c += blockDim.x) bs[c] = bias[c];
+    // phase A: rows 4*ra .. +3, columns 4*ca .. +3 (16 x 16 threads)
+    const int ra = tid >> 4, ca = tid & 15;
+    // phase B: rows 4*rb .. +3, features 8*kb .. +7 (16 x 16 threads)
+    const int rb = tid >> 4, kb = tid & 15;
+    const uint32_t tiles = (n + kBwdRows - 1) / kBwdRows;
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const uint32_t r0 = tile * kBwdRows;
+        __syncthreads();
+        for (int e = tid; e < kBwdRows * K2; e += blockDim.x) {
+            const int rr = e / K2, k = e % K2;
+            const uint32_t row = r0 + rr;
+            Xs[rr * kXsStride + k] = row < n ? (k < H ? hp[size_t(row) * H + k] : m[size_t(row) * H + k - H]) : 0.f;
         }
-        for (int k = 0; k < K2; k++) {
-            float v = 0.f;
-            for (int c = 0; c < H; c++) v = fmaf(dz[c], W[size_t(k) * H + c], v);
-            if (k < H) gprev[size_t(i) * H + k] = g[size_t(i) * H + k] + v;
-            else gm[size_t(i) * H + (k - H)] = v;
+        __syncthreads();
+        {
+            float z[4][4];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) z[i][j] = bs[4 * ca + j];
+            for (int k = 0; k < K2; k++) {
+                const float4 w = *reinterpret_cast<const float4 *>(&Ws[k * H + 4 * ca]);
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const float x = Xs[(4 * ra + i) * kXsStride + k];
+                    z[i][0] = fmaf(x, w.x, z[i][0]);
+                    z[i][1] = fmaf(x, w.y, z[i][1]);
+                    z[i][2] = fmaf(x, w.z, z[i][2]);
+                    z[i][3] = fmaf(x, w.w, z[i][3]);
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const uint32_t row = r0 + 4 * ra + i;
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int c = 4 * ca + j;
+                    const float d = (row < n && z[i][j] > 0.f) ? g[size_t(row) * H + c] : 0.f;
+                    Ds[(4 * ra + i) * kDsStride + c] = d;
+                    if (row < n) dz_out[size_t(row) * H + c] = d;
+                }
+            }
+        }
+        __syncthreads();
+        {
+            float gx[4][8];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 8; j++) gx[i][j] = 0.f;
+            for (int c = 0; c < H; c++) {
+                const float4 w0 = *reinterpret_cast<const float4 *>(&WT[c * K2 + 8 * kb]);
+                const float4 w1 = *reinterpret_cast<const float4 *>(&WT[c * K2 + 8 * kb + 4]);
+                const float w[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const float d = Ds[(4 * rb + i) * kDsStride + c];
+#pragma unroll
+                    for (int j = 0; j < 8; j++) gx[i][j] = fmaf(d, w[j], gx[i][j]);
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const uint32_t row = r0 + 4 * rb + i;
+                if (row >= n) continue;
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    const int k = 8 * kb + j;
+                    if (k < H) gprev[size_t(row) * H + k] = g[size_t(row) * H + k] + gx[i][j];
+                    else gm[size_t(row) * H + (k - H)] = gx[i][j];
+                }
+            }
         }
     }
 }
 
-// dW = X^T dz and db = sum dz, per block over a row range (fixed order), X = [h_prev, m].
-// Block computes all (k, c) entries with one thread per entry group.
-__global__ void k_gnn_layer_wgrad(uint32_t n, const float *__restrict__ hp, const float *__restrict__ m,
-                                  const float *__restrict__ dz, float *__restrict__ blk)
+// dW = X^T dz and db = sum dz over a contiguous row range per block (rows in order),
+// X = [h_prev, m]: register tiles of 4 features x 8 columns per thread, rows staged in
+// shared memory 32 at a time.
+constexpr int kWgRows = 32;
+__global__ void __launch_bounds__(256) k_gnn_layer_wgrad(uint32_t n, const float *__restrict__ hp,
+                                                         const float *__restrict__ m, const float *__restrict__ dz,
+                                                         float *__restrict__ blk)
 {
+    __shared__ float Xs[kWgRows][K2 + 4];
+    __shared__ float Ds[kWgRows][H + 4];
     const uint32_t rows_per = (n + gridDim.x - 1) / gridDim.x;
     const uint32_t r0 = min(n, blockIdx.x * rows_per), r1 = min(n, r0 + rows_per);
+    const int tid = threadIdx.x, kb = tid >> 3, cb = tid & 7;  // features 4kb..4kb+3, columns 8cb..8cb+7
+    float acc[4][8];
+    float accb[8];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] = 0.f;
+#pragma unroll
+    for (int j = 0; j < 8; j++) accb[j] = 0.f;
+    for (uint32_t t0 = r0; t0 < r1; t0 += kWgRows) {
+        const uint32_t cnt = min(uint32_t(kWgRows), r1 - t0);
+        __syncthreads();
+        for (int e = tid; e < kWgRows * K2; e += blockDim.x) {
+            const int rr = e / K2, k = e % K2;
+            const uint32_t row = t0 + rr;
+            Xs[rr][k] = uint32_t(rr) < cnt ? (k < H ? hp[size_t(row) * H + k] : m[size_t(row) * H + k - H]) : 0.f;
+        }
+        for (int e = tid; e < kWgRows * H; e += blockDim.x) {
+            const int rr = e / H, c = e % H;
+            Ds[rr][c] = uint32_t(rr) < cnt ? dz[size_t(t0 + rr) * H + c] : 0.f;
+        }
+        __syncthreads();
+        for (uint32_t rr = 0; rr < cnt; rr++) {
+            float x[4], d[8];
+#pragma unroll
+            for (int i = 0; i < 4; i++) x[i] = Xs[rr][4 * kb + i];
+#pragma unroll
+            for (int j = 0; j < 8; j++) d[j] = Ds[rr][8 * cb + j];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 8; j++) acc[i][j] = fmaf(x[i], d[j], acc[i][j]);
+            if (kb == 0)
+#pragma unroll
+                for (int j = 0; j < 8; j++) accb[j] += d[j];
+        }
+    }
     const int total = K2 * H + H;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-        float v = 0.f;
-        if (e < K2 * H) {
-            const int k = e / H, c = e % H;
-            const float *src = k < H ? hp : m;
-            const int kk = k < H ? k : k - H;
-            for (uint32_t i = r0; i < r1; i++) v = fmaf(src[size_t(i) * H + kk], dz[size_t(i) * H + c], v);
-        } else {
-            const int c = e - K2 * H;
-            for (uint32_t i = r0; i < r1; i++) v += dz[size_t(i) * H + c];
-        }
-        blk[size_t(blockIdx.x) * total + e] = v;
-    }
+    float *out = blk + size_t(blockIdx.x) * total;
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) out[(4 * kb + i) * H + 8 * cb + j] = acc[i][j];
+    if (kb == 0)
+#pragma unroll
+        for (int j = 0; j < 8; j++) out[K2 * H + 8 * cb + j] = accb[j];
 }
 
-// input layer: dpre = gh0 * [pre0 > 0]; dW_in = f^T dpre, db_in = sum dpre (per block)
-__global__ void k_gnn_input_wgrad(uint32_t n, const float *__restrict__ feat, const float *__restrict__ pre0,
-                                  const float *__restrict__ gh0, float *__restrict__ blk)
+// input layer: dpre = gh0 * [pre0 > 0]; dW_in = f^T dpre, db_in = sum dpre over a
+// contiguous row range per block (rows in order); thread = (feature k, column pair).
+__global__ void __launch_bounds__(256) k_gnn_input_wgrad(uint32_t n, const float *__restrict__ feat,
+                                                         const float *__restrict__ pre0,
+                                                         const float *__restrict__ gh0, float *__restrict__ blk)
 {
+    __shared__ float Fs[32][F];
+    __shared__ float Ps[32][H + 2];
     const uint32_t rows_per = (n + gridDim.x - 1) / gridDim.x;
     const uint32_t r0 = min(n, blockIdx.x * rows_per), r1 = min(n, r0 + rows_per);
-    const int total = F * H + H;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-        float v = 0.f;
-        const int c = e < F * H ? e % H : e - F * H;
-        const int k = e < F * H ? e / H : -1;
-        for (uint32_t i = r0; i < r1; i++) {
-            const float dp = pre0[size_t(i) * H + c] > 0.f ? gh0[size_t(i) * H + c] : 0.f;
-            v = k >= 0 ? fmaf(feat[size_t(i) * F + k], dp, v) : v + dp;
+    const int tid = threadIdx.x, k = tid >> 5, c0 = 2 * (tid & 31);
+    float a0 = 0.f, a1 = 0.f, b0 = 0.f, b1 = 0.f;
+    for (uint32_t t0 = r0; t0 < r1; t0 += 32) {
+        const uint32_t cnt = min(32u, r1 - t0);
+        __syncthreads();
+        for (int e = tid; e < 32 * F; e += blockDim.x)
+            Fs[e / F][e % F] = uint32_t(e / F) < cnt ? feat[size_t(t0 + e / F) * F + e % F] : 0.f;
+        for (int e = tid; e < 32 * H; e += blockDim.x) {
+            const int rr = e / H, c = e % H;
+            float dp = 0.f;
+            if (uint32_t(rr) < cnt) {
+                const size_t idx = size_t(t0 + rr) * H + c;
+                dp = pre0[idx] > 0.f ? gh0[idx] : 0.f;
+            }
+            Ps[rr][c] = dp;
         }
-        blk[size_t(blockIdx.x) * total + e] = v;
+        __syncthreads();
+        for (uint32_t rr = 0; rr < cnt; rr++) {
+            const float f = Fs[rr][k];
+            const float d0 = Ps[rr][c0], d1 = Ps[rr][c0 + 1];
+            a0 = fmaf(f, d0, a0);
+            a1 = fmaf(f, d1, a1);
+            if (k == 0) {
+                b0 += d0;
+                b1 += d1;
+            }
+        }
+    }
+    float *out = blk + size_t(blockIdx.x) * (F * H + H);
+    out[k * H + c0] = a0;
+    out[k * H + c0 + 1] = a1;
+    if (k == 0) {
+        out[F * H + c0] = b0;
+        out[F * H + c0 + 1] = b1;
     }
 }
 
@@ -366,6 +511,7 @@ __global__ void k_gnn_sum_blocks(const float *__restrict__ blk, int nblk, int co
 {
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < count; e += gridDim.x * blockDim.x) {
         float v = 0.f;
+#pragma unroll 16
         for (int b = 0; b < nblk; b++) v += blk[size_t(b) * count + e];
         grad[e] = v;
     }
@@ -579,11 +725,18 @@ rsg_status gnn_loss_grad(rsg_context *ctx, rsg_learned *G, const rsg_csr *A, con
     k_gnn_output_bwd<<<gi, kBlock, 0, sm>>>(n, gz, G->h[L], G->params, L, G->s, rms, G->gh, G->blk);
     k_gnn_sum_blocks<<<1, 128, 0, sm>>>(G->blk, gi, H + 1, G->grad + off_wout(L));
     const int gs = std::min(grid_for(ctx, (const void *)k_gnn_spmm, kBlock, 0, (long long)n * 32), kMaxGrid);
-    const int gb = std::min(grid_for(ctx, (const void *)k_gnn_layer_bwd, 128, 0, n), kMaxGrid);
+    static bool bwd_attr = false;
+    if (!bwd_attr) {
+        RSG_CHECK_CUDA(ctx, cudaFuncSetAttribute(k_gnn_layer_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 int(kBwdSmem)));
+        bwd_attr = true;
+    }
+    const int gb = std::min(grid_for(ctx, (const void *)k_gnn_layer_bwd, 256, kBwdSmem,
+                                     (long long)(n + kBwdRows - 1) / kBwdRows * 256), kMaxGrid);
     float *g = G->gh, *g2 = G->gh2;
     for (int l = L - 1; l >= 0; l--) {
         const float *W = G->params + off_layer(l), *b = W + size_t(K2) * H;
-        k_gnn_layer_bwd<<<gb, 128, 0, sm>>>(n, G->h[l], G->m[l], W, b, g, G->dz, g2, G->gm);
+        k_gnn_layer_bwd<<<gb, 256, kBwdSmem, sm>>>(n, G->h[l], G->m[l], W, b, g, G->dz, g2, G->gm);
         k_gnn_layer_wgrad<<<nb, kBlock, 0, sm>>>(n, G->h[l], G->m[l], G->dz, G->blk);
         k_gnn_sum_blocks<<<32, kBlock, 0, sm>>>(G->blk, nb, K2 * H + H, G->grad + off_layer(l));
         // g_prev += W^T-graph gm (the graph weights are symmetric): reuse the SpMM into gm, then add
