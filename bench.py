@@ -198,8 +198,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     by32 = spmv_bytes(n, nnz, 4, 2, 4)
     achieved64 = by64 / kd["cg_dir_fp64"]["cold_s"] / 1e9
     achieved32 = by32 / kd["cg_dir_mixed"]["cold_s"] / 1e9
-    # DRAM bytes (read + write) of one k_mx_dir launch on this workload, from the ncu capture
-    # summarised in profiles/k_mx_dir_heat_lognormal_100.md
+    # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_mx_dir launch on this
+    # workload, from an ncu --set full capture of the register-capped kernel
     traffic = 113.65e6 if N_HEX == 100 else None
 
     # launches per solve: setup (norm, 2 scalings, Jacobi, FP32 copy, init residual + z, fold,
@@ -465,6 +465,7 @@ def run_other(args, rank, world, local_rank, threads):
             rhs.append(bb.cpu().numpy())
             asm.close()
         batch = rsg.Batch(ctx, systems)
+        tune = batch.autotune()  # launch shapes of the batch loop (set-up, not timed)
         b_all = torch.from_numpy(np.concatenate(rhs)).cuda()
         x_all = torch.zeros_like(b_all)
         res = {}
@@ -487,6 +488,7 @@ def run_other(args, rank, world, local_rank, threads):
                      "value": 256 * world / t_best, "unit": "systems/s", "ms_per_step": t_best * 1e3,
                      "higher_is_better": True, "dtype": "f64 / f32-inner",
                      "config": {"workload": "batch256_heat_8to60", "rows": batch.rows, "nnz": batch.nnz,
+                                "autotune": tune,
                                 "parallelism": f"independent shards x{world}", "variants": res}})
         if world == 1 and not args.no_cpu_baseline:
             t0 = time.perf_counter()

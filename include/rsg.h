@@ -111,6 +111,7 @@ typedef struct {
 typedef struct rsg_context rsg_context;
 typedef struct rsg_csr rsg_csr;
 typedef struct rsg_learned rsg_learned;
+typedef struct rsg_batch rsg_batch;
 
 /* ---- context ---- */
 RSG_API rsg_status rsg_context_create(int device, rsg_context **out);
@@ -214,6 +215,9 @@ typedef struct rsg_tune_info {
 } rsg_tune_info;
 RSG_API rsg_status rsg_autotune(rsg_context *ctx, rsg_csr *A, const char *cache_path, rsg_tune_info *out);
 RSG_API rsg_status rsg_tune_get(const rsg_csr *A, rsg_tune_info *out);
+/* The same for a batch (rsg_batch_create): the grid of the batch loop's slice kernels
+ * per precision, by timing 32-iteration batch solves (grid_dir_* = grid_update_*). */
+RSG_API rsg_status rsg_batch_autotune(rsg_context *ctx, rsg_batch *batch, rsg_tune_info *out);
 
 /* FP64 true relative residual ||b - A x|| / ||b|| (device pointers). */
 RSG_API rsg_status rsg_true_relres(rsg_context *ctx, const rsg_csr *A, const double *b, const double *x,
@@ -248,7 +252,6 @@ RSG_API rsg_status rsg_true_relres_noalloc(uint32_t n_rows, const uint32_t *row_
  * or JACOBI) to the FP64 true relative residual conf->rtol (stop_rule must be
  * RSG_STOP_TRUE_RELRES), in FP64 or mixed precision, with its own iteration
  * count and convergence; the whole batch is one device-driven loop. */
-typedef struct rsg_batch rsg_batch;
 RSG_API rsg_status rsg_batch_create(rsg_context *ctx, uint32_t n_systems, const uint32_t *sys_row_begin,
                                     const uint32_t *row_ptr, const uint32_t *col_idx, const double *values,
                                     rsg_batch **out);

@@ -29,6 +29,11 @@ struct rsg_batch {
     uint32_t *d_slice_sys = nullptr;       // system of each slice
     uint32_t *d_sys_slice = nullptr;       // first slice of each system (n_sys + 1)
     uint32_t *d_user2pad = nullptr;        // padded row of each user row
+    // grid of the slice kernels picked by rsg_batch_autotune (0 = the built-in default)
+    int32_t g64 = 0, g32 = 0;
+    double it64 = 0, it32 = 0, it64_default = 0, it32_default = 0;
+    uint32_t tune_candidates = 0;
+    bool tuned = false;
 };
 
 namespace rsg {
@@ -673,7 +678,11 @@ rsg_status rsg_batch_solve(rsg_context *ctx, rsg_batch *B, const rsg_solver_conf
     const BView V{B->d_slice_sys, B->d_sys_slice, nsl, ns};
     const Sell<double> M64 = sell_view<double>(B->A);
     const Sell<float> M32 = sell_view<float>(B->A);
-    const int g = std::min(grid_for(ctx, (const void *)bk_dir<double, false>, kBlock, 0, (long long)nsl * 32), kMaxGrid);
+    const int g_tuned = B->tuned ? (mixed ? B->g32 : B->g64) : 0;
+    const int g = g_tuned > 0
+                      ? g_tuned
+                      : std::min(grid_for(ctx, (const void *)bk_dir<double, false>, kBlock, 0, (long long)nsl * 32),
+                                 kMaxGrid);
     cudaEventRecord(ctx->ev[0], sm);
     const int gr = int(ns);  // reduce kernels: one block per listed system
     bk_init_res<<<g, kBlock, 0, sm>>>(M64, V, L_all, bp, xp, r, part, S);
@@ -805,6 +814,99 @@ rsg_status rsg_batch_solve(rsg_context *ctx, rsg_batch *B, const rsg_solver_conf
     if (summary) *summary = sum;
     if (worst == RSG_ERR_TIMEOUT) return set_error(ctx, RSG_ERR_TIMEOUT, "batch solve hit its hard limit");
     return worst;
+}
+
+
+// Batch autotuner (no reference counterpart): the grid of the slice kernels (direction,
+// update, check) is chosen per precision by timing short fixed-length batch solves
+// (every system runs kTuneIters iterations: rtol 0 is never met) for the built-in
+// default and multiples of the SM count; three solves per candidate, median.
+rsg_status rsg_batch_autotune(rsg_context *ctx, rsg_batch *B, rsg_tune_info *out)
+{
+    if (!ctx || !B) return set_error(ctx, RSG_ERR_INVALID_ARG, "batch_autotune: bad arguments");
+    RSG_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
+    constexpr uint32_t kTuneIters = 32;
+    constexpr int kReps = 3;
+    const size_t nu = B->user_rows;
+    double *b = nullptr, *x = nullptr;
+    if (cudaMalloc(&b, nu * sizeof(double)) != cudaSuccess || cudaMalloc(&x, nu * sizeof(double)) != cudaSuccess) {
+        cudaFree(b);
+        return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "batch_autotune: vectors");
+    }
+    std::vector<double> ones(nu, 1.0);
+    rsg_status s = RSG_OK;
+    if (cudaMemcpy(b, ones.data(), nu * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+        s = set_error(ctx, RSG_ERR_CUDA, "batch_autotune: upload");
+    rsg_solver_conf c;
+    rsg_conf_default(&c);
+    c.n_outer = kTuneIters;
+    c.stop_rule = RSG_STOP_TRUE_RELRES;
+    c.rtol = 0.0;
+    const uint32_t nsl = B->A->n_slices;
+    std::vector<int> cand = {0};
+    for (int k : {1, 2, 3, 4, 6, 8}) cand.push_back(k * ctx->num_sms);
+    cand.push_back(int(std::min<long long>(((long long)nsl * 32 + kBlock - 1) / kBlock, (long long)kMaxGrid)));
+    B->tuned = true;
+    uint32_t count = 0;
+    for (int32_t prec : {RSG_PRECISION_FP64, RSG_PRECISION_MIXED}) {
+        if (s != RSG_OK) break;
+        c.precision = prec;
+        int32_t &gsel = prec == RSG_PRECISION_FP64 ? B->g64 : B->g32;
+        double best = 1e300, def = 0;
+        int bestg = 0;
+        for (int gc : cand) {
+            gsel = gc;
+            double t[kReps];
+            for (int r = 0; r < kReps && s == RSG_OK; r++) {
+                if (cudaMemsetAsync(x, 0, nu * sizeof(double), ctx->stream) != cudaSuccess) {
+                    s = set_error(ctx, RSG_ERR_CUDA, "batch_autotune: memset");
+                    break;
+                }
+                rsg_stats sum;
+                const rsg_status rs = rsg_batch_solve(ctx, B, &c, RSG_PREC_JACOBI, b, x, RSG_MEM_DEVICE, nullptr, &sum);
+                if (rs < 0) {
+                    s = rs;
+                    break;
+                }
+                t[r] = sum.seconds_solve / double(std::max<uint32_t>(sum.iterations, 1));
+                count++;
+            }
+            if (s != RSG_OK) break;
+            std::sort(t, t + kReps);
+            const double tm = t[kReps / 2];
+            if (gc == 0) def = tm;
+            if (tm < best) {
+                best = tm;
+                bestg = gc;
+            }
+        }
+        gsel = bestg;
+        (prec == RSG_PRECISION_FP64 ? B->it64 : B->it32) = best;
+        (prec == RSG_PRECISION_FP64 ? B->it64_default : B->it32_default) = def;
+    }
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(b);
+    cudaFree(x);
+    if (s != RSG_OK) {
+        B->tuned = false;
+        B->g64 = B->g32 = 0;
+        return s;
+    }
+    B->tune_candidates = count;
+    if (out) {
+        std::memset(out, 0, sizeof(*out));
+        out->tuned = 1;
+        out->format = 1;
+        out->rows_per_warp = 32;
+        out->grid_dir_fp64 = out->grid_update_fp64 = uint32_t(B->g64);
+        out->grid_dir_fp32 = out->grid_update_fp32 = uint32_t(B->g32);
+        out->seconds_iter_fp64 = B->it64;
+        out->seconds_iter_fp32 = B->it32;
+        out->seconds_iter_fp64_default = B->it64_default;
+        out->seconds_iter_fp32_default = B->it32_default;
+        out->candidates = count;
+    }
+    return RSG_OK;
 }
 
 }  // extern "C"

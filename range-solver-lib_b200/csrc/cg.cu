@@ -34,6 +34,8 @@ namespace rsg {
 // Resident blocks per SM the FP32 direction kernel is compiled for: capping its registers
 // (48 -> 32) gives the latency-bound gathers more warps; measured 31.1 -> 28.8 us per launch
 // in the solve loop at 1M rows.  The FP64 kernel measured slower with a cap and keeps 48.
+// (Software-pipelining the next slice's matrix loads needed 64-80 registers with spills
+// and measured 38.9-44.5 us.)
 constexpr int kDirMinBlocks32 = 8;
 
 // ---------------- FP64 kernels ----------------

@@ -12,9 +12,9 @@
 // The learned step is abandoned for Jacobi (the reference's preconditioner)
 // as soon as it fails: z not a descent direction (r^T z <= 0), p^T A p <= 0,
 // or no new lowest residual norm for kStall iterations.  Stopping: FP64 true
-// relative residual, recomputed before stopping.  The loop is host-driven (one
-// short synchronisation per iteration): the network's application is a
-// sequence of launches that costs far more than that synchronisation.
+// relative residual, recomputed before stopping.  The loop is host-driven with
+// one short synchronisation per iteration: the scalars (coefficients, alpha)
+// stay on the device, and the host reads back only ||r||^2 and the failure flags.
 #include "gnn.cuh"
 #include "krylov.cuh"
 
@@ -25,15 +25,23 @@ constexpr uint32_t kStall = 25;
 constexpr int kDotsNV = kFcgMaxDirs + 1;
 
 struct DirCoef {
-    double c[kFcgMaxDirs];
     int slot[kFcgMaxDirs];
     int cnt;
+};
+
+// device-side scalars of the loop (inside the solver's small scratch block)
+struct FcgDev {
+    double coef[kFcgMaxDirs];     // z^T A p_j / p_j^T A p_j of the stored directions
+    double pq_slot[kFcgMaxDirs + 1];  // p^T A p of the direction held in each slot
+    double alpha;
+    double rn2;                   // ||r||^2 after the update   } read back together
+    double flags;                 // 1: not a descent direction, 2: p^T A p <= 0 }
 };
 
 // out[0] = r^T z, out[1 + j] = z^T Q[slot j] (j < cnt)
 __global__ void k_fcg_mdots(uint32_t n, const double *__restrict__ r, const double *__restrict__ z,
                             const double *__restrict__ Q, DirCoef dc, double *partials, unsigned int *ticket,
-                            double *out)
+                            FcgDev *dev, int check_descent)
 {
     __shared__ double sh[32 * kDotsNV];
     double acc[kDotsNV];
@@ -47,8 +55,10 @@ __global__ void k_fcg_mdots(uint32_t n, const double *__restrict__ r, const doub
             if (j < dc.cnt) acc[1 + j] += zi * Q[size_t(dc.slot[j]) * n + i];
     }
     double tot[kDotsNV];
-    if (grid_sum<kDotsNV>(acc, partials, ticket, sh, tot) && threadIdx.x == 0)
-        for (int k = 0; k < kDotsNV; k++) out[k] = tot[k];
+    if (grid_sum<kDotsNV>(acc, partials, ticket, sh, tot) && threadIdx.x == 0) {
+        dev->flags = (check_descent && !(tot[0] > 0.0)) ? 1.0 : 0.0;
+        for (int j = 0; j < dc.cnt; j++) dev->coef[j] = tot[1 + j] / dev->pq_slot[dc.slot[j]];
+    }
 }
 
 __global__ void k_fcg_jacobi(uint32_t n, const double *__restrict__ d, const double *__restrict__ r,
@@ -60,20 +70,24 @@ __global__ void k_fcg_jacobi(uint32_t n, const double *__restrict__ d, const dou
 
 // p = z - sum_j c_j P[slot j]
 __global__ void k_fcg_newdir(uint32_t n, const double *__restrict__ z, const double *__restrict__ P, DirCoef dc,
-                             double *__restrict__ p)
+                             const FcgDev *__restrict__ dev, double *__restrict__ p)
 {
+    double c[kFcgMaxDirs];
+#pragma unroll
+    for (int j = 0; j < kFcgMaxDirs; j++) c[j] = j < dc.cnt ? dev->coef[j] : 0.0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double v = z[i];
 #pragma unroll
         for (int j = 0; j < kFcgMaxDirs; j++)
-            if (j < dc.cnt) v = fma(-dc.c[j], P[size_t(dc.slot[j]) * n + i], v);
+            if (j < dc.cnt) v = fma(-c[j], P[size_t(dc.slot[j]) * n + i], v);
         p[i] = v;
     }
 }
 
 // p^T q and p^T r
 __global__ void k_fcg_pdots(uint32_t n, const double *__restrict__ p, const double *__restrict__ q,
-                            const double *__restrict__ r, double *partials, unsigned int *ticket, double *out)
+                            const double *__restrict__ r, double *partials, unsigned int *ticket, FcgDev *dev,
+                            int slot)
 {
     __shared__ double sh[64];
     double acc[2] = {0.0, 0.0};
@@ -83,16 +97,24 @@ __global__ void k_fcg_pdots(uint32_t n, const double *__restrict__ p, const doub
     }
     double tot[2];
     if (grid_sum<2>(acc, partials, ticket, sh, tot) && threadIdx.x == 0) {
-        out[0] = tot[0];
-        out[1] = tot[1];
+        const double pq = tot[0];
+        if (!(pq > 0.0) || !isfinite(pq)) {
+            dev->flags = dev->flags + 2.0;
+        } else {
+            dev->alpha = tot[1] / pq;
+            dev->pq_slot[slot] = pq;
+        }
     }
 }
 
-__global__ void k_fcg_update(uint32_t n, double alpha, const double *__restrict__ p, const double *__restrict__ q,
+// x += alpha p, r -= alpha q, ||r||^2 -- skipped when this iteration failed
+__global__ void k_fcg_update(uint32_t n, const double *__restrict__ p, const double *__restrict__ q,
                              double *__restrict__ x, double *__restrict__ r, double *partials, unsigned int *ticket,
-                             double *out)
+                             FcgDev *dev)
 {
     __shared__ double sh[32];
+    if (dev->flags != 0.0) return;
+    const double alpha = dev->alpha;
     double acc[1] = {0.0};
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         x[i] = fma(alpha, p[i], x[i]);
@@ -101,7 +123,7 @@ __global__ void k_fcg_update(uint32_t n, double alpha, const double *__restrict_
         acc[0] += ri * ri;
     }
     double tot[1];
-    if (grid_sum<1>(acc, partials, ticket, sh, tot) && threadIdx.x == 0) out[0] = tot[0];
+    if (grid_sum<1>(acc, partials, ticket, sh, tot) && threadIdx.x == 0) dev->rn2 = tot[0];
 }
 
 __global__ void k_fcg_resid(uint32_t n, const double *__restrict__ b, const double *__restrict__ ax,
@@ -129,7 +151,7 @@ uint32_t fcg_dirs(uint32_t n_inner) { return std::max<uint32_t>(1, std::min<uint
 size_t fcg_workspace_bytes(uint32_t n, uint32_t m)
 {
     return 2 * arena_bytes(n, sizeof(double)) + 2 * arena_bytes(size_t(m + 1) * n, sizeof(double)) +
-           arena_bytes(64, 8);
+           arena_bytes(64, 8) + arena_bytes(sizeof(FcgDev), 1);
 }
 
 rsg_status fcg_run(rsg_context *ctx, const rsg_csr *A, rsg_learned *G, const double *d, const double *b, double *x,
@@ -141,11 +163,13 @@ rsg_status fcg_run(rsg_context *ctx, const rsg_csr *A, rsg_learned *G, const dou
     double *r = arena_take<double>(ctx, n), *z = arena_take<double>(ctx, n);
     double *P = arena_take<double>(ctx, size_t(slots) * n), *Q = arena_take<double>(ctx, size_t(slots) * n);
     double *sc = arena_take<double>(ctx, 64);
-    if (!sc) return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "fcg workspace");
+    FcgDev *dev = reinterpret_cast<FcgDev *>(arena_take<char>(ctx, sizeof(FcgDev)));
+    if (!sc || !dev) return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "fcg workspace");
     unsigned int *ticket = reinterpret_cast<unsigned int *>(sc + 32);
     double *out = sc;
     double *h = ctx->pinned;
     RSG_CHECK_CUDA(ctx, cudaMemsetAsync(sc, 0, 64 * 8, sm));
+    RSG_CHECK_CUDA(ctx, cudaMemsetAsync(dev, 0, sizeof(FcgDev), sm));
     const int g = std::min(grid_for(ctx, (const void *)k_fcg_update, kBlock, 0, n), kMaxGrid);
     auto fetch = [&](int count) -> rsg_status {
         RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(h, out, count * sizeof(double), cudaMemcpyDeviceToHost, sm));
@@ -163,9 +187,8 @@ rsg_status fcg_run(rsg_context *ctx, const rsg_csr *A, rsg_learned *G, const dou
     bool learned = G != nullptr;
     double best = rn;
     uint32_t since_best = 0;
-    // stored directions, oldest first: slot index and p^T A p
+    // stored directions, oldest first (their p^T A p stay on the device)
     int ring_slot[kFcgMaxDirs];
-    double ring_pq[kFcgMaxDirs];
     uint32_t cnt = 0, next_slot = 0;
     res->iterations = 0;
     res->fallbacks = 0;
@@ -184,25 +207,20 @@ rsg_status fcg_run(rsg_context *ctx, const rsg_csr *A, rsg_learned *G, const dou
         DirCoef dc;
         dc.cnt = int(cnt);
         for (uint32_t j = 0; j < cnt; j++) dc.slot[j] = ring_slot[j];
-        if (learned) RSG_TRY(gnn_forward(ctx, G, A, r, z, nullptr, false, true));
-        else k_fcg_jacobi<<<g, kBlock, 0, sm>>>(n, d, r, z);
-        k_fcg_mdots<<<g, kBlock, 0, sm>>>(n, r, z, Q, dc, partials, ticket, out);
-        RSG_TRY(fetch(1 + int(cnt)));
-        if (learned && !(h[0] > 0.0)) {  // not a descent direction
-            fall_back();
-            dc.cnt = 0;
-            k_fcg_jacobi<<<g, kBlock, 0, sm>>>(n, d, r, z);
-        }
-        for (int j = 0; j < dc.cnt; j++) dc.c[j] = h[1 + j] / ring_pq[j];
         const int slot = int(next_slot);
         double *p = P + size_t(slot) * n, *q = Q + size_t(slot) * n;
-        k_fcg_newdir<<<g, kBlock, 0, sm>>>(n, z, P, dc, p);
+        if (learned) RSG_TRY(gnn_forward(ctx, G, A, r, z, nullptr, false, true));
+        else k_fcg_jacobi<<<g, kBlock, 0, sm>>>(n, d, r, z);
+        k_fcg_mdots<<<g, kBlock, 0, sm>>>(n, r, z, Q, dc, partials, ticket, dev, learned ? 1 : 0);
+        k_fcg_newdir<<<g, kBlock, 0, sm>>>(n, z, P, dc, dev, p);
         RSG_TRY(spmv64(ctx, A, p, q, true));
-        k_fcg_pdots<<<g, kBlock, 0, sm>>>(n, p, q, r, partials, ticket, out);
-        RSG_TRY(fetch(2));
-        const double pq = h[0], pr = h[1];
-        if (!(pq > 0.0) || !std::isfinite(pq)) {
-            if (learned) {
+        k_fcg_pdots<<<g, kBlock, 0, sm>>>(n, p, q, r, partials, ticket, dev, slot);
+        k_fcg_update<<<g, kBlock, 0, sm>>>(n, p, q, x, r, partials, ticket, dev);
+        RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(h, &dev->rn2, 2 * sizeof(double), cudaMemcpyDeviceToHost, sm));
+        RSG_CHECK_CUDA(ctx, cudaStreamSynchronize(sm));
+        const int flags = int(h[1]);
+        if (flags != 0) {  // the iteration was not applied
+            if (learned) {  // not a descent direction, or p^T A p <= 0: hand over to Jacobi
                 fall_back();
                 continue;
             }
@@ -211,14 +229,10 @@ rsg_status fcg_run(rsg_context *ctx, const rsg_csr *A, rsg_learned *G, const dou
         }
         // keep p_k: drop the oldest stored direction when m are held
         if (cnt == m) {
-            for (uint32_t j = 1; j < cnt; j++) {
-                ring_slot[j - 1] = ring_slot[j];
-                ring_pq[j - 1] = ring_pq[j];
-            }
+            for (uint32_t j = 1; j < cnt; j++) ring_slot[j - 1] = ring_slot[j];
             cnt--;
         }
         ring_slot[cnt] = slot;
-        ring_pq[cnt] = pq;
         cnt++;
         // the next free slot is the one no stored direction uses
         for (uint32_t s = 0; s < slots; s++) {
@@ -229,9 +243,6 @@ rsg_status fcg_run(rsg_context *ctx, const rsg_csr *A, rsg_learned *G, const dou
                 break;
             }
         }
-        const double alpha = pr / pq;
-        k_fcg_update<<<g, kBlock, 0, sm>>>(n, alpha, p, q, x, r, partials, ticket, out);
-        RSG_TRY(fetch(1));
         rn = std::sqrt(h[0]);
         res->iterations = it + 1;
         if (!std::isfinite(rn)) {

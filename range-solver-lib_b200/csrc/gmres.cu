@@ -12,6 +12,11 @@
 // Z is stored, so a variable preconditioner (flexible GMRES) needs no change.
 // Each cycle is one captured CUDA graph; the host polls the device state once
 // per cycle.
+// Mixed precision: the Arnoldi vectors V, Z, w and the matrix of the inner
+// steps are FP32 (dot products accumulated in FP64), while the true residual at
+// every restart (FP64 matrix), the Hessenberg matrix, the Givens rotations, the
+// least-squares solve and the solution update x += Z y stay FP64 -- restarted
+// GMRES as iterative refinement with an FP32 inner cycle.
 #include "gmres.cuh"
 #include "gnn.cuh"
 
@@ -85,52 +90,54 @@ __global__ void __launch_bounds__(kBlock) k_gm_residual(Csr<double> M, Sell<doub
     }
 }
 
-// v_k = src / s (0 if s == 0), z_k = P v_k.  src = ro for k = 0, else w.
-template <int PK>
-__global__ void __launch_bounds__(kBlock) k_gm_vz(uint32_t n, uint32_t w_, const double *__restrict__ d,
-                                                  const double *__restrict__ ro, const double *__restrict__ wv,
-                                                  const double *__restrict__ wnorm, double *__restrict__ V,
-                                                  double *__restrict__ Z, const GmresState *st, uint32_t k)
+// v_k = src / s (0 if s == 0), z_k = P v_k.  src = ro for k = 0, else w.  T: vector type
+// of the Arnoldi vectors (double, or float in mixed precision); D: preconditioner values.
+template <int PK, typename T, typename D>
+__global__ void __launch_bounds__(kBlock) k_gm_vz(uint32_t n, uint32_t w_, const D *__restrict__ d,
+                                                  const double *__restrict__ ro, const T *__restrict__ wv,
+                                                  const double *__restrict__ wnorm, T *__restrict__ V,
+                                                  T *__restrict__ Z, const GmresState *st, uint32_t k)
 {
     if (st->done || st->inner_done) return;
     const double s = (k == 0) ? st->beta : wnorm[k];
-    const double *src = (k == 0) ? ro : wv;
-    double *v = V + size_t(k) * n, *z = Z + size_t(k) * n;
+    T *v = V + size_t(k) * n, *z = Z + size_t(k) * n;
     const uint32_t G = PK == 2 ? w_ : 1, ng = n / G;
     for (uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x; gi < ng; gi += gridDim.x * blockDim.x) {
-        double vl[kMaxBlock];
+        T vl[kMaxBlock];
         for (uint32_t j = 0; j < G; j++) {
             const size_t i = size_t(gi) * G + j;
-            vl[j] = (s == 0.0) ? 0.0 : src[i] / s;
+            const double src = (k == 0) ? ro[i] : double(wv[i]);
+            vl[j] = T((s == 0.0) ? 0.0 : src / s);
             v[i] = vl[j];
         }
         if (PK == 0) z[gi] = vl[0];
-        else if (PK == 1) z[gi] = d[gi] * vl[0];
+        else if (PK == 1) z[gi] = T(d[gi]) * vl[0];
         else
             for (uint32_t j = 0; j < G; j++) {
-                const double *row = d + (size_t(gi) * G + j) * G;
-                double acc = 0.0;
-                for (uint32_t l = 0; l < G; l++) acc += row[l] * vl[l];
+                const D *row = d + (size_t(gi) * G + j) * G;
+                T acc = T(0);
+                for (uint32_t l = 0; l < G; l++) acc += T(row[l]) * vl[l];
                 z[size_t(gi) * G + j] = acc;
             }
     }
 }
 
-template <int RPW>
-__global__ void __launch_bounds__(kBlock) k_gm_spmv(Csr<double> M, Sell<double> S, int use_sell, const double *__restrict__ Z,
-                                                    double *__restrict__ wv, GmresState *st, uint32_t k)
+template <int RPW, typename T>
+__global__ void __launch_bounds__(kBlock) k_gm_spmv(Csr<T> M, Sell<T> S, int use_sell, const T *__restrict__ Z,
+                                                    T *__restrict__ wv, GmresState *st, uint32_t k)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (st->done || st->inner_done) return;
-    const double *z = Z + size_t(k) * M.n;
+    const T *z = Z + size_t(k) * M.n;
     auto gx = [&](uint32_t c) { return z[c]; };
-    auto epi = [&](uint32_t row, double v) { wv[row] = v; };
-    for_rows_any<double, RPW>(M, S, use_sell != 0, gx, epi, smem_raw, &st->ticket[7], true);
+    auto epi = [&](uint32_t row, T v) { wv[row] = v; };
+    for_rows_any<T, RPW>(M, S, use_sell != 0, gx, epi, smem_raw, &st->ticket[7], true);
 }
 
 // h_i = v_i^T w for i <= k: blockIdx.y = i.  Last block of the 2-D grid stores column k of H.
-__global__ void __launch_bounds__(kBlock) k_gm_dots(uint32_t n, const double *__restrict__ V,
-                                                    const double *__restrict__ wv, double *__restrict__ H,
+template <typename T>
+__global__ void __launch_bounds__(kBlock) k_gm_dots(uint32_t n, const T *__restrict__ V,
+                                                    const T *__restrict__ wv, double *__restrict__ H,
                                                     double *__restrict__ hv, double *partials, GmresState *st,
                                                     uint32_t k)
 {
@@ -138,9 +145,10 @@ __global__ void __launch_bounds__(kBlock) k_gm_dots(uint32_t n, const double *__
     __shared__ bool is_last;
     if (st->done || st->inner_done) return;
     if (blockIdx.y > k) return;
-    const double *v = V + size_t(blockIdx.y) * n;
+    const T *v = V + size_t(blockIdx.y) * n;
     double acc[1] = {0.0};
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) acc[0] += wv[i] * v[i];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        acc[0] += double(wv[i]) * double(v[i]);
     block_sum<1>(acc, sh);
     const unsigned int nblocks = gridDim.x * (k + 1);
     if (threadIdx.x == 0) {
@@ -165,8 +173,9 @@ __global__ void __launch_bounds__(kBlock) k_gm_dots(uint32_t n, const double *__
 }
 
 // w -= sum_i hv_i v_i; ||w|| -> Givens update of column k (last block).
-__global__ void __launch_bounds__(kBlock) k_gm_correct(uint32_t n, const double *__restrict__ V,
-                                                       double *__restrict__ wv, const double *__restrict__ hv_g,
+template <typename T>
+__global__ void __launch_bounds__(kBlock) k_gm_correct(uint32_t n, const T *__restrict__ V,
+                                                       T *__restrict__ wv, const double *__restrict__ hv_g,
                                                        double *__restrict__ H, double *__restrict__ cs,
                                                        double *__restrict__ sn, double *__restrict__ g,
                                                        double *__restrict__ wnorm, double *partials, GmresState *st,
@@ -179,10 +188,11 @@ __global__ void __launch_bounds__(kBlock) k_gm_correct(uint32_t n, const double 
     __syncthreads();
     double acc[1] = {0.0};
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-        double value = wv[j];
-        for (uint32_t i = 0; i <= k; i++) value -= hv[i] * V[size_t(i) * n + j];
-        wv[j] = value;
-        acc[0] += value * value;
+        double value = double(wv[j]);
+        for (uint32_t i = 0; i <= k; i++) value -= hv[i] * double(V[size_t(i) * n + j]);
+        const T stored = T(value);
+        wv[j] = stored;
+        acc[0] += double(stored) * double(stored);
     }
     double tot[1];
     if (grid_sum<1>(acc, partials, &st->ticket[2], sh, tot) && threadIdx.x == 0) {
@@ -229,7 +239,8 @@ __global__ void k_gm_backsub(double *__restrict__ H, double *__restrict__ g, dou
     }
 }
 
-__global__ void __launch_bounds__(kBlock) k_gm_update(uint32_t n, const double *__restrict__ Z,
+template <typename T>
+__global__ void __launch_bounds__(kBlock) k_gm_update(uint32_t n, const T *__restrict__ Z,
                                                       const double *__restrict__ y_g, double *__restrict__ x,
                                                       GmresState *st)
 {
@@ -240,7 +251,7 @@ __global__ void __launch_bounds__(kBlock) k_gm_update(uint32_t n, const double *
     __syncthreads();
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double xi = x[i];
-        for (uint32_t j = 0; j < len; j++) xi += Z[size_t(j) * n + i] * y[j];
+        for (uint32_t j = 0; j < len; j++) xi += double(Z[size_t(j) * n + i]) * y[j];
         x[i] = xi;
     }
 }
@@ -256,19 +267,26 @@ __global__ void k_gm_cycle_end(GmresState *st)
     }
 }
 
-size_t gmres_workspace_bytes(uint32_t n, uint32_t m, bool)
+size_t gmres_workspace_bytes(uint32_t n, uint32_t m, bool mixed, uint32_t w)
 {
     const size_t vn = arena_bytes(n, sizeof(double));
-    return size_t(m + 1) * vn * 2 + 2 * vn + arena_bytes(size_t(m + 1) * m, sizeof(double)) +
-           6 * arena_bytes(m + 2, sizeof(double));
+    const size_t vt = mixed ? arena_bytes(size_t(m + 1) * n, sizeof(float)) : arena_bytes(size_t(m + 1) * n, 8);
+    return 2 * vt + (mixed ? arena_bytes(n, sizeof(float)) : vn) + vn + arena_bytes(size_t(m + 1) * m, sizeof(double)) +
+           6 * arena_bytes(m + 2, sizeof(double)) + (mixed ? arena_bytes(size_t(n) * w, sizeof(float)) : 0);
 }
 
 rsg_status gmres_carve(rsg_context *ctx, GmresArgs &a, uint32_t n, uint32_t m)
 {
     if (m > kMaxRestart) return set_error(ctx, RSG_ERR_UNSUPPORTED, "GMRES restart length %u > %u", m, kMaxRestart);
-    a.V = arena_take<double>(ctx, size_t(m + 1) * n);
-    a.Z = arena_take<double>(ctx, size_t(m + 1) * n);
-    a.w = arena_take<double>(ctx, n);
+    if (a.mixed) {
+        a.V32 = arena_take<float>(ctx, size_t(m + 1) * n);
+        a.Z32 = arena_take<float>(ctx, size_t(m + 1) * n);
+        a.w32 = arena_take<float>(ctx, n);
+    } else {
+        a.V = arena_take<double>(ctx, size_t(m + 1) * n);
+        a.Z = arena_take<double>(ctx, size_t(m + 1) * n);
+        a.w = arena_take<double>(ctx, n);
+    }
     a.ro = arena_take<double>(ctx, n);
     a.H = arena_take<double>(ctx, size_t(m + 1) * m);
     a.cs = arena_take<double>(ctx, m + 2);
@@ -292,15 +310,22 @@ rsg_status run_typed(rsg_context *ctx, const GmresArgs &a, double *seconds)
     const Csr<double> M = view<double>(a.A, true);
     const size_t s64 = a.A->use_sell ? 0 : tma_smem<double>();
     cudaFuncSetAttribute(k_gm_residual<RPW>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tma_smem<double>()));
-    cudaFuncSetAttribute(k_gm_spmv<RPW>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tma_smem<double>()));
+    cudaFuncSetAttribute(k_gm_spmv<RPW, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         int(tma_smem<double>()));
+    cudaFuncSetAttribute(k_gm_spmv<RPW, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tma_smem<float>()));
     const Sell<double> S = sell_view<double>(a.A);
+    const Csr<float> M32 = view<float>(a.A, true);
+    const Sell<float> S32 = sell_view<float>(a.A);
+    const size_t s32 = a.A->use_sell ? 0 : tma_smem<float>();
     const int us = a.A->use_sell;
     const long long ct = (long long)n * 32 / RPW;
     (void)ct;
-    const int g_sp = spmv_grid(ctx, a.A, (const void *)k_gm_spmv<RPW>, s64, RPW);
+    const int g_sp = spmv_grid(ctx, a.A, (const void *)k_gm_spmv<RPW, double>, s64, RPW);
+    const int g_sp32 = spmv_grid(ctx, a.A, (const void *)k_gm_spmv<RPW, float>, s32, RPW);
     const int g_res = spmv_grid(ctx, a.A, (const void *)k_gm_residual<RPW>, s64, RPW);
-    const int g_vec = std::min(grid_for(ctx, (const void *)k_gm_correct, kBlock, 0, n), kMaxGrid);
-    const int g_dot = std::min(std::min(grid_for(ctx, (const void *)k_gm_dots, kBlock, 0, n), 512), kMaxGrid);
+    const int g_vec = std::min(grid_for(ctx, (const void *)k_gm_correct<double>, kBlock, 0, n), kMaxGrid);
+    const int g_dot =
+        std::min(std::min(grid_for(ctx, (const void *)k_gm_dots<double>, kBlock, 0, n), 512), kMaxGrid);
 
     // One captured graph per cycle; with the learned preconditioner a second graph
     // (Jacobi z_k) is captured as the fallback.
@@ -310,7 +335,18 @@ rsg_status run_typed(rsg_context *ctx, const GmresArgs &a, double *seconds)
         k_gm_residual<RPW><<<g_res, kBlock, s64, ctx->stream>>>(M, S, us, a.b, a.x, a.ro, a.H, a.g, a.partials,
                                                                a.st);
         for (uint32_t k = 0; k < m; k++) {
-            k_gm_vz<PK><<<g_vec, kBlock, 0, ctx->stream>>>(n, a.P.w, a.P.d, a.ro, a.w, a.wnorm, a.V, a.Z, a.st, k);
+            if (a.mixed) {  // FP32 Arnoldi step
+                k_gm_vz<PK, float, float><<<g_vec, kBlock, 0, ctx->stream>>>(n, a.P.w, a.P.d32, a.ro, a.w32,
+                                                                             a.wnorm, a.V32, a.Z32, a.st, k);
+                k_gm_spmv<RPW, float><<<g_sp32, kBlock, s32, ctx->stream>>>(M32, S32, us, a.Z32, a.w32, a.st, k);
+                k_gm_dots<float><<<dim3(g_dot, k + 1), kBlock, 0, ctx->stream>>>(n, a.V32, a.w32, a.H, a.hv,
+                                                                               a.partials, a.st, k);
+                k_gm_correct<float><<<g_vec, kBlock, 0, ctx->stream>>>(n, a.V32, a.w32, a.hv, a.H, a.cs, a.sn, a.g,
+                                                                      a.wnorm, a.partials, a.st, k);
+                continue;
+            }
+            k_gm_vz<PK, double, double><<<g_vec, kBlock, 0, ctx->stream>>>(n, a.P.w, a.P.d, a.ro, a.w, a.wnorm,
+                                                                           a.V, a.Z, a.st, k);
             if (G) {  // flexible GMRES: z_k = M(v_k) from the network (Z is stored, src/rmatrixsolver.cpp:446)
                 const rsg_status gs =
                     gnn_forward(ctx, G, a.A, a.V + size_t(k) * n, a.Z + size_t(k) * n, nullptr, false, true);
@@ -321,13 +357,15 @@ rsg_status run_typed(rsg_context *ctx, const GmresArgs &a, double *seconds)
                     return gs;
                 }
             }
-            k_gm_spmv<RPW><<<g_sp, kBlock, s64, ctx->stream>>>(M, S, us, a.Z, a.w, a.st, k);
-            k_gm_dots<<<dim3(g_dot, k + 1), kBlock, 0, ctx->stream>>>(n, a.V, a.w, a.H, a.hv, a.partials, a.st, k);
-            k_gm_correct<<<g_vec, kBlock, 0, ctx->stream>>>(n, a.V, a.w, a.hv, a.H, a.cs, a.sn, a.g, a.wnorm,
-                                                           a.partials, a.st, k);
+            k_gm_spmv<RPW, double><<<g_sp, kBlock, s64, ctx->stream>>>(M, S, us, a.Z, a.w, a.st, k);
+            k_gm_dots<double><<<dim3(g_dot, k + 1), kBlock, 0, ctx->stream>>>(n, a.V, a.w, a.H, a.hv, a.partials,
+                                                                            a.st, k);
+            k_gm_correct<double><<<g_vec, kBlock, 0, ctx->stream>>>(n, a.V, a.w, a.hv, a.H, a.cs, a.sn, a.g,
+                                                                   a.wnorm, a.partials, a.st, k);
         }
         k_gm_backsub<<<1, 32, 0, ctx->stream>>>(a.H, a.g, a.y, a.st);
-        k_gm_update<<<g_vec, kBlock, 0, ctx->stream>>>(n, a.Z, a.y, a.x, a.st);
+        if (a.mixed) k_gm_update<float><<<g_vec, kBlock, 0, ctx->stream>>>(n, a.Z32, a.y, a.x, a.st);
+        else k_gm_update<double><<<g_vec, kBlock, 0, ctx->stream>>>(n, a.Z, a.y, a.x, a.st);
         k_gm_cycle_end<<<1, 32, 0, ctx->stream>>>(a.st);
         cudaError_t e = cudaStreamEndCapture(ctx->stream, graph);
         if (e != cudaSuccess) return set_error(ctx, RSG_ERR_CUDA, "GMRES capture: %s", cudaGetErrorString(e));

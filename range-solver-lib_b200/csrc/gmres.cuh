@@ -33,14 +33,16 @@ struct GmresArgs {
     GmresState *st;
     uint32_t m;
     bool flexible;
-    // carved buffers
+    // carved buffers (V, Z, w in FP64, or V32, Z32, w32 in mixed precision)
     double *V, *Z, *w, *ro, *H, *cs, *sn, *g, *y, *hv, *wnorm;
+    bool mixed = false;
+    float *V32 = nullptr, *Z32 = nullptr, *w32 = nullptr;
     uint32_t st_max_outer;
     rsg_learned *G = nullptr;   // learned (variable) preconditioner: z_k = M(v_k)
     uint32_t *fallbacks = nullptr;  // out: cycles handed over to Jacobi
 };
 
-size_t gmres_workspace_bytes(uint32_t n, uint32_t m, bool flexible);
+size_t gmres_workspace_bytes(uint32_t n, uint32_t m, bool mixed, uint32_t w);
 rsg_status gmres_carve(rsg_context *ctx, GmresArgs &a, uint32_t n, uint32_t m);
 rsg_status gmres_run(rsg_context *ctx, const GmresArgs &a, double *seconds);
 

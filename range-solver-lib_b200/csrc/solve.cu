@@ -100,8 +100,6 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
     if (c.autotune && !A->tune.valid) RSG_TRY(autotune_run(ctx, A, std::getenv("RSG_TUNE_CACHE")));
     if (c.precision == RSG_PRECISION_MIXED && c.stop_rule != RSG_STOP_TRUE_RELRES)
         return set_error(ctx, RSG_ERR_INVALID_ARG, "mixed precision requires stop_rule TRUE_RELRES");
-    if (c.precision == RSG_PRECISION_MIXED && c.solver_type != RSG_SOLVER_CG)
-        return set_error(ctx, RSG_ERR_UNSUPPORTED, "mixed precision is implemented for CG");
     const uint32_t n = A->n;
     const bool mixed = c.precision == RSG_PRECISION_MIXED;
     const bool gmres = c.solver_type == RSG_SOLVER_GMRES;
@@ -127,7 +125,7 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
         bytes += 5 * vn;                               // r z p0 p1 q
         if (mixed) bytes += 6 * vf + arena_bytes(size_t(n) * w, sizeof(float));
     } else {
-        bytes += gmres_workspace_bytes(n, m, c.flexible != 0);
+        bytes += gmres_workspace_bytes(n, m, mixed, w);
     }
     RSG_TRY(arena_reserve(ctx, bytes));
     double *b_dev = memory == RSG_MEM_HOST ? arena_take<double>(ctx, n) : const_cast<double *>(b);
@@ -274,10 +272,17 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
         a.m = m;
         a.flexible = c.flexible != 0;
         a.G = learned ? G : nullptr;
+        a.mixed = mixed;
         uint32_t gm_fallbacks = 0;
         a.fallbacks = &gm_fallbacks;
         a.st_max_outer = max_it;
         RSG_TRY(gmres_carve(ctx, a, n, m));
+        if (mixed && prec_type != RSG_PREC_NONE) {  // FP32 copy of the preconditioner for the inner steps
+            float *d32 = arena_take<float>(ctx, size_t(n) * w);
+            if (!d32) return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "GMRES workspace");
+            k_to_f32<<<gv, kBlock, 0, ctx->stream>>>(size_t(n) * w, d, d32);
+            a.P.d32 = d32;
+        }
         GmresState h;
         std::memset(&h, 0, sizeof(h));
         h.an = an;

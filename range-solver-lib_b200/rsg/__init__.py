@@ -408,6 +408,12 @@ class Batch:
         self.ctx.check(s, "batch_solve", allow)
         return x, list(per), summ
 
+    def autotune(self) -> dict:
+        """Pick the batch loop's grid per precision by timing short batch solves (rsg_batch_autotune)."""
+        info = _lib.TuneInfo()
+        self.ctx.check(self.ctx.lib.rsg_batch_autotune(self.ctx.h, self.h, C.byref(info)), "batch_autotune")
+        return info.as_dict()
+
     def close(self):
         if self.h and self.ctx.h:
             self.ctx.lib.rsg_batch_destroy(self.ctx.h, self.h)

@@ -139,6 +139,7 @@ SIGNATURES = {
     "rsg_solve_multi": (C.c_int, [_P, _P, C.POINTER(SolverConf), C.c_int32, C.c_uint32, _P, _P, C.c_int32,
                                   C.POINTER(Stats), C.POINTER(Stats)]),
     "rsg_tune_get": (C.c_int, [_P, C.POINTER(TuneInfo)]),
+    "rsg_batch_autotune": (C.c_int, [_P, _P, C.POINTER(TuneInfo)]),
     "rsg_profile_kernel": (C.c_int, [_P, _P, C.c_int32, C.c_uint32, C.c_int32, _DP]),
     "rsg_true_relres_noalloc": (C.c_int, [C.c_uint32, _P, _P, _P, _P, _P, _P, _P]),
     "rsg_batch_create": (C.c_int, [_P, C.c_uint32, _P, _P, _P, _P, _PP]),

@@ -88,3 +88,25 @@ def _coupled(ctx, A1, A2):
     ctx.check(ctx.lib.rsg_batch_create(ctx.h, 2, rb.ctypes.data_as(C.c_void_p), rp.ctypes.data_as(C.c_void_p),
                                        ci.ctypes.data_as(C.c_void_p), val.ctypes.data_as(C.c_void_p), C.byref(h)),
               "batch_create")
+
+
+def test_batch_autotune_keeps_results(ctx):
+    """The batch autotuner only changes launch shapes: tuned solves reach the same tolerance
+    and agree with the untuned ones to rounding."""
+    sys_ = systems([(6, 1.0, 11), (12, 1.2, 12), (4, 0.8, 13), (9, 1.0, 14)])
+    batch = rsg.Batch(ctx, [(A.rp, A.ci, A.val) for A, _ in sys_])
+    b = np.concatenate([bb for _, bb in sys_])
+    results = {}
+    for tag in ("default", "tuned"):
+        if tag == "tuned":
+            info = batch.autotune()
+            assert info["tuned"] == 1 and info["candidates"] >= 2 * 8
+            assert info["seconds_iter_fp64"] <= info["seconds_iter_fp64_default"]
+            assert info["seconds_iter_fp32"] <= info["seconds_iter_fp32_default"]
+        for precision in ("fp64", "mixed"):
+            conf = rsg.make_conf(n_outer=20000, stop_rule="true", rtol=1e-10, precision=precision)
+            x, per, summ = batch.solve(b, conf=conf)
+            assert summ.status == rsg.OK and summ.true_relres <= 1e-10
+            results[(tag, precision)] = x
+    for precision in ("fp64", "mixed"):
+        assert rel_err(results[("tuned", precision)], results[("default", precision)]) < 1e-8

@@ -181,6 +181,32 @@ def test_gmres_nonsymmetric_block_jacobi(ctx):
     assert rel_err(x, np.linalg.solve(D, b)) < 1e-9
 
 
+@pytest.mark.parametrize("prec,block", [(rsg.PREC_JACOBI, 1), (rsg.PREC_BLOCK_JACOBI, 2), (rsg.PREC_NONE, 1)])
+def test_gmres_mixed_precision(ctx, prec, block):
+    """GMRES with FP32 Arnoldi cycles inside FP64 restarts (true residual, Hessenberg,
+    Givens, least squares and x update in FP64) reaches the FP64 tolerance, on an SPD
+    heat system and on a nonsymmetric one."""
+    A, b = heat(10, sigma=1.0, seed=2, source="random")
+    rng = np.random.default_rng(5)
+    n = 80
+    D = np.diag(4.0 + rng.random(n)) + 0.3 * rng.standard_normal((n, n)) * (rng.random((n, n)) < 0.1)
+    cases = [(A, b, oracle_tight(A, b)), (O.csr_from_dense(D), rng.standard_normal(n), None)]
+    for Am, bm, xref in cases:
+        if xref is None:
+            xref = np.linalg.solve(D, bm)
+        M = ctx.matrix(Am.rp, Am.ci, Am.val)
+        its = {}
+        for precision in ("fp64", "mixed"):
+            conf = rsg.make_conf(solver="gmres", n_outer=2000, n_inner=30, stop_rule="true", rtol=1e-10,
+                                 precision=precision)
+            x, st = ctx.solve(M, bm, conf=conf, prec=prec, block_size=block)
+            assert st.status == rsg.OK and st.true_relres <= 1e-10, (precision, st.as_dict())
+            assert O.true_relres(Am, bm, x) <= 1e-10 * 1.01
+            assert rel_err(x, xref) <= 1e-7
+            its[precision] = st.iterations
+        assert its["mixed"] <= 2 * its["fp64"] + 30, its
+
+
 @pytest.mark.parametrize("prec,block", [(rsg.PREC_JACOBI, 1), (rsg.PREC_BLOCK_JACOBI, 3), (rsg.PREC_NONE, 1)])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_stress_cg_preconditioners(ctx, prec, block, precision):
