@@ -219,6 +219,22 @@ RSG_API rsg_status rsg_tune_get(const rsg_csr *A, rsg_tune_info *out);
  * per precision, by timing 32-iteration batch solves (grid_dir_* = grid_update_*). */
 RSG_API rsg_status rsg_batch_autotune(rsg_context *ctx, rsg_batch *batch, rsg_tune_info *out);
 
+/* CSR/RHS dump (no counterpart in the reference): the matrix as the solver holds
+ * it, and optionally a right-hand side (b_device, n doubles, may be NULL), in a
+ * little-endian binary file with a 64-byte "RSGCSR01" header -- reproducible
+ * benchmark and regression inputs.  rsg_csr_load creates *A and, when the file
+ * has a right-hand side and b_device is given, copies it there. */
+RSG_API rsg_status rsg_csr_save(rsg_context *ctx, const rsg_csr *A, const double *b_device, const char *path);
+RSG_API rsg_status rsg_csr_load(rsg_context *ctx, const char *path, rsg_csr **A, double *b_device, uint32_t *n_rows,
+                                uint64_t *nnz, int32_t *has_b);
+
+/* Failure-detection self-test (no counterpart in the reference): a kernel waits,
+ * with the library's bounded mbarrier wait limited to `polls` polls (0: 1024),
+ * for a completion that never comes; it flags the context's error word and
+ * returns, so this call returns RSG_ERR_TIMEOUT and the context stays usable.
+ * Nothing faults or hangs. */
+RSG_API rsg_status rsg_selftest_wait_timeout(rsg_context *ctx, uint32_t polls);
+
 /* FP64 true relative residual ||b - A x|| / ||b|| (device pointers). */
 RSG_API rsg_status rsg_true_relres(rsg_context *ctx, const rsg_csr *A, const double *b, const double *x,
                                    double *relres);
@@ -282,6 +298,10 @@ RSG_API rsg_status rsg_learned_info(const rsg_learned *model, uint32_t *layers, 
 RSG_API rsg_status rsg_learned_get_params(rsg_context *ctx, const rsg_learned *model, float *host, int32_t which);
 RSG_API rsg_status rsg_learned_set_params(rsg_context *ctx, rsg_learned *model, const float *host, int32_t which);
 RSG_API rsg_status rsg_learned_set_step(rsg_learned *model, uint64_t step);
+/* Training checkpoint (parameters, Adam moments, step) in a binary file with a
+ * 64-byte "RSGGNN01" header (version, layers, width, features, parameter count). */
+RSG_API rsg_status rsg_learned_save(rsg_context *ctx, const rsg_learned *model, const char *path);
+RSG_API rsg_status rsg_learned_load(rsg_context *ctx, const char *path, rsg_learned **out);
 /* z = M(r); tensor_cores != 0 runs the dense layers as BF16 MMA with FP32 accumulation, else FP32 */
 RSG_API rsg_status rsg_learned_apply(rsg_context *ctx, rsg_learned *model, const rsg_csr *A, const double *r,
                                      double *z, const double *xyz, int32_t tensor_cores);

@@ -192,6 +192,21 @@ class Context:
         self.check(self.lib.rsg_tune_get(A.h, C.byref(info)), "tune_get")
         return info.as_dict()
 
+    def save_matrix(self, A: "Matrix", path: str, b_dev=None):
+        """CSR/RHS dump of A (and a device right-hand side) in the RSGCSR01 format (rsg_csr_save)."""
+        self.check(self.lib.rsg_csr_save(self.h, A.h, _ptr(b_dev), path.encode()), "csr_save")
+
+    def load_matrix(self, path: str, b_dev=None):
+        """(Matrix, has_b) from an RSGCSR01 file; the right-hand side goes to b_dev when given."""
+        h, n, nnz, hb = C.c_void_p(), C.c_uint32(), C.c_uint64(), C.c_int32()
+        self.check(self.lib.rsg_csr_load(self.h, path.encode(), C.byref(h), _ptr(b_dev), C.byref(n), C.byref(nnz),
+                                         C.byref(hb)), "csr_load")
+        return Matrix(self, h), bool(hb.value)
+
+    def selftest_wait_timeout(self, polls: int = 1024) -> int:
+        """Status of the failure-detection self-test (RSG_ERR_TIMEOUT when detection works)."""
+        return self.lib.rsg_selftest_wait_timeout(self.h, polls)
+
     def true_relres(self, A: "Matrix", b_dev, x_dev) -> float:
         r = C.c_double()
         self.check(self.lib.rsg_true_relres(self.h, A.h, _ptr(b_dev), _ptr(x_dev), C.byref(r)), "true_relres")

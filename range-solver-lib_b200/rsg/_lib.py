@@ -136,6 +136,11 @@ SIGNATURES = {
                             C.POINTER(Stats)]),
     "rsg_true_relres": (C.c_int, [_P, _P, _P, _P, _DP]),
     "rsg_autotune": (C.c_int, [_P, _P, C.c_char_p, C.POINTER(TuneInfo)]),
+    "rsg_csr_save": (C.c_int, [_P, _P, _P, C.c_char_p]),
+    "rsg_csr_load": (C.c_int, [_P, C.c_char_p, _PP, _P, _U32P, _U64P, C.POINTER(C.c_int32)]),
+    "rsg_selftest_wait_timeout": (C.c_int, [_P, C.c_uint32]),
+    "rsg_learned_save": (C.c_int, [_P, _P, C.c_char_p]),
+    "rsg_learned_load": (C.c_int, [_P, C.c_char_p, _PP]),
     "rsg_solve_multi": (C.c_int, [_P, _P, C.POINTER(SolverConf), C.c_int32, C.c_uint32, _P, _P, C.c_int32,
                                   C.POINTER(Stats), C.POINTER(Stats)]),
     "rsg_tune_get": (C.c_int, [_P, C.POINTER(TuneInfo)]),

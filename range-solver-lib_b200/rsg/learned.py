@@ -77,6 +77,19 @@ class Learned:
         m._info()
         return m
 
+    def save_binary(self, path: str):
+        """Checkpoint in the library's RSGGNN01 format (rsg_learned_save)."""
+        self.ctx.check(self.ctx.lib.rsg_learned_save(self.ctx.h, self.h, path.encode()), "learned_save")
+
+    @classmethod
+    def load_binary(cls, ctx, path: str) -> "Learned":
+        h = C.c_void_p()
+        ctx.check(ctx.lib.rsg_learned_load(ctx.h, path.encode(), C.byref(h)), "learned_load")
+        m = cls.__new__(cls)
+        m.ctx, m.h = ctx, h
+        m._info()
+        return m
+
     # ---- compute ----
     def apply(self, A, r_dev, z_dev, xyz_dev=None, tensor_cores: bool = True):
         """z = M(r) on the device (r, z: n doubles; xyz: 3n doubles or None)."""
