@@ -340,6 +340,12 @@ RSG_API rsg_status rsg_assembly_create_stress(rsg_context *ctx, uint32_t n_nodes
                                               rsg_assembly **out);
 RSG_API void       rsg_assembly_destroy(rsg_context *ctx, rsg_assembly *plan);
 RSG_API rsg_status rsg_assembly_info(const rsg_assembly *plan, uint32_t *n_free, uint64_t *nnz);
+/* Solution back into the nodal field (device arrays): node_values[node*dofs + c] =
+ * x[book[node*dofs + c]] for every free DOF, Dirichlet entries untouched -- the map
+ * RSolverHeat/RSolverStress apply after solve (src/rsolverheat.cpp:466-483); with it
+ * a transient step (assemble, solve, scatter) stays on the GPU. */
+RSG_API rsg_status rsg_assembly_scatter(rsg_context *ctx, const rsg_assembly *plan, const double *x_device,
+                                        double *node_values_device);
 
 /* Heat numeric assembly, src/rsolverheat.cpp:361-455 (element loop) and :755-820
  * (theta scheme, Dirichlet lifting, scatter).  Per-tet arrays k_e, q_e, rhoc_e;

@@ -351,6 +351,18 @@ __global__ void __launch_bounds__(128) k_asm_stress_local(
     }
 }
 
+// node_values[node * dofs + c] = x[book[node * dofs + c]] for every free DOF (the
+// Dirichlet values stay): the solution back into the nodal field, e.g. the
+// previous-step temperatures of the next transient assembly.
+__global__ void k_asm_scatter(uint32_t n_entries, const uint32_t *__restrict__ book, const double *__restrict__ x,
+                              double *__restrict__ node_values)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_entries; i += gridDim.x * blockDim.x) {
+        const uint32_t pos = book[i];
+        if (pos != RSG_EOD) node_values[i] = x[pos];
+    }
+}
+
 // RSG_ASM_ROW_THREADS=1 selects the kernels that accumulate in global memory (tests compare the two)
 bool row_threads_forced()
 {
@@ -574,6 +586,19 @@ rsg_status rsg_assemble_stress(rsg_context *ctx, rsg_assembly *p, const double *
             reinterpret_cast<const uint4 *>(p->tets), p->tris, p->book, d[0], d[1], d[2], d[3], d[4], d[5], d[6],
             d[7], transient ? 1 : 0, alpha, dt, val, b_device);
     });
+}
+
+rsg_status rsg_assembly_scatter(rsg_context *ctx, const rsg_assembly *p, const double *x_device,
+                                double *node_values_device)
+{
+    if (!ctx || !p || !x_device || !node_values_device)
+        return set_error(ctx, RSG_ERR_INVALID_ARG, "assembly_scatter: bad arguments");
+    RSG_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
+    const uint32_t ne = p->n_nodes * p->dofs;
+    const int grid = std::min(grid_for(ctx, (const void *)k_asm_scatter, kBlock, 0, ne), kMaxGrid);
+    k_asm_scatter<<<grid, kBlock, 0, ctx->stream>>>(ne, p->book, x_device, node_values_device);
+    RSG_CHECK_CUDA(ctx, cudaGetLastError());
+    return RSG_OK;
 }
 
 }  // extern "C"

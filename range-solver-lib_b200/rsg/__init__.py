@@ -449,30 +449,34 @@ def transient_heat(ctx: Context, problem, n_steps: int, conf: SolverConf | None 
     every step, which rebuilds A and b from scratch (A.clear(), src/rsolverheat.cpp:85)
     with the theta scheme of assemblyMatrix (:768-779), then solves with x = 0 as
     the initial guess.  Here the assembly plan (pattern + scatter map) is built
-    once and each step re-assembles values and RHS on the GPU into the same
-    matrix; the previous step's temperatures are the initial guess.
-    Returns the list of nodal temperature arrays after each step (host numpy).
+    once; each step re-assembles values and right-hand side on the GPU from
+    device-resident element fields and the previous temperatures, solves with the
+    previous step's temperatures as the initial guess, and writes the solution back
+    into the nodal field with rsg_assembly_scatter -- nothing leaves the GPU inside
+    the loop.  Returns [(nodal temperatures after each step (host numpy), Stats)].
     """
     import copy
+    import torch  # device buffers
     p = copy.copy(problem)
     p.transient = True
-    p.node_t = np.array(problem.node_t, np.float64, copy=True)
     asm = Assembly.heat(ctx, p)
-    import torch  # device buffers for b and x
-    b = torch.empty(asm.n_free, dtype=torch.float64, device=f"cuda:{ctx.device}")
+    dev = f"cuda:{ctx.device}"
+    fields = {k: torch.from_numpy(np.ascontiguousarray(getattr(p, k), np.float64)).to(dev)
+              for k in ("k_e", "q_e", "rhoc_e", "node_t")}
+    b = torch.empty(asm.n_free, dtype=torch.float64, device=dev)
     x = torch.zeros_like(b)
     conf = conf or make_conf(n_outer=50000, stop_rule="true", rtol=1e-10, precision=precision)
     free = p.book != 0xFFFFFFFF
-    idx = p.book[free].astype(np.int64)
-    out = []
+    x.copy_(torch.from_numpy(np.ascontiguousarray(p.node_t[free][np.argsort(p.book[free])], np.float64)).to(dev))
+    torch.cuda.synchronize()
+    history, stats = [], []
     for _ in range(n_steps):
-        A = asm.assemble(p, b)
-        torch.cuda.synchronize()
-        x.copy_(torch.from_numpy(p.node_t[free][np.argsort(idx)]).to(b.device))
-        torch.cuda.synchronize()
+        A = asm.assemble(p, b, inputs_on_device=fields)
         _, st = ctx.solve(A, b, x, conf=conf)
-        xs = x.cpu().numpy()
-        p.node_t[free] = xs[idx]
-        out.append((p.node_t.copy(), st))
+        ctx.check(ctx.lib.rsg_assembly_scatter(ctx.h, asm.h, _ptr(x), _ptr(fields["node_t"])), "assembly_scatter")
+        ctx.sync()  # the snapshot below runs on torch's stream, the scatter on the context's
+        history.append(fields["node_t"].clone())
+        stats.append(st)
+    out = [(t.cpu().numpy(), st) for t, st in zip(history, stats)]
     asm.close()
     return out

@@ -165,6 +165,7 @@ SIGNATURES = {
                                              _PP]),
     "rsg_assembly_destroy": (None, [_P, _P]),
     "rsg_assembly_info": (C.c_int, [_P, _U32P, _U64P]),
+    "rsg_assembly_scatter": (C.c_int, [_P, _P, _P, _P]),
     "rsg_assemble_heat": (C.c_int, [_P, _P, _P, _P, _P, _P, C.POINTER(Time), C.c_int32, _PP, _P]),
     "rsg_assemble_stress": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, C.POINTER(Time), C.c_int32, _PP,
                                       _P]),

@@ -176,6 +176,29 @@ def heat_cube(n: int, *, sigma: float = 0.0, seed: int = 0, source: str = "unit"
                        name=f"heat_cube_{n}", meta=dict(n=n, sigma=sigma, seed=seed, source=source))
 
 
+# vacuum permittivity [F/m] as RSolverGeneric::e0 (src/rsolvergeneric.cpp:13)
+E0 = 8.854187817e-12
+
+
+def electrostatic_cube(n: int, *, eps_r: float = 1.0, charge: float = 0.0, v0: float = 0.0, v1: float = 1.0,
+                       sigma: float = 0.0, seed: int = 0) -> HeatProblem:
+    """Electrostatics on the unit cube (potential v0 on x=0, v1 on x=1, other faces insulated).
+
+    RSolverElectrostatics' 3-D volume integrals (src/rsolverelectrostatics.cpp:322-344) are the heat
+    conduction ones with k = eps_r * e0 and a volumetric source of -rho (fe -= rho N detJ w), and its
+    Dirichlet lifting (:800-812) is the heat one, so the heat assembly plan serves them: the returned
+    problem carries k_e = eps_r e0 (lognormal spread sigma when > 0) and q_e = -charge per tet.
+    """
+    p = heat_cube(n, sigma=sigma, seed=seed, source="none")
+    nt = p.mesh.n_tets
+    p.k_e = (np.full(nt, eps_r) if sigma == 0.0 else lognormal(seed, 1, nt, np.log(eps_r), sigma)) * E0
+    p.q_e = np.full(nt, -charge)
+    x = p.mesh.xyz[:, 0]
+    p.node_t = np.where(x == 1.0, v1, np.where(x == 0.0, v0, 0.0))
+    p.name = f"electrostatic_cube_{n}"
+    return p
+
+
 def reseed_heat(p: HeatProblem, *, sigma: float, seed: int, mu: float = 0.0) -> HeatProblem:
     """p with a new lognormal(mu, sigma) conductivity field and random source drawn from seed
     (same mesh, node book and boundary values; the streams heat_cube uses for that seed)."""

@@ -160,3 +160,23 @@ def test_warp_and_thread_row_kernels_bitwise_equal(ctx, torch_cuda, monkeypatch,
         asm.close()
     assert np.array_equal(out[0][0], out[1][0])
     assert np.array_equal(out[0][1], out[1][1])
+
+
+def test_electrostatics_through_the_heat_plan(ctx, torch_cuda):
+    """RSolverElectrostatics' volume integrals are the heat ones with k = eps_r e0 and
+    source -rho: a parallel-plate capacitor (uniform eps_r, no charge) gives the exact
+    linear potential, and a charged lognormal case matches the oracle assembly."""
+    torch = torch_cuda
+    p = W.electrostatic_cube(6, eps_r=4.0, v0=0.0, v1=10.0)
+    asm, M, b = run_heat(ctx, torch, p)
+    x, st = ctx.solve(M, b.cpu().numpy(), conf=rsg.make_conf(n_outer=10000, stop_rule="true", rtol=1e-13))
+    free = p.book != 0xFFFFFFFF
+    order = np.argsort(p.book[free])
+    expect = 10.0 * p.mesh.xyz[free, 0][order]
+    assert np.max(np.abs(x - expect)) < 1e-8
+    asm.close()
+    q = W.electrostatic_cube(7, eps_r=3.0, charge=2e-9, sigma=0.8, seed=5)
+    asm, M, b = run_heat(ctx, torch, q)
+    Ao, bo = O.assemble_heat(q)
+    compare(device_csr(ctx, torch, M), b.cpu().numpy(), Ao, bo)
+    asm.close()
