@@ -338,6 +338,14 @@ RSG_API rsg_status rsg_assembly_create_stress(rsg_context *ctx, uint32_t n_nodes
                                               uint32_t n_tets, const uint32_t *tets, uint32_t n_tris,
                                               const uint32_t *tris, const uint32_t *book, uint32_t n_free,
                                               rsg_assembly **out);
+/* Magnetostatics (vector potential): 3 interleaved DOFs per node (3 * position + component) with a
+ * node's three DOFs enabled or disabled together -- one node book position per node, as
+ * RSolverMagnetostatics::prepare/assemblyMatrix use it (src/rsolvermagnetostatics.cpp:46, :245, :261);
+ * a book that disables some but not all of a node's components is rejected.  The pattern holds full
+ * 3x3 blocks per node pair, the reference's zero entries between components included (:272-282). */
+RSG_API rsg_status rsg_assembly_create_magnetostatics(rsg_context *ctx, uint32_t n_nodes, const double *xyz,
+                                                      uint32_t n_tets, const uint32_t *tets, const uint32_t *book,
+                                                      uint32_t n_free, rsg_assembly **out);
 RSG_API void       rsg_assembly_destroy(rsg_context *ctx, rsg_assembly *plan);
 RSG_API rsg_status rsg_assembly_info(const rsg_assembly *plan, uint32_t *n_free, uint64_t *nnz);
 /* Solution back into the nodal field (device arrays): node_values[node*dofs + c] =
@@ -363,6 +371,16 @@ RSG_API rsg_status rsg_assemble_stress(rsg_context *ctx, rsg_assembly *plan, con
                                        const double *rho_e, const double *gravity, const double *texp_e,
                                        const double *dtemp_e, const double *traction, const double *node_u,
                                        const rsg_time *time, int32_t memory, rsg_csr **A, double *b_device);
+
+/* Magnetostatic numeric assembly, src/rsolvermagnetostatics.cpp:57-137 (element loop) and
+ * :234-287 (lifting, scatter): per tet and node pair -(grad N_m . grad N_n) V on each component,
+ * right-hand side e0 V/4 (grad N_m x J_m) with J the nodal current density.  node_j: current
+ * density (3 per node, the reference's convertElementToNodeVector output, :38-40); node_a:
+ * prescribed potential at disabled nodes (3 per node).  Inputs in `memory`; writes *A and b
+ * as rsg_assemble_heat. */
+RSG_API rsg_status rsg_assemble_magnetostatics(rsg_context *ctx, rsg_assembly *plan, const double *node_j,
+                                               const double *node_a, int32_t memory, rsg_csr **A,
+                                               double *b_device);
 
 #ifdef __cplusplus
 }

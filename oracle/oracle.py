@@ -87,6 +87,8 @@ def lib():
         L.orc_assemble_stress.restype = _P
         L.orc_assemble_stress.argtypes = [C.c_uint32, _P, C.c_uint32, _P, _P, _P, _P, _P, _P, _P, C.c_uint32, _P,
                                           _P, _P, _P, C.c_uint32, C.POINTER(OrcTime)]
+        L.orc_assemble_magnetostatics.restype = _P
+        L.orc_assemble_magnetostatics.argtypes = [C.c_uint32, _P, C.c_uint32, _P, _P, _P, _P, C.c_uint32]
         _LIB = L
     return _LIB
 
@@ -221,4 +223,17 @@ def assemble_stress(p) -> tuple[CSR, np.ndarray]:
     h = lib().orc_assemble_stress(m.n_nodes, _ptr(xyz), m.n_tets, _ptr(tets), _ptr(e), _ptr(nu), _ptr(rho), _ptr(g),
                                   _ptr(te), _ptr(dte), tris.shape[0], _ptr(tris), _ptr(tr), _ptr(nu_), _ptr(book),
                                   p.n_free, C.byref(tm))
+    return _system(h)
+
+
+def assemble_magnetostatics(p) -> tuple[CSR, np.ndarray]:
+    """RSolverMagnetostatics::prepare + assemblyMatrix restated for a rsg.workloads.MagnetostaticProblem."""
+    m = p.mesh
+    xyz = np.ascontiguousarray(m.xyz, np.float64)
+    tets = np.ascontiguousarray(m.tets, np.uint32)
+    j = np.ascontiguousarray(p.node_j, np.float64)
+    a = np.ascontiguousarray(p.node_a, np.float64)
+    book = np.ascontiguousarray(p.book, np.uint32)
+    h = lib().orc_assemble_magnetostatics(m.n_nodes, _ptr(xyz), m.n_tets, _ptr(tets), _ptr(j), _ptr(a), _ptr(book),
+                                          p.n_free)
     return _system(h)

@@ -818,4 +818,57 @@ orc_system *orc_assemble_stress(uint32_t n_nodes, const double *xyz, uint32_t n_
     return finish_system(A, b);
 }
 
+/* Magnetostatics (vector potential, 3 dofs per node interleaved, all three disabled together):
+ * RSolverMagnetostatics::prepare volume loop (src/rsolvermagnetostatics.cpp:57-137) and
+ * assemblyMatrix (:234-287).  Per tet, for node pair (m, n): Ke[3m+c][3n+c] = -(B_m . B_n) detJ w and
+ * zero off the component diagonal (the zero entries are still added to the pattern, :272-282);
+ * fe[3m+c] = N_m detJ w e0 (B_m x J_m)_c with J_m the current density of node m (:110-119), restated
+ * with the exact P1 integrals (constant B = grad N; int N_m = V/4). */
+orc_system *orc_assemble_magnetostatics(uint32_t n_nodes, const double *xyz, uint32_t n_tets, const uint32_t *tets,
+                                        const double *node_j, const double *node_a, const uint32_t *book,
+                                        uint32_t n_free)
+{
+    (void)n_nodes;
+    const double e0 = 8.854187817e-12; /* RSolverGeneric::e0 (src/rsolvergeneric.cpp:13) */
+    RowMap A(n_free);
+    std::vector<double> b(n_free, 0.0);
+    for (uint32_t e = 0; e < n_tets; e++) {
+        const uint32_t *t = tets + 4 * size_t(e);
+        double G[4][3];
+        double V = std::abs(tet_gradients(xyz, t, G)) / 6.0;
+        double Ke[12][12], be[12];
+        for (int i = 0; i < 12; i++)
+            for (int j = 0; j < 12; j++) Ke[i][j] = 0.0;
+        for (int m = 0; m < 4; m++) {
+            for (int n = 0; n < 4; n++) {
+                const double v = (G[m][0] * G[n][0] + G[m][1] * G[n][1] + G[m][2] * G[n][2]) * V;
+                for (int c = 0; c < 3; c++) Ke[3 * m + c][3 * n + c] -= v;
+            }
+            const double fv = V / 4.0 * e0;
+            const double *J = node_j + 3 * size_t(t[m]);
+            const double js[3] = {-G[m][2] * J[1] + G[m][1] * J[2], G[m][2] * J[0] - G[m][0] * J[2],
+                                  -G[m][1] * J[0] + G[m][0] * J[1]};
+            for (int c = 0; c < 3; c++) be[3 * m + c] = fv * js[c];
+        }
+        /* :240-254 -- lifting by the prescribed potential of disabled nodes */
+        for (int m = 0; m < 4; m++)
+            if (book[3 * size_t(t[m])] == kEod)
+                for (int n = 0; n < 12; n++)
+                    for (int c = 0; c < 3; c++) be[n] -= Ke[n][3 * m + c] * node_a[3 * size_t(t[m]) + c];
+        /* :256-286 */
+        for (int m = 0; m < 4; m++) {
+            if (book[3 * size_t(t[m])] == kEod) continue;
+            for (int i = 0; i < 3; i++) {
+                const uint32_t mp = book[3 * size_t(t[m]) + i];
+                b[mp] += be[3 * m + i];
+                for (int n = 0; n < 4; n++) {
+                    if (book[3 * size_t(t[n])] == kEod) continue;
+                    for (int j = 0; j < 3; j++) A.add(mp, book[3 * size_t(t[n]) + j], Ke[3 * m + i][3 * n + j]);
+                }
+            }
+        }
+    }
+    return finish_system(A, b);
+}
+
 }  // extern "C"

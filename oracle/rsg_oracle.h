@@ -14,6 +14,7 @@
  *   src/rsolvergeneric.cpp          DOF numbering (node book)
  *   src/rsolverheat.cpp             P1 tet heat element + theta scheme + lifting
  *   src/rsolverstress.cpp           P1 tet elasticity element, traction, lifting
+ *   src/rsolvermagnetostatics.cpp   P1 tet vector-potential element, curl source, lifting
  *
  * Parity pins: the reference's only known-answer tests
  * (tests/tst_matrix_solver.cpp:33-54 and :56-77) are reproduced by
@@ -100,6 +101,12 @@ orc_system *orc_assemble_stress(uint32_t n_nodes, const double *xyz, uint32_t n_
                                 uint32_t n_tris, const uint32_t *tris, const double *traction /* n_tris*3 */,
                                 const double *node_u /* 3*n_nodes */, const uint32_t *book /* 3*n_nodes */,
                                 uint32_t n_free, const orc_time *time);
+
+/* f4: magnetostatics (vector potential, 3 dofs per node interleaved, a node's three dofs enabled or
+ * disabled together); node_j = nodal current density, node_a = prescribed potential (3*n_nodes each). */
+orc_system *orc_assemble_magnetostatics(uint32_t n_nodes, const double *xyz, uint32_t n_tets, const uint32_t *tets,
+                                        const double *node_j, const double *node_a, const uint32_t *book,
+                                        uint32_t n_free);
 
 #ifdef __cplusplus
 }

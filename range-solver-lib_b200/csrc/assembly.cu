@@ -37,9 +37,12 @@ struct rsg_assembly {
     double *stage = nullptr;   // host inputs staged on the device
     size_t stage_cap = 0;
     uint32_t max_row = 0;      // longest row of the pattern (the thread-local kernels take short rows)
+    int kind = 0;              // rsg::kPlanHeat / kPlanStress / kPlanMagnetostatics
 };
 
 namespace rsg {
+
+enum { kPlanHeat = 1, kPlanStress = 2, kPlanMagnetostatics = 3 };
 
 namespace {
 
@@ -351,6 +354,89 @@ __global__ void __launch_bounds__(128) k_asm_stress_local(
     }
 }
 
+// vacuum permittivity, RSolverGeneric::e0 (src/rsolvergeneric.cpp:13)
+constexpr double kE0 = 8.854187817e-12;
+
+// Contribution of one (row node, component i, adjacent tet) triple to a magnetostatic row
+// (src/rsolvermagnetostatics.cpp:94-119, lifting :240-254): Ar[3n+j] = -(grad N_m . grad N_n) V
+// on the component diagonal (j == i) and an explicit 0 elsewhere, be = e0 V/4 (grad N_m x J)_i
+// with J the row node's current density, minus the lifting by disabled nodes' potentials.
+__device__ __forceinline__ void magneto_adj(uint32_t t, int i, const uint32_t *__restrict__ adj_elem,
+                                            const uint8_t *__restrict__ adj_loc, const double *__restrict__ xyz,
+                                            const uint4 *__restrict__ tets, const uint32_t *__restrict__ book,
+                                            const double *__restrict__ J, const double *__restrict__ node_a,
+                                            double (&Ar)[12], double &be, uint4 &tv)
+{
+    const uint32_t e = adj_elem[t];
+    const int m = adj_loc[t];
+    tv = tets[e];
+    double G[4][3];
+    const double V = tet_geometry(xyz, tv, G);
+    for (int n = 0; n < 4; n++) {
+        const double v = (G[m][0] * G[n][0] + G[m][1] * G[n][1] + G[m][2] * G[n][2]) * V;
+        for (int j = 0; j < 3; j++) Ar[3 * n + j] = j == i ? 0.0 - v : 0.0;
+    }
+    const double js = i == 0 ? -G[m][2] * J[1] + G[m][1] * J[2]
+                    : i == 1 ? G[m][2] * J[0] - G[m][0] * J[2]
+                             : -G[m][1] * J[0] + G[m][0] * J[1];
+    be = V / 4.0 * kE0 * js;
+    for (int n = 0; n < 4; n++) {
+        const uint32_t nd = node_of(tv, n);
+        if (book[3 * size_t(nd)] == RSG_EOD)
+            for (int j = 0; j < 3; j++) be -= Ar[3 * n + j] * node_a[3 * size_t(nd) + j];
+    }
+}
+
+// One thread per row; Local: the row accumulated in a thread-local array (rows of up to
+// kLocalStressRowMax entries), else in global memory.  Same per-entry order either way.
+template <bool Local>
+__global__ void __launch_bounds__(128) k_asm_magneto(
+    uint32_t n_free, const uint32_t *__restrict__ row_node, const uint8_t *__restrict__ row_comp,
+    const uint32_t *__restrict__ rp, const uint32_t *__restrict__ adj_ptr, const uint32_t *__restrict__ adj_elem,
+    const uint8_t *__restrict__ adj_loc, const ushort4 *__restrict__ adj_off, const uint8_t *__restrict__ node_mask,
+    const double *__restrict__ xyz, const uint4 *__restrict__ tets, const uint32_t *__restrict__ book,
+    const double *__restrict__ node_j, const double *__restrict__ node_a, double *__restrict__ val,
+    double *__restrict__ b)
+{
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n_free; r += gridDim.x * blockDim.x) {
+        const uint32_t a = row_node[r], start = rp[r], len = rp[r + 1] - start;
+        const int i = row_comp[r];
+        double acc[Local ? kLocalStressRowMax : 1];
+        if (Local) {
+            for (uint32_t j = 0; j < len; j++) acc[j] = 0.0;
+        } else {
+            for (uint32_t j = 0; j < len; j++) val[start + j] = 0.0;
+        }
+        const double J[3] = {node_j[3 * size_t(a)], node_j[3 * size_t(a) + 1], node_j[3 * size_t(a) + 2]};
+        double bs = 0.0;
+        for (uint32_t t = adj_ptr[a]; t < adj_ptr[a + 1]; t++) {
+            double Ar[12], be;
+            uint4 tv;
+            magneto_adj(t, i, adj_elem, adj_loc, xyz, tets, book, J, node_a, Ar, be, tv);
+            bs += be;
+            const ushort4 off4 = adj_off[t];
+            const uint16_t off[4] = {off4.x, off4.y, off4.z, off4.w};
+            for (int n = 0; n < 4; n++) {
+                if (off[n] == 0xffffu) continue;
+                const uint8_t mask = node_mask[node_of(tv, n)];
+                uint32_t rank = 0;
+                for (int j = 0; j < 3; j++)
+                    if (mask & (1u << j)) {
+                        const uint32_t pos = off[n] + rank++;
+                        if (Local) {
+                            if (pos < kLocalStressRowMax) acc[pos] += Ar[3 * n + j];
+                        } else {
+                            val[start + pos] += Ar[3 * n + j];
+                        }
+                    }
+            }
+        }
+        if (Local)
+            for (uint32_t j = 0; j < len; j++) val[start + j] = acc[j];
+        b[r] = bs;
+    }
+}
+
 // node_values[node * dofs + c] = x[book[node * dofs + c]] for every free DOF (the
 // Dirichlet values stay): the solution back into the nodal field, e.g. the
 // previous-step temperatures of the next transient assembly.
@@ -510,14 +596,37 @@ extern "C" {
 rsg_status rsg_assembly_create_heat(rsg_context *ctx, uint32_t n_nodes, const double *xyz, uint32_t n_tets,
                                     const uint32_t *tets, const uint32_t *book, uint32_t n_free, rsg_assembly **out)
 {
-    return create_plan(ctx, n_nodes, xyz, n_tets, tets, 0, nullptr, book, 1, n_free, out);
+    const rsg_status s = create_plan(ctx, n_nodes, xyz, n_tets, tets, 0, nullptr, book, 1, n_free, out);
+    if (s == RSG_OK) (*out)->kind = kPlanHeat;
+    return s;
 }
 
 rsg_status rsg_assembly_create_stress(rsg_context *ctx, uint32_t n_nodes, const double *xyz, uint32_t n_tets,
                                       const uint32_t *tets, uint32_t n_tris, const uint32_t *tris,
                                       const uint32_t *book, uint32_t n_free, rsg_assembly **out)
 {
-    return create_plan(ctx, n_nodes, xyz, n_tets, tets, n_tris, tris, book, 3, n_free, out);
+    const rsg_status s = create_plan(ctx, n_nodes, xyz, n_tets, tets, n_tris, tris, book, 3, n_free, out);
+    if (s == RSG_OK) (*out)->kind = kPlanStress;
+    return s;
+}
+
+rsg_status rsg_assembly_create_magnetostatics(rsg_context *ctx, uint32_t n_nodes, const double *xyz,
+                                              uint32_t n_tets, const uint32_t *tets, const uint32_t *book,
+                                              uint32_t n_free, rsg_assembly **out)
+{
+    if (!ctx || !book || !out) return set_error(ctx, RSG_ERR_INVALID_ARG, "assembly_create_magnetostatics: bad arguments");
+    // one node book position per node (src/rsolvermagnetostatics.cpp:245, :261): the three
+    // potential components of a node are enabled or disabled together
+    for (uint32_t nd = 0; nd < n_nodes; nd++) {
+        const int eod = int(book[3 * size_t(nd)] == RSG_EOD) + int(book[3 * size_t(nd) + 1] == RSG_EOD) +
+                        int(book[3 * size_t(nd) + 2] == RSG_EOD);
+        if (eod != 0 && eod != 3)
+            return set_error(ctx, RSG_ERR_INVALID_ARG,
+                             "assembly_create_magnetostatics: node %u has some but not all components disabled", nd);
+    }
+    const rsg_status s = create_plan(ctx, n_nodes, xyz, n_tets, tets, 0, nullptr, book, 3, n_free, out);
+    if (s == RSG_OK) (*out)->kind = kPlanMagnetostatics;
+    return s;
 }
 
 void rsg_assembly_destroy(rsg_context *ctx, rsg_assembly *plan)
@@ -541,7 +650,7 @@ rsg_status rsg_assemble_heat(rsg_context *ctx, rsg_assembly *p, const double *k_
                              const double *rhoc_e, const double *node_t, const rsg_time *time, int32_t memory,
                              rsg_csr **A, double *b_device)
 {
-    if (!ctx || !p || !k_e || !q_e || !node_t || !A || !b_device || p->dofs != 1)
+    if (!ctx || !p || !k_e || !q_e || !node_t || !A || !b_device || p->kind != kPlanHeat)
         return set_error(ctx, RSG_ERR_INVALID_ARG, "assemble_heat: bad arguments");
     const bool transient = time && time->transient;
     if (transient && !rhoc_e) return set_error(ctx, RSG_ERR_INVALID_ARG, "assemble_heat: transient needs rhoc_e");
@@ -566,7 +675,7 @@ rsg_status rsg_assemble_stress(rsg_context *ctx, rsg_assembly *p, const double *
                                const rsg_time *time, int32_t memory, rsg_csr **A, double *b_device)
 {
     if (!ctx || !p || !e_mod || !nu || !rho_e || !gravity || !texp_e || !dtemp_e || !node_u || !A || !b_device ||
-        p->dofs != 3 || (p->n_tris && !traction))
+        p->kind != kPlanStress || (p->n_tris && !traction))
         return set_error(ctx, RSG_ERR_INVALID_ARG, "assemble_stress: bad arguments");
     RSG_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
     const bool transient = time && time->transient;
@@ -585,6 +694,26 @@ rsg_status rsg_assemble_stress(rsg_context *ctx, rsg_assembly *p, const double *
             reinterpret_cast<const ushort4 *>(p->adj_off), p->tadj_ptr, p->tadj_tri, p->node_mask, p->xyz,
             reinterpret_cast<const uint4 *>(p->tets), p->tris, p->book, d[0], d[1], d[2], d[3], d[4], d[5], d[6],
             d[7], transient ? 1 : 0, alpha, dt, val, b_device);
+    });
+}
+
+rsg_status rsg_assemble_magnetostatics(rsg_context *ctx, rsg_assembly *p, const double *node_j,
+                                       const double *node_a, int32_t memory, rsg_csr **A, double *b_device)
+{
+    if (!ctx || !p || !node_j || !node_a || !A || !b_device || p->kind != kPlanMagnetostatics)
+        return set_error(ctx, RSG_ERR_INVALID_ARG, "assemble_magnetostatics: bad arguments");
+    RSG_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
+    const double *d[2];
+    RSG_TRY(stage_inputs(ctx, p, memory, {size_t(p->n_nodes) * 3, size_t(p->n_nodes) * 3}, {node_j, node_a}, d));
+    const bool local = p->max_row <= kLocalStressRowMax && !row_threads_forced();
+    auto kern = local ? k_asm_magneto<true> : k_asm_magneto<false>;
+    const int block = 128;
+    const int grid = std::min(grid_for(ctx, (const void *)kern, block, 0, p->n_free), kMaxGrid * 4);
+    return assemble_into(ctx, p, A, [&](double *val) {
+        kern<<<grid, block, 0, ctx->stream>>>(p->n_free, p->row_node, p->row_comp, p->rp, p->adj_ptr, p->adj_elem,
+                                              p->adj_loc, reinterpret_cast<const ushort4 *>(p->adj_off),
+                                              p->node_mask, p->xyz, reinterpret_cast<const uint4 *>(p->tets),
+                                              p->book, d[0], d[1], val, b_device);
     });
 }
 

@@ -293,7 +293,9 @@ class Assembly:
     """Assembly plan (rsg_assembly): pattern + scatter map of one mesh and node book.
 
     heat: RSolverHeat::prepare/assemblyMatrix (src/rsolverheat.cpp:361-455, :755-820);
-    stress: RSolverStress::prepare/assemblyMatrix (src/rsolverstress.cpp:384-715, :1654-1772).
+    stress: RSolverStress::prepare/assemblyMatrix (src/rsolverstress.cpp:384-715, :1654-1772);
+    magnetostatics: RSolverMagnetostatics::prepare/assemblyMatrix (src/rsolvermagnetostatics.cpp:44-145,
+    :234-287).
     """
 
     def __init__(self, ctx: Context, h: C.c_void_p, kind: str):
@@ -328,8 +330,20 @@ class Assembly:
                   "assembly_create_stress")
         return cls(ctx, h, "stress")
 
+    @classmethod
+    def magnetostatics(cls, ctx: Context, p) -> "Assembly":
+        m = p.mesh
+        xyz = np.ascontiguousarray(m.xyz, np.float64)
+        tets = np.ascontiguousarray(m.tets, np.uint32)
+        book = np.ascontiguousarray(p.book, np.uint32)
+        h = C.c_void_p()
+        ctx.check(ctx.lib.rsg_assembly_create_magnetostatics(ctx.h, m.n_nodes, _ptr(xyz), m.n_tets, _ptr(tets),
+                                                             _ptr(book), p.n_free, C.byref(h)),
+                  "assembly_create_magnetostatics")
+        return cls(ctx, h, "magnetostatics")
+
     def _time(self, p) -> Time:
-        return Time(1 if p.transient else 0, p.alpha, p.dt)
+        return Time(1 if getattr(p, "transient", False) else 0, getattr(p, "alpha", 1.0), getattr(p, "dt", 0.0))
 
     def assemble(self, p, b_dev, inputs_on_device: dict | None = None) -> Matrix:
         """Assemble problem p's values into the plan's matrix (created on first use) and b_dev (device)."""
@@ -345,6 +359,13 @@ class Assembly:
                 mem = MEM_HOST
             s = self.ctx.lib.rsg_assemble_heat(self.ctx.h, self.h, *[_ptr(a) for a in args], C.byref(tm), mem,
                                                C.byref(hA), _ptr(b_dev))
+        elif self.kind == "magnetostatics":
+            if inputs_on_device:
+                args, mem = [inputs_on_device["node_j"], inputs_on_device["node_a"]], MEM_DEVICE
+            else:
+                args, mem = [np.ascontiguousarray(a, np.float64) for a in (p.node_j, p.node_a)], MEM_HOST
+            s = self.ctx.lib.rsg_assemble_magnetostatics(self.ctx.h, self.h, *[_ptr(a) for a in args], mem,
+                                                         C.byref(hA), _ptr(b_dev))
         else:
             args = [np.ascontiguousarray(a, np.float64) for a in (p.e_mod, p.nu, p.rho_e, p.gravity, p.texp_e,
                                                                   p.dtemp_e, p.traction, p.node_u)]

@@ -166,6 +166,8 @@ SIGNATURES = {
     "rsg_assembly_destroy": (None, [_P, _P]),
     "rsg_assembly_info": (C.c_int, [_P, _U32P, _U64P]),
     "rsg_assembly_scatter": (C.c_int, [_P, _P, _P, _P]),
+    "rsg_assembly_create_magnetostatics": (C.c_int, [_P, C.c_uint32, _P, C.c_uint32, _P, _P, C.c_uint32, _P]),
+    "rsg_assemble_magnetostatics": (C.c_int, [_P, _P, _P, _P, C.c_int32, _P, _P]),
     "rsg_assemble_heat": (C.c_int, [_P, _P, _P, _P, _P, _P, C.POINTER(Time), C.c_int32, _PP, _P]),
     "rsg_assemble_stress": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, C.POINTER(Time), C.c_int32, _PP,
                                       _P]),

@@ -199,6 +199,51 @@ def electrostatic_cube(n: int, *, eps_r: float = 1.0, charge: float = 0.0, v0: f
     return p
 
 
+@dataclass
+class MagnetostaticProblem:
+    """Magnetostatics on a tet mesh (RSolverMagnetostatics inputs): vector potential, 3 dofs per node
+    interleaved (3 * position + component), a node's three dofs enabled or disabled together."""
+
+    mesh: TetMesh
+    node_j: np.ndarray  # (3 n_nodes,) nodal current density
+    node_a: np.ndarray  # (3 n_nodes,) prescribed potential at disabled nodes
+    disabled: np.ndarray  # (n_nodes,) bool
+    book: np.ndarray  # (3 n_nodes,)
+    n_free: int
+    name: str = ""
+
+
+def magnetostatic_cube(n: int, *, current: str = "coil", a0=(0.0, 0.0, 0.0), a1=(0.0, 0.0, 0.0), j0: float = 1.0e6,
+                       seed: int = 0) -> MagnetostaticProblem:
+    """Unit cube (n^3 hexes, 6 tets each); potential a0 on x=0 and a1 on x=1 (all components).
+
+    current "coil": J = j0 (-(y - 1/2), x - 1/2, 0) inside the cylinder (x-1/2)^2 + (y-1/2)^2 < 1/16
+    (a circulating current about the z axis), zero outside; "random": J ~ j0 U(-1, 1) per node and
+    component; "none": J = 0.  The reference converts element current densities to nodes with
+    range-model-lib's convertElementToNodeVector (src/rsolvermagnetostatics.cpp:38-40); the nodal
+    field is the input here.
+    """
+    mesh = box_tet_mesh(n, n, n)
+    nn = mesh.n_nodes
+    x, y = mesh.xyz[:, 0], mesh.xyz[:, 1]
+    if current == "coil":
+        inside = (x - 0.5) ** 2 + (y - 0.5) ** 2 < 1.0 / 16.0
+        J = np.stack([-(y - 0.5), x - 0.5, np.zeros(nn)], axis=1) * j0 * inside[:, None]
+    elif current == "random":
+        J = (uniform(seed, 5, 3 * nn, -1.0, 1.0) * j0).reshape(nn, 3)
+    elif current == "none":
+        J = np.zeros((nn, 3))
+    else:
+        raise ValueError(current)
+    disabled = (x == 0.0) | (x == 1.0)
+    A = np.zeros((nn, 3))
+    A[x == 0.0] = np.asarray(a0, float)
+    A[x == 1.0] = np.asarray(a1, float)
+    book, n_free = node_book(np.repeat(disabled, 3))
+    return MagnetostaticProblem(mesh, J.reshape(-1).copy(), A.reshape(-1).copy(), disabled, book, n_free,
+                                name=f"magnetostatic_cube_{n}")
+
+
 def reseed_heat(p: HeatProblem, *, sigma: float, seed: int, mu: float = 0.0) -> HeatProblem:
     """p with a new lognormal(mu, sigma) conductivity field and random source drawn from seed
     (same mesh, node book and boundary values; the streams heat_cube uses for that seed)."""

@@ -180,3 +180,71 @@ def test_electrostatics_through_the_heat_plan(ctx, torch_cuda):
     Ao, bo = O.assemble_heat(q)
     compare(device_csr(ctx, torch, M), b.cpu().numpy(), Ao, bo)
     asm.close()
+
+
+def run_magneto(ctx, torch, p):
+    asm = rsg.Assembly.magnetostatics(ctx, p)
+    b = torch.empty(p.n_free, dtype=torch.float64, device="cuda")
+    M = asm.assemble(p, b)
+    ctx.sync()
+    return asm, M, b
+
+
+@pytest.mark.parametrize("current", ["coil", "random"])
+def test_magnetostatics_matches_oracle(ctx, torch_cuda, current):
+    # RSolverMagnetostatics::prepare + assemblyMatrix (src/rsolvermagnetostatics.cpp:44-145, :234-287)
+    torch = torch_cuda
+    p = W.magnetostatic_cube(7, current=current, seed=3, a1=(0.2, -0.1, 0.4))
+    asm, M, b = run_magneto(ctx, torch, p)
+    Ao, bo = O.assemble_magnetostatics(p)
+    assert asm.n_free == Ao.n and asm.nnz == Ao.nnz
+    Ag = device_csr(ctx, torch, M)
+    compare(Ag, b.cpu().numpy(), Ao, bo)
+    # entries coupling different components are exact zeros (rows and columns are 3 * position + component)
+    rows = np.repeat(np.arange(Ag.n), np.diff(Ag.rp.astype(np.int64)))
+    cross = rows % 3 != Ag.ci.astype(np.int64) % 3
+    assert cross.sum() == 2 * (~cross).sum() and not Ag.val[cross].any()
+    # the solve the reference runs on it (CG + Jacobi, :151-153); the matrix is negative definite
+    conf = rsg.make_conf(n_outer=20000, stop_rule="true", rtol=1e-10)
+    x, st = ctx.solve(M, b.cpu().numpy(), conf=conf, prec=rsg.PREC_JACOBI)
+    assert st.true_relres <= 1e-10
+    xo, _ = O.solve(Ao, bo, prec=1, n_outer=20000, stop_rule="true", rtol=1e-12)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-8
+
+
+def test_magnetostatics_thread_local_rows_match_global(ctx, torch_cuda, monkeypatch):
+    torch = torch_cuda
+    p = W.magnetostatic_cube(6, current="random", seed=5, a0=(0.1, 0.2, 0.3))
+    _, M, b = run_magneto(ctx, torch, p)
+    v_local, b_local = device_csr(ctx, torch, M).val.copy(), b.cpu().numpy()
+    monkeypatch.setenv("RSG_ASM_ROW_THREADS", "1")
+    _, M2, b2 = run_magneto(ctx, torch, p)
+    assert np.array_equal(device_csr(ctx, torch, M2).val, v_local)
+    assert np.array_equal(b2.cpu().numpy(), b_local)
+
+
+def test_magnetostatics_patch_test_and_book_check(ctx, torch_cuda):
+    torch = torch_cuda
+    p = W.magnetostatic_cube(6, current="none", a1=(1.0, -2.0, 3.0))
+    asm, M, b = run_magneto(ctx, torch, p)
+    x, st = ctx.solve(M, b.cpu().numpy(), conf=rsg.make_conf(n_outer=20000, stop_rule="true", rtol=1e-13),
+                      prec=rsg.PREC_JACOBI)
+    full = p.node_a.copy()
+    free = p.book != W.EOD
+    full[free] = x[p.book[free]]
+    assert np.abs(full - np.outer(p.mesh.xyz[:, 0], [1.0, -2.0, 3.0]).reshape(-1)).max() < 1e-9
+    # the solution back into the nodal field on the device
+    xd = torch.tensor(x, device="cuda")
+    nodal = torch.tensor(p.node_a, device="cuda")
+    torch.cuda.synchronize()
+    ctx.check(ctx.lib.rsg_assembly_scatter(ctx.h, asm.h, rsg._ptr(xd), rsg._ptr(nodal)), "assembly_scatter")
+    ctx.sync()
+    assert np.array_equal(nodal.cpu().numpy(), full)
+    # one node book position per node: a node with one component disabled is rejected
+    q = W.magnetostatic_cube(3, current="none")
+    bad = q.book.copy()
+    inner = int(np.flatnonzero(~q.disabled)[0])
+    bad[3 * inner + 1] = W.EOD
+    with pytest.raises(rsg.RsgError):
+        q.book = bad
+        rsg.Assembly.magnetostatics(ctx, q)

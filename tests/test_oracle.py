@@ -150,6 +150,46 @@ def test_stress_clamped_beam_solves():
     assert uz.min() < 0  # the free end moves down under the -z traction
 
 
+def test_magnetostatic_assembly_structure():
+    # RSolverMagnetostatics (src/rsolvermagnetostatics.cpp:94-105, :256-286): each component carries
+    # minus the unit-conductivity heat Laplacian; the zero blocks between components are in the pattern
+    p = W.magnetostatic_cube(4, current="random", seed=2)
+    A, b = O.assemble_magnetostatics(p)
+    h = W.heat_cube(4, source="none")
+    H, _ = O.assemble_heat(h)
+    assert A.n == 3 * H.n and len(A.ci) == 9 * len(H.ci)
+    D, DH = A.to_dense(), H.to_dense()
+    for c in range(3):
+        for d in range(3):
+            blk = D[c::3, d::3]
+            if c == d:
+                assert np.array_equal(blk, -DH)  # bitwise: same products, negated
+            else:
+                assert not blk.any()
+    # the source e0 V/4 (grad N_m x J_m) sums grad N_m over a node's tets: zero at interior nodes
+    # for a uniform current, so only boundary rows carry it
+    q = W.magnetostatic_cube(4, current="none")
+    q.node_j = np.tile([1.0e6, -2.0e6, 0.5e6], q.mesh.n_nodes)
+    _, bq = O.assemble_magnetostatics(q)
+    xyz = q.mesh.xyz
+    interior = np.all((xyz > 0.0) & (xyz < 1.0), axis=1)
+    pos = q.book[3 * np.flatnonzero(interior)]
+    scale = np.abs(bq).max()
+    assert scale > 0 and np.abs(bq[pos[:, None] + np.arange(3)]).max() <= 1e-12 * scale
+
+
+def test_magnetostatic_patch_test_linear_potential():
+    # no current, A = 0 on x=0 and (1, -2, 3) on x=1: P1 reproduces the linear potential exactly
+    p = W.magnetostatic_cube(5, current="none", a1=(1.0, -2.0, 3.0))
+    A, b = O.assemble_magnetostatics(p)
+    x, st = O.solve(A, b, prec=1, n_outer=5000, stop_rule="true", rtol=1e-13)
+    full = p.node_a.copy()
+    free = p.book != W.EOD
+    full[free] = x[p.book[free]]
+    expect = np.outer(p.mesh.xyz[:, 0], [1.0, -2.0, 3.0]).reshape(-1)
+    assert np.abs(full - expect).max() < 1e-10
+
+
 def test_rng_is_counter_based():
     a = W.uniform(7, 1, 1000)
     b = W.uniform(7, 1, 1000)
