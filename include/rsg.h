@@ -201,7 +201,9 @@ RSG_API rsg_status rsg_solve_multi(rsg_context *ctx, rsg_csr *A, const rsg_solve
  * candidate too.  The choice stays with A for every later solve.  cache_path
  * (may be NULL): a text file keyed by device, matrix shape and layout; a
  * matching line is used without timing, a new result is appended.  Tuning
- * allocates two n-vectors for the duration of the call. */
+ * allocates two n-vectors for the duration of the call.  After the grids, the
+ * tuner also times the loop with programmatic dependent launch switched the other
+ * way from its default (on for n <= 262144 rows, where launch latency dominates). */
 typedef struct rsg_tune_info {
     int32_t  tuned;                  /* 1 when A carries autotuned shapes */
     int32_t  from_cache;
@@ -211,7 +213,8 @@ typedef struct rsg_tune_info {
     double   seconds_iter_fp64, seconds_iter_fp32;                   /* per CG iteration, chosen shapes */
     double   seconds_iter_fp64_default, seconds_iter_fp32_default;   /* per CG iteration, built-in shapes */
     uint32_t candidates;             /* timed solves */
-    int32_t  reserved[3];
+    int32_t  pdl_fp64, pdl_fp32;     /* 1: the CG loop's kernels use programmatic dependent launch */
+    int32_t  reserved[1];
 } rsg_tune_info;
 RSG_API rsg_status rsg_autotune(rsg_context *ctx, rsg_csr *A, const char *cache_path, rsg_tune_info *out);
 RSG_API rsg_status rsg_tune_get(const rsg_csr *A, rsg_tune_info *out);

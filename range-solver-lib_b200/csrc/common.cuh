@@ -68,6 +68,7 @@ struct rsg_csr {
         bool from_cache = false;
         int32_t rpw = 0;              // CSR-stream rows per warp chunk (<= the largest that fits)
         int32_t g_dir64 = 0, g_dir32 = 0, g_upd64 = 0, g_upd32 = 0;
+        int32_t pdl64 = -1, pdl32 = -1;  // programmatic dependent launch in the CG loop: 1/0, -1 size default
         double it64 = 0, it32 = 0;    // seconds per CG iteration with these shapes
         double it64_default = 0, it32_default = 0;
         uint32_t candidates = 0;
@@ -112,6 +113,14 @@ int grid_for(rsg_context *ctx, const void *kernel, int block, size_t smem, long 
 // ---------------- device helpers ----------------
 
 // std::isnormal on the device: finite, non-zero and not subnormal (false for NaN).
+// Programmatic dependent launch.  A kernel launched with the programmatic stream
+// serialization attribute may be scheduled while its predecessor drains; pdl_wait()
+// blocks until the predecessor has completed and its writes are visible (it returns at
+// once for a normal launch), so it comes before the first access to anything the
+// predecessor writes.  pdl_release() lets the successor be scheduled early.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 __device__ __forceinline__ bool dev_isnormal(double v)
 {
     const double a = fabs(v);

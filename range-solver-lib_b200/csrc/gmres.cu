@@ -30,6 +30,8 @@ __global__ void __launch_bounds__(kBlock) k_gm_residual(Csr<double> M, Sell<doub
                                                         double *__restrict__ H, double *__restrict__ g,
                                                         double *partials, GmresState *st)
 {
+    pdl_wait();
+    pdl_release();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double sh[96];
     if (st->done) return;
@@ -98,6 +100,8 @@ __global__ void __launch_bounds__(kBlock) k_gm_vz(uint32_t n, uint32_t w_, const
                                                   const double *__restrict__ wnorm, T *__restrict__ V,
                                                   T *__restrict__ Z, const GmresState *st, uint32_t k)
 {
+    pdl_wait();
+    pdl_release();
     if (st->done || st->inner_done) return;
     const double s = (k == 0) ? st->beta : wnorm[k];
     T *v = V + size_t(k) * n, *z = Z + size_t(k) * n;
@@ -126,6 +130,8 @@ template <int RPW, typename T>
 __global__ void __launch_bounds__(kBlock) k_gm_spmv(Csr<T> M, Sell<T> S, int use_sell, const T *__restrict__ Z,
                                                     T *__restrict__ wv, GmresState *st, uint32_t k)
 {
+    pdl_wait();
+    pdl_release();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (st->done || st->inner_done) return;
     const T *z = Z + size_t(k) * M.n;
@@ -141,6 +147,8 @@ __global__ void __launch_bounds__(kBlock) k_gm_dots(uint32_t n, const T *__restr
                                                     double *__restrict__ hv, double *partials, GmresState *st,
                                                     uint32_t k)
 {
+    pdl_wait();
+    pdl_release();
     __shared__ double sh[32];
     __shared__ bool is_last;
     if (st->done || st->inner_done) return;
@@ -181,6 +189,8 @@ __global__ void __launch_bounds__(kBlock) k_gm_correct(uint32_t n, const T *__re
                                                        double *__restrict__ wnorm, double *partials, GmresState *st,
                                                        uint32_t k)
 {
+    pdl_wait();
+    pdl_release();
     __shared__ double sh[32];
     __shared__ double hv[kMaxRestart + 1];
     if (st->done || st->inner_done) return;
@@ -228,6 +238,8 @@ __global__ void __launch_bounds__(kBlock) k_gm_correct(uint32_t n, const T *__re
 __global__ void k_gm_backsub(double *__restrict__ H, double *__restrict__ g, double *__restrict__ y,
                              GmresState *st)
 {
+    pdl_wait();
+    pdl_release();
     if (threadIdx.x != 0 || st->done) return;
     const uint32_t m = st->m, it = st->cycle_len;
     if (it == 0) return;
@@ -244,6 +256,8 @@ __global__ void __launch_bounds__(kBlock) k_gm_update(uint32_t n, const T *__res
                                                       const double *__restrict__ y_g, double *__restrict__ x,
                                                       GmresState *st)
 {
+    pdl_wait();
+    pdl_release();
     __shared__ double y[kMaxRestart];
     if (st->done) return;
     const uint32_t len = st->cycle_len;
@@ -258,6 +272,8 @@ __global__ void __launch_bounds__(kBlock) k_gm_update(uint32_t n, const T *__res
 
 __global__ void k_gm_cycle_end(GmresState *st)
 {
+    pdl_wait();
+    pdl_release();
     if (threadIdx.x != 0) return;
     if (st->done) return;
     st->outer++;
@@ -329,24 +345,25 @@ rsg_status run_typed(rsg_context *ctx, const GmresArgs &a, double *seconds)
 
     // One captured graph per cycle; with the learned preconditioner a second graph
     // (Jacobi z_k) is captured as the fallback.
-    auto capture = [&](rsg_learned *G, cudaGraph_t *graph, cudaGraphExec_t *exec) -> rsg_status {
+    auto capture = [&](rsg_learned *G, bool pdl, cudaGraph_t *graph, cudaGraphExec_t *exec) -> rsg_status {
         if (G) RSG_TRY(gnn_prepare(ctx, G, a.A, false));  // no allocation inside the capture
         RSG_CHECK_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-        k_gm_residual<RPW><<<g_res, kBlock, s64, ctx->stream>>>(M, S, us, a.b, a.x, a.ro, a.H, a.g, a.partials,
-                                                               a.st);
+        cudaStream_t st = ctx->stream;
+        launch_k(st, pdl, k_gm_residual<RPW>, g_res, kBlock, s64, M, S, us, a.b, a.x, a.ro, a.H, a.g, a.partials,
+                 a.st);
         for (uint32_t k = 0; k < m; k++) {
             if (a.mixed) {  // FP32 Arnoldi step
-                k_gm_vz<PK, float, float><<<g_vec, kBlock, 0, ctx->stream>>>(n, a.P.w, a.P.d32, a.ro, a.w32,
-                                                                             a.wnorm, a.V32, a.Z32, a.st, k);
-                k_gm_spmv<RPW, float><<<g_sp32, kBlock, s32, ctx->stream>>>(M32, S32, us, a.Z32, a.w32, a.st, k);
-                k_gm_dots<float><<<dim3(g_dot, k + 1), kBlock, 0, ctx->stream>>>(n, a.V32, a.w32, a.H, a.hv,
-                                                                               a.partials, a.st, k);
-                k_gm_correct<float><<<g_vec, kBlock, 0, ctx->stream>>>(n, a.V32, a.w32, a.hv, a.H, a.cs, a.sn, a.g,
-                                                                      a.wnorm, a.partials, a.st, k);
+                launch_k(st, pdl, k_gm_vz<PK, float, float>, g_vec, kBlock, 0, n, a.P.w, a.P.d32, a.ro, a.w32,
+                         a.wnorm, a.V32, a.Z32, a.st, k);
+                launch_k(st, pdl, k_gm_spmv<RPW, float>, g_sp32, kBlock, s32, M32, S32, us, a.Z32, a.w32, a.st, k);
+                launch_k(st, pdl, k_gm_dots<float>, dim3(g_dot, k + 1), kBlock, 0, n, a.V32, a.w32, a.H, a.hv,
+                         a.partials, a.st, k);
+                launch_k(st, pdl, k_gm_correct<float>, g_vec, kBlock, 0, n, a.V32, a.w32, a.hv, a.H, a.cs, a.sn, a.g,
+                         a.wnorm, a.partials, a.st, k);
                 continue;
             }
-            k_gm_vz<PK, double, double><<<g_vec, kBlock, 0, ctx->stream>>>(n, a.P.w, a.P.d, a.ro, a.w, a.wnorm,
-                                                                           a.V, a.Z, a.st, k);
+            launch_k(st, pdl, k_gm_vz<PK, double, double>, g_vec, kBlock, 0, n, a.P.w, a.P.d, a.ro, a.w, a.wnorm,
+                     a.V, a.Z, a.st, k);
             if (G) {  // flexible GMRES: z_k = M(v_k) from the network (Z is stored, src/rmatrixsolver.cpp:446)
                 const rsg_status gs =
                     gnn_forward(ctx, G, a.A, a.V + size_t(k) * n, a.Z + size_t(k) * n, nullptr, false, true);
@@ -357,16 +374,16 @@ rsg_status run_typed(rsg_context *ctx, const GmresArgs &a, double *seconds)
                     return gs;
                 }
             }
-            k_gm_spmv<RPW, double><<<g_sp, kBlock, s64, ctx->stream>>>(M, S, us, a.Z, a.w, a.st, k);
-            k_gm_dots<double><<<dim3(g_dot, k + 1), kBlock, 0, ctx->stream>>>(n, a.V, a.w, a.H, a.hv, a.partials,
-                                                                            a.st, k);
-            k_gm_correct<double><<<g_vec, kBlock, 0, ctx->stream>>>(n, a.V, a.w, a.hv, a.H, a.cs, a.sn, a.g,
-                                                                   a.wnorm, a.partials, a.st, k);
+            launch_k(st, pdl, k_gm_spmv<RPW, double>, g_sp, kBlock, s64, M, S, us, a.Z, a.w, a.st, k);
+            launch_k(st, pdl, k_gm_dots<double>, dim3(g_dot, k + 1), kBlock, 0, n, a.V, a.w, a.H, a.hv, a.partials,
+                     a.st, k);
+            launch_k(st, pdl, k_gm_correct<double>, g_vec, kBlock, 0, n, a.V, a.w, a.hv, a.H, a.cs, a.sn, a.g,
+                     a.wnorm, a.partials, a.st, k);
         }
-        k_gm_backsub<<<1, 32, 0, ctx->stream>>>(a.H, a.g, a.y, a.st);
-        if (a.mixed) k_gm_update<float><<<g_vec, kBlock, 0, ctx->stream>>>(n, a.Z32, a.y, a.x, a.st);
-        else k_gm_update<double><<<g_vec, kBlock, 0, ctx->stream>>>(n, a.Z, a.y, a.x, a.st);
-        k_gm_cycle_end<<<1, 32, 0, ctx->stream>>>(a.st);
+        launch_k(st, pdl, k_gm_backsub, 1, 32, 0, a.H, a.g, a.y, a.st);
+        if (a.mixed) launch_k(st, pdl, k_gm_update<float>, g_vec, kBlock, 0, n, a.Z32, a.y, a.x, a.st);
+        else launch_k(st, pdl, k_gm_update<double>, g_vec, kBlock, 0, n, a.Z, a.y, a.x, a.st);
+        launch_k(st, pdl, k_gm_cycle_end, 1, 32, 0, a.st);
         cudaError_t e = cudaStreamEndCapture(ctx->stream, graph);
         if (e != cudaSuccess) return set_error(ctx, RSG_ERR_CUDA, "GMRES capture: %s", cudaGetErrorString(e));
         e = cudaGraphInstantiate(exec, *graph, 0);
@@ -377,10 +394,21 @@ rsg_status run_typed(rsg_context *ctx, const GmresArgs &a, double *seconds)
         }
         return RSG_OK;
     };
+    // with programmatic dependent launch when the CG policy picks it for A, else (or if the
+    // driver refuses the programmatic edges) plain launches
+    auto capture_any = [&](rsg_learned *G, cudaGraph_t *graph, cudaGraphExec_t *exec) -> rsg_status {
+        const bool pdl = pdl_for(a.A, a.mixed);
+        rsg_status r = capture(G, pdl, graph, exec);
+        if (r != RSG_OK && r != RSG_ERR_OUT_OF_MEMORY && pdl) {
+            (void)cudaGetLastError();
+            r = capture(G, false, graph, exec);
+        }
+        return r;
+    };
     cudaGraph_t graph = nullptr, graph_j = nullptr;
     cudaGraphExec_t exec = nullptr, exec_j = nullptr;
-    rsg_status s = capture(a.G, &graph, &exec);
-    if (s == RSG_OK && a.G) s = capture(nullptr, &graph_j, &exec_j);
+    rsg_status s = capture_any(a.G, &graph, &exec);
+    if (s == RSG_OK && a.G) s = capture_any(nullptr, &graph_j, &exec_j);
     if (s != RSG_OK) {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);

@@ -3,6 +3,8 @@
 
 #include "csr.cuh"
 
+#include <utility>
+
 namespace rsg {
 
 // Device-resident CG state.  Written by the last block of each kernel's grid
@@ -60,6 +62,31 @@ struct CgArgs {
 };
 
 rsg_status autotune_run(rsg_context *ctx, rsg_csr *A, const char *cache_path);
+// Programmatic dependent launch in the CG loop: the size default (n <= kPdlDefaultRows)
+// and the effective choice for A (autotuned value, else the default).
+constexpr uint32_t kPdlDefaultRows = 262144;
+inline bool pdl_default(const rsg_csr *A) { return A->n <= kPdlDefaultRows; }
+bool pdl_for(const rsg_csr *A, bool mixed);
+
+// Launch of a loop kernel; pdl adds the programmatic stream serialization attribute
+// (captured into a graph as a programmatic edge), so the kernel's blocks are scheduled
+// while its predecessor drains and wait in pdl_wait().
+template <typename... P, typename... A>
+void launch_k(cudaStream_t stream, bool pdl, void (*k)(P...), dim3 grid, int block, size_t smem, A &&...args)
+{
+    cudaLaunchAttribute at;
+    at.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at.val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(unsigned(block));
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cfg.attrs = &at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
+}
+
 rsg_status cg_run(rsg_context *ctx, const CgArgs &a, double *seconds);
 
 // ---------------- state transitions (thread 0 of the last block) ----------------

@@ -9,7 +9,8 @@
 // same graph-driven loop as a real solve, so L2 traffic between the kernels is
 // what a solve sees -- and keeps the fastest shapes in A.  The built-in
 // defaults are always a candidate, so tuning never selects shapes that were
-// measured slower than them.
+// measured slower than them.  Last, per precision, the loop is timed with
+// programmatic dependent launch switched the other way from its size default.
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -48,7 +49,7 @@ std::string tune_key(const rsg_context *ctx, const rsg_csr *A)
     for (char &c : name)
         if (c == ' ') c = '_';
     char buf[256];
-    std::snprintf(buf, sizeof(buf), "rsg-tune-v1 %s sms=%d n=%u nnz=%llu maxrow=%u sell=%d", name.c_str(),
+    std::snprintf(buf, sizeof(buf), "rsg-tune-v2 %s sms=%d n=%u nnz=%llu maxrow=%u sell=%d", name.c_str(),
                   ctx->num_sms, A->n, (unsigned long long)A->nnz, A->max_row, A->sval ? 1 : 0);
     return buf;
 }
@@ -67,8 +68,9 @@ bool tune_load(const char *path, const std::string &key, rsg_csr *A)
         rsg_csr::Tune c;
         int us = 0;
         double i64 = 0, i32 = 0;
-        if (std::sscanf(sep + 3, "sell=%d rpw=%d dir64=%d dir32=%d upd64=%d upd32=%d it_us=%lf,%lf", &us, &c.rpw,
-                        &c.g_dir64, &c.g_dir32, &c.g_upd64, &c.g_upd32, &i64, &i32) == 8) {
+        if (std::sscanf(sep + 3, "sell=%d rpw=%d dir64=%d dir32=%d upd64=%d upd32=%d pdl64=%d pdl32=%d it_us=%lf,%lf",
+                        &us, &c.rpw, &c.g_dir64, &c.g_dir32, &c.g_upd64, &c.g_upd32, &c.pdl64, &c.pdl32, &i64,
+                        &i32) == 10) {
             c.it64 = i64 * 1e-6;
             c.it32 = i32 * 1e-6;
             t = c;
@@ -90,8 +92,9 @@ void tune_store(const char *path, const std::string &key, const rsg_csr *A)
     FILE *f = std::fopen(path, "a");
     if (!f) return;
     const rsg_csr::Tune &t = A->tune;
-    std::fprintf(f, "%s : sell=%d rpw=%d dir64=%d dir32=%d upd64=%d upd32=%d it_us=%.3f,%.3f\n", key.c_str(),
-                 A->use_sell ? 1 : 0, t.rpw, t.g_dir64, t.g_dir32, t.g_upd64, t.g_upd32, t.it64 * 1e6, t.it32 * 1e6);
+    std::fprintf(f, "%s : sell=%d rpw=%d dir64=%d dir32=%d upd64=%d upd32=%d pdl64=%d pdl32=%d it_us=%.3f,%.3f\n",
+                 key.c_str(), A->use_sell ? 1 : 0, t.rpw, t.g_dir64, t.g_dir32, t.g_upd64, t.g_upd32, t.pdl64,
+                 t.pdl32, t.it64 * 1e6, t.it32 * 1e6);
     std::fclose(f);
 }
 
@@ -193,6 +196,14 @@ rsg_status autotune_run(rsg_context *ctx, rsg_csr *A, const char *cache_path)
             }
             if (s != RSG_OK) break;
             gu = bu;
+            // programmatic dependent launch: the other setting than the size default
+            int32_t &pd = prec == RSG_PRECISION_FP64 ? A->tune.pdl64 : A->tune.pdl32;
+            pd = pdl_default(A) ? 0 : 1;
+            double tp = 0;
+            if ((s = B.per_iteration(prec, &tp)) != RSG_OK) break;
+            if (tp < tbest) tbest = tp;
+            else pd = -1;
+            (prec == RSG_PRECISION_FP64 ? t.pdl64 : t.pdl32) = pd;
             (prec == RSG_PRECISION_FP64 ? t.g_dir64 : t.g_dir32) = bd;
             (prec == RSG_PRECISION_FP64 ? t.g_upd64 : t.g_upd32) = bu;
             (prec == RSG_PRECISION_FP64 ? t.it64 : t.it32) = tbest;
@@ -246,6 +257,8 @@ rsg_status rsg_tune_get(const rsg_csr *A, rsg_tune_info *out)
     out->seconds_iter_fp64_default = t.it64_default;
     out->seconds_iter_fp32_default = t.it32_default;
     out->candidates = t.candidates;
+    out->pdl_fp64 = pdl_for(A, false) ? 1 : 0;
+    out->pdl_fp32 = pdl_for(A, true) ? 1 : 0;
     return RSG_OK;
 }
 

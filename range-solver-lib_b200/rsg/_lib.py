@@ -96,7 +96,9 @@ class TuneInfo(C.Structure):
         ("seconds_iter_fp64_default", C.c_double),
         ("seconds_iter_fp32_default", C.c_double),
         ("candidates", C.c_uint32),
-        ("reserved", C.c_int32 * 3),
+        ("pdl_fp64", C.c_int32),
+        ("pdl_fp32", C.c_int32),
+        ("reserved", C.c_int32 * 1),
     ]
 
     def as_dict(self) -> dict:

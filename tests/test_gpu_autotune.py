@@ -27,6 +27,7 @@ def test_autotune_shapes_and_same_solution(ctx, system):
     for k in ("grid_dir_fp64", "grid_dir_fp32", "grid_update_fp64", "grid_update_fp32"):
         assert 0 <= info[k] <= 16384, k
     assert info["format"] in (0, 1) and info["rows_per_warp"] in (4, 8, 16, 32)
+    assert info["pdl_fp64"] in (0, 1) and info["pdl_fp32"] in (0, 1)
     # the built-in shapes are a candidate: the choice is never measured slower than them
     assert info["seconds_iter_fp64"] + info["seconds_iter_fp32"] <= \
         info["seconds_iter_fp64_default"] + info["seconds_iter_fp32_default"]
@@ -46,9 +47,10 @@ def test_autotune_cache_roundtrip(ctx, system, tmp_path):
     M2 = ctx.matrix(A.rp, A.ci, A.val)
     second = ctx.autotune(M2, path)
     assert second["from_cache"] == 1
-    for k in ("format", "rows_per_warp", "grid_dir_fp64", "grid_dir_fp32", "grid_update_fp64", "grid_update_fp32"):
+    for k in ("format", "rows_per_warp", "grid_dir_fp64", "grid_dir_fp32", "grid_update_fp64", "grid_update_fp32",
+              "pdl_fp64", "pdl_fp32"):
         assert first[k] == second[k], k
-    assert open(path).read().startswith("rsg-tune-v1 ")
+    assert open(path).read().startswith("rsg-tune-v2 ")
     x, st = ctx.solve(M2, b, conf=rsg.make_conf(n_outer=20000, stop_rule="true", rtol=1e-10))
     assert st.converged == 1
 
@@ -60,3 +62,21 @@ def test_conf_autotune_on_first_solve(ctx, system, monkeypatch):
     x, st = ctx.solve(M, b, conf=rsg.make_conf(n_outer=20000, stop_rule="true", rtol=1e-10, autotune=True))
     assert st.converged == 1 and ctx.tune_info(M)["tuned"] == 1
     assert O.true_relres(A, b, x) <= 1e-10 * 1.01
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_programmatic_launch_gives_identical_bits(ctx, system, monkeypatch, precision, use_graph):
+    # programmatic dependent launch only changes when the loop's blocks are scheduled: every
+    # kernel waits for its predecessor before touching its data, so the solve is bitwise the same
+    A, b = system
+    assert A.n <= 262144  # PDL is on by default at this size
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    conf = rsg.make_conf(n_outer=20000, stop_rule="true", rtol=1e-10, precision=precision, use_graph=use_graph)
+    assert ctx.tune_info(M)["pdl_fp64"] == 1 and ctx.tune_info(M)["pdl_fp32"] == 1
+    x_pdl, st_pdl = ctx.solve(M, b, conf=conf)
+    monkeypatch.setenv("RSG_NO_PDL", "1")
+    assert ctx.tune_info(M)["pdl_fp64"] == 0
+    x_plain, st_plain = ctx.solve(M, b, conf=conf)
+    assert st_pdl.iterations == st_plain.iterations and (x_pdl == x_plain).all()
+    assert O.true_relres(A, b, x_pdl) <= 1e-10 * 1.01
