@@ -179,8 +179,17 @@ __device__ __forceinline__ void finalize_update_mixed(CgState *st, double rz, do
     }
 }
 
+// Residual replacement keeps the search direction while the FP32 recurrence tracked the
+// true residual.  When the true residual comes back more than kRestartGap times larger
+// than the recurrence claimed, the recurrence has drifted too far for the old direction
+// to stay conjugate to the new residual (stiff systems in FP32: on the 64x32x32
+// elasticity beam with a 1e-3 refresh factor the claimed 9.7e-4 was really 1.3e-2, and
+// the continued recurrence then stalled near 1e-2), so the direction restarts from z.
+constexpr double kRestartGap = 2.0;
+
 __device__ __forceinline__ void finalize_check_mixed(CgState *st, double rz, double rn)
 {
+    const double claimed = st->rn;  // the recurrence's residual norm that triggered this check
     st->n_updates++;
     st->fold = 1;
     st->rn = rn;
@@ -194,7 +203,7 @@ __device__ __forceinline__ void finalize_check_mixed(CgState *st, double rz, dou
     } else {
         st->max_r = rn;
         st->rho_new = rz;
-        st->beta = rz / st->rho;
+        st->beta = rn > kRestartGap * claimed ? 0.0 : rz / st->rho;
         st->need_check = 0;
         if (st->it >= st->max_it) {
             st->done = 1;

@@ -344,3 +344,20 @@ def test_csr_stream_path_agrees_with_sell_path(ctx, monkeypatch):
         x2, s2 = ctx.solve(M_csr, b, conf=conf)
         assert s1.true_relres <= 1e-11 and s2.true_relres <= 1e-11
         assert rel_err(x1, x2) < 1e-9
+
+
+@pytest.mark.parametrize("delta", [1e-2, 1e-3])
+def test_mixed_precision_stiff_elasticity_converges(ctx, delta):
+    # the 64x32x32 elasticity beam is stiff enough that the FP32 recurrence drifts from the true
+    # residual; a refresh that finds the true residual far above the claimed one restarts the
+    # search direction instead of keeping a direction that is no longer conjugate (with 1e-3
+    # the kept direction stalled near 1e-2 for 100,000 iterations)
+    p = W.stress_beam()
+    A, b = O.assemble_stress(p)
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    x64, st64 = ctx.solve(M, b, conf=rsg.make_conf(n_outer=20000, stop_rule="true", rtol=1e-10))
+    conf = rsg.make_conf(n_outer=20000, stop_rule="true", rtol=1e-10, precision="mixed", reliable_delta=delta)
+    x, st = ctx.solve(M, b, conf=conf)
+    assert st.converged == 1 and O.true_relres(A, b, x) <= 1e-10 * 1.01
+    assert st.iterations < 6000
+    assert rel_err(x, x64) < 1e-8
