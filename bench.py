@@ -253,7 +253,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--delta", type=float, default=1e-2)
+    ap.add_argument("--delta", type=float, default=1e-3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="heat100: keep the built-in launch shapes")
     ap.add_argument("--workload", default="heat100",

@@ -78,7 +78,8 @@ typedef struct {
     double   rtol;              /* for RSG_STOP_TRUE_RELRES */
     int32_t  precision;         /* rsg_precision */
     int32_t  scale_equations;   /* 1 = reference's equation scaling 1e9*||A||_F/||b|| (src/rmatrixsolver.cpp:164-184) */
-    double   reliable_delta;    /* mixed precision: refresh the FP64 residual when ||r|| drops by this factor */
+    double   reliable_delta;    /* mixed precision: refresh the FP64 residual when ||r|| drops by this factor
+                                   (default 1e-3) */
     int32_t  flexible;          /* GMRES: store Z (flexible / variable preconditioner) */
     int32_t  use_graph;         /* 1 = device-driven loop in one CUDA graph launch (default) */
     uint32_t check_interval;    /* host-driven loop: iterations per convergence poll */

@@ -651,7 +651,7 @@ rsg_status rsg_batch_solve(rsg_context *ctx, rsg_batch *B, const rsg_solver_conf
         h.eps = 0.0;
         h.cvg = conf->cvg;
         h.rtol = conf->rtol;
-        h.delta = conf->reliable_delta > 0.0 && conf->reliable_delta < 1.0 ? conf->reliable_delta : 1.0e-2;
+        h.delta = conf->reliable_delta > 0.0 && conf->reliable_delta < 1.0 ? conf->reliable_delta : kReliableDelta;
         h.sigma = 1.0;
         h.max_it = max_it;
         h.stop_rule = RSG_STOP_TRUE_RELRES;

@@ -1,5 +1,5 @@
 // Context lifetime, error strings, workspace arena, launch sizing.
-#include "common.cuh"
+#include "krylov.cuh"
 
 #include <cstring>
 
@@ -157,7 +157,7 @@ void rsg_conf_default(rsg_solver_conf *c)
     c->rtol = 1.0e-10;
     c->precision = RSG_PRECISION_FP64;
     c->scale_equations = 1;
-    c->reliable_delta = 1.0e-2;
+    c->reliable_delta = rsg::kReliableDelta;
     c->flexible = 0;
     c->use_graph = 1;
     c->check_interval = 16;

@@ -185,7 +185,15 @@ __device__ __forceinline__ void finalize_update_mixed(CgState *st, double rz, do
 // to stay conjugate to the new residual (stiff systems in FP32: on the 64x32x32
 // elasticity beam with a 1e-3 refresh factor the claimed 9.7e-4 was really 1.3e-2, and
 // the continued recurrence then stalled near 1e-2), so the direction restarts from z.
-constexpr double kRestartGap = 2.0;
+// Measured on that beam with a 1e-2 factor: 4138 iterations with a gap of 2, 2587 with
+// 1.25; heat and magnetostatic solves are unchanged between the two.
+constexpr double kRestartGap = 1.25;
+
+// Default refresh factor of the mixed-precision CG (rsg_solver_conf.reliable_delta):
+// 1e-3 measured equal or better than 1e-2 on heat (40^3 to 100^3, several seeds) and on
+// the elasticity beam (2412 against 2587 iterations), 2% more iterations on 40^3
+// magnetostatics.
+constexpr double kReliableDelta = 1.0e-3;
 
 __device__ __forceinline__ void finalize_check_mixed(CgState *st, double rz, double rn)
 {

@@ -237,7 +237,7 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
         h.cvg = c.cvg;
         h.eps = c.eps;
         h.rtol = c.rtol;
-        h.delta = c.reliable_delta > 0.0 && c.reliable_delta < 1.0 ? c.reliable_delta : 1.0e-2;
+        h.delta = c.reliable_delta > 0.0 && c.reliable_delta < 1.0 ? c.reliable_delta : kReliableDelta;
         h.sigma = 1.0;
         h.max_it = max_it;
         h.stop_rule = c.stop_rule;

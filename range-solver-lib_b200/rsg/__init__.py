@@ -35,7 +35,7 @@ def _is_device(a) -> bool:
 
 def make_conf(solver: str | int = "cg", n_outer: int = 1000, n_inner: int = 30, cvg: float = 1e-13,
               eps: float = 1e-14, stop_rule: str | int = "reference", rtol: float = 1e-10,
-              precision: str | int = "fp64", scale_equations: bool = True, reliable_delta: float = 1e-2,
+              precision: str | int = "fp64", scale_equations: bool = True, reliable_delta: float = 1e-3,
               flexible: bool = False, use_graph: bool = True, check_interval: int = 16,
               output_frequency: int = 0, output_file: str | None = None,
               l2_resident_f32: bool = False, autotune: bool = False) -> SolverConf:
