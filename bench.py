@@ -345,6 +345,8 @@ def main():
                    "assembly_numeric_from_host_arrays_s": r["asm_host_ms"] / 1e3,
                    "fp64_ms_per_iteration": r["t_fp64"] / max(st_f.iterations, 1) * 1e3,
                    "mixed_ms_per_iteration": r["t_mixed"] / max(st_m.iterations, 1) * 1e3,
+                   "mixed_loop_s": st_m.seconds_solve, "mixed_setup_s": st_m.seconds_setup,
+                   "fp64_loop_s": st_f.seconds_solve, "fp64_setup_s": st_f.seconds_setup,
                    "autotune": r["tune"]},
         "roofline": {"bound": "hbm", "kernel": "k_mx_dir (fused FP32 CG direction + SpMV)",
                      "achieved": r["achieved32"], "peak": r["peak"], "unit": "GB/s",
