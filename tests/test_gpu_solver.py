@@ -181,6 +181,54 @@ def test_gmres_nonsymmetric_block_jacobi(ctx):
     assert rel_err(x, np.linalg.solve(D, b)) < 1e-9
 
 
+def convection_diffusion(m, peclet, seed=0):
+    """7-point central-difference -div(grad u) + w . grad u on an m^3 grid (Dirichlet 0 outside),
+    with a swirling velocity field w of cell Peclet number up to `peclet`: nonsymmetric, with
+    a positive diagonal, as the systems RSolverFluid hands to GMRES are."""
+    n = m ** 3
+    h = 1.0 / (m + 1)
+    g = (np.arange(m) + 1) * h
+    X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+    w = np.stack([np.sin(np.pi * Y), -np.sin(np.pi * X), 0.5 * np.cos(np.pi * Z)], axis=-1).reshape(n, 3)
+    w *= 2.0 * peclet / h
+    idx = np.arange(n).reshape(m, m, m)
+    rows, cols, vals = [np.arange(n)], [np.arange(n)], [np.full(n, 6.0 / h ** 2)]
+    for ax in range(3):
+        for sgn in (-1, 1):
+            nb = np.roll(idx, -sgn, axis=ax)
+            sl = [slice(None)] * 3
+            sl[ax] = slice(m - 1, m) if sgn == 1 else slice(0, 1)
+            valid = np.ones((m, m, m), bool)
+            valid[tuple(sl)] = False
+            r = idx[valid]
+            rows.append(r)
+            cols.append(nb[valid])
+            vals.append(-1.0 / h ** 2 + sgn * w[r, ax] / (2.0 * h))
+    import scipy.sparse as sp
+    S = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n, n))
+    S.sort_indices()
+    A = O.CSR(n, S.indptr.astype(np.uint32), S.indices.astype(np.uint32), S.data.astype(np.float64))
+    b = np.random.default_rng(seed).uniform(0.0, 1.0, n)
+    return A, b, S
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_gmres_jacobi_on_convection_diffusion(ctx, precision):
+    # the call RSolverFluid makes (src/rsolverfluid.cpp:510-511): GMRES with scalar Jacobi on a
+    # nonsymmetric transport system
+    A, b, S = convection_diffusion(20, peclet=0.8, seed=3)
+    assert abs(S - S.T).max() > 0.1 * abs(S).max() / 6  # genuinely nonsymmetric
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    kw = dict(solver="gmres", n_outer=2000, n_inner=30, stop_rule="true", rtol=1e-10)
+    x, st = ctx.solve(M, b, conf=rsg.make_conf(precision=precision, **kw), prec=rsg.PREC_JACOBI)
+    assert st.converged == 1 and O.true_relres(A, b, x) <= 1e-10 * 1.01
+    xo, sto = O.solve(A, b, prec=1, **dict(kw, rtol=1e-12))
+    assert sto.converged == 1 and rel_err(x, xo) < 1e-8
+    if precision == "fp64":  # same algorithm as the oracle: inner-step counts agree closely
+        x2, st2 = O.solve(A, b, prec=1, **kw)
+        assert abs(int(st.iterations) - int(st2.iterations)) <= 3
+
+
 @pytest.mark.parametrize("prec,block", [(rsg.PREC_JACOBI, 1), (rsg.PREC_BLOCK_JACOBI, 2), (rsg.PREC_NONE, 1)])
 def test_gmres_mixed_precision(ctx, prec, block):
     """GMRES with FP32 Arnoldi cycles inside FP64 restarts (true residual, Hessenberg,
