@@ -257,11 +257,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="heat100: keep the built-in launch shapes")
     ap.add_argument("--workload", default="heat100",
-                    choices=["heat100", "stress", "batch256", "transient40", "learned"],
+                    choices=["heat100", "stress", "batch256", "transient40", "learned", "gmres100", "multi100"],
                     help="heat100 (default, the headline); stress: 64x32x32 elasticity beam; batch256: 256 "
                          "independent heat cubes with 8..60 hexes per side; transient40: 64 backward-Euler steps "
                          "on a 40^3 mesh; learned: train the learned preconditioner on the GPU on seeded "
-                         "60^3 lognormal heat problems, evaluate on held-out seeds and on the 100^3 system")
+                         "60^3 lognormal heat problems, evaluate on held-out seeds and on the 100^3 system; "
+                         "gmres100: restarted GMRES(30) + Jacobi on the 100^3 system, FP64 and mixed; "
+                         "multi100: k = 4, 8, 16 right-hand sides of the 100^3 matrix against single solves")
     ap.add_argument("--train-seeds", type=int, default=100, help="learned: training problems (seeds)")
     ap.add_argument("--eval-seeds", type=int, default=8, help="learned: held-out evaluation seeds")
     ap.add_argument("--learned-hex", type=int, default=60, help="learned: hexes per side of the family mesh")
@@ -418,7 +420,83 @@ def run_other(args, rank, world, local_rank, threads):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    if args.workload == "stress":
+    if args.workload in ("gmres100", "multi100"):
+        p = build_problem(seed=rank)
+        asm = rsg.Assembly.heat(ctx, p)
+        b = torch.empty(asm.n_free, dtype=torch.float64, device="cuda")
+        x = torch.zeros_like(b)
+        A = asm.assemble(p, b)
+
+    if args.workload == "gmres100":
+        res = {}
+        for precision in ("fp64", "mixed"):
+            conf = rsg.make_conf(solver="gmres", n_outer=100000, n_inner=30, stop_rule="true", rtol=RTOL,
+                                 precision=precision)
+            for _ in range(args.warmup):
+                x.zero_()
+                ctx.solve(A, b, x, conf=conf)
+            tot = 0.0
+            for _ in range(args.steps):
+                flush.fill_(1)
+                x.zero_()
+                t, (_, st) = _events_time(lambda: ctx.solve(A, b, x, conf=conf), stream)
+                tot += t
+            res[precision] = {"s": max_over_ranks(tot / args.steps), "inner_iterations": st.iterations,
+                              "restarts": st.outer, "true_relres": st.true_relres}
+        best = min(res, key=lambda k: res[k]["s"])
+        line.update({"metric": f"time-to-solve (s) at FP64 rel. residual 1e-10, GMRES(30) + Jacobi, {N_HEX}^3 heat",
+                     "value": res[best]["s"], "unit": "s", "ms_per_step": res[best]["s"] * 1e3,
+                     "higher_is_better": False, "dtype": "f64 / f32-Arnoldi",
+                     "config": {"workload": f"gmres30_heat_lognormal_{N_HEX}", "n_free": A.n, "nnz": A.nnz,
+                                "best": best, "variants": res}})
+        if world == 1 and not args.no_cpu_baseline:
+            rp, ci, val = A.to_host()
+            cycles = 3
+            xo, sto = O.solve(O.CSR(A.n, rp, ci, val), b.cpu().numpy(), prec=1, solver="gmres", n_outer=cycles,
+                              n_inner=30, stop_rule="true", rtol=RTOL, threads=threads)
+            per_inner = sto.seconds / max(sto.iterations, 1)
+            line["cpu_baseline"] = {"value": per_inner * res["fp64"]["inner_iterations"], "unit": "s",
+                                    "cores": threads, "kind": "port",
+                                    "sample": f"{cycles} restart cycles ({sto.iterations} inner steps) of the "
+                                              "oracle's FP64 GMRES(30), scaled to the GPU run's inner-step count"}
+
+    elif args.workload == "multi100":
+        conf = rsg.make_conf(n_outer=100000, stop_rule="true", rtol=RTOL)
+        rng = np.random.default_rng(rank)
+        res = {}
+        for _ in range(args.warmup):
+            x.zero_()
+            ctx.solve(A, b, x, conf=conf)
+        tot = 0.0
+        for _ in range(args.steps):
+            flush.fill_(1)
+            x.zero_()
+            t, (_, st) = _events_time(lambda: ctx.solve(A, b, x, conf=conf), stream)
+            tot += t
+        res["k1_single_solve"] = {"s_per_rhs": max_over_ranks(tot / args.steps), "iterations": st.iterations}
+        for k in (4, 8, 16):
+            B = torch.from_numpy(np.stack([b.cpu().numpy() * rng.uniform(0.5, 1.5, A.n) for _ in range(k)])).cuda()
+            X = torch.zeros_like(B)
+            for _ in range(args.warmup):
+                X.zero_()
+                ctx.solve_multi(A, B, X, conf=conf)
+            tot = 0.0
+            for _ in range(args.steps):
+                flush.fill_(1)
+                X.zero_()
+                t, (_, per, summ) = _events_time(lambda: ctx.solve_multi(A, B, X, conf=conf), stream)
+                tot += t
+            res[f"k{k}"] = {"s_per_rhs": max_over_ranks(tot / args.steps) / k, "max_iterations": summ.iterations,
+                            "worst_true_relres": max(q.true_relres for q in per)}
+        best = min(res, key=lambda q: res[q]["s_per_rhs"])
+        line.update({"metric": f"seconds per right-hand side at FP64 rel. residual 1e-10, FP64 Jacobi-PCG, "
+                               f"{N_HEX}^3 heat matrix",
+                     "value": res[best]["s_per_rhs"], "unit": "s", "ms_per_step": res[best]["s_per_rhs"] * 1e3,
+                     "higher_is_better": False, "dtype": "f64",
+                     "config": {"workload": f"multi_rhs_heat_lognormal_{N_HEX}", "n_free": A.n, "nnz": A.nnz,
+                                "best": best, "variants": res}})
+
+    elif args.workload == "stress":
         p = W.stress_beam(64, 32, 32)
         asm = rsg.Assembly.stress(ctx, p)
         b = torch.empty(asm.n_free, dtype=torch.float64, device="cuda")
