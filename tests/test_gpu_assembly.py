@@ -248,3 +248,33 @@ def test_magnetostatics_patch_test_and_book_check(ctx, torch_cuda):
     with pytest.raises(rsg.RsgError):
         q.book = bad
         rsg.Assembly.magnetostatics(ctx, q)
+
+
+@pytest.mark.parametrize("forced", ["0", "1"])
+def test_stress_rollers_match_oracle(ctx, torch_cuda, monkeypatch, forced):
+    # rollers disable a subset of a node's components (RSolverStress::generateNodeBook,
+    # src/rsolverstress.cpp:1564-1652): u_y on the y=0 face and u_z on the z=0 face, clamped at x=0;
+    # the pattern then holds 1-3 columns per neighbour node, on both row kernels
+    torch = torch_cuda
+    monkeypatch.setenv("RSG_ASM_ROW_THREADS", forced)
+    p = W.stress_beam(6, 3, 3)
+    xyz = p.mesh.xyz
+    dis = p.disabled.reshape(-1, 3).copy()
+    dis[xyz[:, 1] == 0.0, 1] = True
+    dis[xyz[:, 2] == 0.0, 2] = True
+    p.disabled = dis.reshape(-1)
+    p.book, p.n_free = W.node_book(p.disabled)
+    p.node_u = np.zeros(3 * p.mesh.n_nodes)
+    p.gravity = np.array([0.0, 0.0, -9.81])
+    asm = rsg.Assembly.stress(ctx, p)
+    b = torch.empty(p.n_free, dtype=torch.float64, device="cuda")
+    M = asm.assemble(p, b)
+    ctx.sync()
+    Ao, bo = O.assemble_stress(p)
+    assert asm.n_free == Ao.n and asm.nnz == Ao.nnz
+    compare(device_csr(ctx, torch, M), b.cpu().numpy(), Ao, bo)
+    x, st = ctx.solve(M, b.cpu().numpy(), conf=rsg.make_conf(n_outer=20000, stop_rule="true", rtol=1e-10),
+                      prec=rsg.PREC_JACOBI)
+    assert st.true_relres <= 1e-10
+    xo, _ = O.solve(Ao, bo, prec=1, n_outer=20000, stop_rule="true", rtol=1e-12)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-8
