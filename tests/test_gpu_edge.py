@@ -64,3 +64,26 @@ def test_missing_diagonal_row_gmres(ctx, torch_cuda):
     assert st.converged == 1 and O.true_relres(Z, b, x) <= 1e-10 * 1.01
     xo = np.linalg.solve(D, b)
     assert rel_err(x, xo) < 1e-8
+
+
+def test_block_jacobi_width_shrinks_to_a_divisor(ctx, torch_cuda):
+    # BLOCK_JACOBI shrinks the block width until it divides n (5 on 12 rows -> 4), as the oracle
+    # restating RMatrixPreconditioner does; the GPU build and a solve with it agree with the oracle
+    A, b = spd_banded(12, seed=5)
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    blocks = torch_cuda.empty(12 * 5, dtype=torch_cuda.float64, device="cuda")
+    torch_cuda.cuda.synchronize()
+    w = ctx.block_jacobi(M, 5, blocks)
+    ctx.sync()
+    B, w_ref = O.block_jacobi(A, 5)
+    assert w == w_ref == 4
+    assert np.allclose(blocks.cpu().numpy()[: 12 * w].reshape(12, w), B, rtol=1e-12,
+                       atol=1e-16 * np.abs(B).max())
+    A2, b2 = spd_banded(96, seed=6)
+    M2 = ctx.matrix(A2.rp, A2.ci, A2.val)
+    for precision in ("fp64", "mixed"):
+        conf = rsg.make_conf(n_outer=5000, stop_rule="true", rtol=1e-10, precision=precision)
+        x, st = ctx.solve(M2, b2, conf=conf, prec=rsg.PREC_BLOCK_JACOBI, block_size=5)
+        assert st.converged == 1 and O.true_relres(A2, b2, x) <= 1e-10 * 1.01
+        xo, _ = O.solve(A2, b2, prec=2, block_size=5, n_outer=5000, stop_rule="true", rtol=1e-13)
+        assert rel_err(x, xo) < 1e-8
