@@ -87,3 +87,24 @@ def test_block_jacobi_width_shrinks_to_a_divisor(ctx, torch_cuda):
         assert st.converged == 1 and O.true_relres(A2, b2, x) <= 1e-10 * 1.01
         xo, _ = O.solve(A2, b2, prec=2, block_size=5, n_outer=5000, stop_rule="true", rtol=1e-13)
         assert rel_err(x, xo) < 1e-8
+
+
+@pytest.mark.parametrize("solver,precision", [("cg", "fp64"), ("cg", "mixed"), ("gmres", "fp64")])
+def test_incoming_x_is_the_initial_guess(ctx, solver, precision):
+    # x is in/out and its incoming values are the initial guess (RMatrixSolver::solve scales it with
+    # b, src/rmatrixsolver.cpp:164-198): a guess near the solution converges in fewer iterations to
+    # the same answer, with the same count as the oracle started from the same guess (FP64 CG)
+    A, b = spd_banded(600, seed=9)
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    kw = dict(solver=solver, n_outer=5000, n_inner=30, stop_rule="true", rtol=1e-10)
+    conf = rsg.make_conf(precision=precision, **kw)
+    x_cold, st_cold = ctx.solve(M, b, conf=conf)
+    xo, _ = O.solve(A, b, prec=1, **dict(kw, rtol=1e-13))
+    guess = xo * (1.0 + 1e-6 * np.random.default_rng(1).standard_normal(A.n))
+    x_warm, st_warm = ctx.solve(M, b, guess.copy(), conf=conf)
+    assert st_warm.converged == 1 and O.true_relres(A, b, x_warm) <= 1e-10 * 1.01
+    assert st_warm.iterations < st_cold.iterations
+    assert rel_err(x_warm, xo) < 1e-8 and rel_err(x_cold, xo) < 1e-8
+    if solver == "cg" and precision == "fp64":
+        _, sto = O.solve(A, b, guess.copy(), prec=1, **kw)
+        assert abs(int(st_warm.iterations) - int(sto.iterations)) <= 2
