@@ -89,7 +89,11 @@ __device__ __forceinline__ void heat_adj(uint32_t t, const uint32_t *__restrict_
     double G[4][3];
     const double V = tet_geometry(xyz, tv, G);
     const double k = k_e[e];
-    for (int n = 0; n < 4; n++) Ar[n] = (G[m][0] * G[n][0] + G[m][1] * G[n][1] + G[m][2] * G[n][2]) * k * V;
+    // the row node's gradient, selected without indexing G by the run-time m (which would put G
+    // in local memory)
+    double gm[3];
+    for (int c = 0; c < 3; c++) gm[c] = m == 0 ? G[0][c] : m == 1 ? G[1][c] : m == 2 ? G[2][c] : G[3][c];
+    for (int n = 0; n < 4; n++) Ar[n] = (gm[0] * G[n][0] + gm[1] * G[n][1] + gm[2] * G[n][2]) * k * V;
     const double fe = q_e[e] * V / 4.0;
     if (transient) {
         const double rc = rhoc_e[e];
@@ -135,10 +139,14 @@ __global__ void __launch_bounds__(kBlock) k_asm_heat(
     }
 }
 
-// One thread per row with the row accumulated in a thread-local array (rows of up to
-// kLocalRowMax entries): the same per-entry order as k_asm_heat without the
-// read-modify-write round trips through global memory.
+// One thread per row with the row accumulated in shared memory (rows of up to kLocalRowMax
+// entries, the launch sizes it for the plan's longest row; entry j of a thread at
+// acc_s[j * blockDim.x + threadIdx.x]): the same per-entry order
+// as k_asm_heat without read-modify-write round trips through global memory.  A thread-local
+// array indexed by the column offset cannot stay in registers: it went through local memory,
+// 515 MB of DRAM writes per launch at 100^3 against 127 MB of results.
 constexpr uint32_t kLocalRowMax = 32;
+constexpr size_t kHeatLocalSmem = size_t(kLocalRowMax) * kBlock * sizeof(double);
 
 __global__ void __launch_bounds__(kBlock) k_asm_heat_local(
     uint32_t n_free, const uint32_t *__restrict__ row_node, const uint32_t *__restrict__ rp,
@@ -148,11 +156,12 @@ __global__ void __launch_bounds__(kBlock) k_asm_heat_local(
     const double *__restrict__ rhoc_e, const double *__restrict__ node_t, int transient, double alpha, double dt,
     double *__restrict__ val, double *__restrict__ b)
 {
+    extern __shared__ double acc_s[];
+    double *acc = acc_s + threadIdx.x;
+    const uint32_t stride = blockDim.x;
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n_free; r += gridDim.x * blockDim.x) {
-        const uint32_t a = row_node[r], start = rp[r], len = rp[r + 1] - start;
-        double acc[kLocalRowMax];
-#pragma unroll
-        for (uint32_t j = 0; j < kLocalRowMax; j++) acc[j] = 0.0;
+        const uint32_t a = row_node[r], start = rp[r], len = min(rp[r + 1] - start, kLocalRowMax);
+        for (uint32_t j = 0; j < len; j++) acc[j * stride] = 0.0;
         double bs = 0.0;
         for (uint32_t t = adj_ptr[a]; t < adj_ptr[a + 1]; t++) {
             double Ar[4], be;
@@ -161,9 +170,9 @@ __global__ void __launch_bounds__(kBlock) k_asm_heat_local(
             const uint16_t off[4] = {off4.x, off4.y, off4.z, off4.w};
             bs += be;
             for (int n = 0; n < 4; n++)
-                if (off[n] < kLocalRowMax) acc[off[n]] += Ar[n];
+                if (off[n] < len) acc[off[n] * stride] += Ar[n];
         }
-        for (uint32_t j = 0; j < len; j++) val[start + j] = acc[j];
+        for (uint32_t j = 0; j < len; j++) val[start + j] = acc[j * stride];
         b[r] = bs;
     }
 }
@@ -659,10 +668,16 @@ rsg_status rsg_assemble_heat(rsg_context *ctx, rsg_assembly *p, const double *k_
     RSG_TRY(stage_inputs(ctx, p, memory, {p->n_tets, p->n_tets, p->n_tets, p->n_nodes},
                          {k_e, q_e, transient ? rhoc_e : nullptr, node_t}, d));
     const double alpha = time ? time->alpha : 1.0, dt = time ? time->dt : 0.0;
-    auto kern = p->max_row <= kLocalRowMax && !row_threads_forced() ? k_asm_heat_local : k_asm_heat;
-    const int grid = std::min(grid_for(ctx, (const void *)kern, kBlock, 0, p->n_free), kMaxGrid * 4);
+    const bool local = p->max_row <= kLocalRowMax && !row_threads_forced();
+    auto kern = local ? k_asm_heat_local : k_asm_heat;
+    // shared memory for the plan's longest row only (15 entries on tet meshes of structured hexes)
+    const size_t smem = local ? size_t(std::max<uint32_t>(p->max_row, 1)) * kBlock * sizeof(double) : 0;
+    if (local)
+        RSG_CHECK_CUDA(ctx, cudaFuncSetAttribute(k_asm_heat_local, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 int(kHeatLocalSmem)));
+    const int grid = std::min(grid_for(ctx, (const void *)kern, kBlock, smem, p->n_free), kMaxGrid * 4);
     return assemble_into(ctx, p, A, [&](double *val) {
-        kern<<<grid, kBlock, 0, ctx->stream>>>(p->n_free, p->row_node, p->rp, p->adj_ptr, p->adj_elem, p->adj_loc,
+        kern<<<grid, kBlock, smem, ctx->stream>>>(p->n_free, p->row_node, p->rp, p->adj_ptr, p->adj_elem, p->adj_loc,
                                               reinterpret_cast<const ushort4 *>(p->adj_off), p->xyz,
                                               reinterpret_cast<const uint4 *>(p->tets), p->book, d[0], d[1], d[2],
                                               d[3], transient ? 1 : 0, alpha, dt, val, b_device);

@@ -112,7 +112,6 @@ int grid_for(rsg_context *ctx, const void *kernel, int block, size_t smem, long 
 
 // ---------------- device helpers ----------------
 
-// std::isnormal on the device: finite, non-zero and not subnormal (false for NaN).
 // Programmatic dependent launch.  A kernel launched with the programmatic stream
 // serialization attribute may be scheduled while its predecessor drains; pdl_wait()
 // blocks until the predecessor has completed and its writes are visible (it returns at
@@ -121,6 +120,7 @@ int grid_for(rsg_context *ctx, const void *kernel, int block, size_t smem, long 
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
+// std::isnormal on the device: finite, non-zero and not subnormal (false for NaN).
 __device__ __forceinline__ bool dev_isnormal(double v)
 {
     const double a = fabs(v);
