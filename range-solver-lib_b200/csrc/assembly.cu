@@ -68,6 +68,13 @@ __device__ __forceinline__ double tet_geometry(const double *__restrict__ xyz, c
     return fabs(det) / 6.0;
 }
 
+// Row m of the gradient matrix selected without indexing G by a run-time m (which would put G
+// in local memory).
+__device__ __forceinline__ void grad_row(const double G[4][3], int m, double gm[3])
+{
+    for (int c = 0; c < 3; c++) gm[c] = m == 0 ? G[0][c] : m == 1 ? G[1][c] : m == 2 ? G[2][c] : G[3][c];
+}
+
 __device__ __forceinline__ uint32_t node_of(const uint4 t, int k)
 {
     return k == 0 ? t.x : k == 1 ? t.y : k == 2 ? t.z : t.w;
@@ -89,10 +96,8 @@ __device__ __forceinline__ void heat_adj(uint32_t t, const uint32_t *__restrict_
     double G[4][3];
     const double V = tet_geometry(xyz, tv, G);
     const double k = k_e[e];
-    // the row node's gradient, selected without indexing G by the run-time m (which would put G
-    // in local memory)
     double gm[3];
-    for (int c = 0; c < 3; c++) gm[c] = m == 0 ? G[0][c] : m == 1 ? G[1][c] : m == 2 ? G[2][c] : G[3][c];
+    grad_row(G, m, gm);
     for (int n = 0; n < 4; n++) Ar[n] = (gm[0] * G[n][0] + gm[1] * G[n][1] + gm[2] * G[n][2]) * k * V;
     const double fe = q_e[e] * V / 4.0;
     if (transient) {
@@ -241,7 +246,9 @@ __device__ __forceinline__ void stress_adj(uint32_t t, int i, const uint32_t *__
     for (int p = 0; p < 6; p++)
         for (int q = 0; q < 6; q++) De[p][q] *= f;
     double Bm[6], BD[6];
-    be_row(G[m], i, Bm);
+    double gm[3];
+    grad_row(G, m, gm);
+    be_row(gm, i, Bm);
     for (int q = 0; q < 6; q++) {
         double s = 0.0;
         for (int k = 0; k < 6; k++) s += Bm[k] * De[k][q];
@@ -316,9 +323,11 @@ __global__ void __launch_bounds__(128) k_asm_stress(
     }
 }
 
-// One thread per row with the row accumulated in a thread-local array (rows of up to
-// kLocalStressRowMax entries), as k_asm_heat_local.
+// One thread per row with the row accumulated in shared memory (rows of up to
+// kLocalStressRowMax entries, the launch sizes it for the plan's longest row), as k_asm_heat_local.
 constexpr uint32_t kLocalStressRowMax = 96;
+constexpr int kStressBlock = 128;
+constexpr size_t kStressLocalSmemMax = size_t(kLocalStressRowMax) * kStressBlock * sizeof(double);
 
 __global__ void __launch_bounds__(128) k_asm_stress_local(
     uint32_t n_free, const uint32_t *__restrict__ row_node, const uint8_t *__restrict__ row_comp,
@@ -331,11 +340,13 @@ __global__ void __launch_bounds__(128) k_asm_stress_local(
     const double *__restrict__ traction, const double *__restrict__ node_u, int transient, double alpha, double dt,
     double *__restrict__ val, double *__restrict__ b)
 {
+    extern __shared__ double acc_s[];
+    double *acc = acc_s + threadIdx.x;
+    const uint32_t stride = blockDim.x;
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n_free; r += gridDim.x * blockDim.x) {
-        const uint32_t a = row_node[r], start = rp[r], len = rp[r + 1] - start;
+        const uint32_t a = row_node[r], start = rp[r], len = min(rp[r + 1] - start, kLocalStressRowMax);
         const int i = row_comp[r];
-        double acc[kLocalStressRowMax];
-        for (uint32_t j = 0; j < len; j++) acc[j] = 0.0;
+        for (uint32_t j = 0; j < len; j++) acc[j * stride] = 0.0;
         double bs = 0.0;
         for (uint32_t t = tadj_ptr[a]; t < tadj_ptr[a + 1]; t++)
             bs += traction_fe(tadj_tri[t], i, xyz, tris, traction, transient, dt);
@@ -354,11 +365,11 @@ __global__ void __launch_bounds__(128) k_asm_stress_local(
                 for (int j = 0; j < 3; j++)
                     if (mask & (1u << j)) {
                         const uint32_t pos = off[n] + rank++;
-                        if (pos < kLocalStressRowMax) acc[pos] += Ar[3 * n + j];
+                        if (pos < len) acc[pos * stride] += Ar[3 * n + j];
                     }
             }
         }
-        for (uint32_t j = 0; j < len; j++) val[start + j] = acc[j];
+        for (uint32_t j = 0; j < len; j++) val[start + j] = acc[j * stride];
         b[r] = bs;
     }
 }
@@ -381,13 +392,15 @@ __device__ __forceinline__ void magneto_adj(uint32_t t, int i, const uint32_t *_
     tv = tets[e];
     double G[4][3];
     const double V = tet_geometry(xyz, tv, G);
+    double gm[3];
+    grad_row(G, m, gm);
     for (int n = 0; n < 4; n++) {
-        const double v = (G[m][0] * G[n][0] + G[m][1] * G[n][1] + G[m][2] * G[n][2]) * V;
+        const double v = (gm[0] * G[n][0] + gm[1] * G[n][1] + gm[2] * G[n][2]) * V;
         for (int j = 0; j < 3; j++) Ar[3 * n + j] = j == i ? 0.0 - v : 0.0;
     }
-    const double js = i == 0 ? -G[m][2] * J[1] + G[m][1] * J[2]
-                    : i == 1 ? G[m][2] * J[0] - G[m][0] * J[2]
-                             : -G[m][1] * J[0] + G[m][0] * J[1];
+    const double js = i == 0 ? -gm[2] * J[1] + gm[1] * J[2]
+                    : i == 1 ? gm[2] * J[0] - gm[0] * J[2]
+                             : -gm[1] * J[0] + gm[0] * J[1];
     be = V / 4.0 * kE0 * js;
     for (int n = 0; n < 4; n++) {
         const uint32_t nd = node_of(tv, n);
@@ -396,8 +409,9 @@ __device__ __forceinline__ void magneto_adj(uint32_t t, int i, const uint32_t *_
     }
 }
 
-// One thread per row; Local: the row accumulated in a thread-local array (rows of up to
-// kLocalStressRowMax entries), else in global memory.  Same per-entry order either way.
+// One thread per row; Local: the row accumulated in shared memory (rows of up to
+// kLocalStressRowMax entries, sized for the plan's longest row), else in global memory.  Same
+// per-entry order either way.
 template <bool Local>
 __global__ void __launch_bounds__(128) k_asm_magneto(
     uint32_t n_free, const uint32_t *__restrict__ row_node, const uint8_t *__restrict__ row_comp,
@@ -407,12 +421,15 @@ __global__ void __launch_bounds__(128) k_asm_magneto(
     const double *__restrict__ node_j, const double *__restrict__ node_a, double *__restrict__ val,
     double *__restrict__ b)
 {
+    extern __shared__ double acc_s[];  // Local only
+    double *acc = acc_s + threadIdx.x;
+    const uint32_t stride = blockDim.x;
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n_free; r += gridDim.x * blockDim.x) {
-        const uint32_t a = row_node[r], start = rp[r], len = rp[r + 1] - start;
+        const uint32_t a = row_node[r], start = rp[r];
+        const uint32_t len = Local ? min(rp[r + 1] - start, kLocalStressRowMax) : rp[r + 1] - start;
         const int i = row_comp[r];
-        double acc[Local ? kLocalStressRowMax : 1];
         if (Local) {
-            for (uint32_t j = 0; j < len; j++) acc[j] = 0.0;
+            for (uint32_t j = 0; j < len; j++) acc[j * stride] = 0.0;
         } else {
             for (uint32_t j = 0; j < len; j++) val[start + j] = 0.0;
         }
@@ -433,7 +450,7 @@ __global__ void __launch_bounds__(128) k_asm_magneto(
                     if (mask & (1u << j)) {
                         const uint32_t pos = off[n] + rank++;
                         if (Local) {
-                            if (pos < kLocalStressRowMax) acc[pos] += Ar[3 * n + j];
+                            if (pos < len) acc[pos * stride] += Ar[3 * n + j];
                         } else {
                             val[start + pos] += Ar[3 * n + j];
                         }
@@ -441,7 +458,7 @@ __global__ void __launch_bounds__(128) k_asm_magneto(
             }
         }
         if (Local)
-            for (uint32_t j = 0; j < len; j++) val[start + j] = acc[j];
+            for (uint32_t j = 0; j < len; j++) val[start + j] = acc[j * stride];
         b[r] = bs;
     }
 }
@@ -700,11 +717,16 @@ rsg_status rsg_assemble_stress(rsg_context *ctx, rsg_assembly *p, const double *
                           size_t(p->n_nodes) * 3},
                          {e_mod, nu, rho_e, gravity, texp_e, dtemp_e, p->n_tris ? traction : nullptr, node_u}, d));
     const double alpha = time ? time->alpha : 1.0, dt = time ? time->dt : 0.0;
-    auto kern = p->max_row <= kLocalStressRowMax && !row_threads_forced() ? k_asm_stress_local : k_asm_stress;
-    const int block = 128;
-    const int grid = std::min(grid_for(ctx, (const void *)kern, block, 0, p->n_free), kMaxGrid * 4);
+    const bool local = p->max_row <= kLocalStressRowMax && !row_threads_forced();
+    auto kern = local ? k_asm_stress_local : k_asm_stress;
+    const int block = kStressBlock;
+    const size_t smem = local ? size_t(std::max<uint32_t>(p->max_row, 1)) * block * sizeof(double) : 0;
+    if (local)
+        RSG_CHECK_CUDA(ctx, cudaFuncSetAttribute(k_asm_stress_local, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 int(kStressLocalSmemMax)));
+    const int grid = std::min(grid_for(ctx, (const void *)kern, block, smem, p->n_free), kMaxGrid * 4);
     return assemble_into(ctx, p, A, [&](double *val) {
-        kern<<<grid, block, 0, ctx->stream>>>(
+        kern<<<grid, block, smem, ctx->stream>>>(
             p->n_free, p->row_node, p->row_comp, p->rp, p->adj_ptr, p->adj_elem, p->adj_loc,
             reinterpret_cast<const ushort4 *>(p->adj_off), p->tadj_ptr, p->tadj_tri, p->node_mask, p->xyz,
             reinterpret_cast<const uint4 *>(p->tets), p->tris, p->book, d[0], d[1], d[2], d[3], d[4], d[5], d[6],
@@ -722,10 +744,14 @@ rsg_status rsg_assemble_magnetostatics(rsg_context *ctx, rsg_assembly *p, const 
     RSG_TRY(stage_inputs(ctx, p, memory, {size_t(p->n_nodes) * 3, size_t(p->n_nodes) * 3}, {node_j, node_a}, d));
     const bool local = p->max_row <= kLocalStressRowMax && !row_threads_forced();
     auto kern = local ? k_asm_magneto<true> : k_asm_magneto<false>;
-    const int block = 128;
-    const int grid = std::min(grid_for(ctx, (const void *)kern, block, 0, p->n_free), kMaxGrid * 4);
+    const int block = kStressBlock;
+    const size_t smem = local ? size_t(std::max<uint32_t>(p->max_row, 1)) * block * sizeof(double) : 0;
+    if (local)
+        RSG_CHECK_CUDA(ctx, cudaFuncSetAttribute(k_asm_magneto<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 int(kStressLocalSmemMax)));
+    const int grid = std::min(grid_for(ctx, (const void *)kern, block, smem, p->n_free), kMaxGrid * 4);
     return assemble_into(ctx, p, A, [&](double *val) {
-        kern<<<grid, block, 0, ctx->stream>>>(p->n_free, p->row_node, p->row_comp, p->rp, p->adj_ptr, p->adj_elem,
+        kern<<<grid, block, smem, ctx->stream>>>(p->n_free, p->row_node, p->row_comp, p->rp, p->adj_ptr, p->adj_elem,
                                               p->adj_loc, reinterpret_cast<const ushort4 *>(p->adj_off),
                                               p->node_mask, p->xyz, reinterpret_cast<const uint4 *>(p->tets),
                                               p->book, d[0], d[1], val, b_device);

@@ -367,9 +367,12 @@ class Assembly:
             s = self.ctx.lib.rsg_assemble_magnetostatics(self.ctx.h, self.h, *[_ptr(a) for a in args], mem,
                                                          C.byref(hA), _ptr(b_dev))
         else:
-            args = [np.ascontiguousarray(a, np.float64) for a in (p.e_mod, p.nu, p.rho_e, p.gravity, p.texp_e,
-                                                                  p.dtemp_e, p.traction, p.node_u)]
-            s = self.ctx.lib.rsg_assemble_stress(self.ctx.h, self.h, *[_ptr(a) for a in args], C.byref(tm), MEM_HOST,
+            keys = ("e_mod", "nu", "rho_e", "gravity", "texp_e", "dtemp_e", "traction", "node_u")
+            if inputs_on_device:
+                args, mem = [inputs_on_device[k] for k in keys], MEM_DEVICE
+            else:
+                args, mem = [np.ascontiguousarray(getattr(p, k), np.float64) for k in keys], MEM_HOST
+            s = self.ctx.lib.rsg_assemble_stress(self.ctx.h, self.h, *[_ptr(a) for a in args], C.byref(tm), mem,
                                                  C.byref(hA), _ptr(b_dev))
         self.ctx.check(s, f"assemble_{self.kind}")
         if self.A is None:
