@@ -345,7 +345,8 @@ RSG_API rsg_status rsg_assembly_create_stress(rsg_context *ctx, uint32_t n_nodes
 /* Magnetostatics (vector potential): 3 interleaved DOFs per node (3 * position + component) with a
  * node's three DOFs enabled or disabled together -- one node book position per node, as
  * RSolverMagnetostatics::prepare/assemblyMatrix use it (src/rsolvermagnetostatics.cpp:46, :245, :261);
- * a book that disables some but not all of a node's components is rejected.  The pattern holds full
+ * a book that disables some but not all of a node's components, or places them elsewhere than at
+ * 3 * position + c, is rejected.  The pattern holds full
  * 3x3 blocks per node pair, the reference's zero entries between components included (:272-282). */
 RSG_API rsg_status rsg_assembly_create_magnetostatics(rsg_context *ctx, uint32_t n_nodes, const double *xyz,
                                                       uint32_t n_tets, const uint32_t *tets, const uint32_t *book,

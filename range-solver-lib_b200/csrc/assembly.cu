@@ -409,10 +409,7 @@ __device__ __forceinline__ void magneto_adj(uint32_t t, int i, const uint32_t *_
     }
 }
 
-// One thread per row; Local: the row accumulated in shared memory (rows of up to
-// kLocalStressRowMax entries, sized for the plan's longest row), else in global memory.  Same
-// per-entry order either way.
-template <bool Local>
+// One thread per row, the row accumulated in global memory (any row length).
 __global__ void __launch_bounds__(128) k_asm_magneto(
     uint32_t n_free, const uint32_t *__restrict__ row_node, const uint8_t *__restrict__ row_comp,
     const uint32_t *__restrict__ rp, const uint32_t *__restrict__ adj_ptr, const uint32_t *__restrict__ adj_elem,
@@ -421,18 +418,10 @@ __global__ void __launch_bounds__(128) k_asm_magneto(
     const double *__restrict__ node_j, const double *__restrict__ node_a, double *__restrict__ val,
     double *__restrict__ b)
 {
-    extern __shared__ double acc_s[];  // Local only
-    double *acc = acc_s + threadIdx.x;
-    const uint32_t stride = blockDim.x;
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n_free; r += gridDim.x * blockDim.x) {
-        const uint32_t a = row_node[r], start = rp[r];
-        const uint32_t len = Local ? min(rp[r + 1] - start, kLocalStressRowMax) : rp[r + 1] - start;
+        const uint32_t a = row_node[r], start = rp[r], len = rp[r + 1] - start;
         const int i = row_comp[r];
-        if (Local) {
-            for (uint32_t j = 0; j < len; j++) acc[j * stride] = 0.0;
-        } else {
-            for (uint32_t j = 0; j < len; j++) val[start + j] = 0.0;
-        }
+        for (uint32_t j = 0; j < len; j++) val[start + j] = 0.0;
         const double J[3] = {node_j[3 * size_t(a)], node_j[3 * size_t(a) + 1], node_j[3 * size_t(a) + 2]};
         double bs = 0.0;
         for (uint32_t t = adj_ptr[a]; t < adj_ptr[a + 1]; t++) {
@@ -447,19 +436,70 @@ __global__ void __launch_bounds__(128) k_asm_magneto(
                 const uint8_t mask = node_mask[node_of(tv, n)];
                 uint32_t rank = 0;
                 for (int j = 0; j < 3; j++)
-                    if (mask & (1u << j)) {
-                        const uint32_t pos = off[n] + rank++;
-                        if (Local) {
-                            if (pos < len) acc[pos * stride] += Ar[3 * n + j];
-                        } else {
-                            val[start + pos] += Ar[3 * n + j];
-                        }
-                    }
+                    if (mask & (1u << j)) val[start + off[n] + rank++] += Ar[3 * n + j];
             }
         }
-        if (Local)
-            for (uint32_t j = 0; j < len; j++) val[start + j] = acc[j * stride];
         b[r] = bs;
+    }
+}
+
+// One thread per free node.  Its three component rows (3p, 3p+1, 3p+2: a node's components are
+// enabled or disabled together, checked when the plan is made) share the column pattern, the
+// element geometry and the -(grad N_m . grad N_n) V values of the diagonal blocks, so each
+// adjacent tet's geometry is computed once for the three rows, and one shared-memory slot per
+// neighbour node accumulates the diagonal-block value.  Entry (n, j) of row i is that sum when
+// j == i and an exact +0.0 otherwise; the right-hand side of each row follows magneto_adj's
+// sequence.  The bits equal the row kernel's (tests compare them).
+__global__ void __launch_bounds__(128) k_asm_magneto_node(
+    uint32_t n_free_nodes, const uint32_t *__restrict__ row_node, const uint32_t *__restrict__ rp,
+    const uint32_t *__restrict__ adj_ptr, const uint32_t *__restrict__ adj_elem, const uint8_t *__restrict__ adj_loc,
+    const ushort4 *__restrict__ adj_off, const double *__restrict__ xyz, const uint4 *__restrict__ tets,
+    const uint32_t *__restrict__ book, const double *__restrict__ node_j, const double *__restrict__ node_a,
+    double *__restrict__ val, double *__restrict__ b)
+{
+    extern __shared__ double acc_s[];
+    double *acc = acc_s + threadIdx.x;
+    const uint32_t stride = blockDim.x;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n_free_nodes; q += gridDim.x * blockDim.x) {
+        const uint32_t r0 = 3 * q, a = row_node[r0], len = rp[r0 + 1] - rp[r0];
+        const uint32_t slots = min(len / 3, kLocalStressRowMax / 3);
+        for (uint32_t s = 0; s < slots; s++) acc[s * stride] = 0.0;
+        const double J[3] = {node_j[3 * size_t(a)], node_j[3 * size_t(a) + 1], node_j[3 * size_t(a) + 2]};
+        double bs[3] = {0.0, 0.0, 0.0};
+        for (uint32_t t = adj_ptr[a]; t < adj_ptr[a + 1]; t++) {
+            const uint32_t e = adj_elem[t];
+            const int m = adj_loc[t];
+            const uint4 tv = tets[e];
+            double G[4][3];
+            const double V = tet_geometry(xyz, tv, G);
+            double gm[3];
+            grad_row(G, m, gm);
+            double dv[4];  // diagonal-block value of the pair (m, n)
+            for (int n = 0; n < 4; n++) dv[n] = 0.0 - (gm[0] * G[n][0] + gm[1] * G[n][1] + gm[2] * G[n][2]) * V;
+            const double js[3] = {-gm[2] * J[1] + gm[1] * J[2], gm[2] * J[0] - gm[0] * J[2],
+                                  -gm[1] * J[0] + gm[0] * J[1]};
+            double be[3];
+            for (int i = 0; i < 3; i++) be[i] = V / 4.0 * kE0 * js[i];
+            for (int n = 0; n < 4; n++) {
+                const uint32_t nd = node_of(tv, n);
+                if (book[3 * size_t(nd)] == RSG_EOD)
+                    for (int i = 0; i < 3; i++)
+                        for (int j = 0; j < 3; j++) be[i] -= (j == i ? dv[n] : 0.0) * node_a[3 * size_t(nd) + j];
+            }
+            for (int i = 0; i < 3; i++) bs[i] += be[i];
+            const ushort4 off4 = adj_off[t];
+            const uint16_t off[4] = {off4.x, off4.y, off4.z, off4.w};
+            for (int n = 0; n < 4; n++)
+                if (off[n] != 0xffffu && off[n] / 3u < slots) acc[(off[n] / 3u) * stride] += dv[n];
+        }
+        for (int i = 0; i < 3; i++) {
+            const uint32_t start = rp[r0 + i];
+            for (uint32_t s = 0; s < slots; s++) {
+                const double d = acc[s * stride];
+                for (int j = 0; j < 3; j++) val[start + 3 * s + j] = j == i ? d : 0.0;
+            }
+            b[r0 + i] = bs[i];
+        }
     }
 }
 
@@ -642,13 +682,17 @@ rsg_status rsg_assembly_create_magnetostatics(rsg_context *ctx, uint32_t n_nodes
 {
     if (!ctx || !book || !out) return set_error(ctx, RSG_ERR_INVALID_ARG, "assembly_create_magnetostatics: bad arguments");
     // one node book position per node (src/rsolvermagnetostatics.cpp:245, :261): the three
-    // potential components of a node are enabled or disabled together
+    // potential components of a node are enabled or disabled together, at 3 * position + c
     for (uint32_t nd = 0; nd < n_nodes; nd++) {
         const int eod = int(book[3 * size_t(nd)] == RSG_EOD) + int(book[3 * size_t(nd) + 1] == RSG_EOD) +
                         int(book[3 * size_t(nd) + 2] == RSG_EOD);
         if (eod != 0 && eod != 3)
             return set_error(ctx, RSG_ERR_INVALID_ARG,
                              "assembly_create_magnetostatics: node %u has some but not all components disabled", nd);
+        const uint32_t p0 = book[3 * size_t(nd)];
+        if (eod == 0 && (p0 % 3 != 0 || book[3 * size_t(nd) + 1] != p0 + 1 || book[3 * size_t(nd) + 2] != p0 + 2))
+            return set_error(ctx, RSG_ERR_INVALID_ARG,
+                             "assembly_create_magnetostatics: node %u: components must sit at 3*position + c", nd);
     }
     const rsg_status s = create_plan(ctx, n_nodes, xyz, n_tets, tets, 0, nullptr, book, 3, n_free, out);
     if (s == RSG_OK) (*out)->kind = kPlanMagnetostatics;
@@ -742,19 +786,25 @@ rsg_status rsg_assemble_magnetostatics(rsg_context *ctx, rsg_assembly *p, const 
     RSG_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
     const double *d[2];
     RSG_TRY(stage_inputs(ctx, p, memory, {size_t(p->n_nodes) * 3, size_t(p->n_nodes) * 3}, {node_j, node_a}, d));
-    const bool local = p->max_row <= kLocalStressRowMax && !row_threads_forced();
-    auto kern = local ? k_asm_magneto<true> : k_asm_magneto<false>;
     const int block = kStressBlock;
-    const size_t smem = local ? size_t(std::max<uint32_t>(p->max_row, 1)) * block * sizeof(double) : 0;
-    if (local)
-        RSG_CHECK_CUDA(ctx, cudaFuncSetAttribute(k_asm_magneto<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 int(kStressLocalSmemMax)));
-    const int grid = std::min(grid_for(ctx, (const void *)kern, block, smem, p->n_free), kMaxGrid * 4);
+    if (p->max_row <= kLocalStressRowMax && !row_threads_forced()) {
+        const uint32_t nodes = p->n_free / 3;
+        const size_t smem = size_t(std::max<uint32_t>(p->max_row / 3, 1)) * block * sizeof(double);
+        const int grid = std::min(grid_for(ctx, (const void *)k_asm_magneto_node, block, smem, nodes), kMaxGrid * 4);
+        return assemble_into(ctx, p, A, [&](double *val) {
+            k_asm_magneto_node<<<grid, block, smem, ctx->stream>>>(
+                nodes, p->row_node, p->rp, p->adj_ptr, p->adj_elem, p->adj_loc,
+                reinterpret_cast<const ushort4 *>(p->adj_off), p->xyz, reinterpret_cast<const uint4 *>(p->tets),
+                p->book, d[0], d[1], val, b_device);
+        });
+    }
+    const int grid = std::min(grid_for(ctx, (const void *)k_asm_magneto, block, 0, p->n_free), kMaxGrid * 4);
     return assemble_into(ctx, p, A, [&](double *val) {
-        kern<<<grid, block, smem, ctx->stream>>>(p->n_free, p->row_node, p->row_comp, p->rp, p->adj_ptr, p->adj_elem,
-                                              p->adj_loc, reinterpret_cast<const ushort4 *>(p->adj_off),
-                                              p->node_mask, p->xyz, reinterpret_cast<const uint4 *>(p->tets),
-                                              p->book, d[0], d[1], val, b_device);
+        k_asm_magneto<<<grid, block, 0, ctx->stream>>>(p->n_free, p->row_node, p->row_comp, p->rp, p->adj_ptr,
+                                                       p->adj_elem, p->adj_loc,
+                                                       reinterpret_cast<const ushort4 *>(p->adj_off), p->node_mask,
+                                                       p->xyz, reinterpret_cast<const uint4 *>(p->tets), p->book,
+                                                       d[0], d[1], val, b_device);
     });
 }
 

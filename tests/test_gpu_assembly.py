@@ -242,11 +242,18 @@ def test_magnetostatics_patch_test_and_book_check(ctx, torch_cuda):
     assert np.array_equal(nodal.cpu().numpy(), full)
     # one node book position per node: a node with one component disabled is rejected
     q = W.magnetostatic_cube(3, current="none")
+    good = q.book.copy()
     bad = q.book.copy()
     inner = int(np.flatnonzero(~q.disabled)[0])
     bad[3 * inner + 1] = W.EOD
     with pytest.raises(rsg.RsgError):
         q.book = bad
+        rsg.Assembly.magnetostatics(ctx, q)
+    # and its three components sit at 3 * position + c
+    swapped = good.copy()
+    swapped[3 * inner], swapped[3 * inner + 1] = good[3 * inner + 1], good[3 * inner]
+    with pytest.raises(rsg.RsgError):
+        q.book = swapped
         rsg.Assembly.magnetostatics(ctx, q)
 
 
