@@ -168,7 +168,9 @@ RSG_API rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_conf
  * of the solver's kernels on matrix A over `reps` launches on the context
  * stream, measured with CUDA events.  flush_l2 != 0 writes a buffer larger
  * than L2 before every launch (excluded from the timing), giving the
- * HBM-bound time; 0 measures back-to-back launches as inside a solve. */
+ * HBM-bound time; 0 measures back-to-back launches as inside a solve.  The CG
+ * kernels are launched with the solve loop's shapes (A's autotuned grids when it
+ * has them, else the built-in defaults). */
 typedef enum {
     RSG_KERNEL_CG_DIR_FP64 = 0,    /* p = z + beta p, q = A p, p^T q   (FP64 CSR) */
     RSG_KERNEL_CG_DIR_MIXED = 1,   /* same with FP32 values and 16-bit column offsets */

@@ -759,9 +759,13 @@ rsg_status profile_typed(rsg_context *ctx, const rsg_csr *A, int kernel, uint32_
     const int us = A->use_sell;
     const long long ct = (long long)n * 32 / RPW;
     (void)ct;
-    const int g64 = spmv_grid(ctx, A, (const void *)k_cg_dir<RPW>, s64, RPW);
-    const int g32 = spmv_grid(ctx, A, (const void *)k_mx_dir<RPW>, s32, RPW);
+    // the solve loop's launch shapes: autotuned when A carries them, else the built-in defaults
+    const rsg_csr::Tune &T = A->tune;
+    const int g64 = T.valid && T.g_dir64 > 0 ? T.g_dir64 : spmv_grid(ctx, A, (const void *)k_cg_dir<RPW>, s64, RPW);
+    const int g32 = T.valid && T.g_dir32 > 0 ? T.g_dir32 : spmv_grid(ctx, A, (const void *)k_mx_dir<RPW>, s32, RPW);
     const int gv = std::min(grid_for(ctx, (const void *)k_cg_update<1>, kBlock, 0, n), kMaxGrid);
+    const int gv64 = T.valid && T.g_upd64 > 0 ? T.g_upd64 : gv;
+    const int gv32 = T.valid && T.g_upd32 > 0 ? T.g_upd32 : gv;
     const Csr<double> M64 = view<double>(A, true);
     const Csr<float> M32 = view<float>(A, true);
     auto launch = [&]() {
@@ -775,11 +779,11 @@ rsg_status profile_typed(rsg_context *ctx, const rsg_csr *A, int kernel, uint32_
                                                              v32[4], partials, st);
             break;
         case RSG_KERNEL_CG_UPDATE_FP64:
-            k_cg_update<1><<<gv, kBlock, 0, ctx->stream>>>(n, 1, v64[4], v64[0], v64[1], v64[2], v64[3], v64[4],
+            k_cg_update<1><<<gv64, kBlock, 0, ctx->stream>>>(n, 1, v64[4], v64[0], v64[1], v64[2], v64[3], v64[4],
                                                           partials, st);
             break;
         case RSG_KERNEL_CG_UPDATE_MIXED:
-            k_mx_update<1><<<gv, kBlock, 0, ctx->stream>>>(n, 1, v32[5], v32[0], v32[1], v32[2], v32[3], v32[4],
+            k_mx_update<1><<<gv32, kBlock, 0, ctx->stream>>>(n, 1, v32[5], v32[0], v32[1], v32[2], v32[3], v32[4],
                                                           partials, st);
             break;
         case RSG_KERNEL_SPMV_FP64:
