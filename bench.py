@@ -39,6 +39,10 @@ UNIT = "s"
 N_HEX = int(os.environ.get("RSG_BENCH_N", "100"))
 SIGMA = 1.5
 RTOL = 1e-10
+# DRAM bytes of one k_mx_dir launch on heat_lognormal_100 and where the figure comes from
+TRAFFIC_MX_DIR = 113.65e6
+TRAFFIC_SOURCE = ("ncu --set full capture of k_mx_dir on heat_lognormal_100, dram__bytes_read.sum + "
+                  "dram__bytes_write.sum of one launch (profiles/k_mx_dir_heat_lognormal_100.md)")
 
 
 def load_peaks() -> tuple[float, str]:
@@ -185,6 +189,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     x_m = x.clone()
     _, st_f = ctx.solve(A, b, x.zero_(), conf=conf_fp64)
     err_vs_fp64 = float(torch.linalg.norm(x_m - x) / torch.linalg.norm(x))
+    x_mixed_host, x_fp64_host = x_m.cpu().numpy(), x.cpu().numpy()
 
     # dominant kernels, timed live (HBM-bound: L2 flushed before each launch)
     kd = {}
@@ -199,8 +204,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     achieved64 = by64 / kd["cg_dir_fp64"]["cold_s"] / 1e9
     achieved32 = by32 / kd["cg_dir_mixed"]["cold_s"] / 1e9
     # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_mx_dir launch on this
-    # workload, from an ncu --set full capture of the register-capped kernel
-    traffic = 113.65e6 if N_HEX == 100 else None
+    # workload: not measurable inside this run (ncu replays kernels), so it is the figure of the
+    # ncu capture named in TRAFFIC_SOURCE, taken of the same kernel on the same workload
+    traffic = TRAFFIC_MX_DIR if N_HEX == 100 else None
 
     # launches per solve: setup (norm, 2 scalings, Jacobi, FP32 copy, init residual + z, fold,
     # unscale, true residual) + per 2-iteration graph body (3 kernels per iteration + tail)
@@ -236,6 +242,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         "clocks": sampler.summary(), "e2e_s": e2e_s, "tune": tune,
         "h2d": int(nnz * 8 + 2 * n * 8), "d2h": int(n * 8), "launches": launches(st_m, True),
         "launches_fp64": launches(st_f, False), "ctx": ctx, "A": A, "b": b, "rp": rp_h, "ci": ci_h, "val": val_h,
+        "x_mixed": x_mixed_host, "x_fp64": x_fp64_host, "problem": p,
     }
     return out
 
@@ -245,6 +252,28 @@ def cpu_baseline(rp, ci, val, b, threads: int) -> dict:
     Ah = O.CSR(len(rp) - 1, rp, ci, val)
     x, st = O.solve(Ah, b, prec=1, n_outer=50000, stop_rule="true", rtol=RTOL, threads=threads)
     return {"value": st.seconds, "iterations": st.iterations, "relres": st.true_relres}
+
+
+def oracle_check(r: dict, threads: int) -> dict:
+    """Parity of the timed GPU results with the oracle (untimed): the oracle assembles the same
+    problem on the host and solves it to a tight FP64 true residual (1e-12); the GPU matrix is
+    compared entry by entry and both GPU solutions by ||x - x_ref|| / ||x_ref|| and by the true
+    residual the oracle recomputes on its own system."""
+    from oracle import oracle as O
+    Ao, bo = O.assemble_heat(r["problem"])
+    same_pattern = bool(np.array_equal(Ao.rp, r["rp"]) and np.array_equal(Ao.ci, r["ci"]))
+    rowmax = np.maximum.reduceat(np.abs(Ao.val), Ao.rp[:-1].astype(np.int64))
+    scale = np.repeat(rowmax, np.diff(Ao.rp.astype(np.int64)))
+    entry_err = float(np.max(np.abs(r["val"] - Ao.val) / np.maximum(np.abs(Ao.val), scale))) if same_pattern else None
+    rhs_err = float(np.max(np.abs(r["b"].cpu().numpy() - bo)) / np.max(np.abs(bo)))
+    x_ref, st = O.solve(Ao, bo, prec=1, n_outer=50000, stop_rule="true", rtol=1e-12, threads=threads)
+    nref = np.linalg.norm(x_ref)
+    return {"assembly_same_pattern": same_pattern, "assembly_max_rel_entry_err": entry_err,
+            "rhs_max_rel_err": rhs_err, "oracle_tight_relres": st.true_relres,
+            "err_vs_oracle_mixed": float(np.linalg.norm(r["x_mixed"] - x_ref) / nref),
+            "err_vs_oracle_fp64": float(np.linalg.norm(r["x_fp64"] - x_ref) / nref),
+            "oracle_relres_of_mixed_x": O.true_relres(Ao, bo, r["x_mixed"]),
+            "oracle_relres_of_fp64_x": O.true_relres(Ao, bo, r["x_fp64"])}
 
 
 def main():
@@ -329,8 +358,10 @@ def main():
         return
 
     cpu = None
+    parity = None
     if world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(r["rp"], r["ci"], r["val"], r["b"].cpu().numpy(), threads)
+        parity = oracle_check(r, threads)
     st_m, st_f = r["st_m"], r["st_f"]
     kd = r["kd"]
     line = {
@@ -342,6 +373,8 @@ def main():
                    "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}",
                    "iterations": st_m.iterations, "residual_refreshes": st_m.outer,
                    "true_relres": st_m.true_relres, "err_vs_fp64_solution": r["err_vs_fp64"],
+                   "err_vs_oracle": parity["err_vs_oracle_mixed"] if parity else None,
+                   "oracle_parity": parity,
                    "plain_fp64_pcg_s": r["t_fp64"], "plain_fp64_iterations": st_f.iterations,
                    "plain_fp64_true_relres": st_f.true_relres,
                    "speedup_vs_plain_fp64": r["t_fp64"] / r["t_mixed"],
@@ -355,6 +388,7 @@ def main():
         "roofline": {"bound": "hbm", "kernel": "k_mx_dir (fused FP32 CG direction + SpMV)",
                      "achieved": r["achieved32"], "peak": r["peak"], "unit": "GB/s",
                      "frac": r["achieved32"] / r["peak"], "traffic": r["traffic"],
+                     "traffic_source": TRAFFIC_SOURCE if r["traffic"] is not None else None,
                      "algorithmic_bytes": r["by32"], "avg_launch_s": kd["cg_dir_mixed"]["cold_s"],
                      "peak_source": r["peak_kind"]},
         "roofline_fp64": {"bound": "hbm", "kernel": "k_cg_dir (fused FP64 CG direction + SpMV)",

@@ -257,9 +257,11 @@ RSG_API rsg_status rsg_true_relres(rsg_context *ctx, const rsg_csr *A, const dou
  * loads the library until the process exits; n_rows above
  * RSG_NOALLOC_MAX_ROWS is rejected with RSG_ERR_INVALID_ARG.  Calls share that
  * array: calls whose kernels overlap on the GPU race and give wrong results,
- * so order them on one stream.  The first call on a device looks up the
- * array's address with that device current; make it before any stream
- * capture.  A column index >= n_rows is not read and makes the result NaN. */
+ * so order them on one stream.  Each call looks up the array's address on
+ * the current device (no allocation), so the entry point stays usable after
+ * the application calls cudaDeviceReset; the first call on a device may load
+ * the library's device code there, so make it before any stream capture.  A
+ * column index >= n_rows is not read and makes the result NaN. */
 #define RSG_NOALLOC_MAX_ROWS 2097152u
 RSG_API rsg_status rsg_true_relres_noalloc(uint32_t n_rows, const uint32_t *row_ptr, const uint32_t *col_idx,
                                            const double *values, const double *b, const double *x, double *out3,
@@ -317,6 +319,44 @@ RSG_API rsg_status rsg_learned_loss_grad(rsg_context *ctx, rsg_learned *model, c
 /* forward (tensor cores) + backward + one Adam step with learning rate lr */
 RSG_API rsg_status rsg_learned_train_step(rsg_context *ctx, rsg_learned *model, const rsg_csr *A, const double *r,
                                           const double *xyz, float lr, double *loss);
+
+/* ---- node books (DOF numbering) ----
+ * The model's elements and element groups as plain arrays (host memory): element e has the nodes
+ * elem_nodes[elem_begin[e] .. elem_begin[e+1]) -- any element type (points, lines, triangles,
+ * tetrahedra); group g holds the elements group_elems[group_begin[g] .. group_begin[g+1]).
+ * computable (n_elements flags) marks the elements the solver computes (RSolverGeneric's
+ * computableElements); NULL = all.  Indexes out of range or decreasing begin arrays are rejected
+ * with RSG_ERR_INVALID_ARG.  The book receives the free position of every DOF in index order, or
+ * 0xffffffff (RConstants::eod) for a disabled one; *n_free the number of free DOFs.  These run on the
+ * host and need no context. */
+typedef struct {
+    uint32_t n_nodes;
+    uint32_t n_elements;
+    const uint32_t *elem_begin;   /* n_elements + 1 */
+    const uint32_t *elem_nodes;
+    uint32_t n_groups;
+    const uint32_t *group_begin;  /* n_groups + 1 */
+    const uint32_t *group_elems;
+    const uint8_t *computable;    /* n_elements, or NULL */
+} rsg_model_groups;
+
+/* RSolverGeneric::generateNodeBook + rebuildNodeBook (src/rsolvergeneric.cpp:498-582): one DOF per
+ * node; the nodes of every group with group_explicit_bc[g] != 0 (an explicit boundary condition of
+ * the problem type) and the nodes no computable element touches are disabled.  book: n_nodes. */
+RSG_API rsg_status rsg_node_book_generic(const rsg_model_groups *model, const uint8_t *group_explicit_bc,
+                                         uint32_t *book, uint32_t *n_free);
+
+/* Displacement conditions of an element group for rsg_node_book_stress (bit mask: a group may carry several). */
+enum {
+    RSG_BC_DISPLACEMENT = 1,         /* R_BOUNDARY_CONDITION_DISPLACEMENT: all three components */
+    RSG_BC_DISPLACEMENT_NORMAL = 2,  /* R_BOUNDARY_CONDITION_DISPLACEMENT_NORMAL: all three components */
+    RSG_BC_DISPLACEMENT_ROLLER = 4   /* R_BOUNDARY_CONDITION_DISPLACEMENT_ROLLER: y and z on a line group, else x */
+};
+/* RSolverStress::generateNodeBook (src/rsolverstress.cpp:1564-1652): three interleaved DOFs per node
+ * (position 3 node + component); group_bc[g] is a mask of RSG_BC_* and group_is_line[g] != 0 marks a
+ * line (edge) group.  Nodes no computable element touches lose all three components.  book: 3 n_nodes. */
+RSG_API rsg_status rsg_node_book_stress(const rsg_model_groups *model, const uint8_t *group_bc,
+                                        const uint8_t *group_is_line, uint32_t *book, uint32_t *n_free);
 
 /* ---- assembly (RSolverHeat / RSolverStress prepare + assemblyMatrix) ----
  * A plan is the sparsity pattern of the free-DOF system plus the

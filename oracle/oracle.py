@@ -75,6 +75,10 @@ def lib():
         L.orc_true_relres.argtypes = [C.c_uint32, _P, _P, _P, _P, _P]
         L.orc_node_book.restype = C.c_uint32
         L.orc_node_book.argtypes = [C.c_uint32, _P, _P]
+        L.orc_node_book_generic.restype = C.c_uint32
+        L.orc_node_book_generic.argtypes = [C.c_uint32, C.c_uint32, _P, _P, C.c_uint32, _P, _P, _P, _P, _P]
+        L.orc_node_book_stress.restype = C.c_uint32
+        L.orc_node_book_stress.argtypes = [C.c_uint32, C.c_uint32, _P, _P, C.c_uint32, _P, _P, _P, _P, _P, _P]
         L.orc_system_n.restype = C.c_uint32
         L.orc_system_n.argtypes = [_P]
         L.orc_system_nnz.restype = C.c_uint64
@@ -179,6 +183,31 @@ def solve(A: CSR, b: np.ndarray, x0: np.ndarray | None = None, *, prec: int = 1,
     if rc != 0:
         raise RuntimeError(f"oracle solve failed: {rc}")
     return x, st
+
+
+def node_book_generic(n_nodes, elem_begin, elem_nodes, group_begin, group_elems, explicit_bc, computable=None):
+    """RSolverGeneric::generateNodeBook (src/rsolvergeneric.cpp:498-582): (book, n_free)."""
+    arrs = [np.ascontiguousarray(a, np.uint32) for a in (elem_begin, elem_nodes, group_begin, group_elems)]
+    flags = np.ascontiguousarray(explicit_bc, np.uint8)
+    comp = None if computable is None else np.ascontiguousarray(computable, np.uint8)
+    book = np.empty(n_nodes, np.uint32)
+    n_free = lib().orc_node_book_generic(n_nodes, len(arrs[0]) - 1, _ptr(arrs[0]), _ptr(arrs[1]), len(arrs[2]) - 1,
+                                         _ptr(arrs[2]), _ptr(arrs[3]), None if comp is None else _ptr(comp),
+                                         _ptr(flags), _ptr(book))
+    return book, int(n_free)
+
+
+def node_book_stress(n_nodes, elem_begin, elem_nodes, group_begin, group_elems, bc, is_line, computable=None):
+    """RSolverStress::generateNodeBook (src/rsolverstress.cpp:1564-1652): (book of 3 n_nodes, n_free)."""
+    arrs = [np.ascontiguousarray(a, np.uint32) for a in (elem_begin, elem_nodes, group_begin, group_elems)]
+    bcs = np.ascontiguousarray(bc, np.uint8)
+    line = np.ascontiguousarray(is_line, np.uint8)
+    comp = None if computable is None else np.ascontiguousarray(computable, np.uint8)
+    book = np.empty(3 * n_nodes, np.uint32)
+    n_free = lib().orc_node_book_stress(n_nodes, len(arrs[0]) - 1, _ptr(arrs[0]), _ptr(arrs[1]), len(arrs[2]) - 1,
+                                        _ptr(arrs[2]), _ptr(arrs[3]), None if comp is None else _ptr(comp),
+                                        _ptr(bcs), _ptr(line), _ptr(book))
+    return book, int(n_free)
 
 
 def _system(h) -> tuple[CSR, np.ndarray]:

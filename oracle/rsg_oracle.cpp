@@ -628,6 +628,70 @@ uint32_t orc_node_book(uint32_t n, const uint8_t *disabled, uint32_t *book)
     return next;
 }
 
+/* src/rsolvergeneric.cpp:536-558: nodes of computable elements are computable, the others disabled */
+static void orc_disable_not_computable(uint32_t n_nodes, uint32_t n_elements, const uint32_t *elem_begin,
+                                       const uint32_t *elem_nodes, const uint8_t *computable, uint32_t dofs,
+                                       std::vector<uint8_t> &disabled)
+{
+    std::vector<uint8_t> computable_nodes(n_nodes, 0);
+    for (uint32_t i = 0; i < n_elements; i++)
+        if (!computable || computable[i])
+            for (uint32_t j = elem_begin[i]; j < elem_begin[i + 1]; j++) computable_nodes[elem_nodes[j]] = 1;
+    for (uint32_t i = 0; i < n_nodes; i++)
+        if (!computable_nodes[i])
+            for (uint32_t c = 0; c < dofs; c++) disabled[size_t(dofs) * i + c] = 1;
+}
+
+uint32_t orc_node_book_generic(uint32_t n_nodes, uint32_t n_elements, const uint32_t *elem_begin,
+                               const uint32_t *elem_nodes, uint32_t n_groups, const uint32_t *group_begin,
+                               const uint32_t *group_elems, const uint8_t *computable, const uint8_t *explicit_bc,
+                               uint32_t *book)
+{
+    /* src/rsolvergeneric.cpp:508-535: every node of a group with an explicit condition is disabled */
+    std::vector<uint8_t> disabled(n_nodes, 0);
+    for (uint32_t g = 0; g < n_groups; g++) {
+        if (!explicit_bc[g]) continue;
+        for (uint32_t j = group_begin[g]; j < group_begin[g + 1]; j++) {
+            const uint32_t e = group_elems[j];
+            for (uint32_t k = elem_begin[e]; k < elem_begin[e + 1]; k++) disabled[elem_nodes[k]] = 1;
+        }
+    }
+    orc_disable_not_computable(n_nodes, n_elements, elem_begin, elem_nodes, computable, 1, disabled);
+    return orc_node_book(n_nodes, disabled.data(), book);
+}
+
+uint32_t orc_node_book_stress(uint32_t n_nodes, uint32_t n_elements, const uint32_t *elem_begin,
+                              const uint32_t *elem_nodes, uint32_t n_groups, const uint32_t *group_begin,
+                              const uint32_t *group_elems, const uint8_t *computable, const uint8_t *bc,
+                              const uint8_t *is_line, uint32_t *book)
+{
+    /* src/rsolverstress.cpp:1569-1629: displacement / normal displacement disable x, y, z; a roller
+     * disables y and z on a line group, x elsewhere; groups without any of these are skipped */
+    std::vector<uint8_t> disabled(size_t(n_nodes) * 3, 0);
+    for (uint32_t g = 0; g < n_groups; g++) {
+        bool dx = false, dy = false, dz = false;
+        if (bc[g] & 3u) dx = dy = dz = true;
+        if (bc[g] & 4u) {
+            if (is_line[g]) dy = dz = true;
+            else dx = true;
+        }
+        if (!dx && !dy && !dz) continue;
+        for (uint32_t j = group_begin[g]; j < group_begin[g + 1]; j++) {
+            const uint32_t e = group_elems[j];
+            for (uint32_t k = elem_begin[e]; k < elem_begin[e + 1]; k++) {
+                const uint32_t node = elem_nodes[k];
+                if (dx) disabled[3 * size_t(node) + 0] = 1;
+                if (dy) disabled[3 * size_t(node) + 1] = 1;
+                if (dz) disabled[3 * size_t(node) + 2] = 1;
+            }
+        }
+    }
+    /* :1630-1651 */
+    orc_disable_not_computable(n_nodes, n_elements, elem_begin, elem_nodes, computable, 3, disabled);
+    /* RBook::disable renumbers the enabled positions consecutively, as rebuildNodeBook does */
+    return orc_node_book(3 * n_nodes, disabled.data(), book);
+}
+
 uint32_t orc_system_n(const orc_system *s) { return s->n; }
 uint64_t orc_system_nnz(const orc_system *s) { return s->ci.size(); }
 void orc_system_copy(const orc_system *s, uint32_t *rp, uint32_t *ci, double *val, double *b)

@@ -74,6 +74,19 @@ double orc_true_relres(uint32_t n, const uint32_t *rp, const uint32_t *ci, const
 
 /* a10: node book (RSolverGeneric::rebuildNodeBook).  book[i] = position or 0xffffffff. */
 uint32_t orc_node_book(uint32_t n, const uint8_t *disabled, uint32_t *book);
+/* RSolverGeneric::generateNodeBook (src/rsolvergeneric.cpp:498-561) + rebuildNodeBook: elements
+ * e have nodes elem_nodes[elem_begin[e]..elem_begin[e+1]); group g holds group_elems[group_begin[g]..];
+ * explicit_bc per group; computable per element (NULL = all).  Returns n_free. */
+uint32_t orc_node_book_generic(uint32_t n_nodes, uint32_t n_elements, const uint32_t *elem_begin,
+                               const uint32_t *elem_nodes, uint32_t n_groups, const uint32_t *group_begin,
+                               const uint32_t *group_elems, const uint8_t *computable, const uint8_t *explicit_bc,
+                               uint32_t *book);
+/* RSolverStress::generateNodeBook (src/rsolverstress.cpp:1564-1652): bc bit mask per group
+ * (1 displacement, 2 normal displacement, 4 roller), is_line per group.  book: 3 n_nodes. */
+uint32_t orc_node_book_stress(uint32_t n_nodes, uint32_t n_elements, const uint32_t *elem_begin,
+                              const uint32_t *elem_nodes, uint32_t n_groups, const uint32_t *group_begin,
+                              const uint32_t *group_elems, const uint8_t *computable, const uint8_t *bc,
+                              const uint8_t *is_line, uint32_t *book);
 
 /* Assembled system handle (CSR with sorted columns + RHS). */
 typedef struct orc_system orc_system;

@@ -11,6 +11,13 @@ namespace rsg {
 constexpr int kGnnHidden = 64;
 constexpr int kGnnFeatures = 8;
 constexpr int kGnnGradBlocks = 256;
+// Parameters of an L-layer model: W_in (features x hidden) and b_in, per layer W (2 hidden x hidden) and b,
+// w_out (hidden) and b_out.
+constexpr uint64_t gnn_param_count(int layers)
+{
+    return uint64_t(kGnnFeatures) * kGnnHidden + kGnnHidden +
+           uint64_t(layers) * (2ull * kGnnHidden * kGnnHidden + kGnnHidden) + kGnnHidden + 1;
+}
 }  // namespace rsg
 
 struct rsg_learned {

@@ -15,6 +15,7 @@
 // RSG_ERR_TIMEOUT and the context stays usable.
 #include <cstdio>
 #include <cstring>
+#include <exception>
 #include <vector>
 
 #include "gnn.cuh"
@@ -41,6 +42,16 @@ static_assert(sizeof(GnnHeader) == 64, "checkpoint header is 64 bytes");
 
 bool write_all(FILE *f, const void *p, size_t bytes) { return bytes == 0 || std::fwrite(p, 1, bytes, f) == bytes; }
 bool read_all(FILE *f, void *p, size_t bytes) { return bytes == 0 || std::fread(p, 1, bytes, f) == bytes; }
+
+// Bytes between the current position and the end of the file (the position is kept).
+uint64_t file_bytes_left(FILE *f)
+{
+    const long here = std::ftell(f);
+    if (here < 0 || std::fseek(f, 0, SEEK_END) != 0) return 0;
+    const long end = std::ftell(f);
+    std::fseek(f, here, SEEK_SET);
+    return end > here ? uint64_t(end - here) : 0;
+}
 
 // Waits for phase 0 of an mbarrier that expects one arrival which never happens;
 // the wait gives up after `limit` polls and flags *err.
@@ -104,12 +115,38 @@ rsg_status rsg_csr_load(rsg_context *ctx, const char *path, rsg_csr **A, double 
         std::fclose(f);
         return set_error(ctx, RSG_ERR_INVALID_ARG, "csr_load: %s is not an RSGCSR01 file", path);
     }
-    std::vector<uint32_t> rp(size_t(h.n) + 1), ci(h.nnz);
-    std::vector<double> val(h.nnz), b(h.has_b ? h.n : 0);
-    const bool ok = read_all(f, rp.data(), rp.size() * 4) && read_all(f, ci.data(), ci.size() * 4) &&
-                    read_all(f, val.data(), val.size() * 8) && read_all(f, b.data(), b.size() * 8);
+    // The header is untrusted: check it against the file's size before sizing any buffer from it.
+    const uint64_t payload = file_bytes_left(f);
+    const uint64_t want = (uint64_t(h.n) + 1) * 4 + h.nnz * 12 + (h.has_b ? uint64_t(h.n) * 8 : 0);
+    if (h.n == 0 || h.nnz > 0xffffffffull || h.has_b > 1 || payload != want) {
+        std::fclose(f);
+        return set_error(ctx, RSG_ERR_INVALID_ARG,
+                         "csr_load: %s: header (n %u, nnz %llu, has_b %u) does not match the file's %llu payload bytes",
+                         path, h.n, (unsigned long long)h.nnz, h.has_b, (unsigned long long)payload);
+    }
+    std::vector<uint32_t> rp, ci;
+    std::vector<double> val, b;
+    bool ok = false;
+    try {
+        rp.resize(size_t(h.n) + 1);
+        ci.resize(h.nnz);
+        val.resize(h.nnz);
+        b.resize(h.has_b ? h.n : 0);
+        ok = read_all(f, rp.data(), rp.size() * 4) && read_all(f, ci.data(), ci.size() * 4) &&
+             read_all(f, val.data(), val.size() * 8) && read_all(f, b.data(), b.size() * 8);
+    } catch (const std::exception &) {
+        std::fclose(f);
+        return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "csr_load: no host memory for %s", path);
+    }
     std::fclose(f);
     if (!ok) return set_error(ctx, RSG_ERR_INVALID_ARG, "csr_load: %s is truncated", path);
+    // rsg_csr_create copies rp[n] column indexes and values: they must be the nnz the header sized.
+    if (rp[0] != 0 || rp[h.n] != h.nnz)
+        return set_error(ctx, RSG_ERR_INVALID_ARG, "csr_load: %s: row_ptr[0] = %u, row_ptr[n] = %u, nnz = %llu", path,
+                         rp[0], rp[h.n], (unsigned long long)h.nnz);
+    for (uint32_t i = 0; i < h.n; i++)
+        if (rp[i + 1] < rp[i])
+            return set_error(ctx, RSG_ERR_INVALID_ARG, "csr_load: %s: row_ptr decreases at row %u", path, i);
     if (n_rows) *n_rows = h.n;
     if (nnz) *nnz = h.nnz;
     if (has_b) *has_b = int32_t(h.has_b);
@@ -163,20 +200,32 @@ rsg_status rsg_learned_load(rsg_context *ctx, const char *path, rsg_learned **ou
         return set_error(ctx, RSG_ERR_UNSUPPORTED, "learned_load: %u layers of width %u with %u features", h.layers,
                          h.hidden, h.features);
     }
-    std::vector<float> buf(h.n_params * 3);
-    const bool ok = read_all(f, buf.data(), buf.size() * 4);
+    // The parameter count follows from the layer count; compare before sizing anything from the header.
+    const uint64_t expect = gnn_param_count(int(h.layers));
+    const uint64_t payload = file_bytes_left(f);
+    if (h.n_params != expect || payload != expect * 3 * 4) {
+        std::fclose(f);
+        return set_error(ctx, RSG_ERR_INVALID_ARG,
+                         "learned_load: %s holds %llu parameters in %llu bytes; %u layers need %llu", path,
+                         (unsigned long long)h.n_params, (unsigned long long)payload, h.layers,
+                         (unsigned long long)expect);
+    }
+    std::vector<float> buf;
+    bool ok = false;
+    try {
+        buf.resize(expect * 3);
+        ok = read_all(f, buf.data(), buf.size() * 4);
+    } catch (const std::exception &) {
+        std::fclose(f);
+        return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "learned_load: no host memory for %s", path);
+    }
     std::fclose(f);
     if (!ok) return set_error(ctx, RSG_ERR_INVALID_ARG, "learned_load: %s is truncated", path);
     rsg_learned *G = nullptr;
     RSG_TRY(rsg_learned_create(ctx, h.layers, 0, &G));
-    if (G->n_params != h.n_params) {
-        rsg_learned_destroy(ctx, G);
-        return set_error(ctx, RSG_ERR_INVALID_ARG, "learned_load: %llu parameters, expected %llu",
-                         (unsigned long long)h.n_params, (unsigned long long)G->n_params);
-    }
     rsg_status s = rsg_learned_set_params(ctx, G, buf.data(), 0);
-    if (s == RSG_OK) s = rsg_learned_set_params(ctx, G, buf.data() + h.n_params, 2);
-    if (s == RSG_OK) s = rsg_learned_set_params(ctx, G, buf.data() + 2 * h.n_params, 3);
+    if (s == RSG_OK) s = rsg_learned_set_params(ctx, G, buf.data() + expect, 2);
+    if (s == RSG_OK) s = rsg_learned_set_params(ctx, G, buf.data() + 2 * expect, 3);
     if (s != RSG_OK) {
         rsg_learned_destroy(ctx, G);
         return s;

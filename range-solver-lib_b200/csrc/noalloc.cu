@@ -16,12 +16,12 @@
 // share it and it keeps the last call's contents, so the ticket is cleared
 // before each launch, and calls whose kernels overlap on the GPU (different
 // streams, no ordering between them) race on the array and give wrong
-// results: order such calls on one stream.  The first call on a device looks up
-// the array's device address (cudaGetSymbolAddress) with that device current;
-// make that first call before any stream capture.
+// results: order such calls on one stream.  Every call looks up the array's
+// device address (cudaGetSymbolAddress) with the caller's device current, so the
+// entry point stays valid across a cudaDeviceReset in the host application; the
+// first call on a device also loads the library's device code there if the CUDA
+// runtime has not done so yet, so make that first call before any stream capture.
 #include <cuda_runtime.h>
-
-#include <mutex>
 
 #include "../../include/rsg.h"
 
@@ -30,7 +30,6 @@ namespace {
 constexpr uint32_t kChunks = RSG_NOALLOC_MAX_ROWS / 32u;
 constexpr uint32_t kHeader = 32;  // doubles reserved in front of the partials; word 0 holds the ticket
 constexpr int kThreads = 256;
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) double g_noalloc_scratch[kHeader + 2 * size_t(kChunks)];
 
@@ -109,21 +108,14 @@ __global__ void __launch_bounds__(kThreads) k_true_relres_noalloc(uint32_t n, co
     }
 }
 
-std::mutex g_setup_mu;
-double *g_scratch_ptr[kMaxDevices] = {};
-
-// Device address of the scratch array on the current device (looked up once per device).
+// Device address of the scratch array on the current device.  The lookup is repeated on every call (a host-side
+// query that allocates nothing): a cached address would go stale if the host application reset the device
+// (cudaDeviceReset), which unloads the library's device code and places the array anew on the next load.
 rsg_status scratch_for_current_device(double **ptr)
 {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return RSG_ERR_CUDA;
-    std::lock_guard<std::mutex> lock(g_setup_mu);
-    if (!g_scratch_ptr[dev]) {
-        void *p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return RSG_ERR_CUDA;
-        g_scratch_ptr[dev] = static_cast<double *>(p);
-    }
-    *ptr = g_scratch_ptr[dev];
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return RSG_ERR_CUDA;
+    *ptr = static_cast<double *>(p);
     return RSG_OK;
 }
 

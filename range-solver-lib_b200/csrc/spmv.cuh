@@ -6,8 +6,9 @@
 //      contiguous range; the 32 lanes read it with 16-byte vector loads of
 //      values and column indexes (fully coalesced, no per-row divergence),
 //      multiply by the gathered x and park the products in shared memory;
-//   2. row phase: 32/RPW lanes per row sum that row's products and hand the
-//      result to the caller's epilogue.
+//   2. row phase: FP32 -- 32/RPW lanes per row sum that row's products; FP64 --
+//      one lane per row adds them serially in CSR column order (the
+//      reference's multiplyRow arithmetic); the sum goes to the caller's epilogue.
 // Chunks whose nonzeros exceed kCap fall back to warp-per-row.
 //
 // The x operand is a functor so callers fuse vector updates into the gather
@@ -124,98 +125,33 @@ struct VecLoad<float> {
     }
 };
 
-// Row product for one row by a whole warp (long rows).
+// Row product for one row by a whole warp (rows too long to stage).  FP32 (inner
+// solver only): lanes take strided elements and a shuffle tree adds them.  FP64:
+// lane 0 sums the row serially in CSR column order with separate multiply and
+// add, the reference's multiplyRow arithmetic (src/rmatrixsolver.cpp:111-119),
+// so every FP64 path gives the same bits as the SELL-32 path.
 template <typename V, typename A, class GX>
 __device__ __forceinline__ A warp_row(const Csr<V> &M, uint32_t row, GX &gx, int lane)
 {
     const uint32_t s = M.rp[row], e = M.rp[row + 1];
     const int base = int(row & ~31u);
     A acc = A(0);
-    for (uint32_t j = s + lane; j < e; j += 32) {
-        uint32_t c = M.off ? uint32_t(base + int(M.off[j])) : M.ci[j];
-        acc += A(M.val[j]) * A(gx(c));
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    return acc;
-}
-
-// Process rows [row0, row0 + RPW) of M with one warp.  `prod` is this warp's
-// kCap-element shared buffer.  Accumulation type A (double for FP64, float for FP32).
-template <typename V, typename A, int RPW, class GX, class EPI>
-__device__ __forceinline__ void warp_chunk(const Csr<V> &M, uint32_t row0, GX &gx, EPI &epi, A *prod, int lane)
-{
-    static_assert(32 % RPW == 0, "RPW must divide 32");
-    constexpr int L = 32 / RPW;  // lanes per row in the row phase
-    constexpr int W = VecLoad<V>::W;
-    const uint32_t nrows = min(uint32_t(RPW), M.n - row0);
-    // lane i < nrows holds rp[row0 + i]; every lane also reads the chunk end
-    const uint32_t end = __ldg(&M.rp[row0 + nrows]);
-    const uint32_t my_rp = (lane < int(nrows)) ? __ldg(&M.rp[row0 + lane]) : end;
-    const uint32_t start = __shfl_sync(0xffffffffu, my_rp, 0);
-    const int base = int(row0 & ~31u);
-
-    if (end - start <= kCap) {
-        // Issue every matrix load of the chunk first, then every gather, so that
-        // a warp keeps up to kCap/(32 W) + 1 independent 16-byte loads in flight.
-        constexpr int MAXIT = int(kCap) / (32 * W) + 1;
-        const uint32_t g = start & ~uint32_t(W - 1);
-        V v[MAXIT][W];
-        uint32_t c[MAXIT][W];
-#pragma unroll
-        for (int it = 0; it < MAXIT; it++) {
-            const uint32_t j0 = g + (uint32_t(it) * 32u + uint32_t(lane)) * W;
-            if (j0 < end) {
-                VecLoad<V>::vals(M.val + j0, v[it]);
-                if (M.off) {
-                    int o[W];
-                    VecLoad<V>::offs(M.off + j0, o);
-#pragma unroll
-                    for (int k = 0; k < W; k++) c[it][k] = uint32_t(base + o[k]);
-                } else {
-                    VecLoad<V>::cols(M.ci + j0, c[it]);
-                }
+    if constexpr (std::is_same<A, double>::value) {
+        if (lane == 0)
+            for (uint32_t j = s; j < e; j++) {
+                const uint32_t c = M.off ? uint32_t(base + int(M.off[j])) : M.ci[j];
+                acc = __dadd_rn(acc, __dmul_rn(double(M.val[j]), double(gx(c))));
             }
-        }
-#pragma unroll
-        for (int it = 0; it < MAXIT; it++) {
-            const uint32_t j0 = g + (uint32_t(it) * 32u + uint32_t(lane)) * W;
-#pragma unroll
-            for (int k = 0; k < W; k++) {
-                const uint32_t j = j0 + k;
-                if (j0 < end && j >= start && j < end) prod[j - start] = A(v[it][k]) * A(gx(c[it][k]));
-            }
-        }
-        __syncwarp();
-        const int r = lane / L, sub = lane % L;
-        const uint32_t rs = __shfl_sync(0xffffffffu, my_rp, r) - start;
-        const uint32_t nx = __shfl_sync(0xffffffffu, my_rp, min(r + 1, 31));
-        const uint32_t re = ((r + 1 < int(nrows)) ? nx : end) - start;
-        A acc = A(0);
-        if (r < int(nrows))
-            for (uint32_t k = rs + sub; k < re; k += L) acc += prod[k];
-#pragma unroll
-        for (int o = L / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (sub == 0 && r < int(nrows)) epi(row0 + r, acc);
-        __syncwarp();
+        return __shfl_sync(0xffffffffu, acc, 0);
     } else {
-        for (uint32_t r = 0; r < nrows; r++) {
-            A acc = warp_row<V, A>(M, row0 + r, gx, lane);
-            if (lane == 0) epi(row0 + r, acc);
+        for (uint32_t j = s + lane; j < e; j += 32) {
+            const uint32_t c = M.off ? uint32_t(base + int(M.off[j])) : M.ci[j];
+            acc += A(M.val[j]) * A(gx(c));
         }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        return acc;
     }
-}
-
-// Grid-stride driver over all row chunks.  Every thread of the block must call it.
-template <typename V, typename A, int RPW, class GX, class EPI>
-__device__ __forceinline__ void for_rows(const Csr<V> &M, GX &gx, EPI &epi, A *smem_prod)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    A *prod = smem_prod + size_t(warp) * kCap;
-    const uint32_t n_chunks = (M.n + RPW - 1) / RPW;
-    const uint32_t warps_total = gridDim.x * (blockDim.x >> 5);
-    for (uint32_t c = blockIdx.x * (blockDim.x >> 5) + warp; c < n_chunks; c += warps_total)
-        warp_chunk<V, A, RPW>(M, c * RPW, gx, epi, prod, lane);
 }
 
 // ---------------------------------------------------------------------------
@@ -298,6 +234,10 @@ struct Stage {
     static constexpr uint32_t kWarpBytes = kStages * kBytes + 16 * kStages;
 };
 
+// Product rounded on its own (never contracted into a later add).
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return a * b; }
+
 template <typename V>
 constexpr size_t tma_smem() { return size_t(kWarpsPerBlock) * Stage<V>::kWarpBytes; }
 
@@ -379,13 +319,13 @@ __device__ __forceinline__ void for_rows_tma(const Csr<V> &M, GX &gx, EPI &epi, 
 #pragma unroll 4
                 for (uint32_t j = start + lane; j < end; j += 32) {
                     const uint32_t k = j - a0;
-                    sv[k] = sv[k] * V(gx(uint32_t(base + int(so[k]))));
+                    sv[k] = mul_rn(sv[k], V(gx(uint32_t(base + int(so[k])))));
                 }
             } else {
 #pragma unroll 4
                 for (uint32_t j = start + lane; j < end; j += 32) {
                     const uint32_t k = j - a0;
-                    sv[k] = sv[k] * V(gx(sc[k]));
+                    sv[k] = mul_rn(sv[k], V(gx(sc[k])));
                 }
             }
             __syncwarp();
@@ -394,10 +334,17 @@ __device__ __forceinline__ void for_rows_tma(const Csr<V> &M, GX &gx, EPI &epi, 
             const uint32_t nx = __shfl_sync(0xffffffffu, my_rp, min(r + 1, 31));
             const uint32_t re = ((r + 1 < int(nrows)) ? nx : end) - a0;
             V acc = V(0);
-            if (r < int(nrows))
-                for (uint32_t k = rs + sub; k < re; k += L) acc += sv[k];
+            if constexpr (std::is_same<V, double>::value) {
+                // FP64: one lane per row adds the row's rounded products serially in CSR column order
+                // (multiplyRow, src/rmatrixsolver.cpp:111-119); the products were rounded on their own above.
+                if (sub == 0 && r < int(nrows))
+                    for (uint32_t k = rs; k < re; k++) acc = __dadd_rn(acc, sv[k]);
+            } else {
+                if (r < int(nrows))
+                    for (uint32_t k = rs + sub; k < re; k += L) acc += sv[k];
 #pragma unroll
-            for (int o = L / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+                for (int o = L / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            }
             if (sub == 0 && r < int(nrows)) epi(row0 + r, acc);
             __syncwarp();
             fence_async_shared();  // generic writes to the stage precede the next async copy into it

@@ -289,6 +289,62 @@ class Solver:
         return self.ctx.solve(M, b, x, self.conf, prec, block_size)
 
 
+class ModelGroups:
+    """The model's elements and element groups as flat arrays for the node-book entry points.
+
+    elements: list of node-id sequences (any element type), or a 2-D array (one element per row);
+    groups: list of element-id sequences; computable: per-element flags or None (all computable).
+    """
+
+    def __init__(self, n_nodes: int, elements, groups, computable=None):
+        if isinstance(elements, np.ndarray) and elements.ndim == 2:
+            k = elements.shape[1]
+            self.elem_nodes = np.ascontiguousarray(elements.reshape(-1), np.uint32)
+            self.elem_begin = np.arange(0, k * elements.shape[0] + 1, k, dtype=np.uint32)
+        else:
+            lens = [len(e) for e in elements]
+            self.elem_begin = np.zeros(len(lens) + 1, np.uint32)
+            self.elem_begin[1:] = np.cumsum(lens)
+            self.elem_nodes = np.ascontiguousarray(np.concatenate([np.asarray(e, np.uint32) for e in elements])
+                                                   if elements else np.zeros(0, np.uint32))
+        glens = [len(g) for g in groups]
+        self.group_begin = np.zeros(len(glens) + 1, np.uint32)
+        self.group_begin[1:] = np.cumsum(glens)
+        self.group_elems = np.ascontiguousarray(np.concatenate([np.asarray(g, np.uint32) for g in groups])
+                                                if groups else np.zeros(0, np.uint32))
+        self.computable = None if computable is None else np.ascontiguousarray(computable, np.uint8)
+        self.c = _lib.ModelGroups(n_nodes, len(self.elem_begin) - 1, _ptr(self.elem_begin).value,
+                                  _ptr(self.elem_nodes).value, len(glens), _ptr(self.group_begin).value,
+                                  _ptr(self.group_elems).value,
+                                  None if self.computable is None else _ptr(self.computable).value)
+        self.n_nodes = n_nodes
+
+
+def node_book_generic(model: ModelGroups, explicit_bc) -> tuple[np.ndarray, int]:
+    """RSolverGeneric::generateNodeBook (rsg_node_book_generic): (book, n_free)."""
+    lib = _lib.load()
+    flags = np.ascontiguousarray(explicit_bc, np.uint8)
+    book = np.empty(model.n_nodes, np.uint32)
+    n_free = C.c_uint32()
+    s = lib.rsg_node_book_generic(C.byref(model.c), _ptr(flags), _ptr(book), C.byref(n_free))
+    if s != OK:
+        raise _lib.RsgError(s, "node_book_generic: " + lib.rsg_status_string(s).decode())
+    return book, n_free.value
+
+
+def node_book_stress(model: ModelGroups, group_bc, group_is_line) -> tuple[np.ndarray, int]:
+    """RSolverStress::generateNodeBook (rsg_node_book_stress): (book of 3 n_nodes positions, n_free)."""
+    lib = _lib.load()
+    bc = np.ascontiguousarray(group_bc, np.uint8)
+    line = np.ascontiguousarray(group_is_line, np.uint8)
+    book = np.empty(3 * model.n_nodes, np.uint32)
+    n_free = C.c_uint32()
+    s = lib.rsg_node_book_stress(C.byref(model.c), _ptr(bc), _ptr(line), _ptr(book), C.byref(n_free))
+    if s != OK:
+        raise _lib.RsgError(s, "node_book_stress: " + lib.rsg_status_string(s).decode())
+    return book, n_free.value
+
+
 class Assembly:
     """Assembly plan (rsg_assembly): pattern + scatter map of one mesh and node book.
 

@@ -32,6 +32,7 @@ STOP_REFERENCE, STOP_TRUE_RELRES = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 MEM_HOST, MEM_DEVICE = 0, 1
 NOALLOC_MAX_ROWS = 2097152
+BC_DISPLACEMENT, BC_DISPLACEMENT_NORMAL, BC_DISPLACEMENT_ROLLER = 1, 2, 4
 
 
 class SolverConf(C.Structure):
@@ -105,6 +106,19 @@ class TuneInfo(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
+class ModelGroups(C.Structure):
+    _fields_ = [
+        ("n_nodes", C.c_uint32),
+        ("n_elements", C.c_uint32),
+        ("elem_begin", C.c_void_p),
+        ("elem_nodes", C.c_void_p),
+        ("n_groups", C.c_uint32),
+        ("group_begin", C.c_void_p),
+        ("group_elems", C.c_void_p),
+        ("computable", C.c_void_p),
+    ]
+
+
 class Time(C.Structure):
     _fields_ = [("transient", C.c_int32), ("alpha", C.c_double), ("dt", C.c_double)]
 
@@ -162,6 +176,8 @@ SIGNATURES = {
     "rsg_learned_apply": (C.c_int, [_P, _P, _P, _P, _P, _P, C.c_int32]),
     "rsg_learned_loss_grad": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, _DP]),
     "rsg_learned_train_step": (C.c_int, [_P, _P, _P, _P, _P, C.c_float, _DP]),
+    "rsg_node_book_generic": (C.c_int, [C.POINTER(ModelGroups), _P, _P, _U32P]),
+    "rsg_node_book_stress": (C.c_int, [C.POINTER(ModelGroups), _P, _P, _P, _U32P]),
     "rsg_assembly_create_heat": (C.c_int, [_P, C.c_uint32, _P, C.c_uint32, _P, _P, C.c_uint32, _PP]),
     "rsg_assembly_create_stress": (C.c_int, [_P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32, _P, _P, C.c_uint32,
                                              _PP]),

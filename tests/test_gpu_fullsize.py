@@ -1,0 +1,130 @@
+"""Benchmark configurations at full size against the CPU oracle, through the C ABI.
+
+Every system here is the one the benchmarks time, at its full size:
+  * 100^3 lognormal heat (sigma 1.5, seed 0; 1,009,899 unknowns, 14.9M stored entries);
+  * the 64x32x32 elasticity beam (209,088 unknowns);
+  * 32 systems of the 256-system batch (8..60 hexes per side, drawn as the batch benchmark draws them).
+Bar (the same as the small cases): the GPU-assembled pattern equals the oracle's, every entry and
+right-hand-side value within 1e-13 relative (absolute floor 1e-13 of the row's largest entry for
+entries that cancel to rounding noise); every GPU solution reaches the FP64 true relative residual
+1e-10, recomputed by the oracle on the oracle's system, and agrees with the oracle's tight solution
+(rtol 1e-12) to ||x - x_ref|| / ||x_ref|| <= 1e-8.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import rsg
+from oracle import oracle as O
+from rsg import workloads as W
+from conftest import rel_err
+from test_gpu_assembly import compare
+
+pytestmark = pytest.mark.gpu
+
+THREADS = os.cpu_count() or 1
+_CACHE = {}
+
+
+def oracle_tight(A, b, prec=1, block=1):
+    x, st = O.solve(A, b, prec=prec, block_size=block, n_outer=200000, stop_rule="true", rtol=1e-12,
+                    threads=THREADS)
+    assert st.converged == 1 and st.true_relres <= 1e-12
+    return x
+
+
+def heat100():
+    if "heat100" not in _CACHE:
+        p = W.heat_cube(100, sigma=1.5, seed=0, source="random")
+        Ao, bo = O.assemble_heat(p)
+        _CACHE["heat100"] = (p, Ao, bo, oracle_tight(Ao, bo))
+    return _CACHE["heat100"]
+
+
+def test_heat100_assembly_matches_oracle_per_entry(ctx, torch_cuda):
+    torch = torch_cuda
+    p, Ao, bo, _ = heat100()
+    assert (Ao.n, Ao.nnz) == (1009899, 14908095)
+    asm = rsg.Assembly.heat(ctx, p)
+    b = torch.empty(asm.n_free, dtype=torch.float64, device="cuda")
+    M = asm.assemble(p, b)
+    ctx.sync()
+    rp, ci, val = M.to_host()
+    compare(O.CSR(M.n, rp, ci, val), b.cpu().numpy(), Ao, bo)
+    assert M.frobenius == pytest.approx(O.frobenius(Ao), rel=1e-13)
+    asm.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_heat100_solution_matches_oracle(ctx, torch_cuda, precision):
+    """The headline system: GPU assembly, then the benchmark's solve (Jacobi-PCG to the FP64 true
+    relative residual 1e-10) in FP64 and in mixed precision."""
+    torch = torch_cuda
+    p, Ao, bo, x_ref = heat100()
+    asm = rsg.Assembly.heat(ctx, p)
+    b = torch.empty(asm.n_free, dtype=torch.float64, device="cuda")
+    M = asm.assemble(p, b)
+    x = torch.zeros_like(b)
+    ctx.sync()
+    conf = rsg.make_conf(n_outer=50000, stop_rule="true", rtol=1e-10, precision=precision)
+    _, st = ctx.solve(M, b, x, conf=conf)
+    xh = x.cpu().numpy()
+    assert st.status == rsg.OK and st.converged == 1
+    relres = O.true_relres(Ao, bo, xh)
+    assert relres <= 1e-10 * 1.01 and st.true_relres == pytest.approx(relres, rel=1e-6)
+    assert rel_err(xh, x_ref) <= 1e-8
+    # the same number of iterations as the oracle's FP64 Jacobi-PCG to 1e-10, give or take
+    # the mixed-precision refreshes
+    _, so = O.solve(Ao, bo, prec=1, n_outer=50000, stop_rule="true", rtol=1e-10, threads=THREADS)
+    assert abs(int(st.iterations) - int(so.iterations)) <= (3 if precision == "fp64" else 0.15 * so.iterations)
+    asm.close()
+
+
+@pytest.mark.parametrize("prec,block,precision", [(1, 1, "fp64"), (1, 1, "mixed"), (2, 3, "fp64"), (2, 3, "mixed")])
+def test_elasticity_beam_64x32x32_matches_oracle(ctx, torch_cuda, prec, block, precision):
+    torch = torch_cuda
+    if "beam" not in _CACHE:
+        p = W.stress_beam(64, 32, 32)
+        Ao, bo = O.assemble_stress(p)
+        _CACHE["beam"] = (p, Ao, bo, {})
+    p, Ao, bo, refs = _CACHE["beam"]
+    assert Ao.n == 209088
+    if (prec, block) not in refs:
+        refs[(prec, block)] = oracle_tight(Ao, bo, prec=prec, block=block)
+    asm = rsg.Assembly.stress(ctx, p)
+    b = torch.empty(asm.n_free, dtype=torch.float64, device="cuda")
+    M = asm.assemble(p, b)
+    ctx.sync()
+    if precision == "fp64" and prec == 1:
+        rp, ci, val = M.to_host()
+        compare(O.CSR(M.n, rp, ci, val), b.cpu().numpy(), Ao, bo)
+    x = torch.zeros_like(b)
+    conf = rsg.make_conf(n_outer=100000, stop_rule="true", rtol=1e-10, precision=precision)
+    _, st = ctx.solve(M, b, x, conf=conf, prec=prec, block_size=block)
+    xh = x.cpu().numpy()
+    assert st.status == rsg.OK and O.true_relres(Ao, bo, xh) <= 1e-10 * 1.01
+    assert rel_err(xh, refs[(prec, block)]) <= 1e-8
+    asm.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_of_32_from_the_benchmark_distribution(ctx, precision):
+    """The first 32 systems of the 256-system batch benchmark (hexes per side drawn uniformly from
+    8..60 with the benchmark's generator, lognormal(0, 1) conductivity), solved as one batch."""
+    if "batch" not in _CACHE:
+        sizes = np.random.default_rng(1000).integers(8, 61, 256)[:32]
+        sys_ = [O.assemble_heat(W.heat_cube(int(n), sigma=1.0, seed=i, source="random")) for i, n in enumerate(sizes)]
+        _CACHE["batch"] = (sizes, sys_, [oracle_tight(A, b) for A, b in sys_])
+    sizes, sys_, refs = _CACHE["batch"]
+    assert sizes.min() < 20 and sizes.max() > 50  # the draw spans the distribution
+    batch = rsg.Batch(ctx, [(A.rp, A.ci, A.val) for A, _ in sys_])
+    b = np.concatenate([bb for _, bb in sys_])
+    conf = rsg.make_conf(n_outer=100000, stop_rule="true", rtol=1e-10, precision=precision)
+    x, per, summ = batch.solve(b, conf=conf)
+    assert summ.status == rsg.OK
+    for (A, bb), xs, st, xr in zip(sys_, batch.split(x), per, refs):
+        assert st.status == rsg.OK and st.converged == 1
+        assert O.true_relres(A, bb, xs) <= 1e-10 * 1.01
+        assert rel_err(xs, xr) <= 1e-8
+    batch.close()

@@ -54,6 +54,56 @@ def test_csr_dump_roundtrip(ctx, torch_cuda, tmp_path):
         ctx.load_matrix(str(tmp_path / "bad.rsgcsr"))
 
 
+def _corrupt(raw: bytes, offset: int, value: np.ndarray) -> bytes:
+    b = bytearray(raw)
+    v = value.tobytes()
+    b[offset:offset + len(v)] = v
+    return bytes(b)
+
+
+def test_corrupt_csr_dumps_are_rejected_before_any_copy(ctx, torch_cuda, tmp_path):
+    """An untrusted header or row pointer never sizes a read past the file's arrays: a last row
+    pointer above the stored nnz, a header nnz that does not match the payload, an absurd row
+    count and a decreasing row pointer all return RSG_ERR_INVALID_ARG, and the context stays usable."""
+    A, b = O.assemble_heat(W.heat_cube(4, sigma=1.0, seed=2, source="random"))
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    path = tmp_path / "ok.rsgcsr"
+    ctx.save_matrix(M, str(path))
+    raw = path.read_bytes()
+    n = A.n
+    cases = {
+        "rp_end_above_nnz": _corrupt(raw, 64 + 4 * n, np.array([A.nnz + 1000], np.uint32)),
+        "header_nnz_too_big": _corrupt(raw, 16, np.array([A.nnz + 7], np.uint64)),
+        "header_n_huge": _corrupt(raw, 8, np.array([0xFFFFFFF0], np.uint32)),
+        "rp_decreasing": _corrupt(raw, 64 + 4 * 3, np.array([0], np.uint32)),
+        "truncated": raw[:-8],
+    }
+    for name, data in cases.items():
+        f = tmp_path / f"{name}.rsgcsr"
+        f.write_bytes(data)
+        with pytest.raises(rsg.RsgError) as e:
+            ctx.load_matrix(str(f))
+        assert e.value.status == rsg._lib.ERR_INVALID_ARG, name
+    M2, _ = ctx.load_matrix(str(path))
+    assert np.array_equal(M2.to_host()[2], A.val)
+
+
+def test_corrupt_checkpoint_is_rejected_before_allocating(ctx, tmp_path):
+    m = RL.Learned(ctx, layers=2, seed=1)
+    path = tmp_path / "m.rsggnn"
+    m.save_binary(str(path))
+    raw = path.read_bytes()
+    for name, data in {"n_params_huge": _corrupt(raw, 24, np.array([1 << 60], np.uint64)),
+                       "n_params_off_by_one": _corrupt(raw, 24, np.array([m.n_params + 1], np.uint64)),
+                       "truncated": raw[:-4]}.items():
+        f = tmp_path / f"{name}.rsggnn"
+        f.write_bytes(data)
+        with pytest.raises(rsg.RsgError) as e:
+            RL.Learned.load_binary(ctx, str(f))
+        assert e.value.status == rsg._lib.ERR_INVALID_ARG, name
+    m.close()
+
+
 def test_learned_binary_checkpoint(ctx, torch_cuda, tmp_path):
     torch = torch_cuda
     A, b = O.assemble_heat(W.heat_cube(6, sigma=1.0, seed=3, source="random"))

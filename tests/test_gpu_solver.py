@@ -68,8 +68,12 @@ def test_golden_vectors_gpu(ctx):
     assert np.allclose(x, [3, 2, 2], atol=1e-6)
 
 
+@pytest.mark.parametrize("layout", ["sell", "csr_stream"])
 @pytest.mark.parametrize("which", ["heat", "ragged", "stress"])
-def test_spmv_fp64_and_fp32_match_oracle(ctx, torch_cuda, which):
+def test_spmv_fp64_and_fp32_match_oracle(ctx, torch_cuda, monkeypatch, which, layout):
+    """FP64: every row equals the oracle's serial multiplyRow sum bit for bit, on the SELL-32
+    layout and on the TMA-staged CSR stream (rows longer than the staging buffer included).
+    FP32 (inner solver only): within 2e-6 of the row's absolute sum."""
     torch = torch_cuda
     if which == "heat":
         A, _ = heat(12, sigma=1.0, seed=1)
@@ -77,7 +81,10 @@ def test_spmv_fp64_and_fp32_match_oracle(ctx, torch_cuda, which):
         A = ragged_csr()
     else:
         A, _ = stress(6, 3, 3)
+    if layout == "csr_stream":
+        monkeypatch.setenv("RSG_NO_SELL", "1")
     M = ctx.matrix(A.rp, A.ci, A.val)
+    monkeypatch.delenv("RSG_NO_SELL", raising=False)
     assert M.frobenius == pytest.approx(O.frobenius(A), rel=1e-13)
     x = np.random.default_rng(2).standard_normal(A.n)
     y_ref = O.spmv(A, x)
@@ -87,7 +94,7 @@ def test_spmv_fp64_and_fp32_match_oracle(ctx, torch_cuda, which):
     torch.cuda.synchronize()  # the library runs on its own stream
     ctx.spmv(M, xd, yd)
     ctx.sync()
-    assert np.all(np.abs(yd.cpu().numpy() - y_ref) <= 1e-13 * absrow + 1e-300)
+    assert np.array_equal(yd.cpu().numpy(), y_ref)
     x32 = torch.tensor(x, device="cuda", dtype=torch.float32)
     y32 = torch.empty_like(x32)
     torch.cuda.synchronize()
