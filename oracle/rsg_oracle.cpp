@@ -567,6 +567,11 @@ int orc_solve(const orc_conf *conf, uint32_t n, const uint32_t *rp, const uint32
     /* src/rmatrixsolver.cpp:158-201 (solve) */
     orc_stats st;
     std::memset(&st, 0, sizeof(st));
+    /* a requested team size holds for this call only */
+    struct TeamSize {
+        int prev = omp_get_max_threads();
+        ~TeamSize() { omp_set_num_threads(prev); }
+    } team;
     if (conf->n_threads > 0) omp_set_num_threads(conf->n_threads);
 
     Precond P;

@@ -22,6 +22,8 @@ def test_reference_arm_json_line():
         assert k in d, k
     assert d["impl"] == "reference" and d["steps"] == 2 and d["warmup"] == 3 and d["higher_is_better"] is False
     assert d["value"] > 0 and d["unit"] == "s" and abs(d["ms_per_step"] - 1e3 * d["value"]) < 1e-9
-    assert d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["kind"] == "port"
+    from oracle import ref as R
+    assert d["cpu_baseline"]["value"] == d["value"]
+    assert d["cpu_baseline"]["kind"] == ("reference" if R.available() else "port")
     assert d["e2e"] == {"value": d["value"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert d["config"]["workload"] == "heat_lognormal_10" and d["config"]["true_relres"] <= 1e-10
