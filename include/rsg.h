@@ -44,12 +44,14 @@ typedef enum {
 /* RMatrixSolverConf::Type (range-model-lib; used at src/rmatrixsolver.cpp:186-196) */
 typedef enum { RSG_SOLVER_CG = 0, RSG_SOLVER_GMRES = 1 } rsg_solver_type;
 
-/* RMatrixPreconditionerType (include/rmatrixpreconditioner.h:7-16), plus the learned one. */
+/* RMatrixPreconditionerType (include/rmatrixpreconditioner.h:7-16), plus two without a reference
+ * counterpart: the learned one and a multilevel aggregation preconditioner (rsg_amg_*). */
 typedef enum {
     RSG_PREC_NONE = 0,
     RSG_PREC_JACOBI = 1,
     RSG_PREC_BLOCK_JACOBI = 2,
-    RSG_PREC_LEARNED = 3
+    RSG_PREC_LEARNED = 3,
+    RSG_PREC_AMG = 4
 } rsg_prec_type;
 
 typedef enum {
@@ -89,7 +91,8 @@ typedef struct {
                                    (slower than evict_first on SELL-32 in measurements, so not applied there) */
     int32_t  autotune;          /* 1: autotune A's launch shapes on its first solve (rsg_autotune, with the
                                    cache file named by the RSG_TUNE_CACHE environment variable if set) */
-    int32_t  reserved[5];
+    int32_t  amg_sweeps;        /* RSG_PREC_AMG: damped-Jacobi sweeps per side of the V-cycle, 1 or 2 (0: 2) */
+    int32_t  reserved[4];
 } rsg_solver_conf;
 
 typedef struct {
@@ -177,7 +180,9 @@ typedef enum {
     RSG_KERNEL_CG_UPDATE_FP64 = 2, /* x, r update + Jacobi + dots */
     RSG_KERNEL_CG_UPDATE_MIXED = 3,
     RSG_KERNEL_SPMV_FP64 = 4,
-    RSG_KERNEL_SPMV_FP32 = 5
+    RSG_KERNEL_SPMV_FP32 = 5,
+    RSG_KERNEL_AMG_SWEEP = 6       /* RSG_PREC_AMG: finest-level smoothing sweep with the coarse correction
+                                      fused into its gather (builds A's hierarchy first if it has none) */
 } rsg_kernel_id;
 RSG_API rsg_status rsg_profile_kernel(rsg_context *ctx, const rsg_csr *A, int32_t kernel, uint32_t reps,
                                       int32_t flush_l2, double *seconds);
@@ -240,6 +245,34 @@ RSG_API rsg_status rsg_csr_load(rsg_context *ctx, const char *path, rsg_csr **A,
  * returns, so this call returns RSG_ERR_TIMEOUT and the context stays usable.
  * Nothing faults or hangs. */
 RSG_API rsg_status rsg_selftest_wait_timeout(rsg_context *ctx, uint32_t polls);
+
+/* ---- multilevel aggregation preconditioner (RSG_PREC_AMG) ----
+ * No counterpart in the reference (its preconditioners are NONE / JACOBI / BLOCK_JACOBI); it fills
+ * the same slot, P.compute(r, z) in solveCG (src/rmatrixsolver.cpp:258).  Built on the GPU from the
+ * matrix's current values at every rsg_solve that asks for it: aggregates rooted at a distance-2
+ * independent set of the strength graph (|a_ij| >= 0.08 sqrt(|a_ii a_jj|)), piecewise-constant
+ * prolongation, Galerkin coarse matrices added in a fixed order (deterministic), down to at most
+ * 128 rows, inverted densely.  Applied as a symmetric FP32 V-cycle (damped Jacobi, weight 2/3, with
+ * conf.amg_sweeps sweeps per side and a coarse correction scaled by 1.6 / 1.8) inside the
+ * mixed-precision CG (precision MIXED, stop_rule TRUE_RELRES), which keeps the result at FP64 accuracy. */
+typedef struct {
+    uint32_t levels;            /* levels including the finest */
+    uint32_t dense_coarsest;    /* 1: the last level is applied through its dense inverse */
+    uint32_t rows[16];
+    uint64_t nnz[16];
+    uint32_t mis_rounds;        /* synchronous rounds of the independent-set construction, all levels */
+    uint32_t reserved;
+    double   seconds_setup;     /* wall time of the set-up */
+} rsg_amg_info;
+/* Build (or rebuild) A's hierarchy from A's current values; info may be NULL. */
+RSG_API rsg_status rsg_amg_setup(rsg_context *ctx, rsg_csr *A, rsg_amg_info *info);
+/* Copy level `level` of the last hierarchy to host arrays (any may be NULL): agg (rows of the level)
+ * maps each row to its aggregate, the row of level + 1 (not for the last level); row_ptr / col_idx /
+ * values are the level's CSR (level 0: A itself). */
+RSG_API rsg_status rsg_amg_level(rsg_context *ctx, const rsg_csr *A, uint32_t level, uint32_t *agg, uint32_t *row_ptr,
+                                 uint32_t *col_idx, double *values);
+/* z = one V-cycle applied to r (device arrays of n_rows doubles; FP32 inside), sweeps 1 or 2. */
+RSG_API rsg_status rsg_amg_apply(rsg_context *ctx, rsg_csr *A, const double *r, double *z, uint32_t sweeps);
 
 /* FP64 true relative residual ||b - A x|| / ||b|| (device pointers). */
 RSG_API rsg_status rsg_true_relres(rsg_context *ctx, const rsg_csr *A, const double *b, const double *x,

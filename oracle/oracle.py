@@ -75,6 +75,19 @@ def lib():
         L.orc_true_relres.argtypes = [C.c_uint32, _P, _P, _P, _P, _P]
         L.orc_node_book.restype = C.c_uint32
         L.orc_node_book.argtypes = [C.c_uint32, _P, _P]
+        L.orc_amg_build.restype = C.c_void_p
+        L.orc_amg_build.argtypes = [C.c_uint32, _P, _P, _P]
+        L.orc_amg_levels.restype = C.c_uint32
+        L.orc_amg_levels.argtypes = [_P]
+        L.orc_amg_dense_coarsest.restype = C.c_int32
+        L.orc_amg_dense_coarsest.argtypes = [_P]
+        L.orc_amg_rows.restype = C.c_uint32
+        L.orc_amg_rows.argtypes = [_P, C.c_uint32]
+        L.orc_amg_nnz.restype = C.c_uint64
+        L.orc_amg_nnz.argtypes = [_P, C.c_uint32]
+        L.orc_amg_level.argtypes = [_P, C.c_uint32, _P, _P, _P, _P]
+        L.orc_amg_apply.argtypes = [_P, _P, _P, C.c_uint32]
+        L.orc_amg_free.argtypes = [_P]
         L.orc_node_book_generic.restype = C.c_uint32
         L.orc_node_book_generic.argtypes = [C.c_uint32, C.c_uint32, _P, _P, C.c_uint32, _P, _P, _P, _P, _P]
         L.orc_node_book_stress.restype = C.c_uint32
@@ -208,6 +221,45 @@ def node_book_stress(n_nodes, elem_begin, elem_nodes, group_begin, group_elems, 
                                         _ptr(arrs[2]), _ptr(arrs[3]), None if comp is None else _ptr(comp),
                                         _ptr(bcs), _ptr(line), _ptr(book))
     return book, int(n_free)
+
+
+class Amg:
+    """The multilevel aggregation preconditioner built on the host (the checker of RSG_PREC_AMG)."""
+
+    def __init__(self, A: CSR):
+        self.h = C.c_void_p(lib().orc_amg_build(A.n, _ptr(A.rp), _ptr(A.ci), _ptr(A.val)))
+        L = lib()
+        self.levels = int(L.orc_amg_levels(self.h))
+        self.dense_coarsest = bool(L.orc_amg_dense_coarsest(self.h))
+        self.rows = [int(L.orc_amg_rows(self.h, l)) for l in range(self.levels)]
+        self.nnz = [int(L.orc_amg_nnz(self.h, l)) for l in range(self.levels)]
+
+    def level(self, l: int):
+        """(agg or None, CSR) of level l."""
+        n, nnz = self.rows[l], self.nnz[l]
+        agg = np.empty(n, np.uint32) if l + 1 < self.levels else None
+        rp = np.empty(n + 1, np.uint32)
+        ci = np.empty(nnz, np.uint32)
+        val = np.empty(nnz, np.float64)
+        lib().orc_amg_level(self.h, l, None if agg is None else _ptr(agg), _ptr(rp), _ptr(ci), _ptr(val))
+        return agg, CSR(n, rp, ci, val)
+
+    def apply(self, r: np.ndarray, sweeps: int = 2) -> np.ndarray:
+        r = np.ascontiguousarray(r, np.float64)
+        z = np.empty_like(r)
+        lib().orc_amg_apply(self.h, _ptr(r), _ptr(z), sweeps)
+        return z
+
+    def close(self):
+        if self.h:
+            lib().orc_amg_free(self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _system(h) -> tuple[CSR, np.ndarray]:

@@ -941,3 +941,329 @@ orc_system *orc_assemble_magnetostatics(uint32_t n_nodes, const double *xyz, uin
 }
 
 }  // extern "C"
+
+/* ------------------------------------------------------------------------------------------------
+ * Multilevel aggregation preconditioner (no reference counterpart).  Serial restatement of the
+ * CUDA library's set-up (range-solver-lib_b200/csrc/amg.cu): every integer decision and every
+ * floating-point sum is taken in the same order, so the hierarchy is identical bit for bit; the
+ * V-cycle runs in FP64 here (FP32 on the GPU).
+ * ------------------------------------------------------------------------------------------------ */
+namespace {
+
+constexpr uint32_t kAmgCoarsest = 128, kAmgMaxEntries = 4096, kAmgUnset = 0xffffffffu;
+constexpr double kAmgTheta = 0.08, kAmgOmega = 2.0 / 3.0, kAmgScale1 = 1.6, kAmgScale2 = 1.8;
+
+uint32_t amg_hash(uint32_t x)
+{
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+uint64_t amg_key(uint32_t i) { return (uint64_t(amg_hash(i) >> 2) << 32) | i; }
+
+struct AmgLev {
+    uint32_t n = 0;
+    std::vector<uint32_t> rp, ci, agg, agg_ptr, agg_rows;
+    std::vector<double> val, diag, dw;
+};
+
+}  // namespace
+
+struct orc_amg {
+    std::vector<AmgLev> L;
+    bool dense = false;
+    std::vector<double> inv;  /* dense inverse of the last level */
+};
+
+namespace {
+
+void amg_level_diag(AmgLev &l)
+{
+    l.diag.assign(l.n, 0.0);
+    l.dw.assign(l.n, 0.0);
+    for (uint32_t i = 0; i < l.n; i++) {
+        double d = 0.0;
+        for (uint32_t j = l.rp[i]; j < l.rp[i + 1]; j++)
+            if (l.ci[j] == i) d = l.val[j];
+        l.diag[i] = d;
+        l.dw[i] = d != 0.0 ? kAmgOmega / d : 0.0;
+    }
+}
+
+/* aggregates of level F; returns the coarse size, the largest entry count of a coarse row and the
+ * largest aggregate */
+uint32_t amg_aggregate(AmgLev &F, uint32_t &emax, uint32_t &smax)
+{
+    const uint32_t n = F.n;
+    std::vector<uint8_t> strong(F.ci.size(), 0);
+    for (uint32_t i = 0; i < n; i++)
+        for (uint32_t j = F.rp[i]; j < F.rp[i + 1]; j++) {
+            const uint32_t c = F.ci[j];
+            strong[j] = (c != i && c < n && std::abs(F.val[j]) >= kAmgTheta * std::sqrt(std::abs(F.diag[i] * F.diag[c])) &&
+                         F.val[j] != 0.0) ? 1 : 0;
+        }
+    /* synchronous rounds: state 0 out, 1 undecided, 2 root */
+    std::vector<uint64_t> T(n), M1(n), M2(n);
+    for (uint32_t i = 0; i < n; i++) T[i] = (uint64_t(1) << 62) | amg_key(i);
+    auto nbmax = [&](const std::vector<uint64_t> &in, std::vector<uint64_t> &out) {
+        for (uint32_t i = 0; i < n; i++) {
+            uint64_t m = in[i];
+            for (uint32_t j = F.rp[i]; j < F.rp[i + 1]; j++)
+                if (strong[j]) m = std::max(m, in[F.ci[j]]);
+            out[i] = m;
+        }
+    };
+    for (;;) {
+        nbmax(T, M1);
+        nbmax(M1, M2);
+        uint32_t left = 0;
+        for (uint32_t i = 0; i < n; i++) {
+            if ((T[i] >> 62) != 1) continue;
+            if (M2[i] == T[i]) T[i] = (uint64_t(2) << 62) | amg_key(i);
+            else if ((M2[i] >> 62) == 2) T[i] = amg_key(i);
+            else left++;
+        }
+        if (!left) break;
+    }
+    std::vector<uint32_t> rank(n, 0);
+    uint32_t nc = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        rank[i] = nc;
+        if ((T[i] >> 62) == 2) nc++;
+    }
+    std::vector<uint32_t> a1(n, kAmgUnset);
+    for (uint32_t i = 0; i < n; i++) {
+        if ((T[i] >> 62) == 2) {
+            a1[i] = rank[i];
+            continue;
+        }
+        uint64_t best = 0;
+        for (uint32_t j = F.rp[i]; j < F.rp[i + 1]; j++)
+            if (strong[j] && (T[F.ci[j]] >> 62) == 2) best = std::max(best, T[F.ci[j]]);
+        if (best) a1[i] = rank[uint32_t(best & 0xffffffffu)];
+    }
+    F.agg.assign(n, kAmgUnset);
+    uint32_t left = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        uint32_t a = a1[i];
+        if (a == kAmgUnset) {
+            uint64_t best = 0;
+            for (uint32_t j = F.rp[i]; j < F.rp[i + 1]; j++) {
+                const uint32_t c = F.ci[j];
+                if (!strong[j] || a1[c] == kAmgUnset) continue;
+                if (amg_key(c) + 1 > best) {
+                    best = amg_key(c) + 1;
+                    a = a1[c];
+                }
+            }
+            if (a == kAmgUnset) left++;
+        }
+        F.agg[i] = a;
+    }
+    if (left) {
+        uint32_t next = nc;
+        for (uint32_t i = 0; i < n; i++)
+            if (F.agg[i] == kAmgUnset) F.agg[i] = next++;
+        nc = next;
+    }
+    F.agg_ptr.assign(size_t(nc) + 1, 0);
+    for (uint32_t i = 0; i < n; i++) F.agg_ptr[F.agg[i] + 1]++;
+    for (uint32_t a = 0; a < nc; a++) F.agg_ptr[a + 1] += F.agg_ptr[a];
+    F.agg_rows.assign(n, 0);
+    std::vector<uint32_t> cur(F.agg_ptr.begin(), F.agg_ptr.end() - 1);
+    for (uint32_t i = 0; i < n; i++) F.agg_rows[cur[F.agg[i]]++] = i;  /* ascending within each aggregate */
+    emax = smax = 0;
+    for (uint32_t a = 0; a < nc; a++) {
+        uint32_t e = 0;
+        for (uint32_t k = F.agg_ptr[a]; k < F.agg_ptr[a + 1]; k++) e += F.rp[F.agg_rows[k] + 1] - F.rp[F.agg_rows[k]];
+        emax = std::max(emax, e);
+        smax = std::max(smax, F.agg_ptr[a + 1] - F.agg_ptr[a]);
+    }
+    return nc;
+}
+
+/* C = P^T A P: entries of coarse row I in (J ascending, then the order of the aggregate's rows and
+ * of the entries within each row), each run of equal J added serially */
+void amg_galerkin(const AmgLev &F, AmgLev &C, uint32_t nc)
+{
+    C.n = nc;
+    C.rp.assign(size_t(nc) + 1, 0);
+    C.ci.clear();
+    C.val.clear();
+    std::vector<std::pair<uint32_t, uint32_t>> ent;  /* (J, staging position) */
+    std::vector<double> v;
+    for (uint32_t I = 0; I < nc; I++) {
+        ent.clear();
+        v.clear();
+        for (uint32_t k = F.agg_ptr[I]; k < F.agg_ptr[I + 1]; k++) {
+            const uint32_t i = F.agg_rows[k];
+            for (uint32_t j = F.rp[i]; j < F.rp[i + 1]; j++) {
+                ent.emplace_back(F.agg[F.ci[j]], uint32_t(v.size()));
+                v.push_back(F.val[j]);
+            }
+        }
+        std::sort(ent.begin(), ent.end());
+        for (size_t t = 0; t < ent.size();) {
+            const uint32_t J = ent[t].first;
+            double s = 0.0;
+            for (; t < ent.size() && ent[t].first == J; t++) s += v[ent[t].second];
+            C.ci.push_back(J);
+            C.val.push_back(s);
+        }
+        C.rp[I + 1] = uint32_t(C.ci.size());
+    }
+}
+
+/* in-place Gauss-Jordan inverse without pivoting (SPD); a non-positive pivot zeroes its row and column */
+void amg_dense_inverse(const AmgLev &l, std::vector<double> &a)
+{
+    const uint32_t n = l.n;
+    a.assign(size_t(n) * n, 0.0);
+    for (uint32_t i = 0; i < n; i++)
+        for (uint32_t j = l.rp[i]; j < l.rp[i + 1]; j++)
+            if (l.ci[j] < n) a[size_t(i) * n + l.ci[j]] = l.val[j];
+    for (uint32_t k = 0; k < n; k++) {
+        const double p = a[size_t(k) * n + k];
+        if (!(p > 0.0)) {
+            for (uint32_t t = 0; t < n; t++) a[size_t(k) * n + t] = a[size_t(t) * n + k] = 0.0;
+            continue;
+        }
+        const double pinv = 1.0 / p;
+        for (uint32_t j = 0; j < n; j++) a[size_t(k) * n + j] = (j == k) ? pinv : a[size_t(k) * n + j] * pinv;
+        for (uint32_t i = 0; i < n; i++) {
+            if (i == k) continue;
+            for (uint32_t j = 0; j < n; j++)
+                if (j != k) a[size_t(i) * n + j] -= a[size_t(i) * n + k] * a[size_t(k) * n + j];
+        }
+        for (uint32_t i = 0; i < n; i++)
+            if (i != k) a[size_t(i) * n + k] = -a[size_t(i) * n + k] * pinv;
+    }
+}
+
+/* out = x + dw (b - A x) (smooth) or b - A x (residual) */
+void amg_sweep(const AmgLev &l, const std::vector<double> &b, const std::vector<double> &x, std::vector<double> &out,
+               bool smooth)
+{
+    for (uint32_t i = 0; i < l.n; i++) {
+        double ax = 0.0;
+        for (uint32_t j = l.rp[i]; j < l.rp[i + 1]; j++) ax += l.val[j] * x[l.ci[j]];
+        const double res = b[i] - ax;
+        out[i] = smooth ? x[i] + l.dw[i] * res : res;
+    }
+}
+
+void amg_cycle(const orc_amg &H, size_t lv, const std::vector<double> &b, std::vector<double> &e, uint32_t sweeps)
+{
+    const AmgLev &F = H.L[lv];
+    const uint32_t n = F.n;
+    e.assign(n, 0.0);
+    if (lv + 1 == H.L.size()) {
+        if (H.dense) {
+            for (uint32_t i = 0; i < n; i++) {
+                double s = 0.0;
+                for (uint32_t j = 0; j < n; j++) s += H.inv[size_t(i) * n + j] * b[j];
+                e[i] = s;
+            }
+        } else {  /* coarsening stalled: nine damped-Jacobi sweeps from zero */
+            std::vector<double> x(n, 0.0), y(n);
+            for (int k = 0; k < 9; k++) {
+                amg_sweep(F, b, x, y, true);
+                x.swap(y);
+            }
+            e = x;
+        }
+        return;
+    }
+    const double s = sweeps == 2 ? kAmgScale2 : kAmgScale1;
+    std::vector<double> x(n, 0.0), t(n), r(n);
+    amg_sweep(F, b, x, t, true);           /* x = dw b */
+    x.swap(t);
+    for (uint32_t k = 1; k < sweeps; k++) {
+        amg_sweep(F, b, x, t, true);
+        x.swap(t);
+    }
+    amg_sweep(F, b, x, r, false);
+    const AmgLev &C = H.L[lv + 1];
+    std::vector<double> bc(C.n, 0.0), ec;
+    for (uint32_t I = 0; I < C.n; I++) {
+        double acc = 0.0;
+        for (uint32_t k = F.agg_ptr[I]; k < F.agg_ptr[I + 1]; k++) acc += r[F.agg_rows[k]];
+        bc[I] = acc;
+    }
+    amg_cycle(H, lv + 1, bc, ec, sweeps);
+    for (uint32_t i = 0; i < n; i++) x[i] += s * ec[F.agg[i]];
+    for (uint32_t k = 0; k < sweeps; k++) {
+        amg_sweep(F, b, x, t, true);
+        x.swap(t);
+    }
+    e = x;
+}
+
+}  // namespace
+
+extern "C" {
+
+orc_amg *orc_amg_build(uint32_t n, const uint32_t *rp, const uint32_t *ci, const double *val)
+{
+    auto *H = new orc_amg;
+    H->L.emplace_back();
+    AmgLev &L0 = H->L.back();
+    L0.n = n;
+    L0.rp.assign(rp, rp + n + 1);
+    L0.ci.assign(ci, ci + rp[n]);
+    L0.val.assign(val, val + rp[n]);
+    amg_level_diag(L0);
+    while (H->L.size() < 12) {
+        AmgLev &F = H->L.back();
+        if (F.n <= kAmgCoarsest) {
+            H->dense = true;
+            break;
+        }
+        uint32_t emax = 0, smax = 0;
+        const uint32_t nc = amg_aggregate(F, emax, smax);
+        if (nc == 0 || uint64_t(nc) * 10 > uint64_t(F.n) * 9 || emax > kAmgMaxEntries || smax > kAmgMaxEntries) {
+            F.agg.clear();
+            break;
+        }
+        AmgLev C;
+        amg_galerkin(F, C, nc);
+        amg_level_diag(C);
+        H->L.push_back(std::move(C));
+    }
+    if (H->dense) amg_dense_inverse(H->L.back(), H->inv);
+    return H;
+}
+
+uint32_t orc_amg_levels(const orc_amg *h) { return uint32_t(h->L.size()); }
+int32_t orc_amg_dense_coarsest(const orc_amg *h) { return h->dense ? 1 : 0; }
+uint32_t orc_amg_rows(const orc_amg *h, uint32_t level) { return h->L[level].n; }
+uint64_t orc_amg_nnz(const orc_amg *h, uint32_t level) { return h->L[level].ci.size(); }
+
+void orc_amg_level(const orc_amg *h, uint32_t level, uint32_t *agg, uint32_t *row_ptr, uint32_t *col_idx,
+                   double *values)
+{
+    const AmgLev &l = h->L[level];
+    if (agg && !l.agg.empty()) std::memcpy(agg, l.agg.data(), l.agg.size() * sizeof(uint32_t));
+    if (row_ptr) std::memcpy(row_ptr, l.rp.data(), l.rp.size() * sizeof(uint32_t));
+    if (col_idx) std::memcpy(col_idx, l.ci.data(), l.ci.size() * sizeof(uint32_t));
+    if (values) std::memcpy(values, l.val.data(), l.val.size() * sizeof(double));
+}
+
+void orc_amg_apply(const orc_amg *h, const double *r, double *z, uint32_t sweeps)
+{
+    const AmgLev &F = h->L[0];
+    std::vector<double> b(r, r + F.n), e;
+    if (h->L.size() == 1 && !h->dense) {  /* no coarse level: damped Jacobi */
+        for (uint32_t i = 0; i < F.n; i++) z[i] = F.dw[i] * r[i];
+        return;
+    }
+    amg_cycle(*h, 0, b, e, sweeps);
+    std::memcpy(z, e.data(), F.n * sizeof(double));
+}
+
+void orc_amg_free(orc_amg *h) { delete h; }
+
+}  // extern "C"

@@ -1,0 +1,1134 @@
+// Multilevel aggregation preconditioner (RSG_PREC_AMG): hierarchy set-up and V-cycle on the GPU.
+//
+// No counterpart in the reference (its preconditioners are NONE / JACOBI / BLOCK_JACOBI,
+// src/rmatrixpreconditioner.cpp); it serves the same slot, P.compute(r, z) in solveCG
+// (src/rmatrixsolver.cpp:258), as a fixed symmetric positive definite operator.
+//
+// Set-up, per level, all on the GPU and deterministic (integer work, and floating-point sums in
+// a fixed order):
+//   1. strength: j is a strong neighbour of i when |a_ij| >= theta sqrt(|a_ii a_jj|);
+//   2. roots: a distance-2 independent set of the strength graph by synchronous rounds over the
+//      tuples (state, hash(i), i) -- an undecided node whose tuple is the largest within distance 2
+//      becomes a root, one that sees a root within distance 2 drops out;
+//   3. aggregates: every root opens one (numbered in root index order); a node with a strong root
+//      neighbour joins the one with the largest key, then a node with a strong neighbour that has
+//      joined takes that neighbour's aggregate (largest key again); anything left is a singleton;
+//   4. Galerkin product with the piecewise-constant prolongation: coarse entry (I, J) is the sum of
+//      a_ij over i in I, j in J, added in the order of the fine rows of I (ascending) and of the
+//      entries within each row -- one CTA per coarse row stages the entries, sorts them by
+//      (J, position) and adds each run serially;
+//   5. until the level has at most kAmgCoarsest rows, whose dense inverse (in-place Gauss-Jordan,
+//      FP64, no pivoting: the Galerkin matrices of an SPD matrix are SPD) is kept in FP32.
+// The host reads back a handful of counters per level (set sizes), nothing else.
+//
+// V-cycle (FP32), per level with right-hand side b, diagonal weights dw = omega / a_ii:
+//   pre-smoothing from x = 0 (one or two damped-Jacobi sweeps), residual, restriction (sum over the
+//   aggregate, in ascending row order), the coarse level, prolongation scaled by s, post-smoothing
+//   with the same sweeps.  Every sweep is one pass over the level's matrix with the smoother fused
+//   into the gather; the finest level reads the matrix's FP32 SELL-32 (or CSR-stream) copy, the
+//   coarse levels their CSR with 8 lanes per row.
+#include "amg.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <vector>
+
+namespace rsg {
+
+// ---------------------------------------------------------------- keys ----------------------
+
+// 32-bit integer hash (the "lowbias32" finalizer published by C. Wellons).
+__host__ __device__ __forceinline__ uint32_t amg_hash(uint32_t x)
+{
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+// 62-bit priority of node i: 30 hash bits above the index (unique).
+__host__ __device__ __forceinline__ uint64_t amg_key(uint32_t i) { return (uint64_t(amg_hash(i) >> 2) << 32) | i; }
+constexpr uint64_t kStateShift = 62;
+__device__ __forceinline__ uint32_t tup_state(uint64_t t) { return uint32_t(t >> kStateShift); }
+__device__ __forceinline__ uint32_t tup_index(uint64_t t) { return uint32_t(t & 0xffffffffu); }
+
+namespace {
+
+// ---------------------------------------------------------------- scan ----------------------
+
+constexpr int kScanThreads = 256;
+constexpr int kScanTile = 1024;  // 4 elements per thread
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *sh, uint32_t &total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+    }
+    __syncthreads();
+    if (lane == 31) sh[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < nw ? sh[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += t;
+        }
+        if (lane < nw) sh[32 + lane] = w;
+    }
+    __syncthreads();
+    total = sh[32 + nw - 1];
+    const uint32_t warp_off = warp ? sh[32 + warp - 1] : 0u;
+    return warp_off + inc - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const uint32_t *__restrict__ in, uint32_t n,
+                                                             uint32_t *__restrict__ sums)
+{
+    __shared__ uint32_t sh[64];
+    const size_t base = size_t(blockIdx.x) * kScanTile + size_t(threadIdx.x) * 4;
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+        if (base + k < n) s += in[base + k];
+    uint32_t total;
+    block_exclusive_scan(s, sh, total);
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_sums(uint32_t *sums, uint32_t nb)
+{
+    __shared__ uint32_t sh[64];
+    uint32_t carry = 0;
+    for (uint32_t c0 = 0; c0 < nb; c0 += kScanThreads) {
+        const uint32_t i = c0 + threadIdx.x;
+        const uint32_t v = i < nb ? sums[i] : 0u;
+        uint32_t total;
+        const uint32_t ex = block_exclusive_scan(v, sh, total);
+        if (i < nb) sums[i] = carry + ex;
+        carry += total;
+        __syncthreads();
+    }
+}
+
+// out[i] = sum of in[0..i); out[n] = the total (out holds n + 1 entries).
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(const uint32_t *__restrict__ in, uint32_t n,
+                                                             const uint32_t *__restrict__ sums,
+                                                             uint32_t *__restrict__ out)
+{
+    __shared__ uint32_t sh[64];
+    const size_t base = size_t(blockIdx.x) * kScanTile + size_t(threadIdx.x) * 4;
+    uint32_t v[4], s = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        v[k] = base + k < n ? in[base + k] : 0u;
+        s += v[k];
+    }
+    uint32_t total;
+    uint32_t run = sums[blockIdx.x] + block_exclusive_scan(s, sh, total);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        if (base + k < n) out[base + k] = run;
+        run += v[k];
+        if (base + k + 1 == n) out[n] = run;
+    }
+}
+
+// Exclusive scan of in[0..n) into out[0..n]; the total lands in *total_dev (device word).
+rsg_status scan_u32(rsg_context *ctx, AmgHierarchy *H, const uint32_t *in, uint32_t n, uint32_t *out)
+{
+    const uint32_t nb = (n + kScanTile - 1) / kScanTile;
+    if (n == 0) {
+        RSG_CHECK_CUDA(ctx, cudaMemsetAsync(out, 0, sizeof(uint32_t), ctx->stream));
+        return RSG_OK;
+    }
+    if (!H->scan_blocks.ensure(nb)) return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: scan workspace");
+    k_scan_tiles<<<nb, kScanThreads, 0, ctx->stream>>>(in, n, H->scan_blocks.p);
+    k_scan_sums<<<1, kScanThreads, 0, ctx->stream>>>(H->scan_blocks.p, nb);
+    k_scan_apply<<<nb, kScanThreads, 0, ctx->stream>>>(in, n, H->scan_blocks.p, out);
+    RSG_CHECK_CUDA(ctx, cudaGetLastError());
+    return RSG_OK;
+}
+
+// ---------------------------------------------------------------- set-up kernels ------------
+
+inline int grid_rows(uint64_t rows, int per_block = kBlock) { return int(std::min<uint64_t>((rows + per_block - 1) / per_block, 65535ull * 16)); }
+
+__global__ void k_amg_diag(uint32_t n, const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ci,
+                           const double *__restrict__ val, double *__restrict__ diag, float *__restrict__ dw)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double d = 0.0;
+        for (uint32_t j = rp[i]; j < rp[i + 1]; j++)
+            if (ci[j] == i) d = val[j];
+        diag[i] = d;
+        dw[i] = d != 0.0 ? float(double(kAmgOmega) / d) : 0.f;
+    }
+}
+
+__global__ void k_amg_strength(uint32_t n, const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ci,
+                               const double *__restrict__ val, const double *__restrict__ diag, double theta,
+                               uint8_t *__restrict__ smask)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double di = diag[i];
+        for (uint32_t j = rp[i]; j < rp[i + 1]; j++) {
+            const uint32_t c = ci[j];
+            bool s = false;
+            if (c != i && c < n) s = fabs(val[j]) >= theta * sqrt(fabs(di * diag[c])) && val[j] != 0.0;
+            smask[j] = s ? 1 : 0;
+        }
+    }
+}
+
+__global__ void k_amg_mis_init(uint32_t n, uint64_t *__restrict__ T)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        T[i] = (uint64_t(1) << kStateShift) | amg_key(i);
+}
+
+// out_i = max(in_i, max over strong neighbours j of in_j)
+__global__ void k_amg_nbmax(uint32_t n, const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ci,
+                            const uint8_t *__restrict__ smask, const uint64_t *__restrict__ in,
+                            uint64_t *__restrict__ out)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint64_t m = in[i];
+        for (uint32_t j = rp[i]; j < rp[i + 1]; j++)
+            if (smask[j]) m = max(m, in[ci[j]]);
+        out[i] = m;
+    }
+}
+
+// One synchronous round: an undecided node whose tuple is the distance-2 maximum becomes a root;
+// one that sees a root within distance 2 drops out.  flags[0] counts the nodes still undecided.
+__global__ void k_amg_mis_decide(uint32_t n, uint64_t *__restrict__ T, const uint64_t *__restrict__ M2,
+                                 unsigned int *flags)
+{
+    unsigned int left = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint64_t t = T[i];
+        if (tup_state(t) != 1) continue;
+        const uint64_t m = M2[i];
+        if (m == t) T[i] = (uint64_t(2) << kStateShift) | amg_key(i);
+        else if (tup_state(m) == 2) T[i] = amg_key(i);
+        else left++;
+    }
+    left = __reduce_add_sync(0xffffffffu, left);
+    if ((threadIdx.x & 31) == 0 && left) atomicAdd(&flags[0], left);
+}
+
+__global__ void k_amg_root_flags(uint32_t n, const uint64_t *__restrict__ T, uint32_t *__restrict__ flag)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        flag[i] = tup_state(T[i]) == 2 ? 1u : 0u;
+}
+
+// Roots take their number; others join the strong root neighbour with the largest tuple.
+__global__ void k_amg_join1(uint32_t n, const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ci,
+                            const uint8_t *__restrict__ smask, const uint64_t *__restrict__ T,
+                            const uint32_t *__restrict__ root_rank, uint32_t *__restrict__ agg)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (tup_state(T[i]) == 2) {
+            agg[i] = root_rank[i];
+            continue;
+        }
+        uint64_t best = 0;
+        for (uint32_t j = rp[i]; j < rp[i + 1]; j++) {
+            if (!smask[j]) continue;
+            const uint64_t t = T[ci[j]];
+            if (tup_state(t) == 2) best = max(best, t);
+        }
+        agg[i] = best ? root_rank[tup_index(best)] : kAmgUnset;
+    }
+}
+
+// A node left out joins the aggregate of its strong neighbour with the largest key among those
+// that joined in the first pass; flags[1] counts nodes still without an aggregate.
+__global__ void k_amg_join2(uint32_t n, const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ci,
+                            const uint8_t *__restrict__ smask, const uint32_t *__restrict__ agg_in,
+                            uint32_t *__restrict__ agg_out, unsigned int *flags)
+{
+    unsigned int left = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t a = agg_in[i];
+        if (a == kAmgUnset) {
+            uint64_t best = 0;
+            uint32_t pick = kAmgUnset;
+            for (uint32_t j = rp[i]; j < rp[i + 1]; j++) {
+                if (!smask[j]) continue;
+                const uint32_t c = ci[j];
+                if (agg_in[c] == kAmgUnset) continue;
+                const uint64_t k = amg_key(c) + 1;
+                if (k > best) {
+                    best = k;
+                    pick = agg_in[c];
+                }
+            }
+            a = pick;
+            if (a == kAmgUnset) left++;
+        }
+        agg_out[i] = a;
+    }
+    left = __reduce_add_sync(0xffffffffu, left);
+    if ((threadIdx.x & 31) == 0 && left) atomicAdd(&flags[1], left);
+}
+
+__global__ void k_amg_unset_flags(uint32_t n, const uint32_t *__restrict__ agg, uint32_t *__restrict__ flag)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        flag[i] = agg[i] == kAmgUnset ? 1u : 0u;
+}
+
+__global__ void k_amg_singletons(uint32_t n, uint32_t first, const uint32_t *__restrict__ rank,
+                                 uint32_t *__restrict__ agg)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (agg[i] == kAmgUnset) agg[i] = first + rank[i];
+}
+
+__global__ void k_amg_count(uint32_t n, const uint32_t *__restrict__ agg, uint32_t *__restrict__ cnt)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        atomicAdd(&cnt[agg[i]], 1u);
+}
+
+__global__ void k_amg_fill(uint32_t n, const uint32_t *__restrict__ agg, const uint32_t *__restrict__ ptr,
+                           uint32_t *__restrict__ cursor, uint32_t *__restrict__ rows)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t a = agg[i];
+        rows[ptr[a] + atomicAdd(&cursor[a], 1u)] = i;
+    }
+}
+
+// Sort each aggregate's rows ascending (insertion sort: aggregates are small) and record the
+// number of fine entries the aggregate's rows hold (flags[2] = the largest; flags[3] = the largest
+// aggregate).
+__global__ void k_amg_sort_agg(uint32_t nc, const uint32_t *__restrict__ ptr, uint32_t *__restrict__ rows,
+                               const uint32_t *__restrict__ rp, uint32_t *__restrict__ entries, unsigned int *flags)
+{
+    for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < nc; a += gridDim.x * blockDim.x) {
+        const uint32_t b = ptr[a], e = ptr[a + 1];
+        uint32_t tot = 0;
+        for (uint32_t k = b + 1; k < e; k++) {
+            const uint32_t v = rows[k];
+            uint32_t m = k;
+            while (m > b && rows[m - 1] > v) {
+                rows[m] = rows[m - 1];
+                m--;
+            }
+            rows[m] = v;
+        }
+        for (uint32_t k = b; k < e; k++) tot += rp[rows[k] + 1] - rp[rows[k]];
+        entries[a] = tot;
+        atomicMax(&flags[2], tot);
+        atomicMax(&flags[3], e - b);
+    }
+}
+
+// Galerkin coarse row I (one CTA): stage the entries of the aggregate's fine rows as keys
+// (J << 32 | position) with J the aggregate of the column, sort, add each run of equal J serially
+// in position order, and write the row's distinct (J, sum) pairs compacted at eoff[I].
+constexpr int kGalThreads = 128;
+__global__ void __launch_bounds__(kGalThreads) k_amg_galerkin(uint32_t nc, const uint32_t *__restrict__ ptr,
+                                                              const uint32_t *__restrict__ rows,
+                                                              const uint32_t *__restrict__ rp,
+                                                              const uint32_t *__restrict__ ci,
+                                                              const double *__restrict__ val,
+                                                              const uint32_t *__restrict__ agg,
+                                                              const uint32_t *__restrict__ eoff,
+                                                              uint32_t *__restrict__ tcol, double *__restrict__ tval,
+                                                              uint32_t *__restrict__ count)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ uint32_t sh_scan[64];
+    const uint32_t I = blockIdx.x;
+    if (I >= nc) return;
+    const uint32_t b = ptr[I], e = ptr[I + 1];
+    const uint32_t E = eoff[I + 1] - eoff[I];
+    uint32_t P = 32;
+    while (P < E) P <<= 1;
+    uint64_t *key = reinterpret_cast<uint64_t *>(smem);
+    double *sval = reinterpret_cast<double *>(key + P);
+    uint32_t *rstart = reinterpret_cast<uint32_t *>(sval + P);  // staging offset of each fine row
+    // staging offsets of the aggregate's rows (serial prefix: aggregates are short)
+    if (threadIdx.x == 0) {
+        uint32_t o = 0;
+        for (uint32_t k = b; k < e; k++) {
+            rstart[k - b] = o;
+            o += rp[rows[k] + 1] - rp[rows[k]];
+        }
+        rstart[e - b] = o;
+    }
+    __syncthreads();
+    const uint32_t nr = e - b;
+    for (uint32_t t = threadIdx.x; t < P; t += blockDim.x) {
+        if (t < E) {
+            uint32_t lo = 0, hi = nr;  // the row holding staging slot t: rstart[lo] <= t < rstart[lo+1]
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (rstart[mid] <= t) lo = mid;
+                else hi = mid;
+            }
+            const uint32_t i = rows[b + lo];
+            const uint32_t j = rp[i] + (t - rstart[lo]);
+            key[t] = (uint64_t(agg[ci[j]]) << 32) | t;
+            sval[t] = val[j];
+        } else {
+            key[t] = ~uint64_t(0);
+        }
+    }
+    __syncthreads();
+    // bitonic sort of the keys
+    for (uint32_t k = 2; k <= P; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t t = threadIdx.x; t < P; t += blockDim.x) {
+                const uint32_t u = t ^ j;
+                if (u > t) {
+                    const bool up = (t & k) == 0;
+                    const uint64_t a = key[t], c = key[u];
+                    if ((a > c) == up) {
+                        key[t] = c;
+                        key[u] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    // heads of runs of equal J, ranked in order
+    uint32_t base_rank = 0;
+    for (uint32_t t0 = 0; t0 < E; t0 += blockDim.x) {
+        const uint32_t t = t0 + threadIdx.x;
+        const bool head = t < E && (t == 0 || (key[t] >> 32) != (key[t - 1] >> 32));
+        uint32_t total;
+        const uint32_t rank = base_rank + block_exclusive_scan(head ? 1u : 0u, sh_scan, total);
+        if (head) {
+            const uint32_t J = uint32_t(key[t] >> 32);
+            double s = 0.0;
+            for (uint32_t k = t; k < E && uint32_t(key[k] >> 32) == J; k++) s += sval[uint32_t(key[k] & 0xffffffffu)];
+            tcol[size_t(eoff[I]) + rank] = J;
+            tval[size_t(eoff[I]) + rank] = s;
+        }
+        base_rank += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) count[I] = base_rank;
+}
+
+__global__ void k_amg_compact(uint32_t nc, const uint32_t *__restrict__ eoff, const uint32_t *__restrict__ count,
+                              const uint32_t *__restrict__ rp_c, const uint32_t *__restrict__ tcol,
+                              const double *__restrict__ tval, uint32_t *__restrict__ ci_c, double *__restrict__ val_c,
+                              float *__restrict__ val32_c)
+{
+    for (uint32_t I = blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += gridDim.x * blockDim.x) {
+        const uint32_t src = eoff[I], dst = rp_c[I];
+        for (uint32_t k = 0; k < count[I]; k++) {
+            ci_c[dst + k] = tcol[src + k];
+            val_c[dst + k] = tval[src + k];
+            val32_c[dst + k] = float(tval[src + k]);
+        }
+    }
+}
+
+// Dense inverse of the coarsest level (n <= kAmgCoarsest) by in-place Gauss-Jordan elimination in
+// shared memory (FP64, no pivoting: the matrix is SPD).  A pivot that is not positive leaves its
+// row and column at zero (the coarse correction then ignores that direction).
+__global__ void k_amg_dense_inverse(uint32_t n, const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ci,
+                                    const double *__restrict__ val, float *__restrict__ inv)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    double *a = reinterpret_cast<double *>(smem);
+    __shared__ double pinv;
+    __shared__ int skip;
+    for (uint32_t t = threadIdx.x; t < n * n; t += blockDim.x) a[t] = 0.0;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+        for (uint32_t j = rp[i]; j < rp[i + 1]; j++)
+            if (ci[j] < n) a[i * n + ci[j]] = val[j];
+    __syncthreads();
+    for (uint32_t k = 0; k < n; k++) {
+        if (threadIdx.x == 0) {
+            const double p = a[k * n + k];
+            skip = !(p > 0.0);
+            pinv = skip ? 0.0 : 1.0 / p;
+        }
+        __syncthreads();
+        if (skip) {
+            for (uint32_t t = threadIdx.x; t < n; t += blockDim.x) {
+                a[k * n + t] = 0.0;
+                a[t * n + k] = 0.0;
+            }
+            __syncthreads();
+            continue;
+        }
+        // row k scaled: a[k][j] *= pinv (j != k), a[k][k] = pinv
+        for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) a[k * n + j] = (j == k) ? pinv : a[k * n + j] * pinv;
+        __syncthreads();
+        // other rows: a[i][j] -= a[i][k] * a[k][j] (j != k), a[i][k] = -a[i][k] * pinv
+        for (uint32_t t = threadIdx.x; t < n * n; t += blockDim.x) {
+            const uint32_t i = t / n, j = t % n;
+            if (i == k || j == k) continue;
+            a[t] -= a[i * n + k] * a[k * n + j];
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+            if (i != k) a[i * n + k] = -a[i * n + k] * pinv;
+        __syncthreads();
+    }
+    for (uint32_t t = threadIdx.x; t < n * n; t += blockDim.x) inv[t] = float(a[t]);
+}
+
+__global__ void k_amg_d2f(uint32_t n, const double *__restrict__ src, float *__restrict__ dst)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = float(src[i]);
+}
+__global__ void k_amg_f2d(uint32_t n, const float *__restrict__ src, double *__restrict__ dst)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = double(src[i]);
+}
+
+// ---------------------------------------------------------------- V-cycle kernels -----------
+
+// Source of the iterate a sweep starts from (x in x + dw (b - A x)):
+//   kSrcDwB:     x = dw b             (the first sweep from x = 0, never stored)
+//   kSrcX:       x = xs               (a stored iterate)
+//   kSrcDwBCorr: x = dw b + s P e_c   (one sweep per side: coarse correction of the pre-smoothed x)
+//   kSrcXCorr:   x = xs + s P e_c     (two sweeps per side)
+enum { kSrcDwB = 0, kSrcX = 1, kSrcDwBCorr = 2, kSrcXCorr = 3 };
+// Output: kOutRes writes r = b - A x, kOutSmooth writes x + dw (b - A x).
+enum { kOutRes = 0, kOutSmooth = 1 };
+
+struct SweepArgs {
+    const float *b, *dw, *xs, *ec;
+    const uint32_t *agg;
+    float s;
+    float *out;
+};
+
+template <int SRC>
+__device__ __forceinline__ float sweep_x(const SweepArgs &a, uint32_t c)
+{
+    float x = (SRC == kSrcDwB || SRC == kSrcDwBCorr) ? a.dw[c] * a.b[c] : a.xs[c];
+    if (SRC == kSrcDwBCorr || SRC == kSrcXCorr) x = fmaf(a.s, a.ec[a.agg[c]], x);
+    return x;
+}
+
+__device__ __forceinline__ void amg_finalize(CgState *st, double rz, int mode, double *rz_out)
+{
+    if (!st) {
+        if (rz_out) *rz_out = rz;
+        return;
+    }
+    if (mode == 0) {
+        st->rho_new = rz;
+        st->rho = rz;
+        st->beta = 0.0;
+    } else if (st->need_check) {
+        finalize_check_mixed(st, rz, st->check_rn);
+    } else {
+        st->rho_new = rz;
+        st->beta = rz / st->rho;
+    }
+}
+
+// Sweep over the finest level (the caller's matrix, FP32 copy).  FINAL: the output is z of the
+// preconditioner; r^T z is reduced and the CG state finalized.
+template <int RPW, int SRC, int OUT, bool FINAL>
+__global__ void __launch_bounds__(kBlock) k_amg_fine(Csr<float> M, Sell<float> S, int use_sell, SweepArgs a,
+                                                     double *partials, unsigned int *ticket, CgState *st, int mode,
+                                                     double *rz_out)
+{
+    pdl_wait();
+    pdl_release();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double sh[32];
+    if (st && st->done) return;
+    Dot2 rz;
+    auto gx = [&](uint32_t c) { return sweep_x<SRC>(a, c); };
+    auto epi = [&](uint32_t row, float ax) {
+        const float res = a.b[row] - ax;
+        float o;
+        if (OUT == kOutRes) o = res;
+        else o = fmaf(a.dw[row], res, sweep_x<SRC>(a, row));
+        a.out[row] = o;
+        if (FINAL) rz.add_prod(a.b[row], o);
+    };
+    unsigned int *errw = st ? &st->ticket[7] : (ticket ? ticket + 1 : nullptr);
+    for_rows_any<float, RPW>(M, S, use_sell != 0, gx, epi, smem_raw, errw, true);
+    if (FINAL) {
+        double acc[1] = {rz.value()};
+        double tot[1];
+        if (grid_sum<1>(acc, partials, ticket, sh, tot) && threadIdx.x == 0) amg_finalize(st, tot[0], mode, rz_out);
+    }
+}
+
+// Sweep over a coarse level (CSR, 8 lanes per row).
+constexpr int kLanes = 8;
+template <int SRC, int OUT>
+__global__ void __launch_bounds__(kBlock) k_amg_coarse(uint32_t n, const uint32_t *__restrict__ rp,
+                                                       const uint32_t *__restrict__ ci, const float *__restrict__ val,
+                                                       SweepArgs a, const CgState *st)
+{
+    pdl_wait();
+    pdl_release();
+    if (st && st->done) return;
+    const int lane = threadIdx.x & (kLanes - 1);
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // warp index
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t sub = (threadIdx.x & 31) / kLanes;                   // row within the warp's group of 4
+    for (uint32_t base = gw * (32 / kLanes); base < n; base += warps * (32 / kLanes)) {
+        const uint32_t row = base + sub;
+        float acc = 0.f;
+        if (row < n)
+            for (uint32_t j = rp[row] + lane; j < rp[row + 1]; j += kLanes) acc = fmaf(val[j], sweep_x<SRC>(a, ci[j]), acc);
+#pragma unroll
+        for (int o = kLanes / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0 && row < n) {
+            const float res = a.b[row] - acc;
+            a.out[row] = OUT == kOutRes ? res : fmaf(a.dw[row], res, sweep_x<SRC>(a, row));
+        }
+    }
+}
+
+// b_c[I] = sum of r over the aggregate's rows (ascending order).
+__global__ void k_amg_restrict(uint32_t nc, const uint32_t *__restrict__ ptr, const uint32_t *__restrict__ rows,
+                               const float *__restrict__ r, float *__restrict__ bc, const CgState *st)
+{
+    pdl_wait();
+    pdl_release();
+    if (st && st->done) return;
+    for (uint32_t I = blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += gridDim.x * blockDim.x) {
+        float s = 0.f;
+        for (uint32_t k = ptr[I]; k < ptr[I + 1]; k++) s += r[rows[k]];
+        bc[I] = s;
+    }
+}
+
+// e = inv b on the coarsest level (dense, one CTA).
+__global__ void k_amg_dense_apply(uint32_t n, const float *__restrict__ inv, const float *__restrict__ b,
+                                  float *__restrict__ e, const CgState *st)
+{
+    pdl_wait();
+    pdl_release();
+    if (st && st->done) return;
+    __shared__ float sb[kAmgCoarsest];
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sb[i] = b[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (uint32_t i = warp; i < n; i += nw) {
+        float s = 0.f;
+        for (uint32_t j = lane; j < n; j += 32) s = fmaf(inv[size_t(i) * n + j], sb[j], s);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) e[i] = s;
+    }
+}
+
+// Single-level fallbacks (a matrix with no coarse level): z = inv r when the matrix itself is
+// small enough to invert densely, else one damped-Jacobi step z = dw r; then r^T z.
+__global__ void k_amg_jacobi(uint32_t n, const float *__restrict__ dw, const float *__restrict__ r,
+                             float *__restrict__ z, const CgState *st)
+{
+    pdl_wait();
+    pdl_release();
+    if (st && st->done) return;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) z[i] = dw[i] * r[i];
+}
+
+__global__ void k_amg_rz(uint32_t n, const float *__restrict__ r, const float *__restrict__ z, double *partials,
+                         unsigned int *ticket, CgState *st, int mode, double *rz_out)
+{
+    pdl_wait();
+    pdl_release();
+    __shared__ double sh[32];
+    if (st && st->done) return;
+    Dot2 rz;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) rz.add_prod(r[i], z[i]);
+    double acc[1] = {rz.value()};
+    double tot[1];
+    if (grid_sum<1>(acc, partials, ticket, sh, tot) && threadIdx.x == 0) amg_finalize(st, tot[0], mode, rz_out);
+}
+
+// ---------------------------------------------------------------- host: set-up --------------
+
+rsg_status read_flags(rsg_context *ctx, AmgHierarchy *H, int count)
+{
+    RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(H->flags_h, H->flags, count * sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                                        ctx->stream));
+    RSG_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return RSG_OK;
+}
+
+rsg_status read_u32(rsg_context *ctx, AmgHierarchy *H, const uint32_t *dev, uint32_t *host)
+{
+    RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(H->flags_h + 8, dev, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    RSG_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    *host = H->flags_h[8];
+    return RSG_OK;
+}
+
+// Aggregates of level l (sets F.agg, F.agg_ptr, F.agg_rows and the next level's size).
+rsg_status build_aggregates(rsg_context *ctx, AmgHierarchy *H, AmgLevel &F, uint32_t *n_coarse, uint32_t *max_entries,
+                            uint32_t *max_size)
+{
+    const uint32_t n = F.n;
+    const int g = grid_rows(n);
+    cudaStream_t s = ctx->stream;
+    if (!H->T.ensure(n) || !H->M1.ensure(n) || !H->M2.ensure(n) || !H->smask.ensure(F.nnz + 1) ||
+        !H->u1.ensure(size_t(n) + 1) || !H->u2.ensure(size_t(n) + 1) || !F.agg.ensure(n))
+        return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: set-up workspace");
+    k_amg_strength<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, F.val, F.diag.p, kAmgTheta, H->smask.p);
+    k_amg_mis_init<<<g, kBlock, 0, s>>>(n, H->T.p);
+    RSG_CHECK_CUDA(ctx, cudaGetLastError());
+    // synchronous rounds until no node is undecided (checked every two rounds)
+    for (uint32_t round = 0;; round += 2) {
+        RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->flags, 0, sizeof(unsigned int), s));
+        for (int k = 0; k < 2; k++) {
+            k_amg_nbmax<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, H->smask.p, H->T.p, H->M1.p);
+            k_amg_nbmax<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, H->smask.p, H->M1.p, H->M2.p);
+            if (k == 1) RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->flags, 0, sizeof(unsigned int), s));
+            k_amg_mis_decide<<<g, kBlock, 0, s>>>(n, H->T.p, H->M2.p, H->flags);
+        }
+        RSG_TRY(read_flags(ctx, H, 1));
+        H->mis_rounds += 2;
+        if (H->flags_h[0] == 0) break;
+        if (round > 256) return set_error(ctx, RSG_ERR_CUDA, "amg: independent set did not converge");
+    }
+    // root numbering, joins
+    k_amg_root_flags<<<g, kBlock, 0, s>>>(n, H->T.p, H->u1.p);
+    RSG_TRY(scan_u32(ctx, H, H->u1.p, n, H->u2.p));
+    uint32_t nc = 0;
+    RSG_TRY(read_u32(ctx, H, H->u2.p + n, &nc));
+    k_amg_join1<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, H->smask.p, H->T.p, H->u2.p, H->u1.p);
+    RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->flags, 0, 4 * sizeof(unsigned int), s));
+    k_amg_join2<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, H->smask.p, H->u1.p, F.agg.p, H->flags);
+    RSG_TRY(read_flags(ctx, H, 2));
+    if (H->flags_h[1] > 0) {  // singletons for nodes without any strong path to a root
+        k_amg_unset_flags<<<g, kBlock, 0, s>>>(n, F.agg.p, H->u1.p);
+        RSG_TRY(scan_u32(ctx, H, H->u1.p, n, H->u2.p));
+        k_amg_singletons<<<g, kBlock, 0, s>>>(n, nc, H->u2.p, F.agg.p);
+        nc += H->flags_h[1];
+    }
+    // aggregate lists
+    if (!F.agg_ptr.ensure(size_t(nc) + 1) || !F.agg_rows.ensure(n) || !H->u3.ensure(size_t(nc) + 1))
+        return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: aggregate lists");
+    RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->u3.p, 0, size_t(nc) * sizeof(uint32_t), s));
+    k_amg_count<<<g, kBlock, 0, s>>>(n, F.agg.p, H->u3.p);
+    RSG_TRY(scan_u32(ctx, H, H->u3.p, nc, F.agg_ptr.p));
+    RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->u3.p, 0, size_t(nc) * sizeof(uint32_t), s));
+    k_amg_fill<<<g, kBlock, 0, s>>>(n, F.agg.p, F.agg_ptr.p, H->u3.p, F.agg_rows.p);
+    RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->flags + 2, 0, 2 * sizeof(unsigned int), s));
+    k_amg_sort_agg<<<grid_rows(nc), kBlock, 0, s>>>(nc, F.agg_ptr.p, F.agg_rows.p, F.rp, H->u3.p, H->flags);
+    RSG_CHECK_CUDA(ctx, cudaGetLastError());
+    RSG_TRY(read_flags(ctx, H, 4));
+    *n_coarse = nc;
+    *max_entries = H->flags_h[2];
+    *max_size = H->flags_h[3];
+    return RSG_OK;
+}
+
+// Coarse matrix C = P^T A P of level F into level Cl (F.agg_* and H->u3 = entries per coarse row).
+rsg_status build_galerkin(rsg_context *ctx, AmgHierarchy *H, AmgLevel &F, AmgLevel &Cl, uint32_t nc, uint32_t emax,
+                          uint32_t max_size)
+{
+    cudaStream_t s = ctx->stream;
+    // staging offsets (one slot per fine entry)
+    if (!H->u1.ensure(size_t(nc) + 1) || !H->u2.ensure(size_t(nc) + 1) || !H->tcol.ensure(F.nnz + 1) ||
+        !H->tval.ensure(F.nnz + 1))
+        return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: Galerkin staging");
+    RSG_TRY(scan_u32(ctx, H, H->u3.p, nc, H->u1.p));  // eoff
+    uint32_t P = 32;
+    while (P < emax) P <<= 1;
+    // keys and values (16 bytes per padded slot), then the staging offsets of the aggregate's rows
+    const size_t smem = size_t(P) * 16 + (size_t(max_size) + 1) * sizeof(uint32_t);
+    cudaFuncSetAttribute(k_amg_galerkin, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    k_amg_galerkin<<<nc, kGalThreads, smem, s>>>(nc, F.agg_ptr.p, F.agg_rows.p, F.rp, F.ci, F.val, F.agg.p, H->u1.p,
+                                                  H->tcol.p, H->tval.p, H->u2.p);
+    RSG_CHECK_CUDA(ctx, cudaGetLastError());
+    // coarse row pointer, then compact
+    if (!Cl.own_rp.ensure(size_t(nc) + 1)) return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: coarse matrix");
+    RSG_TRY(scan_u32(ctx, H, H->u2.p, nc, Cl.own_rp.p));
+    uint32_t nnz = 0;
+    RSG_TRY(read_u32(ctx, H, Cl.own_rp.p + nc, &nnz));
+    if (!Cl.own_ci.ensure(size_t(nnz) + 1) || !Cl.own_val.ensure(size_t(nnz) + 1) || !Cl.own_val32.ensure(size_t(nnz) + 1))
+        return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: coarse matrix");
+    k_amg_compact<<<grid_rows(nc), kBlock, 0, s>>>(nc, H->u1.p, H->u2.p, Cl.own_rp.p, H->tcol.p, H->tval.p,
+                                                   Cl.own_ci.p, Cl.own_val.p, Cl.own_val32.p);
+    RSG_CHECK_CUDA(ctx, cudaGetLastError());
+    Cl.n = nc;
+    Cl.nnz = nnz;
+    Cl.rp = Cl.own_rp.p;
+    Cl.ci = Cl.own_ci.p;
+    Cl.val = Cl.own_val.p;
+    Cl.val32 = Cl.own_val32.p;
+    return RSG_OK;
+}
+
+rsg_status level_vectors(rsg_context *ctx, AmgLevel &l)
+{
+    if (!l.diag.ensure(l.n) || !l.dw.ensure(l.n) || !l.b.ensure(l.n) || !l.r.ensure(l.n) || !l.x1.ensure(l.n) ||
+        !l.x2.ensure(l.n) || !l.e.ensure(l.n))
+        return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: level vectors");
+    k_amg_diag<<<grid_rows(l.n), kBlock, 0, ctx->stream>>>(l.n, l.rp, l.ci, l.val, l.diag.p, l.dw.p);
+    RSG_CHECK_CUDA(ctx, cudaGetLastError());
+    return RSG_OK;
+}
+
+}  // namespace
+
+void amg_free(AmgHierarchy *H)
+{
+    if (!H) return;
+    for (auto &l : H->L) {
+        l.own_rp.release();
+        l.own_ci.release();
+        l.own_val.release();
+        l.own_val32.release();
+        l.diag.release();
+        l.dw.release();
+        l.agg.release();
+        l.agg_ptr.release();
+        l.agg_rows.release();
+        l.b.release();
+        l.r.release();
+        l.x1.release();
+        l.x2.release();
+        l.e.release();
+    }
+    H->coarse_inv.release();
+    H->T.release();
+    H->M1.release();
+    H->M2.release();
+    H->smask.release();
+    H->u1.release();
+    H->u2.release();
+    H->u3.release();
+    H->scan_blocks.release();
+    H->tcol.release();
+    H->tval.release();
+    if (H->flags) cudaFree(H->flags);
+    if (H->flags_h) cudaFreeHost(H->flags_h);
+    delete H;
+}
+
+void amg_release(void *h) { amg_free(static_cast<AmgHierarchy *>(h)); }
+
+AmgHierarchy *amg_of(const rsg_csr *A) { return static_cast<AmgHierarchy *>(A->amg); }
+
+rsg_status amg_setup(rsg_context *ctx, rsg_csr *A)
+{
+    const auto t0 = std::chrono::steady_clock::now();
+    AmgHierarchy *H = amg_of(A);
+    if (!H) {
+        H = new AmgHierarchy;
+        if (cudaMalloc(&H->flags, 16 * sizeof(unsigned int)) != cudaSuccess ||
+            cudaMallocHost(&H->flags_h, 16 * sizeof(unsigned int)) != cudaSuccess) {
+            amg_free(H);
+            return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: counters");
+        }
+        A->amg = H;
+    }
+    H->mis_rounds = 0;
+    H->levels = 1;
+    H->dense_coarsest = false;
+    AmgLevel &L0 = H->L[0];
+    L0.n = A->n;
+    L0.nnz = A->nnz;
+    L0.rp = A->rp;
+    L0.ci = A->ci;
+    L0.val = A->val;
+    L0.val32 = A->val32;
+    RSG_TRY(level_vectors(ctx, L0));
+    while (H->levels < kAmgMaxLevels) {
+        AmgLevel &F = H->L[H->levels - 1];
+        if (F.n <= kAmgCoarsest) {
+            H->dense_coarsest = true;
+            break;
+        }
+        uint32_t nc = 0, emax = 0, max_size = 0;
+        RSG_TRY(build_aggregates(ctx, H, F, &nc, &emax, &max_size));
+        // stop when coarsening stalls or a coarse row would not fit the staging buffer
+        if (nc == 0 || uint64_t(nc) * 10 > uint64_t(F.n) * 9 || emax > kAmgMaxEntries || max_size > kAmgMaxEntries)
+            break;
+        AmgLevel &Cl = H->L[H->levels];
+        RSG_TRY(build_galerkin(ctx, H, F, Cl, nc, emax, max_size));
+        RSG_TRY(level_vectors(ctx, Cl));
+        H->levels++;
+    }
+    AmgLevel &last = H->L[H->levels - 1];
+    if (H->dense_coarsest) {
+        if (!H->coarse_inv.ensure(size_t(kAmgCoarsest) * kAmgCoarsest))
+            return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: coarse inverse");
+        const size_t smem = size_t(last.n) * last.n * sizeof(double);
+        cudaFuncSetAttribute(k_amg_dense_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        k_amg_dense_inverse<<<1, 512, smem, ctx->stream>>>(last.n, last.rp, last.ci, last.val, H->coarse_inv.p);
+        RSG_CHECK_CUDA(ctx, cudaGetLastError());
+    }
+    RSG_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    H->seconds_setup = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return RSG_OK;
+}
+
+// ---------------------------------------------------------------- host: V-cycle -------------
+
+namespace {
+
+int coarse_grid(rsg_context *ctx, uint32_t n)
+{
+    const long long threads = (long long)n * kLanes;
+    return std::max(1, std::min<int>(int((threads + kBlock - 1) / kBlock), ctx->num_sms * 8));
+}
+
+template <int RPW>
+struct FineLaunch {
+    Csr<float> M;
+    Sell<float> S;
+    int use_sell, grid;
+    size_t smem;
+};
+
+template <int RPW, int SRC, int OUT, bool FINAL>
+void fine_sweep(rsg_context *ctx, const FineLaunch<RPW> &f, const SweepArgs &a, double *partials,
+                unsigned int *ticket, CgState *st, int mode, double *rz_out, bool pdl)
+{
+    launch_k(ctx->stream, pdl, k_amg_fine<RPW, SRC, OUT, FINAL>, f.grid, kBlock, f.smem, f.M, f.S, f.use_sell, a,
+             partials, ticket, st, mode, rz_out);
+}
+
+template <int SRC, int OUT>
+void coarse_sweep(rsg_context *ctx, const AmgLevel &l, const SweepArgs &a, const CgState *st, bool pdl)
+{
+    launch_k(ctx->stream, pdl, k_amg_coarse<SRC, OUT>, coarse_grid(ctx, l.n), kBlock, 0, l.n, l.rp, l.ci, l.val32, a,
+             st);
+}
+
+// Pre-smoothing, residual and restriction of level l (b given), then the coarser levels, then
+// prolongation and post-smoothing into `out`.  Level 0 is handled by the caller (fine kernels).
+void coarse_levels(rsg_context *ctx, const AmgHierarchy *H, int l, int sweeps, const CgState *st, bool pdl);
+
+void down_restrict(rsg_context *ctx, const AmgHierarchy *H, int l, const CgState *st, bool pdl)
+{
+    const AmgLevel &F = H->L[l], &C = H->L[l + 1];
+    launch_k(ctx->stream, pdl, k_amg_restrict, grid_rows(C.n), kBlock, 0, C.n, (const uint32_t *)F.agg_ptr.p,
+             (const uint32_t *)F.agg_rows.p, (const float *)F.r.p, C.b.p, st);
+}
+
+void coarse_levels(rsg_context *ctx, const AmgHierarchy *H, int l, int sweeps, const CgState *st, bool pdl)
+{
+    const AmgLevel &F = H->L[l];
+    const bool last = (l == H->levels - 1);
+    if (last) {
+        if (H->dense_coarsest) {
+            launch_k(ctx->stream, pdl, k_amg_dense_apply, 1, 256, 0, F.n, (const float *)H->coarse_inv.p,
+                     (const float *)F.b.p, F.e.p, st);
+        } else {  // coarsening stalled above the dense limit: smoothing sweeps only
+            SweepArgs a{F.b.p, F.dw.p, nullptr, nullptr, nullptr, 0.f, F.x1.p};
+            coarse_sweep<kSrcDwB, kOutSmooth>(ctx, F, a, st, pdl);
+            for (int k = 0; k < 7; k++) {
+                SweepArgs a2{F.b.p, F.dw.p, (k & 1) ? F.x2.p : F.x1.p, nullptr, nullptr, 0.f, (k & 1) ? F.x1.p : F.x2.p};
+                coarse_sweep<kSrcX, kOutSmooth>(ctx, F, a2, st, pdl);
+            }
+            SweepArgs a3{F.b.p, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, F.e.p};
+            coarse_sweep<kSrcX, kOutSmooth>(ctx, F, a3, st, pdl);
+        }
+        return;
+    }
+    const AmgLevel &C = H->L[l + 1];
+    const float s = sweeps == 2 ? kAmgScale2 : kAmgScale1;
+    if (sweeps == 2) {
+        SweepArgs a1{F.b.p, F.dw.p, nullptr, nullptr, nullptr, 0.f, F.x1.p};
+        coarse_sweep<kSrcDwB, kOutSmooth>(ctx, F, a1, st, pdl);
+        SweepArgs a2{F.b.p, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, F.r.p};
+        coarse_sweep<kSrcX, kOutRes>(ctx, F, a2, st, pdl);
+    } else {
+        SweepArgs a1{F.b.p, F.dw.p, nullptr, nullptr, nullptr, 0.f, F.r.p};
+        coarse_sweep<kSrcDwB, kOutRes>(ctx, F, a1, st, pdl);
+    }
+    down_restrict(ctx, H, l, st, pdl);
+    coarse_levels(ctx, H, l + 1, sweeps, st, pdl);
+    if (sweeps == 2) {
+        SweepArgs u1{F.b.p, F.dw.p, F.x1.p, C.e.p, F.agg.p, s, F.x2.p};
+        coarse_sweep<kSrcXCorr, kOutSmooth>(ctx, F, u1, st, pdl);
+        SweepArgs u2{F.b.p, F.dw.p, F.x2.p, nullptr, nullptr, 0.f, F.e.p};
+        coarse_sweep<kSrcX, kOutSmooth>(ctx, F, u2, st, pdl);
+    } else {
+        SweepArgs u1{F.b.p, F.dw.p, nullptr, C.e.p, F.agg.p, s, F.e.p};
+        coarse_sweep<kSrcDwBCorr, kOutSmooth>(ctx, F, u1, st, pdl);
+    }
+}
+
+template <int RPW>
+rsg_status vcycle_typed(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H, const float *r, float *z,
+                        int sweeps, double *partials, unsigned int *ticket, CgState *st, int mode, double *rz_out,
+                        bool pdl)
+{
+    FineLaunch<RPW> f;
+    f.M = view<float>(A, true);
+    f.S = sell_view<float>(A);
+    f.use_sell = A->use_sell;
+    f.smem = A->use_sell ? 0 : tma_smem<float>();
+    if (!A->use_sell) {
+        cudaFuncSetAttribute(k_amg_fine<RPW, kSrcDwB, kOutRes, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(f.smem));
+        cudaFuncSetAttribute(k_amg_fine<RPW, kSrcDwB, kOutSmooth, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(f.smem));
+        cudaFuncSetAttribute(k_amg_fine<RPW, kSrcX, kOutRes, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(f.smem));
+        cudaFuncSetAttribute(k_amg_fine<RPW, kSrcXCorr, kOutSmooth, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(f.smem));
+        cudaFuncSetAttribute(k_amg_fine<RPW, kSrcX, kOutSmooth, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(f.smem));
+        cudaFuncSetAttribute(k_amg_fine<RPW, kSrcDwBCorr, kOutSmooth, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(f.smem));
+    }
+    f.grid = spmv_grid(ctx, A, (const void *)k_amg_fine<RPW, kSrcX, kOutSmooth, true>, f.smem, RPW);
+    const AmgLevel &F = H->L[0];
+    if (H->levels < 2) {
+        if (H->dense_coarsest)
+            launch_k(ctx->stream, pdl, k_amg_dense_apply, 1, 256, 0, F.n, (const float *)H->coarse_inv.p, r, z,
+                     (const CgState *)st);
+        else
+            launch_k(ctx->stream, pdl, k_amg_jacobi, grid_rows(F.n), kBlock, 0, F.n, (const float *)F.dw.p, r, z,
+                     (const CgState *)st);
+        const int g = std::min(grid_rows(F.n), kMaxGrid);
+        launch_k(ctx->stream, pdl, k_amg_rz, g, kBlock, 0, F.n, r, (const float *)z, partials, ticket, st, mode, rz_out);
+        return RSG_OK;
+    }
+    const AmgLevel &C = H->L[1];
+    const float s = sweeps == 2 ? kAmgScale2 : kAmgScale1;
+    if (sweeps == 2) {
+        SweepArgs a1{r, F.dw.p, nullptr, nullptr, nullptr, 0.f, F.x1.p};
+        fine_sweep<RPW, kSrcDwB, kOutSmooth, false>(ctx, f, a1, partials, ticket, st, mode, rz_out, pdl);
+        SweepArgs a2{r, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, F.r.p};
+        fine_sweep<RPW, kSrcX, kOutRes, false>(ctx, f, a2, partials, ticket, st, mode, rz_out, pdl);
+    } else {
+        SweepArgs a1{r, F.dw.p, nullptr, nullptr, nullptr, 0.f, F.r.p};
+        fine_sweep<RPW, kSrcDwB, kOutRes, false>(ctx, f, a1, partials, ticket, st, mode, rz_out, pdl);
+    }
+    down_restrict(ctx, H, 0, st, pdl);
+    coarse_levels(ctx, H, 1, sweeps, st, pdl);
+    if (sweeps == 2) {
+        SweepArgs u1{r, F.dw.p, F.x1.p, C.e.p, F.agg.p, s, F.x2.p};
+        fine_sweep<RPW, kSrcXCorr, kOutSmooth, false>(ctx, f, u1, partials, ticket, st, mode, rz_out, pdl);
+        SweepArgs u2{r, F.dw.p, F.x2.p, nullptr, nullptr, 0.f, z};
+        fine_sweep<RPW, kSrcX, kOutSmooth, true>(ctx, f, u2, partials, ticket, st, mode, rz_out, pdl);
+    } else {
+        SweepArgs u1{r, F.dw.p, nullptr, C.e.p, F.agg.p, s, z};
+        fine_sweep<RPW, kSrcDwBCorr, kOutSmooth, true>(ctx, f, u1, partials, ticket, st, mode, rz_out, pdl);
+    }
+    return RSG_OK;
+}
+
+}  // namespace
+
+namespace {
+template <int RPW>
+rsg_status profile_typed_sweep(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H, const float *r, float *z)
+{
+    FineLaunch<RPW> f;
+    f.M = view<float>(A, true);
+    f.S = sell_view<float>(A);
+    f.use_sell = A->use_sell;
+    f.smem = A->use_sell ? 0 : tma_smem<float>();
+    if (!A->use_sell)
+        cudaFuncSetAttribute(k_amg_fine<RPW, kSrcDwBCorr, kOutSmooth, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(f.smem));
+    f.grid = spmv_grid(ctx, A, (const void *)k_amg_fine<RPW, kSrcX, kOutSmooth, true>, f.smem, RPW);
+    const AmgLevel &F = H->L[0];
+    SweepArgs a{r, F.dw.p, nullptr, H->L[1].e.p, F.agg.p, kAmgScale1, z};
+    fine_sweep<RPW, kSrcDwBCorr, kOutSmooth, false>(ctx, f, a, nullptr, nullptr, nullptr, 0, nullptr, false);
+    RSG_CHECK_CUDA(ctx, cudaGetLastError());
+    return RSG_OK;
+}
+}  // namespace
+
+rsg_status amg_profile_launch(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H, const float *r, float *z)
+{
+    if (!H || H->levels < 2) return set_error(ctx, RSG_ERR_UNSUPPORTED, "amg: the matrix has no coarse level");
+    RSG_RPW_DISPATCH(pick_rpw(A), return profile_typed_sweep<RPW>(ctx, A, H, r, z));
+    return RSG_ERR_UNSUPPORTED;
+}
+
+rsg_status amg_vcycle(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H, const float *r, float *z, int sweeps,
+                      double *partials, unsigned int *ticket, CgState *st, int mode, double *rz_out, bool pdl)
+{
+    if (!H || H->levels < 1) return set_error(ctx, RSG_ERR_INVALID_ARG, "amg: no hierarchy");
+    RSG_RPW_DISPATCH(pick_rpw(A),
+                     return vcycle_typed<RPW>(ctx, A, H, r, z, sweeps, partials, ticket, st, mode, rz_out, pdl));
+    return RSG_ERR_UNSUPPORTED;
+}
+
+}  // namespace rsg
+
+// ---------------------------------------------------------------- C ABI -----------------------
+
+using namespace rsg;
+
+extern "C" {
+
+rsg_status rsg_amg_setup(rsg_context *ctx, rsg_csr *A, rsg_amg_info *info)
+{
+    if (!ctx || !A) return set_error(ctx, RSG_ERR_INVALID_ARG, "amg_setup: bad arguments");
+    RSG_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
+    RSG_TRY(amg_setup(ctx, A));
+    if (info) {
+        const AmgHierarchy *H = amg_of(A);
+        std::memset(info, 0, sizeof(*info));
+        info->levels = uint32_t(H->levels);
+        info->dense_coarsest = H->dense_coarsest ? 1u : 0u;
+        for (int l = 0; l < H->levels && l < 16; l++) {
+            info->rows[l] = H->L[l].n;
+            info->nnz[l] = H->L[l].nnz;
+        }
+        info->mis_rounds = H->mis_rounds;
+        info->seconds_setup = H->seconds_setup;
+    }
+    return RSG_OK;
+}
+
+rsg_status rsg_amg_level(rsg_context *ctx, const rsg_csr *A, uint32_t level, uint32_t *agg, uint32_t *row_ptr,
+                         uint32_t *col_idx, double *values)
+{
+    const AmgHierarchy *H = A ? amg_of(A) : nullptr;
+    if (!ctx || !H || level >= uint32_t(H->levels)) return set_error(ctx, RSG_ERR_INVALID_ARG, "amg_level: bad level");
+    RSG_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
+    RSG_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    const AmgLevel &l = H->L[level];
+    if (agg) {
+        if (int(level) + 1 >= H->levels) return set_error(ctx, RSG_ERR_INVALID_ARG, "amg_level: the last level has no aggregates");
+        RSG_CHECK_CUDA(ctx, cudaMemcpy(agg, l.agg.p, size_t(l.n) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    }
+    if (row_ptr) RSG_CHECK_CUDA(ctx, cudaMemcpy(row_ptr, l.rp, (size_t(l.n) + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (col_idx) RSG_CHECK_CUDA(ctx, cudaMemcpy(col_idx, l.ci, size_t(l.nnz) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (values) RSG_CHECK_CUDA(ctx, cudaMemcpy(values, l.val, size_t(l.nnz) * sizeof(double), cudaMemcpyDeviceToHost));
+    return RSG_OK;
+}
+
+rsg_status rsg_amg_apply(rsg_context *ctx, rsg_csr *A, const double *r, double *z, uint32_t sweeps)
+{
+    AmgHierarchy *H = A ? amg_of(A) : nullptr;
+    if (!ctx || !H || !r || !z || (sweeps != 1 && sweeps != 2))
+        return set_error(ctx, RSG_ERR_INVALID_ARG, "amg_apply: bad arguments (call rsg_amg_setup first)");
+    RSG_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
+    const uint32_t n = A->n;
+    // FP32 copies of r and z in level 0's b and e (unused by the V-cycle on the finest level)
+    AmgLevel &L0 = H->L[0];
+    const size_t red = arena_bytes(kMaxGrid, sizeof(double)) + arena_bytes(8, sizeof(double));
+    RSG_TRY(arena_reserve(ctx, red));
+    double *partials = arena_take<double>(ctx, kMaxGrid);
+    double *scal = arena_take<double>(ctx, 8);
+    unsigned int *ticket = reinterpret_cast<unsigned int *>(scal + 4);
+    RSG_CHECK_CUDA(ctx, cudaMemsetAsync(scal, 0, 8 * sizeof(double), ctx->stream));
+    const int g = std::min(grid_rows(n), kMaxGrid);
+    k_amg_d2f<<<g, kBlock, 0, ctx->stream>>>(n, r, L0.b.p);
+    RSG_TRY(amg_vcycle(ctx, A, H, L0.b.p, L0.e.p, int(sweeps), partials, ticket, nullptr, 0, scal, false));
+    k_amg_f2d<<<g, kBlock, 0, ctx->stream>>>(n, L0.e.p, z);
+    RSG_CHECK_CUDA(ctx, cudaGetLastError());
+    RSG_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return RSG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,100 @@
+// Internal interface of the multilevel aggregation preconditioner (RSG_PREC_AMG).
+//
+// No counterpart in the reference, whose preconditioners are NONE / JACOBI / BLOCK_JACOBI
+// (src/rmatrixpreconditioner.cpp).  The hierarchy is built on the GPU from the matrix's current
+// values (strength of connection, aggregates rooted at a distance-2 independent set of hashed
+// priorities, piecewise-constant prolongation, Galerkin coarse matrices summed in a fixed order,
+// dense inverse of the coarsest level) and applied as a symmetric FP32 V-cycle with damped-Jacobi
+// smoothing and a scaled coarse correction, so that CG sees one fixed SPD operator.
+#pragma once
+
+#include "krylov.cuh"
+
+namespace rsg {
+
+constexpr int kAmgMaxLevels = 12;
+constexpr uint32_t kAmgCoarsest = 128;     // rows at or below which a level is inverted densely
+constexpr uint32_t kAmgMaxEntries = 4096;  // fine entries gathered into one coarse row (Galerkin staging)
+constexpr double kAmgTheta = 0.08;         // strength threshold |a_ij| >= theta sqrt(|a_ii a_jj|)
+constexpr float kAmgOmega = 2.0f / 3.0f;   // damped-Jacobi weight of the smoother
+constexpr float kAmgScale1 = 1.6f;         // coarse-correction scale, one smoothing sweep per side
+constexpr float kAmgScale2 = 1.8f;         // coarse-correction scale, two sweeps per side
+constexpr uint32_t kAmgUnset = 0xffffffffu;
+
+// Device buffer that only grows (reallocated when a larger size is asked for).
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t cap = 0;
+    bool ensure(size_t count)
+    {
+        if (count <= cap && p) return true;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        const size_t want = count + count / 4 + 64;
+        if (cudaMalloc(&p, want * sizeof(T)) != cudaSuccess) return false;
+        cap = want;
+        return true;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+struct AmgLevel {
+    uint32_t n = 0;
+    uint64_t nnz = 0;
+    // the level's matrix: level 0 points at the caller's matrix, coarser levels use the owned buffers
+    const uint32_t *rp = nullptr, *ci = nullptr;
+    const double *val = nullptr;
+    const float *val32 = nullptr;
+    DevBuf<uint32_t> own_rp, own_ci;
+    DevBuf<double> own_val;
+    DevBuf<float> own_val32;
+    DevBuf<double> diag;                   // a_ii (FP64, strength test)
+    DevBuf<float> dw;                      // omega / a_ii (0 for a zero diagonal)
+    DevBuf<uint32_t> agg;                  // row of this level -> row of the next level
+    DevBuf<uint32_t> agg_ptr, agg_rows;    // next-level row -> rows of this level (ascending)
+    DevBuf<float> b, r, x1, x2, e;         // V-cycle vectors (b and e unused on level 0)
+};
+
+struct AmgHierarchy {
+    int levels = 0;                 // levels in use, the finest included
+    AmgLevel L[kAmgMaxLevels];
+    bool dense_coarsest = false;    // the last level is applied through coarse_inv
+    DevBuf<float> coarse_inv;       // dense inverse of the last level (row-major)
+    // setup scratch
+    DevBuf<uint64_t> T, M1, M2;     // independent-set tuples and their neighbourhood maxima
+    DevBuf<uint8_t> smask;          // strong-connection flag per stored entry
+    DevBuf<uint32_t> u1, u2, u3;    // per-row counters / scan output
+    DevBuf<uint32_t> scan_blocks;   // scan workspace
+    DevBuf<uint32_t> tcol;          // Galerkin staging: columns
+    DevBuf<double> tval;            // Galerkin staging: values
+    unsigned int *flags = nullptr;  // device counters read back by the host (16 words)
+    unsigned int *flags_h = nullptr;  // pinned host copy
+    double seconds_setup = 0.0;
+    uint32_t mis_rounds = 0;
+};
+
+void amg_free(AmgHierarchy *H);
+// (Re)builds A's hierarchy from A's current values; A owns it afterwards (freed with A).
+rsg_status amg_setup(rsg_context *ctx, rsg_csr *A);
+AmgHierarchy *amg_of(const rsg_csr *A);
+
+// z = V(r) on the context stream (FP32; sweeps = 1 or 2 smoothing sweeps per side).  The final
+// kernel adds r^T z (compensated) over its grid and, when st is given, finalizes the CG state:
+// mode 0 starts the recurrence (rho = r^T z, beta = 0), mode 1 continues it (beta = rho_new / rho,
+// or the residual-replacement rule after a true-residual check).  Without st the sum goes to
+// *rz_out.  partials holds >= kMaxGrid doubles; ticket is a zeroed grid-reduction counter.
+rsg_status amg_vcycle(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H, const float *r, float *z, int sweeps,
+                      double *partials, unsigned int *ticket, CgState *st, int mode, double *rz_out, bool pdl);
+
+// One launch of the finest level's post-smoothing sweep with the prolongated coarse correction
+// fused into its gather (z = x + dw (r - A x), x = dw r + s P e_c), for kernel timing.
+rsg_status amg_profile_launch(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H, const float *r, float *z);
+
+}  // namespace rsg

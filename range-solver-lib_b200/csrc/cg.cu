@@ -25,6 +25,7 @@
 // device state, so a whole solve is a single graph launch.  The tail kernel
 // also counts bodies and forces termination past a hard limit, so the loop
 // always ends even if the state were corrupted.
+#include "amg.cuh"
 #include "krylov.cuh"
 
 #include <cmath>
@@ -74,6 +75,8 @@ __device__ __forceinline__ double prec_group64(uint32_t g, uint32_t w, const dou
     if (PK == 0) {
         z[g] = rl[0];
         return rl[0] * rl[0];
+    } else if (PK == 3) {
+        return 0.0;  // multilevel: mixed precision only (rejected in FP64)
     } else if (PK == 1) {
         const double zi = d[g] * rl[0];
         z[g] = zi;
@@ -269,6 +272,8 @@ __device__ __forceinline__ void prec_group32(uint32_t g, uint32_t w, const float
         const float zi = d[g] * rl[0];
         z[g] = zi;
         rz.add_prod(rl[0], zi);
+    } else if (PK == 3) {
+        // multilevel: z comes from the V-cycle kernels that follow
     } else {
         for (uint32_t k = 0; k < w; k++) {
             const float *row = d + (size_t(g) * w + k) * w;
@@ -369,8 +374,9 @@ __global__ void __launch_bounds__(kBlock) k_mx_update(uint32_t n, uint32_t w, co
     const float alpha = float(st->alpha);
     Dot2 rz, rr;
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
-    if (PK < 2) {
-        // four rows per thread with 16-byte loads (vectors are 256-byte aligned)
+    if (PK < 2 || PK == 3) {
+        // four rows per thread with 16-byte loads (vectors are 256-byte aligned); with the multilevel
+        // preconditioner (PK 3) z and r^T z come from the V-cycle that follows
         const uint32_t nq = n / 4;
         for (uint32_t i4 = tid; i4 < nq; i4 += stride) {
             const float4 pv = reinterpret_cast<const float4 *>(p)[i4];
@@ -393,11 +399,13 @@ __global__ void __launch_bounds__(kBlock) k_mx_update(uint32_t n, uint32_t w, co
             zv.w = PK == 1 ? dv.w * rv.w : rv.w;
             reinterpret_cast<float4 *>(y)[i4] = yv;
             reinterpret_cast<float4 *>(r)[i4] = rv;
-            reinterpret_cast<float4 *>(z)[i4] = zv;
-            rz.add_prod(rv.x, zv.x);
-            rz.add_prod(rv.y, zv.y);
-            rz.add_prod(rv.z, zv.z);
-            rz.add_prod(rv.w, zv.w);
+            if (PK != 3) {
+                reinterpret_cast<float4 *>(z)[i4] = zv;
+                rz.add_prod(rv.x, zv.x);
+                rz.add_prod(rv.y, zv.y);
+                rz.add_prod(rv.z, zv.z);
+                rz.add_prod(rv.w, zv.w);
+            }
             rr.add_prod(rv.x, rv.x);
             rr.add_prod(rv.y, rv.y);
             rr.add_prod(rv.z, rv.z);
@@ -408,8 +416,10 @@ __global__ void __launch_bounds__(kBlock) k_mx_update(uint32_t n, uint32_t w, co
             const float ri = fmaf(-alpha, q[i], r[i]);
             const float zi = PK == 1 ? d[i] * ri : ri;
             r[i] = ri;
-            z[i] = zi;
-            rz.add_prod(ri, zi);
+            if (PK != 3) {
+                z[i] = zi;
+                rz.add_prod(ri, zi);
+            }
             rr.add_prod(ri, ri);
         }
     } else {
@@ -466,7 +476,7 @@ __global__ void __launch_bounds__(kBlock) k_mx_check(Csr<double> M, Sell<double>
     double acc[2] = {rz.value(), rr[0]};
     double tot[2];
     if (grid_sum<2>(acc, partials, &st->ticket[2], sh, tot) && threadIdx.x == 0) {
-        if (PK == 2) st->check_rn = sqrt(tot[1]);
+        if (PK >= 2) st->check_rn = sqrt(tot[1]);  // the preconditioner pass that follows finalizes
         else finalize_check_mixed(st, tot[0], sqrt(tot[1]));
     }
 }
@@ -545,6 +555,8 @@ void launch_init(rsg_context *ctx, const CgArgs &a, const Launch &L)
     else
         k_mx_prec<PK><<<L.g_vec, kBlock, 0, ctx->stream>>>(a.A->n, a.P.w, a.P.d32, a.r, a.r32, a.z32, a.partials,
                                                           a.st, 0);
+    if (PK == 3)  // z0 = V(r0), rho = r0^T z0
+        amg_vcycle(ctx, a.A, a.amg, a.r32, a.z32, a.amg_sweeps, a.partials, &a.st->ticket[5], a.st, 0, nullptr, false);
 }
 
 template <int RPW, int PK>
@@ -582,6 +594,9 @@ void launch_body(rsg_context *ctx, const CgArgs &a, const Launch &L, cudaGraphCo
             if (PK == 2)
                 launch_k(st, pdl, k_mx_prec<PK>, L.g_vec, kBlock, 0, n, a.P.w, a.P.d32, (const double *)nullptr,
                          a.r32, a.z32, a.partials, a.st, 1);
+            if (PK == 3)
+                amg_vcycle(ctx, a.A, a.amg, a.r32, a.z32, a.amg_sweeps, a.partials, &a.st->ticket[5], a.st, 1,
+                           nullptr, pdl);
         }
     }
     launch_k(st, pdl, k_tail, 1, 32, 0, a.st, h, use_cond);
@@ -789,6 +804,9 @@ rsg_status profile_typed(rsg_context *ctx, const rsg_csr *A, int kernel, uint32_
         case RSG_KERNEL_SPMV_FP64:
             spmv64(ctx, A, v64[0], v64[1], true);
             break;
+        case RSG_KERNEL_AMG_SWEEP:
+            amg_profile_launch(ctx, A, amg_of(A), v32[0], v32[1]);
+            break;
         default:
             spmv32(ctx, A, v32[0], v32[1], true);
             break;
@@ -832,6 +850,10 @@ rsg_status cg_run(rsg_context *ctx, const CgArgs &a, double *seconds)
     switch (a.P.kind) {
     case 0: RSG_RPW_DISPATCH(rpw, return (run_typed<RPW, 0>(ctx, a, seconds)));
     case 1: RSG_RPW_DISPATCH(rpw, return (run_typed<RPW, 1>(ctx, a, seconds)));
+    case 3:
+        if (!a.mixed || !a.amg)
+            return set_error(ctx, RSG_ERR_UNSUPPORTED, "the multilevel preconditioner runs in the mixed-precision CG");
+        RSG_RPW_DISPATCH(rpw, return (run_typed<RPW, 3>(ctx, a, seconds)));
     default: RSG_RPW_DISPATCH(rpw, return (run_typed<RPW, 2>(ctx, a, seconds)));
     }
     return RSG_ERR_UNSUPPORTED;
@@ -844,9 +866,13 @@ using namespace rsg;
 extern "C" rsg_status rsg_profile_kernel(rsg_context *ctx, const rsg_csr *A, int32_t kernel, uint32_t reps,
                                          int32_t flush_l2, double *seconds)
 {
-    if (!ctx || !A || !seconds || kernel < 0 || kernel > RSG_KERNEL_SPMV_FP32)
+    if (!ctx || !A || !seconds || kernel < 0 || kernel > RSG_KERNEL_AMG_SWEEP)
         return set_error(ctx, RSG_ERR_INVALID_ARG, "profile_kernel: bad arguments");
     RSG_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (kernel == RSG_KERNEL_AMG_SWEEP) {
+        if (!amg_of(A)) RSG_TRY(amg_setup(ctx, const_cast<rsg_csr *>(A)));
+        if (amg_of(A)->levels < 2) return set_error(ctx, RSG_ERR_UNSUPPORTED, "profile_kernel: no coarse level");
+    }
     RSG_RPW_DISPATCH(pick_rpw(A), return profile_typed<RPW>(ctx, A, kernel, reps, flush_l2, seconds));
     return RSG_ERR_UNSUPPORTED;
 }

@@ -73,6 +73,7 @@ struct rsg_csr {
         double it64_default = 0, it32_default = 0;
         uint32_t candidates = 0;
     } tune;
+    void *amg = nullptr;              // multilevel preconditioner hierarchy (amg.cu), freed with the matrix
 };
 
 namespace rsg {

@@ -220,6 +220,7 @@ static void free_sell(rsg_csr *A)
 static void free_csr(rsg_csr *A)
 {
     if (!A) return;
+    rsg::amg_release(A->amg);
     free_sell(A);
     cudaFree(A->rp);
     cudaFree(A->ci);

@@ -49,6 +49,8 @@ rsg_status csr_create_ex(rsg_context *ctx, uint32_t n, const uint32_t *rp, const
 // Recompute ||A||_F and the FP32 copy after the values were rewritten in place.
 rsg_status csr_refresh(rsg_context *ctx, rsg_csr *A);
 rsg_status jacobi_build(rsg_context *ctx, const rsg_csr *A, double *d);
+// Frees a matrix's multilevel preconditioner hierarchy (amg.cu).
+void amg_release(void *hierarchy);
 uint32_t block_width(uint32_t n, uint32_t block_size);
 rsg_status block_jacobi_build(rsg_context *ctx, const rsg_csr *A, uint32_t w, double *blocks, unsigned int *flag);
 // out3 = {||b-Ax||, ||b||, relres}; partials >= 2*grid doubles.

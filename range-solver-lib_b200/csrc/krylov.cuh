@@ -38,8 +38,10 @@ struct CgState {
     double *trend_hist;
 };
 
+struct AmgHierarchy;
+
 struct Precond {
-    int kind = 0;                 // 0 none, 1 Jacobi, 2 block Jacobi
+    int kind = 0;                 // 0 none, 1 Jacobi, 2 block Jacobi, 3 multilevel (amg.cu)
     uint32_t w = 1;
     const double *d = nullptr;    // Jacobi inverse diagonal / blocks (n*w)
     const float *d32 = nullptr;   // FP32 copies for the mixed-precision inner solver
@@ -59,6 +61,8 @@ struct CgArgs {
     bool mixed;
     bool use_graph;
     uint32_t check_interval;
+    const AmgHierarchy *amg;      // kind 3: the matrix's hierarchy
+    int amg_sweeps;               // kind 3: smoothing sweeps per side of the V-cycle (1 or 2)
 };
 
 rsg_status autotune_run(rsg_context *ctx, rsg_csr *A, const char *cache_path);

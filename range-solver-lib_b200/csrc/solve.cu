@@ -9,6 +9,7 @@
 // in RIterationInfo's formats (src/riterationinfo.cpp:111-193) when asked.
 #include <cstdlib>
 
+#include "amg.cuh"
 #include "gmres.cuh"
 #include "gnn.cuh"
 #include "krylov.cuh"
@@ -86,8 +87,11 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
     std::memset(&st_out, 0, sizeof(st_out));
     if (c.solver_type != RSG_SOLVER_CG && c.solver_type != RSG_SOLVER_GMRES)
         return set_error(ctx, RSG_ERR_INVALID_ARG, "Unknown matrix solver type '%d'", c.solver_type);
-    if (prec_type < RSG_PREC_NONE || prec_type > RSG_PREC_LEARNED)
+    if (prec_type < RSG_PREC_NONE || prec_type > RSG_PREC_AMG)
         return set_error(ctx, RSG_ERR_INVALID_ARG, "Invalid matrix preconditioner type '%d'", prec_type);
+    if (prec_type == RSG_PREC_AMG && (c.solver_type != RSG_SOLVER_CG || c.precision != RSG_PRECISION_MIXED))
+        return set_error(ctx, RSG_ERR_UNSUPPORTED,
+                         "the multilevel preconditioner runs in the mixed-precision CG (solver CG, precision MIXED)");
     rsg_learned *G = static_cast<rsg_learned *>(const_cast<void *>(c.learned));
     if ((prec_type == RSG_PREC_LEARNED || c.learned_initial_guess) && !G)
         return set_error(ctx, RSG_ERR_INVALID_ARG, "learned preconditioner requested without conf.learned");
@@ -148,9 +152,11 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
 
     // ---- preconditioner ----
     Precond P;
-    P.kind = learned ? RSG_PREC_JACOBI : prec_type;
+    P.kind = learned ? RSG_PREC_JACOBI : (prec_type == RSG_PREC_AMG ? 3 : prec_type);
     P.w = w;
-    if (prec_type == RSG_PREC_JACOBI || learned) {
+    if (prec_type == RSG_PREC_AMG) {
+        RSG_TRY(amg_setup(ctx, A));  // rebuilt from the current values on every solve
+    } else if (prec_type == RSG_PREC_JACOBI || learned) {
         RSG_TRY(jacobi_build(ctx, A, d));
     } else if (prec_type == RSG_PREC_BLOCK_JACOBI) {
         unsigned int *flag = ticket + 8;
@@ -227,10 +233,13 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
             RSG_CHECK_CUDA(ctx, cudaMemsetAsync(a.p32a, 0, size_t(n) * sizeof(float), ctx->stream));
             RSG_CHECK_CUDA(ctx, cudaMemsetAsync(a.p32b, 0, size_t(n) * sizeof(float), ctx->stream));
             RSG_CHECK_CUDA(ctx, cudaMemsetAsync(a.y32, 0, size_t(n) * sizeof(float), ctx->stream));
-            if (prec_type != RSG_PREC_NONE) k_to_f32<<<gv, kBlock, 0, ctx->stream>>>(size_t(n) * w, d, d32);
+            if (prec_type == RSG_PREC_JACOBI || prec_type == RSG_PREC_BLOCK_JACOBI)
+                k_to_f32<<<gv, kBlock, 0, ctx->stream>>>(size_t(n) * w, d, d32);
             P.d32 = d32;
         }
         a.P = P;
+        a.amg = prec_type == RSG_PREC_AMG ? amg_of(A) : nullptr;
+        a.amg_sweeps = c.amg_sweeps == 1 ? 1 : 2;
         CgState h;
         std::memset(&h, 0, sizeof(h));
         h.an = an;

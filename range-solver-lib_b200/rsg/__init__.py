@@ -15,7 +15,8 @@ import numpy as np
 
 from . import _lib
 from ._lib import (BREAKDOWN, ERR_INVALID_ARG, ERR_SINGULAR, ERR_UNSUPPORTED, MEM_DEVICE, MEM_HOST, NOT_CONVERGED,
-                   OK, PREC_BLOCK_JACOBI, PREC_JACOBI, PREC_LEARNED, PREC_NONE, PRECISION_FP64, PRECISION_MIXED,
+                   OK, PREC_AMG, PREC_BLOCK_JACOBI, PREC_JACOBI, PREC_LEARNED, PREC_NONE, PRECISION_FP64,
+                   PRECISION_MIXED,
                    SOLVER_CG, SOLVER_GMRES, STOP_REFERENCE, STOP_TRUE_RELRES, RsgError, SolverConf, Stats, Time)
 
 __all__ = ["Context", "Matrix", "Assembly", "Batch", "make_conf", "RsgError", "SolverConf", "Stats", "Solver"]
@@ -38,7 +39,7 @@ def make_conf(solver: str | int = "cg", n_outer: int = 1000, n_inner: int = 30, 
               precision: str | int = "fp64", scale_equations: bool = True, reliable_delta: float = 1e-3,
               flexible: bool = False, use_graph: bool = True, check_interval: int = 16,
               output_frequency: int = 0, output_file: str | None = None,
-              l2_resident_f32: bool = False, autotune: bool = False) -> SolverConf:
+              l2_resident_f32: bool = False, autotune: bool = False, amg_sweeps: int = 2) -> SolverConf:
     c = SolverConf()
     _lib.load().rsg_conf_default(C.byref(c))
     c.solver_type = solver if isinstance(solver, int) else {"cg": SOLVER_CG, "gmres": SOLVER_GMRES}[solver]
@@ -60,6 +61,7 @@ def make_conf(solver: str | int = "cg", n_outer: int = 1000, n_inner: int = 30, 
     c.output_file = output_file.encode() if output_file else None
     c.l2_resident_f32 = 1 if l2_resident_f32 else 0
     c.autotune = 1 if autotune else 0
+    c.amg_sweeps = amg_sweeps
     return c
 
 
@@ -157,6 +159,28 @@ class Context:
                                          C.byref(summ))
         self.check(s, "solve_multi", allow)
         return X, list(per), summ
+
+    # ---- multilevel aggregation preconditioner ----
+    def amg_setup(self, A: "Matrix") -> dict:
+        """Build A's hierarchy from its current values (rsg_amg_setup); returns its shape."""
+        info = _lib.AmgInfo()
+        self.check(self.lib.rsg_amg_setup(self.h, A.h, C.byref(info)), "amg_setup")
+        L = info.levels
+        return {"levels": L, "dense_coarsest": bool(info.dense_coarsest), "rows": list(info.rows[:L]),
+                "nnz": list(info.nnz[:L]), "mis_rounds": info.mis_rounds, "seconds_setup": info.seconds_setup}
+
+    def amg_level(self, A: "Matrix", level: int, n_rows: int, nnz: int, with_agg: bool = True):
+        """(agg or None, row_ptr, col_idx, values) of one level of A's last hierarchy."""
+        agg = np.empty(n_rows, np.uint32) if with_agg else None
+        rp = np.empty(n_rows + 1, np.uint32)
+        ci = np.empty(nnz, np.uint32)
+        val = np.empty(nnz, np.float64)
+        self.check(self.lib.rsg_amg_level(self.h, A.h, level, _ptr(agg), _ptr(rp), _ptr(ci), _ptr(val)), "amg_level")
+        return agg, rp, ci, val
+
+    def amg_apply(self, A: "Matrix", r_dev, z_dev, sweeps: int = 2):
+        """z = one V-cycle applied to r (device FP64 arrays)."""
+        self.check(self.lib.rsg_amg_apply(self.h, A.h, _ptr(r_dev), _ptr(z_dev), sweeps), "amg_apply")
 
     def spmv(self, A: "Matrix", x_dev, y_dev):
         self.check(self.lib.rsg_spmv(self.h, A.h, _ptr(x_dev), _ptr(y_dev)), "spmv")

@@ -27,7 +27,7 @@ ERR_SINGULAR = -5
 ERR_TIMEOUT = -6
 
 SOLVER_CG, SOLVER_GMRES = 0, 1
-PREC_NONE, PREC_JACOBI, PREC_BLOCK_JACOBI, PREC_LEARNED = 0, 1, 2, 3
+PREC_NONE, PREC_JACOBI, PREC_BLOCK_JACOBI, PREC_LEARNED, PREC_AMG = 0, 1, 2, 3, 4
 STOP_REFERENCE, STOP_TRUE_RELRES = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 MEM_HOST, MEM_DEVICE = 0, 1
@@ -56,7 +56,8 @@ class SolverConf(C.Structure):
         ("learned_initial_guess", C.c_int32),
         ("l2_resident_f32", C.c_int32),
         ("autotune", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("amg_sweeps", C.c_int32),
+        ("reserved", C.c_int32 * 4),
     ]
 
 
@@ -119,6 +120,18 @@ class ModelGroups(C.Structure):
     ]
 
 
+class AmgInfo(C.Structure):
+    _fields_ = [
+        ("levels", C.c_uint32),
+        ("dense_coarsest", C.c_uint32),
+        ("rows", C.c_uint32 * 16),
+        ("nnz", C.c_uint64 * 16),
+        ("mis_rounds", C.c_uint32),
+        ("reserved", C.c_uint32),
+        ("seconds_setup", C.c_double),
+    ]
+
+
 class Time(C.Structure):
     _fields_ = [("transient", C.c_int32), ("alpha", C.c_double), ("dt", C.c_double)]
 
@@ -162,6 +175,9 @@ SIGNATURES = {
     "rsg_tune_get": (C.c_int, [_P, C.POINTER(TuneInfo)]),
     "rsg_batch_autotune": (C.c_int, [_P, _P, C.POINTER(TuneInfo)]),
     "rsg_profile_kernel": (C.c_int, [_P, _P, C.c_int32, C.c_uint32, C.c_int32, _DP]),
+    "rsg_amg_setup": (C.c_int, [_P, _P, C.POINTER(AmgInfo)]),
+    "rsg_amg_level": (C.c_int, [_P, _P, C.c_uint32, _P, _P, _P, _P]),
+    "rsg_amg_apply": (C.c_int, [_P, _P, _P, _P, C.c_uint32]),
     "rsg_true_relres_noalloc": (C.c_int, [C.c_uint32, _P, _P, _P, _P, _P, _P, _P]),
     "rsg_batch_create": (C.c_int, [_P, C.c_uint32, _P, _P, _P, _P, _PP]),
     "rsg_batch_destroy": (None, [_P, _P]),

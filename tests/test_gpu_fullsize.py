@@ -8,7 +8,8 @@ Bar (the same as the small cases): the GPU-assembled pattern equals the oracle's
 right-hand-side value within 1e-13 relative (absolute floor 1e-13 of the row's largest entry for
 entries that cancel to rounding noise); every GPU solution reaches the FP64 true relative residual
 1e-10, recomputed by the oracle on the oracle's system, and agrees with the oracle's tight solution
-(rtol 1e-12) to ||x - x_ref|| / ||x_ref|| <= 1e-8.
+(rtol 1e-12; 1e-11 for the stiff beam, whose FP64 iteration stagnates above 1e-12) to
+||x - x_ref|| / ||x_ref|| <= 1e-8.
 """
 import os
 
@@ -27,10 +28,10 @@ THREADS = os.cpu_count() or 1
 _CACHE = {}
 
 
-def oracle_tight(A, b, prec=1, block=1):
-    x, st = O.solve(A, b, prec=prec, block_size=block, n_outer=200000, stop_rule="true", rtol=1e-12,
+def oracle_tight(A, b, prec=1, block=1, rtol=1e-12, n_outer=200000):
+    x, st = O.solve(A, b, prec=prec, block_size=block, n_outer=n_outer, stop_rule="true", rtol=rtol,
                     threads=THREADS)
-    assert st.converged == 1 and st.true_relres <= 1e-12
+    assert st.converged == 1 and st.true_relres <= rtol
     return x
 
 
@@ -91,7 +92,9 @@ def test_elasticity_beam_64x32x32_matches_oracle(ctx, torch_cuda, prec, block, p
     p, Ao, bo, refs = _CACHE["beam"]
     assert Ao.n == 209088
     if (prec, block) not in refs:
-        refs[(prec, block)] = oracle_tight(Ao, bo, prec=prec, block=block)
+        # the stiff beam's Jacobi-PCG stagnates above 1e-12 in FP64 (attainable accuracy), so its
+        # reference solution is taken at 1e-11, still ten times below the GPU's 1e-10
+        refs[(prec, block)] = oracle_tight(Ao, bo, prec=prec, block=block, rtol=1e-11, n_outer=40000)
     asm = rsg.Assembly.stress(ctx, p)
     b = torch.empty(asm.n_free, dtype=torch.float64, device="cuda")
     M = asm.assemble(p, b)
