@@ -193,11 +193,13 @@ __global__ void k_amg_mis_init(uint32_t n, uint64_t *__restrict__ T)
         T[i] = (uint64_t(1) << kStateShift) | amg_key(i);
 }
 
-// out_i = max(in_i, max over strong neighbours j of in_j)
+// out_i = max(in_i, max over strong neighbours j of in_j).  Rounds are launched in batches; once a
+// round has left no node undecided (*prev == 0) the later rounds return at once.
 __global__ void k_amg_nbmax(uint32_t n, const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ci,
                             const uint8_t *__restrict__ smask, const uint64_t *__restrict__ in,
-                            uint64_t *__restrict__ out)
+                            uint64_t *__restrict__ out, const unsigned int *prev)
 {
+    if (prev && *prev == 0) return;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint64_t m = in[i];
         for (uint32_t j = rp[i]; j < rp[i + 1]; j++)
@@ -207,10 +209,12 @@ __global__ void k_amg_nbmax(uint32_t n, const uint32_t *__restrict__ rp, const u
 }
 
 // One synchronous round: an undecided node whose tuple is the distance-2 maximum becomes a root;
-// one that sees a root within distance 2 drops out.  flags[0] counts the nodes still undecided.
+// one that sees a root within distance 2 drops out.  *count (zeroed beforehand) receives the number
+// of nodes still undecided; nothing is done once the previous round left none (*prev == 0).
 __global__ void k_amg_mis_decide(uint32_t n, uint64_t *__restrict__ T, const uint64_t *__restrict__ M2,
-                                 unsigned int *flags)
+                                 const unsigned int *prev, unsigned int *count)
 {
+    if (prev && *prev == 0) return;
     unsigned int left = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint64_t t = T[i];
@@ -221,7 +225,7 @@ __global__ void k_amg_mis_decide(uint32_t n, uint64_t *__restrict__ T, const uin
         else left++;
     }
     left = __reduce_add_sync(0xffffffffu, left);
-    if ((threadIdx.x & 31) == 0 && left) atomicAdd(&flags[0], left);
+    if ((threadIdx.x & 31) == 0 && left) atomicAdd(count, left);
 }
 
 __global__ void k_amg_root_flags(uint32_t n, const uint64_t *__restrict__ T, uint32_t *__restrict__ flag)
@@ -599,9 +603,11 @@ __global__ void __launch_bounds__(kBlock) k_amg_coarse(uint32_t n, const uint32_
     }
 }
 
-// b_c[I] = sum of r over the aggregate's rows (ascending order).
+// b_c[I] = sum of r over the aggregate's rows (ascending order), and the coarse level's first
+// smoothing step x0_c = dw_c b_c.
 __global__ void k_amg_restrict(uint32_t nc, const uint32_t *__restrict__ ptr, const uint32_t *__restrict__ rows,
-                               const float *__restrict__ r, float *__restrict__ bc, const CgState *st)
+                               const float *__restrict__ r, const float *__restrict__ dwc, float *__restrict__ bc,
+                               float *__restrict__ x0c, const CgState *st)
 {
     pdl_wait();
     pdl_release();
@@ -610,6 +616,7 @@ __global__ void k_amg_restrict(uint32_t nc, const uint32_t *__restrict__ ptr, co
         float s = 0.f;
         for (uint32_t k = ptr[I]; k < ptr[I + 1]; k++) s += r[rows[k]];
         bc[I] = s;
+        x0c[I] = dwc[I] * s;
     }
 }
 
@@ -689,20 +696,26 @@ rsg_status build_aggregates(rsg_context *ctx, AmgHierarchy *H, AmgLevel &F, uint
     k_amg_strength<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, F.val, F.diag.p, kAmgTheta, H->smask.p);
     k_amg_mis_init<<<g, kBlock, 0, s>>>(n, H->T.p);
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
-    // synchronous rounds until no node is undecided (checked every two rounds)
-    for (uint32_t round = 0;; round += 2) {
-        RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->flags, 0, sizeof(unsigned int), s));
-        for (int k = 0; k < 2; k++) {
-            k_amg_nbmax<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, H->smask.p, H->T.p, H->M1.p);
-            k_amg_nbmax<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, H->smask.p, H->M1.p, H->M2.p);
-            if (k == 1) RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->flags, 0, sizeof(unsigned int), s));
-            k_amg_mis_decide<<<g, kBlock, 0, s>>>(n, H->T.p, H->M2.p, H->flags);
+    // synchronous rounds until no node is undecided: launched in batches of kRoundBatch with one
+    // undecided-node counter per round (rounds after the last one needed return at once); the host
+    // reads the batch's last counter
+    constexpr uint32_t kRoundBatch = 8, kMaxRounds = 128;
+    if (!H->rounds.ensure(kMaxRounds)) return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: round counters");
+    RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->rounds.p, 0, kMaxRounds * sizeof(unsigned int), s));
+    uint32_t round = 0;
+    for (;;) {
+        for (uint32_t k = 0; k < kRoundBatch; k++, round++) {
+            const unsigned int *prev = round ? H->rounds.p + round - 1 : nullptr;
+            k_amg_nbmax<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, H->smask.p, H->T.p, H->M1.p, prev);
+            k_amg_nbmax<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, H->smask.p, H->M1.p, H->M2.p, prev);
+            k_amg_mis_decide<<<g, kBlock, 0, s>>>(n, H->T.p, H->M2.p, prev, H->rounds.p + round);
         }
-        RSG_TRY(read_flags(ctx, H, 1));
-        H->mis_rounds += 2;
+        RSG_CHECK_CUDA(ctx, cudaGetLastError());
+        RSG_TRY(read_u32(ctx, H, H->rounds.p + round - 1, &H->flags_h[0]));
         if (H->flags_h[0] == 0) break;
-        if (round > 256) return set_error(ctx, RSG_ERR_CUDA, "amg: independent set did not converge");
+        if (round + kRoundBatch > kMaxRounds) return set_error(ctx, RSG_ERR_CUDA, "amg: independent set did not converge");
     }
+    H->mis_rounds += round;
     // root numbering, joins
     k_amg_root_flags<<<g, kBlock, 0, s>>>(n, H->T.p, H->u1.p);
     RSG_TRY(scan_u32(ctx, H, H->u1.p, n, H->u2.p));
@@ -813,6 +826,7 @@ void amg_free(AmgHierarchy *H)
     H->u2.release();
     H->u3.release();
     H->scan_blocks.release();
+    H->rounds.release();
     H->tcol.release();
     H->tval.release();
     if (H->flags) cudaFree(H->flags);
@@ -911,15 +925,14 @@ void coarse_sweep(rsg_context *ctx, const AmgLevel &l, const SweepArgs &a, const
              st);
 }
 
-// Pre-smoothing, residual and restriction of level l (b given), then the coarser levels, then
-// prolongation and post-smoothing into `out`.  Level 0 is handled by the caller (fine kernels).
-void coarse_levels(rsg_context *ctx, const AmgHierarchy *H, int l, int sweeps, const CgState *st, bool pdl);
-
+// Level l >= 1 (b and x0 = dw b given by the restriction): pre-smoothing, residual, restriction,
+// the coarser levels, prolongation and post-smoothing into e.  The finest level is done by the caller
+// (fine kernels).  Buffers: x1 holds x0 on entry; with two sweeps x2 holds the pre-smoothed iterate.
 void down_restrict(rsg_context *ctx, const AmgHierarchy *H, int l, const CgState *st, bool pdl)
 {
     const AmgLevel &F = H->L[l], &C = H->L[l + 1];
     launch_k(ctx->stream, pdl, k_amg_restrict, grid_rows(C.n), kBlock, 0, C.n, (const uint32_t *)F.agg_ptr.p,
-             (const uint32_t *)F.agg_rows.p, (const float *)F.r.p, C.b.p, st);
+             (const uint32_t *)F.agg_rows.p, (const float *)F.r.p, (const float *)C.dw.p, C.b.p, C.x1.p, st);
 }
 
 void coarse_levels(rsg_context *ctx, const AmgHierarchy *H, int l, int sweeps, const CgState *st, bool pdl)
@@ -930,46 +943,44 @@ void coarse_levels(rsg_context *ctx, const AmgHierarchy *H, int l, int sweeps, c
         if (H->dense_coarsest) {
             launch_k(ctx->stream, pdl, k_amg_dense_apply, 1, 256, 0, F.n, (const float *)H->coarse_inv.p,
                      (const float *)F.b.p, F.e.p, st);
-        } else {  // coarsening stalled above the dense limit: smoothing sweeps only
-            SweepArgs a{F.b.p, F.dw.p, nullptr, nullptr, nullptr, 0.f, F.x1.p};
-            coarse_sweep<kSrcDwB, kOutSmooth>(ctx, F, a, st, pdl);
+        } else {  // coarsening stalled above the dense limit: nine damped-Jacobi sweeps from zero
+            float *src = F.x1.p, *dst = F.x2.p;
             for (int k = 0; k < 7; k++) {
-                SweepArgs a2{F.b.p, F.dw.p, (k & 1) ? F.x2.p : F.x1.p, nullptr, nullptr, 0.f, (k & 1) ? F.x1.p : F.x2.p};
-                coarse_sweep<kSrcX, kOutSmooth>(ctx, F, a2, st, pdl);
+                SweepArgs a{F.b.p, F.dw.p, src, nullptr, nullptr, 0.f, dst};
+                coarse_sweep<kSrcX, kOutSmooth>(ctx, F, a, st, pdl);
+                std::swap(src, dst);
             }
-            SweepArgs a3{F.b.p, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, F.e.p};
-            coarse_sweep<kSrcX, kOutSmooth>(ctx, F, a3, st, pdl);
+            SweepArgs a{F.b.p, F.dw.p, src, nullptr, nullptr, 0.f, F.e.p};
+            coarse_sweep<kSrcX, kOutSmooth>(ctx, F, a, st, pdl);
         }
         return;
     }
     const AmgLevel &C = H->L[l + 1];
     const float s = sweeps == 2 ? kAmgScale2 : kAmgScale1;
     if (sweeps == 2) {
-        SweepArgs a1{F.b.p, F.dw.p, nullptr, nullptr, nullptr, 0.f, F.x1.p};
-        coarse_sweep<kSrcDwB, kOutSmooth>(ctx, F, a1, st, pdl);
-        SweepArgs a2{F.b.p, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, F.r.p};
+        SweepArgs a1{F.b.p, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, F.x2.p};
+        coarse_sweep<kSrcX, kOutSmooth>(ctx, F, a1, st, pdl);
+        SweepArgs a2{F.b.p, F.dw.p, F.x2.p, nullptr, nullptr, 0.f, F.r.p};
         coarse_sweep<kSrcX, kOutRes>(ctx, F, a2, st, pdl);
     } else {
-        SweepArgs a1{F.b.p, F.dw.p, nullptr, nullptr, nullptr, 0.f, F.r.p};
-        coarse_sweep<kSrcDwB, kOutRes>(ctx, F, a1, st, pdl);
+        SweepArgs a1{F.b.p, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, F.r.p};
+        coarse_sweep<kSrcX, kOutRes>(ctx, F, a1, st, pdl);
     }
     down_restrict(ctx, H, l, st, pdl);
     coarse_levels(ctx, H, l + 1, sweeps, st, pdl);
     if (sweeps == 2) {
-        SweepArgs u1{F.b.p, F.dw.p, F.x1.p, C.e.p, F.agg.p, s, F.x2.p};
+        SweepArgs u1{F.b.p, F.dw.p, F.x2.p, C.e.p, F.agg.p, s, F.x1.p};
         coarse_sweep<kSrcXCorr, kOutSmooth>(ctx, F, u1, st, pdl);
-        SweepArgs u2{F.b.p, F.dw.p, F.x2.p, nullptr, nullptr, 0.f, F.e.p};
+        SweepArgs u2{F.b.p, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, F.e.p};
         coarse_sweep<kSrcX, kOutSmooth>(ctx, F, u2, st, pdl);
     } else {
-        SweepArgs u1{F.b.p, F.dw.p, nullptr, C.e.p, F.agg.p, s, F.e.p};
-        coarse_sweep<kSrcDwBCorr, kOutSmooth>(ctx, F, u1, st, pdl);
+        SweepArgs u1{F.b.p, F.dw.p, F.x1.p, C.e.p, F.agg.p, s, F.e.p};
+        coarse_sweep<kSrcXCorr, kOutSmooth>(ctx, F, u1, st, pdl);
     }
 }
 
 template <int RPW>
-rsg_status vcycle_typed(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H, const float *r, float *z,
-                        int sweeps, double *partials, unsigned int *ticket, CgState *st, int mode, double *rz_out,
-                        bool pdl)
+FineLaunch<RPW> fine_launch(rsg_context *ctx, const rsg_csr *A)
 {
     FineLaunch<RPW> f;
     f.M = view<float>(A, true);
@@ -977,15 +988,29 @@ rsg_status vcycle_typed(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *
     f.use_sell = A->use_sell;
     f.smem = A->use_sell ? 0 : tma_smem<float>();
     if (!A->use_sell) {
-        cudaFuncSetAttribute(k_amg_fine<RPW, kSrcDwB, kOutRes, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(f.smem));
-        cudaFuncSetAttribute(k_amg_fine<RPW, kSrcDwB, kOutSmooth, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(f.smem));
-        cudaFuncSetAttribute(k_amg_fine<RPW, kSrcX, kOutRes, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(f.smem));
-        cudaFuncSetAttribute(k_amg_fine<RPW, kSrcXCorr, kOutSmooth, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(f.smem));
-        cudaFuncSetAttribute(k_amg_fine<RPW, kSrcX, kOutSmooth, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(f.smem));
-        cudaFuncSetAttribute(k_amg_fine<RPW, kSrcDwBCorr, kOutSmooth, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(f.smem));
+        const int sm = int(f.smem);
+        cudaFuncSetAttribute(k_amg_fine<RPW, kSrcX, kOutRes, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        cudaFuncSetAttribute(k_amg_fine<RPW, kSrcX, kOutSmooth, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        cudaFuncSetAttribute(k_amg_fine<RPW, kSrcXCorr, kOutSmooth, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        cudaFuncSetAttribute(k_amg_fine<RPW, kSrcX, kOutSmooth, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        cudaFuncSetAttribute(k_amg_fine<RPW, kSrcXCorr, kOutSmooth, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     }
     f.grid = spmv_grid(ctx, A, (const void *)k_amg_fine<RPW, kSrcX, kOutSmooth, true>, f.smem, RPW);
+    return f;
+}
+
+// x0 (= dw r) in the finest level's x1 buffer, computed by the caller or here.
+template <int RPW>
+rsg_status vcycle_typed(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H, const float *r, const float *x0,
+                        float *z, int sweeps, double *partials, unsigned int *ticket, CgState *st, int mode,
+                        double *rz_out, bool pdl)
+{
     const AmgLevel &F = H->L[0];
+    if (!x0) {
+        launch_k(ctx->stream, pdl, k_amg_jacobi, grid_rows(F.n), kBlock, 0, F.n, (const float *)F.dw.p, r, F.x1.p,
+                 (const CgState *)st);
+        x0 = F.x1.p;
+    }
     if (H->levels < 2) {
         if (H->dense_coarsest)
             launch_k(ctx->stream, pdl, k_amg_dense_apply, 1, 256, 0, F.n, (const float *)H->coarse_inv.p, r, z,
@@ -997,27 +1022,29 @@ rsg_status vcycle_typed(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *
         launch_k(ctx->stream, pdl, k_amg_rz, g, kBlock, 0, F.n, r, (const float *)z, partials, ticket, st, mode, rz_out);
         return RSG_OK;
     }
+    const FineLaunch<RPW> f = fine_launch<RPW>(ctx, A);
     const AmgLevel &C = H->L[1];
     const float s = sweeps == 2 ? kAmgScale2 : kAmgScale1;
+    float *x1 = F.x1.p, *x2 = F.x2.p;
     if (sweeps == 2) {
-        SweepArgs a1{r, F.dw.p, nullptr, nullptr, nullptr, 0.f, F.x1.p};
-        fine_sweep<RPW, kSrcDwB, kOutSmooth, false>(ctx, f, a1, partials, ticket, st, mode, rz_out, pdl);
-        SweepArgs a2{r, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, F.r.p};
+        SweepArgs a1{r, F.dw.p, x0, nullptr, nullptr, 0.f, x2};
+        fine_sweep<RPW, kSrcX, kOutSmooth, false>(ctx, f, a1, partials, ticket, st, mode, rz_out, pdl);
+        SweepArgs a2{r, F.dw.p, x2, nullptr, nullptr, 0.f, F.r.p};
         fine_sweep<RPW, kSrcX, kOutRes, false>(ctx, f, a2, partials, ticket, st, mode, rz_out, pdl);
     } else {
-        SweepArgs a1{r, F.dw.p, nullptr, nullptr, nullptr, 0.f, F.r.p};
-        fine_sweep<RPW, kSrcDwB, kOutRes, false>(ctx, f, a1, partials, ticket, st, mode, rz_out, pdl);
+        SweepArgs a1{r, F.dw.p, x0, nullptr, nullptr, 0.f, F.r.p};
+        fine_sweep<RPW, kSrcX, kOutRes, false>(ctx, f, a1, partials, ticket, st, mode, rz_out, pdl);
     }
     down_restrict(ctx, H, 0, st, pdl);
     coarse_levels(ctx, H, 1, sweeps, st, pdl);
     if (sweeps == 2) {
-        SweepArgs u1{r, F.dw.p, F.x1.p, C.e.p, F.agg.p, s, F.x2.p};
+        SweepArgs u1{r, F.dw.p, x2, C.e.p, F.agg.p, s, x1};
         fine_sweep<RPW, kSrcXCorr, kOutSmooth, false>(ctx, f, u1, partials, ticket, st, mode, rz_out, pdl);
-        SweepArgs u2{r, F.dw.p, F.x2.p, nullptr, nullptr, 0.f, z};
+        SweepArgs u2{r, F.dw.p, x1, nullptr, nullptr, 0.f, z};
         fine_sweep<RPW, kSrcX, kOutSmooth, true>(ctx, f, u2, partials, ticket, st, mode, rz_out, pdl);
     } else {
-        SweepArgs u1{r, F.dw.p, nullptr, C.e.p, F.agg.p, s, z};
-        fine_sweep<RPW, kSrcDwBCorr, kOutSmooth, true>(ctx, f, u1, partials, ticket, st, mode, rz_out, pdl);
+        SweepArgs u1{r, F.dw.p, x0, C.e.p, F.agg.p, s, z};
+        fine_sweep<RPW, kSrcXCorr, kOutSmooth, true>(ctx, f, u1, partials, ticket, st, mode, rz_out, pdl);
     }
     return RSG_OK;
 }
@@ -1028,18 +1055,10 @@ namespace {
 template <int RPW>
 rsg_status profile_typed_sweep(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H, const float *r, float *z)
 {
-    FineLaunch<RPW> f;
-    f.M = view<float>(A, true);
-    f.S = sell_view<float>(A);
-    f.use_sell = A->use_sell;
-    f.smem = A->use_sell ? 0 : tma_smem<float>();
-    if (!A->use_sell)
-        cudaFuncSetAttribute(k_amg_fine<RPW, kSrcDwBCorr, kOutSmooth, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(f.smem));
-    f.grid = spmv_grid(ctx, A, (const void *)k_amg_fine<RPW, kSrcX, kOutSmooth, true>, f.smem, RPW);
+    const FineLaunch<RPW> f = fine_launch<RPW>(ctx, A);
     const AmgLevel &F = H->L[0];
-    SweepArgs a{r, F.dw.p, nullptr, H->L[1].e.p, F.agg.p, kAmgScale1, z};
-    fine_sweep<RPW, kSrcDwBCorr, kOutSmooth, false>(ctx, f, a, nullptr, nullptr, nullptr, 0, nullptr, false);
+    SweepArgs a{r, F.dw.p, F.x1.p, H->L[1].e.p, F.agg.p, kAmgScale1, z};
+    fine_sweep<RPW, kSrcXCorr, kOutSmooth, false>(ctx, f, a, nullptr, nullptr, nullptr, 0, nullptr, false);
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
     return RSG_OK;
 }
@@ -1052,12 +1071,13 @@ rsg_status amg_profile_launch(rsg_context *ctx, const rsg_csr *A, const AmgHiera
     return RSG_ERR_UNSUPPORTED;
 }
 
-rsg_status amg_vcycle(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H, const float *r, float *z, int sweeps,
-                      double *partials, unsigned int *ticket, CgState *st, int mode, double *rz_out, bool pdl)
+rsg_status amg_vcycle(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H, const float *r, const float *x0,
+                      float *z, int sweeps, double *partials, unsigned int *ticket, CgState *st, int mode,
+                      double *rz_out, bool pdl)
 {
     if (!H || H->levels < 1) return set_error(ctx, RSG_ERR_INVALID_ARG, "amg: no hierarchy");
     RSG_RPW_DISPATCH(pick_rpw(A),
-                     return vcycle_typed<RPW>(ctx, A, H, r, z, sweeps, partials, ticket, st, mode, rz_out, pdl));
+                     return vcycle_typed<RPW>(ctx, A, H, r, x0, z, sweeps, partials, ticket, st, mode, rz_out, pdl));
     return RSG_ERR_UNSUPPORTED;
 }
 
@@ -1124,7 +1144,7 @@ rsg_status rsg_amg_apply(rsg_context *ctx, rsg_csr *A, const double *r, double *
     RSG_CHECK_CUDA(ctx, cudaMemsetAsync(scal, 0, 8 * sizeof(double), ctx->stream));
     const int g = std::min(grid_rows(n), kMaxGrid);
     k_amg_d2f<<<g, kBlock, 0, ctx->stream>>>(n, r, L0.b.p);
-    RSG_TRY(amg_vcycle(ctx, A, H, L0.b.p, L0.e.p, int(sweeps), partials, ticket, nullptr, 0, scal, false));
+    RSG_TRY(amg_vcycle(ctx, A, H, L0.b.p, nullptr, L0.e.p, int(sweeps), partials, ticket, nullptr, 0, scal, false));
     k_amg_f2d<<<g, kBlock, 0, ctx->stream>>>(n, L0.e.p, z);
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
     RSG_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

@@ -59,7 +59,7 @@ struct AmgLevel {
     DevBuf<float> dw;                      // omega / a_ii (0 for a zero diagonal)
     DevBuf<uint32_t> agg;                  // row of this level -> row of the next level
     DevBuf<uint32_t> agg_ptr, agg_rows;    // next-level row -> rows of this level (ascending)
-    DevBuf<float> b, r, x1, x2, e;         // V-cycle vectors (b and e unused on level 0)
+    DevBuf<float> b, r, x1, x2, e;         // V-cycle vectors; x1 starts as x0 = dw b (b and e unused on level 0)
 };
 
 struct AmgHierarchy {
@@ -72,6 +72,7 @@ struct AmgHierarchy {
     DevBuf<uint8_t> smask;          // strong-connection flag per stored entry
     DevBuf<uint32_t> u1, u2, u3;    // per-row counters / scan output
     DevBuf<uint32_t> scan_blocks;   // scan workspace
+    DevBuf<unsigned int> rounds;    // undecided nodes after each independent-set round
     DevBuf<uint32_t> tcol;          // Galerkin staging: columns
     DevBuf<double> tval;            // Galerkin staging: values
     unsigned int *flags = nullptr;  // device counters read back by the host (16 words)
@@ -90,8 +91,13 @@ AmgHierarchy *amg_of(const rsg_csr *A);
 // mode 0 starts the recurrence (rho = r^T z, beta = 0), mode 1 continues it (beta = rho_new / rho,
 // or the residual-replacement rule after a true-residual check).  Without st the sum goes to
 // *rz_out.  partials holds >= kMaxGrid doubles; ticket is a zeroed grid-reduction counter.
-rsg_status amg_vcycle(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H, const float *r, float *z, int sweeps,
-                      double *partials, unsigned int *ticket, CgState *st, int mode, double *rz_out, bool pdl);
+// x0 = (omega / a_ii) r, the first smoothing step, computed by the caller's streaming pass (the CG
+// update / check kernels) in the finest level's x0 buffer (amg_finest_x0), or NULL to compute it here.
+rsg_status amg_vcycle(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H, const float *r, const float *x0,
+                      float *z, int sweeps, double *partials, unsigned int *ticket, CgState *st, int mode,
+                      double *rz_out, bool pdl);
+inline const float *amg_finest_weights(const AmgHierarchy *H) { return H->L[0].dw.p; }
+inline float *amg_finest_x0(const AmgHierarchy *H) { return H->L[0].x1.p; }
 
 // One launch of the finest level's post-smoothing sweep with the prolongated coarse correction
 // fused into its gather (z = x + dw (r - A x), x = dw r + s P e_c), for kernel timing.

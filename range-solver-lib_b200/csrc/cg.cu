@@ -273,7 +273,8 @@ __device__ __forceinline__ void prec_group32(uint32_t g, uint32_t w, const float
         z[g] = zi;
         rz.add_prod(rl[0], zi);
     } else if (PK == 3) {
-        // multilevel: z comes from the V-cycle kernels that follow
+        // multilevel: z receives the V-cycle's first smoothing step d r; r^T z comes from the V-cycle
+        z[g] = d[g] * rl[0];
     } else {
         for (uint32_t k = 0; k < w; k++) {
             const float *row = d + (size_t(g) * w + k) * w;
@@ -376,14 +377,16 @@ __global__ void __launch_bounds__(kBlock) k_mx_update(uint32_t n, uint32_t w, co
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
     if (PK < 2 || PK == 3) {
         // four rows per thread with 16-byte loads (vectors are 256-byte aligned); with the multilevel
-        // preconditioner (PK 3) z and r^T z come from the V-cycle that follows
+        // preconditioner (PK 3) z receives the V-cycle's first smoothing step d r (d = omega / a_ii),
+        // and the preconditioned z and r^T z come from the V-cycle that follows
         const uint32_t nq = n / 4;
         for (uint32_t i4 = tid; i4 < nq; i4 += stride) {
             const float4 pv = reinterpret_cast<const float4 *>(p)[i4];
             const float4 qv = reinterpret_cast<const float4 *>(q)[i4];
             float4 yv = reinterpret_cast<const float4 *>(y)[i4];
             float4 rv = reinterpret_cast<const float4 *>(r)[i4];
-            const float4 dv = PK == 1 ? reinterpret_cast<const float4 *>(d)[i4] : make_float4(1.f, 1.f, 1.f, 1.f);
+            const float4 dv = (PK == 1 || PK == 3) ? reinterpret_cast<const float4 *>(d)[i4]
+                                                   : make_float4(1.f, 1.f, 1.f, 1.f);
             float4 zv;
             yv.x = fmaf(alpha, pv.x, yv.x);
             yv.y = fmaf(alpha, pv.y, yv.y);
@@ -393,14 +396,14 @@ __global__ void __launch_bounds__(kBlock) k_mx_update(uint32_t n, uint32_t w, co
             rv.y = fmaf(-alpha, qv.y, rv.y);
             rv.z = fmaf(-alpha, qv.z, rv.z);
             rv.w = fmaf(-alpha, qv.w, rv.w);
-            zv.x = PK == 1 ? dv.x * rv.x : rv.x;
-            zv.y = PK == 1 ? dv.y * rv.y : rv.y;
-            zv.z = PK == 1 ? dv.z * rv.z : rv.z;
-            zv.w = PK == 1 ? dv.w * rv.w : rv.w;
+            zv.x = (PK == 1 || PK == 3) ? dv.x * rv.x : rv.x;
+            zv.y = (PK == 1 || PK == 3) ? dv.y * rv.y : rv.y;
+            zv.z = (PK == 1 || PK == 3) ? dv.z * rv.z : rv.z;
+            zv.w = (PK == 1 || PK == 3) ? dv.w * rv.w : rv.w;
             reinterpret_cast<float4 *>(y)[i4] = yv;
             reinterpret_cast<float4 *>(r)[i4] = rv;
+            reinterpret_cast<float4 *>(z)[i4] = zv;
             if (PK != 3) {
-                reinterpret_cast<float4 *>(z)[i4] = zv;
                 rz.add_prod(rv.x, zv.x);
                 rz.add_prod(rv.y, zv.y);
                 rz.add_prod(rv.z, zv.z);
@@ -414,12 +417,10 @@ __global__ void __launch_bounds__(kBlock) k_mx_update(uint32_t n, uint32_t w, co
         for (uint32_t i = nq * 4 + tid; i < n; i += stride) {
             y[i] = fmaf(alpha, p[i], y[i]);
             const float ri = fmaf(-alpha, q[i], r[i]);
-            const float zi = PK == 1 ? d[i] * ri : ri;
+            const float zi = (PK == 1 || PK == 3) ? d[i] * ri : ri;
             r[i] = ri;
-            if (PK != 3) {
-                z[i] = zi;
-                rz.add_prod(ri, zi);
-            }
+            z[i] = zi;
+            if (PK != 3) rz.add_prod(ri, zi);
             rr.add_prod(ri, ri);
         }
     } else {
@@ -470,6 +471,8 @@ __global__ void __launch_bounds__(kBlock) k_mx_check(Csr<double> M, Sell<double>
             const float zf = d[row] * rf;
             z[row] = zf;
             rz.add_prod(rf, zf);
+        } else if (PK == 3) {
+            z[row] = d[row] * rf;  // the V-cycle's first smoothing step
         }
     };
     for_rows_any<double, RPW>(M, S, use_sell != 0, gx, epi, smem_raw, &st->ticket[7], true);
@@ -553,10 +556,11 @@ void launch_init(rsg_context *ctx, const CgArgs &a, const Launch &L)
     if (!a.mixed)
         k_cg_prec<PK><<<L.g_vec, kBlock, 0, ctx->stream>>>(a.A->n, a.P.w, a.P.d, a.r, a.z, a.partials, a.st, 0);
     else
-        k_mx_prec<PK><<<L.g_vec, kBlock, 0, ctx->stream>>>(a.A->n, a.P.w, a.P.d32, a.r, a.r32, a.z32, a.partials,
-                                                          a.st, 0);
+        k_mx_prec<PK><<<L.g_vec, kBlock, 0, ctx->stream>>>(a.A->n, a.P.w, a.P.d32, a.r, a.r32,
+                                                          PK == 3 ? a.amg_x0 : a.z32, a.partials, a.st, 0);
     if (PK == 3)  // z0 = V(r0), rho = r0^T z0
-        amg_vcycle(ctx, a.A, a.amg, a.r32, a.z32, a.amg_sweeps, a.partials, &a.st->ticket[5], a.st, 0, nullptr, false);
+        amg_vcycle(ctx, a.A, a.amg, a.r32, a.amg_x0, a.z32, a.amg_sweeps, a.partials, &a.st->ticket[5], a.st, 0,
+                   nullptr, false);
 }
 
 template <int RPW, int PK>
@@ -587,16 +591,17 @@ void launch_body(rsg_context *ctx, const CgArgs &a, const Launch &L, cudaGraphCo
             float *po = half ? a.p32b : a.p32a, *pn = half ? a.p32a : a.p32b;
             launch_k(st, pdl, k_mx_dir<RPW>, L.g_dir32, kBlock, L.s32, M32, S32, us, a.z32, po, pn, a.q32, a.x,
                      a.y32, a.partials, a.st);
+            float *zx = PK == 3 ? a.amg_x0 : a.z32;  // multilevel: the V-cycle's first smoothing step
             launch_k(st, pdl, k_mx_update<PK>, L.g_upd32, kBlock, 0, n, a.P.w, a.P.d32, pn, a.q32, a.y32, a.r32,
-                     a.z32, a.partials, a.st);
+                     zx, a.partials, a.st);
             launch_k(st, pdl, k_mx_check<RPW, PK>, L.g_spmv64, kBlock, L.s64, M64, S64, us, a.P.d32, a.b, a.x,
-                     a.y32, a.r32, a.z32, a.partials, a.st);
+                     a.y32, a.r32, zx, a.partials, a.st);
             if (PK == 2)
                 launch_k(st, pdl, k_mx_prec<PK>, L.g_vec, kBlock, 0, n, a.P.w, a.P.d32, (const double *)nullptr,
                          a.r32, a.z32, a.partials, a.st, 1);
             if (PK == 3)
-                amg_vcycle(ctx, a.A, a.amg, a.r32, a.z32, a.amg_sweeps, a.partials, &a.st->ticket[5], a.st, 1,
-                           nullptr, pdl);
+                amg_vcycle(ctx, a.A, a.amg, a.r32, a.amg_x0, a.z32, a.amg_sweeps, a.partials, &a.st->ticket[5],
+                           a.st, 1, nullptr, pdl);
         }
     }
     launch_k(st, pdl, k_tail, 1, 32, 0, a.st, h, use_cond);

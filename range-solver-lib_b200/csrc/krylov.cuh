@@ -63,6 +63,7 @@ struct CgArgs {
     uint32_t check_interval;
     const AmgHierarchy *amg;      // kind 3: the matrix's hierarchy
     int amg_sweeps;               // kind 3: smoothing sweeps per side of the V-cycle (1 or 2)
+    float *amg_x0;                // kind 3: omega D^-1 r, written by the update / check kernels (P.d32 = omega / a_ii)
 };
 
 rsg_status autotune_run(rsg_context *ctx, rsg_csr *A, const char *cache_path);
