@@ -208,18 +208,23 @@ __global__ void k_amg_nbmax(uint32_t n, const uint32_t *__restrict__ rp, const u
     }
 }
 
-// One synchronous round: an undecided node whose tuple is the distance-2 maximum becomes a root;
-// one that sees a root within distance 2 drops out.  *count (zeroed beforehand) receives the number
-// of nodes still undecided; nothing is done once the previous round left none (*prev == 0).
-__global__ void k_amg_mis_decide(uint32_t n, uint64_t *__restrict__ T, const uint64_t *__restrict__ M2,
-                                 const unsigned int *prev, unsigned int *count)
+// Second half of a synchronous round, fused with the decision: for every node still undecided,
+// M2_i = max(M1_i, max over strong neighbours j of M1_j) (decided nodes need no M2); the node becomes
+// a root when M2_i is its own tuple and drops out when M2_i belongs to a root.  *count (zeroed
+// beforehand) receives the number of nodes still undecided; nothing is done once the previous round
+// left none (*prev == 0).
+__global__ void k_amg_mis_round2(uint32_t n, const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ci,
+                                 const uint8_t *__restrict__ smask, const uint64_t *__restrict__ M1,
+                                 uint64_t *__restrict__ T, const unsigned int *prev, unsigned int *count)
 {
     if (prev && *prev == 0) return;
     unsigned int left = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint64_t t = T[i];
         if (tup_state(t) != 1) continue;
-        const uint64_t m = M2[i];
+        uint64_t m = M1[i];
+        for (uint32_t j = rp[i]; j < rp[i + 1]; j++)
+            if (smask[j]) m = max(m, M1[ci[j]]);
         if (m == t) T[i] = (uint64_t(2) << kStateShift) | amg_key(i);
         else if (tup_state(m) == 2) T[i] = amg_key(i);
         else left++;
@@ -428,17 +433,151 @@ __global__ void __launch_bounds__(kGalThreads) k_amg_galerkin(uint32_t nc, const
     if (threadIdx.x == 0) count[I] = base_rank;
 }
 
+// The same coarse rows with one warp per row and no sort: the warp walks the aggregate's entries in
+// staging order (fine rows ascending, entries in CSR order) 32 at a time, keeps one accumulator per
+// distinct J in shared memory (in order of first occurrence), and adds each 32-entry chunk's values
+// into the accumulators serially in lane order -- so every sum is taken in staging order, as in the
+// sorting kernel above.  The row's (J, sum) pairs are then written in ascending J.  A row with more
+// than kGalUnique distinct columns sets flags[5] (the caller then runs the sorting kernel).
+constexpr int kGalWarps = 4;
+constexpr int kGalUnique = 256;
+__global__ void __launch_bounds__(32 * kGalWarps) k_amg_galerkin_warp(
+    uint32_t nc, const uint32_t *__restrict__ ptr, const uint32_t *__restrict__ rows, const uint32_t *__restrict__ rp,
+    const uint32_t *__restrict__ ci, const double *__restrict__ val, const uint32_t *__restrict__ agg,
+    const uint32_t *__restrict__ eoff, uint32_t *__restrict__ tcol, double *__restrict__ tval,
+    uint32_t *__restrict__ count, unsigned int *flags)
+{
+    __shared__ uint32_t ucol[kGalWarps][kGalUnique];
+    __shared__ double uacc[kGalWarps][kGalUnique];
+    __shared__ uint32_t cslot[kGalWarps][32];
+    __shared__ double cval[kGalWarps][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t *uc = ucol[w];
+    double *ua = uacc[w];
+    for (uint32_t I = blockIdx.x * kGalWarps + w; I < nc; I += gridDim.x * kGalWarps) {
+        uint32_t U = 0;
+        bool overflow = false;
+        for (uint32_t k = ptr[I]; k < ptr[I + 1] && !overflow; k++) {
+            const uint32_t i = rows[k];
+            for (uint32_t j0 = rp[i]; j0 < rp[i + 1] && !overflow; j0 += 32) {
+                const uint32_t j = j0 + lane;
+                const bool valid = j < rp[i + 1];
+                const uint32_t J = valid ? agg[ci[j]] : kAmgUnset;
+                const double v = valid ? val[j] : 0.0;
+                uint32_t slot = kAmgUnset;
+                if (valid)
+                    for (uint32_t u = 0; u < U; u++)
+                        if (uc[u] == J) {
+                            slot = u;
+                            break;
+                        }
+                // new columns take slots in order of first occurrence (lane order)
+                const bool fresh = valid && slot == kAmgUnset;
+                const unsigned int fresh_mask = __ballot_sync(0xffffffffu, fresh);
+                const unsigned int same = __match_any_sync(0xffffffffu, fresh ? J : kAmgUnset);
+                const int leader = __ffs(same) - 1;
+                const bool is_leader = fresh && leader == lane;
+                const unsigned int leaders = __ballot_sync(0xffffffffu, is_leader);
+                if (U + __popc(leaders) > uint32_t(kGalUnique)) {
+                    overflow = true;
+                    break;
+                }
+                if (is_leader) {
+                    const uint32_t sl = U + __popc(leaders & ((1u << lane) - 1u));
+                    uc[sl] = J;
+                    ua[sl] = 0.0;
+                    slot = sl;
+                }
+                __syncwarp();
+                if (fresh && !is_leader) slot = U + __popc(leaders & ((1u << leader) - 1u));
+                U += __popc(leaders);
+                (void)fresh_mask;
+                cslot[w][lane] = slot;
+                cval[w][lane] = v;
+                __syncwarp();
+                // the lowest lane of each group of equal slots adds the group's values in lane order
+                const unsigned int grp = __match_any_sync(0xffffffffu, slot);
+                if (valid && (__ffs(grp) - 1) == lane) {
+                    double acc = ua[slot];
+                    for (unsigned int m = grp; m; m &= m - 1) acc += cval[w][__ffs(m) - 1];
+                    ua[slot] = acc;
+                }
+                __syncwarp();
+            }
+        }
+        if (overflow) {
+            if (lane == 0) {
+                atomicOr(&flags[5], 1u);
+                count[I] = 0;
+            }
+            __syncwarp();
+            continue;
+        }
+        // ascending J: each pair's rank among the row's distinct columns
+        for (uint32_t t = lane; t < U; t += 32) {
+            const uint32_t J = uc[t];
+            uint32_t rank = 0;
+            for (uint32_t u = 0; u < U; u++) rank += uc[u] < J ? 1u : 0u;
+            tcol[size_t(eoff[I]) + rank] = J;
+            tval[size_t(eoff[I]) + rank] = ua[t];
+        }
+        if (lane == 0) count[I] = U;
+        __syncwarp();
+    }
+}
+
 __global__ void k_amg_compact(uint32_t nc, const uint32_t *__restrict__ eoff, const uint32_t *__restrict__ count,
                               const uint32_t *__restrict__ rp_c, const uint32_t *__restrict__ tcol,
                               const double *__restrict__ tval, uint32_t *__restrict__ ci_c, double *__restrict__ val_c,
                               float *__restrict__ val32_c)
 {
     for (uint32_t I = blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += gridDim.x * blockDim.x) {
+        // (the longest row was recorded by k_amg_row_max)
         const uint32_t src = eoff[I], dst = rp_c[I];
         for (uint32_t k = 0; k < count[I]; k++) {
             ci_c[dst + k] = tcol[src + k];
             val_c[dst + k] = tval[src + k];
             val32_c[dst + k] = float(tval[src + k]);
+        }
+    }
+}
+
+// flags[6] = the longest coarse row.
+__global__ void k_amg_row_max(uint32_t nc, const uint32_t *__restrict__ count, unsigned int *flags)
+{
+    unsigned int m = 0;
+    for (uint32_t I = blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += gridDim.x * blockDim.x) m = max(m, count[I]);
+    m = __reduce_max_sync(0xffffffffu, m);
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(&flags[6], m);
+}
+
+// SELL-32 copy of a coarse level (the layout of spmv.cuh: slice s = rows 32 s .. 32 s + 31, element k
+// of lane l at slice_ptr[s] + (k / 4) 128 + 4 l + k % 4, rows padded to the slice's longest row
+// rounded up to 4).  len4 / elems: per slice; elems is scanned into slice_ptr.
+__global__ void k_amg_sell_len(uint32_t n, uint32_t n_slices, const uint32_t *__restrict__ rp,
+                               uint32_t *__restrict__ len4, uint32_t *__restrict__ elems)
+{
+    for (uint32_t sl = blockIdx.x * blockDim.x + threadIdx.x; sl < n_slices; sl += gridDim.x * blockDim.x) {
+        uint32_t m = 0;
+        for (uint32_t r = sl * 32u; r < min(n, sl * 32u + 32u); r++) m = max(m, rp[r + 1] - rp[r]);
+        const uint32_t l4 = (m + 3u) / 4u;
+        len4[sl] = l4;
+        elems[sl] = l4 * 128u;
+    }
+}
+
+__global__ void k_amg_sell_fill(uint32_t n, const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ci,
+                                const float *__restrict__ val, const uint32_t *__restrict__ sptr,
+                                const uint32_t *__restrict__ len4, uint32_t *__restrict__ scol, float *__restrict__ sval)
+{
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+        const uint32_t sl = row >> 5, lane = row & 31u;
+        const size_t base = size_t(sptr[sl]) + 4u * lane;
+        const uint32_t len = rp[row + 1] - rp[row], padded = len4[sl] * 4u;
+        for (uint32_t k = 0; k < padded; k++) {
+            const size_t e = base + size_t(k >> 2) * 128u + (k & 3u);
+            scol[e] = k < len ? ci[rp[row] + k] : row;
+            sval[e] = k < len ? val[rp[row] + k] : 0.f;
         }
     }
 }
@@ -575,7 +714,33 @@ __global__ void __launch_bounds__(kBlock) k_amg_fine(Csr<float> M, Sell<float> S
     }
 }
 
-// Sweep over a coarse level (CSR, 8 lanes per row).
+// Sweep over a coarse level in its SELL-32 copy (one thread per row, as the finest level).
+template <int SRC, int OUT>
+__global__ void __launch_bounds__(kBlock) k_amg_coarse_sell(Sell<float> S, SweepArgs a, const CgState *st)
+{
+    pdl_wait();
+    pdl_release();
+    if (st && st->done) return;
+    auto gx = [&](uint32_t c) { return sweep_x<SRC>(a, c); };
+    auto epi = [&](uint32_t row, float ax) {
+        const float res = a.b[row] - ax;
+        a.out[row] = OUT == kOutRes ? res : fmaf(a.dw[row], res, sweep_x<SRC>(a, row));
+    };
+    for_rows_sell<float>(S, gx, epi);
+}
+
+// x_out = xs + s P e_c (the prolongated, scaled coarse correction), one streaming pass.
+__global__ void k_amg_prolong(uint32_t n, const float *__restrict__ xs, const uint32_t *__restrict__ agg,
+                              const float *__restrict__ ec, float s, float *__restrict__ out, const CgState *st)
+{
+    pdl_wait();
+    pdl_release();
+    if (st && st->done) return;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = fmaf(s, ec[agg[i]], xs[i]);
+}
+
+// Sweep over a coarse level (CSR, 8 lanes per row): the stalled-coarsening fallback only.
 constexpr int kLanes = 8;
 template <int SRC, int OUT>
 __global__ void __launch_bounds__(kBlock) k_amg_coarse(uint32_t n, const uint32_t *__restrict__ rp,
@@ -690,7 +855,7 @@ rsg_status build_aggregates(rsg_context *ctx, AmgHierarchy *H, AmgLevel &F, uint
     const uint32_t n = F.n;
     const int g = grid_rows(n);
     cudaStream_t s = ctx->stream;
-    if (!H->T.ensure(n) || !H->M1.ensure(n) || !H->M2.ensure(n) || !H->smask.ensure(F.nnz + 1) ||
+    if (!H->T.ensure(n) || !H->M1.ensure(n) || !H->smask.ensure(F.nnz + 1) ||
         !H->u1.ensure(size_t(n) + 1) || !H->u2.ensure(size_t(n) + 1) || !F.agg.ensure(n))
         return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: set-up workspace");
     k_amg_strength<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, F.val, F.diag.p, kAmgTheta, H->smask.p);
@@ -707,8 +872,8 @@ rsg_status build_aggregates(rsg_context *ctx, AmgHierarchy *H, AmgLevel &F, uint
         for (uint32_t k = 0; k < kRoundBatch; k++, round++) {
             const unsigned int *prev = round ? H->rounds.p + round - 1 : nullptr;
             k_amg_nbmax<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, H->smask.p, H->T.p, H->M1.p, prev);
-            k_amg_nbmax<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, H->smask.p, H->M1.p, H->M2.p, prev);
-            k_amg_mis_decide<<<g, kBlock, 0, s>>>(n, H->T.p, H->M2.p, prev, H->rounds.p + round);
+            k_amg_mis_round2<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, H->smask.p, H->M1.p, H->T.p, prev,
+                                                  H->rounds.p + round);
         }
         RSG_CHECK_CUDA(ctx, cudaGetLastError());
         RSG_TRY(read_u32(ctx, H, H->rounds.p + round - 1, &H->flags_h[0]));
@@ -763,15 +928,29 @@ rsg_status build_galerkin(rsg_context *ctx, AmgHierarchy *H, AmgLevel &F, AmgLev
     while (P < emax) P <<= 1;
     // keys and values (16 bytes per padded slot), then the staging offsets of the aggregate's rows
     const size_t smem = size_t(P) * 16 + (size_t(max_size) + 1) * sizeof(uint32_t);
-    cudaFuncSetAttribute(k_amg_galerkin, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    k_amg_galerkin<<<nc, kGalThreads, smem, s>>>(nc, F.agg_ptr.p, F.agg_rows.p, F.rp, F.ci, F.val, F.agg.p, H->u1.p,
-                                                  H->tcol.p, H->tval.p, H->u2.p);
+    // one warp per coarse row; rows with more distinct columns than the warp kernel keeps fall back to
+    // the sorting kernel (one CTA per row) for the whole level
+    RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->flags + 5, 0, sizeof(unsigned int), s));
+    k_amg_galerkin_warp<<<int(std::min<uint64_t>((nc + kGalWarps - 1) / kGalWarps, 65535ull * 8)), 32 * kGalWarps, 0,
+                          s>>>(nc, F.agg_ptr.p, F.agg_rows.p, F.rp, F.ci, F.val, F.agg.p, H->u1.p, H->tcol.p,
+                               H->tval.p, H->u2.p, H->flags);
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
+    RSG_TRY(read_flags(ctx, H, 6));
+    if (H->flags_h[5]) {
+        cudaFuncSetAttribute(k_amg_galerkin, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        k_amg_galerkin<<<nc, kGalThreads, smem, s>>>(nc, F.agg_ptr.p, F.agg_rows.p, F.rp, F.ci, F.val, F.agg.p,
+                                                      H->u1.p, H->tcol.p, H->tval.p, H->u2.p);
+        RSG_CHECK_CUDA(ctx, cudaGetLastError());
+    }
     // coarse row pointer, then compact
     if (!Cl.own_rp.ensure(size_t(nc) + 1)) return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: coarse matrix");
     RSG_TRY(scan_u32(ctx, H, H->u2.p, nc, Cl.own_rp.p));
-    uint32_t nnz = 0;
-    RSG_TRY(read_u32(ctx, H, Cl.own_rp.p + nc, &nnz));
+    RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->flags + 6, 0, sizeof(unsigned int), s));
+    k_amg_row_max<<<std::min(grid_rows(nc), 1024), kBlock, 0, s>>>(nc, H->u2.p, H->flags);
+    RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(H->flags_h + 9, Cl.own_rp.p + nc, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    RSG_TRY(read_flags(ctx, H, 7));  // one synchronisation for the coarse nnz and the longest row
+    const uint32_t nnz = H->flags_h[9];
+    Cl.max_row = H->flags_h[6];
     if (!Cl.own_ci.ensure(size_t(nnz) + 1) || !Cl.own_val.ensure(size_t(nnz) + 1) || !Cl.own_val32.ensure(size_t(nnz) + 1))
         return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: coarse matrix");
     k_amg_compact<<<grid_rows(nc), kBlock, 0, s>>>(nc, H->u1.p, H->u2.p, Cl.own_rp.p, H->tcol.p, H->tval.p,
@@ -783,6 +962,17 @@ rsg_status build_galerkin(rsg_context *ctx, AmgHierarchy *H, AmgLevel &F, AmgLev
     Cl.ci = Cl.own_ci.p;
     Cl.val = Cl.own_val.p;
     Cl.val32 = Cl.own_val32.p;
+    // SELL-32 copy for the sweeps, sized from the longest row (no further synchronisation)
+    Cl.n_slices = (nc + 31u) / 32u;
+    const size_t cap = size_t(Cl.n_slices) * 128u * ((size_t(Cl.max_row) + 3u) / 4u) + 128u;
+    if (!Cl.s_ptr.ensure(size_t(Cl.n_slices) + 1) || !Cl.s_len4.ensure(Cl.n_slices) || !Cl.s_col.ensure(cap) ||
+        !Cl.s_val.ensure(cap) || !H->u3.ensure(size_t(Cl.n_slices) + 1))
+        return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: coarse SELL copy");
+    k_amg_sell_len<<<grid_rows(Cl.n_slices), kBlock, 0, s>>>(nc, Cl.n_slices, Cl.rp, Cl.s_len4.p, H->u3.p);
+    RSG_TRY(scan_u32(ctx, H, H->u3.p, Cl.n_slices, Cl.s_ptr.p));
+    k_amg_sell_fill<<<grid_rows(nc), kBlock, 0, s>>>(nc, Cl.rp, Cl.ci, Cl.val32, Cl.s_ptr.p, Cl.s_len4.p, Cl.s_col.p,
+                                                     Cl.s_val.p);
+    RSG_CHECK_CUDA(ctx, cudaGetLastError());
     return RSG_OK;
 }
 
@@ -816,11 +1006,14 @@ void amg_free(AmgHierarchy *H)
         l.x1.release();
         l.x2.release();
         l.e.release();
+        l.s_ptr.release();
+        l.s_len4.release();
+        l.s_col.release();
+        l.s_val.release();
     }
     H->coarse_inv.release();
     H->T.release();
     H->M1.release();
-    H->M2.release();
     H->smask.release();
     H->u1.release();
     H->u2.release();
@@ -921,8 +1114,15 @@ void fine_sweep(rsg_context *ctx, const FineLaunch<RPW> &f, const SweepArgs &a, 
 template <int SRC, int OUT>
 void coarse_sweep(rsg_context *ctx, const AmgLevel &l, const SweepArgs &a, const CgState *st, bool pdl)
 {
-    launch_k(ctx->stream, pdl, k_amg_coarse<SRC, OUT>, coarse_grid(ctx, l.n), kBlock, 0, l.n, l.rp, l.ci, l.val32, a,
-             st);
+    if (l.n_slices) {
+        const Sell<float> S{l.rp, l.s_ptr.p, l.s_len4.p, l.s_val.p, nullptr, l.s_col.p, l.n, l.n_slices};
+        const int g = std::max(1, std::min<int>(int((uint64_t(l.n_slices) * 32 + kBlock - 1) / kBlock),
+                                                ctx->num_sms * 8));
+        launch_k(ctx->stream, pdl, k_amg_coarse_sell<SRC, OUT>, g, kBlock, 0, S, a, st);
+    } else {
+        launch_k(ctx->stream, pdl, k_amg_coarse<SRC, OUT>, coarse_grid(ctx, l.n), kBlock, 0, l.n, l.rp, l.ci, l.val32,
+                 a, st);
+    }
 }
 
 // Level l >= 1 (b and x0 = dw b given by the restriction): pre-smoothing, residual, restriction,
@@ -1037,14 +1237,20 @@ rsg_status vcycle_typed(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *
     }
     down_restrict(ctx, H, 0, st, pdl);
     coarse_levels(ctx, H, 1, sweeps, st, pdl);
+    // the coarse correction in its own streaming pass, so that the post-smoothing sweeps gather one vector
+    const int gp = std::min(grid_rows(F.n), kMaxGrid);
     if (sweeps == 2) {
-        SweepArgs u1{r, F.dw.p, x2, C.e.p, F.agg.p, s, x1};
-        fine_sweep<RPW, kSrcXCorr, kOutSmooth, false>(ctx, f, u1, partials, ticket, st, mode, rz_out, pdl);
-        SweepArgs u2{r, F.dw.p, x1, nullptr, nullptr, 0.f, z};
+        launch_k(ctx->stream, pdl, k_amg_prolong, gp, kBlock, 0, F.n, (const float *)x2, (const uint32_t *)F.agg.p,
+                 (const float *)C.e.p, s, x1, (const CgState *)st);
+        SweepArgs u1{r, F.dw.p, x1, nullptr, nullptr, 0.f, x2};
+        fine_sweep<RPW, kSrcX, kOutSmooth, false>(ctx, f, u1, partials, ticket, st, mode, rz_out, pdl);
+        SweepArgs u2{r, F.dw.p, x2, nullptr, nullptr, 0.f, z};
         fine_sweep<RPW, kSrcX, kOutSmooth, true>(ctx, f, u2, partials, ticket, st, mode, rz_out, pdl);
     } else {
-        SweepArgs u1{r, F.dw.p, x0, C.e.p, F.agg.p, s, z};
-        fine_sweep<RPW, kSrcXCorr, kOutSmooth, true>(ctx, f, u1, partials, ticket, st, mode, rz_out, pdl);
+        launch_k(ctx->stream, pdl, k_amg_prolong, gp, kBlock, 0, F.n, x0, (const uint32_t *)F.agg.p,
+                 (const float *)C.e.p, s, x2, (const CgState *)st);
+        SweepArgs u1{r, F.dw.p, x2, nullptr, nullptr, 0.f, z};
+        fine_sweep<RPW, kSrcX, kOutSmooth, true>(ctx, f, u1, partials, ticket, st, mode, rz_out, pdl);
     }
     return RSG_OK;
 }

@@ -60,6 +60,11 @@ struct AmgLevel {
     DevBuf<uint32_t> agg;                  // row of this level -> row of the next level
     DevBuf<uint32_t> agg_ptr, agg_rows;    // next-level row -> rows of this level (ascending)
     DevBuf<float> b, r, x1, x2, e;         // V-cycle vectors; x1 starts as x0 = dw b (b and e unused on level 0)
+    // SELL-32 copy of a coarse level for the sweeps (FP32 values, uint32 columns; see spmv.cuh)
+    uint32_t n_slices = 0;
+    uint32_t max_row = 0;
+    DevBuf<uint32_t> s_ptr, s_len4, s_col;
+    DevBuf<float> s_val;
 };
 
 struct AmgHierarchy {
@@ -68,7 +73,7 @@ struct AmgHierarchy {
     bool dense_coarsest = false;    // the last level is applied through coarse_inv
     DevBuf<float> coarse_inv;       // dense inverse of the last level (row-major)
     // setup scratch
-    DevBuf<uint64_t> T, M1, M2;     // independent-set tuples and their neighbourhood maxima
+    DevBuf<uint64_t> T, M1;         // independent-set tuples and their neighbourhood maxima
     DevBuf<uint8_t> smask;          // strong-connection flag per stored entry
     DevBuf<uint32_t> u1, u2, u3;    // per-row counters / scan output
     DevBuf<uint32_t> scan_blocks;   // scan workspace
