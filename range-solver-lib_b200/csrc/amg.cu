@@ -29,8 +29,6 @@
 //   coarse levels their CSR with 8 lanes per row.
 #include "amg.cuh"
 
-#include <cooperative_groups.h>
-
 #include <algorithm>
 #include <chrono>
 #include <cstring>
@@ -742,115 +740,6 @@ __global__ void k_amg_prolong(uint32_t n, const float *__restrict__ xs, const ui
         out[i] = fmaf(s, ec[agg[i]], xs[i]);
 }
 
-// ---- the bottom of the V-cycle in one thread-block cluster ----
-// Levels of at most kBottomRows rows are latency-bound: a separate launch per sweep costs far more
-// than its work.  One cluster of kBottomCtas CTAs runs all of them -- every sweep, restriction, the
-// coarsest solve and the prolongations -- with a hardware cluster barrier (release / acquire at
-// cluster scope) between steps.  Vectors written inside the kernel are read through L2 (ld.global.cg)
-// so that a CTA never sees a stale L1 line of another CTA's output.
-constexpr uint32_t kBottomRows = 32768;
-constexpr int kBottomCtas = 8, kBottomThreads = 1024;
-
-struct BottomLevel {
-    uint32_t n;
-    const uint32_t *rp, *ci;
-    const float *val, *dw;
-    float *b, *x1, *x2, *r, *e;
-    const uint32_t *agg, *agg_ptr, *agg_rows;  // towards the next level (not for the last)
-};
-struct BottomArgs {
-    int count;                  // levels handled, the coarsest included
-    int sweeps;
-    float s;
-    int dense;                  // the last level is applied through inv
-    const float *inv;
-    BottomLevel lv[kAmgMaxLevels];
-};
-
-// out = x + dw (b - A x) (smooth) or b - A x (residual), x = src or src + s P ec (corr)
-__device__ __forceinline__ void bottom_sweep(const BottomLevel &L, const float *src, const float *ec, float s,
-                                             bool corr, bool smooth, float *out, uint32_t tid, uint32_t nthr)
-{
-    for (uint32_t row = tid; row < L.n; row += nthr) {
-        float acc = 0.f;
-        for (uint32_t j = L.rp[row]; j < L.rp[row + 1]; j++) {
-            const uint32_t c = L.ci[j];
-            float x = __ldcg(src + c);
-            if (corr) x = fmaf(s, __ldcg(ec + L.agg[c]), x);
-            acc = fmaf(L.val[j], x, acc);
-        }
-        const float res = __ldcg(L.b + row) - acc;
-        float o = res;
-        if (smooth) {
-            float x = __ldcg(src + row);
-            if (corr) x = fmaf(s, __ldcg(ec + L.agg[row]), x);
-            o = fmaf(L.dw[row], res, x);
-        }
-        __stcg(out + row, o);
-    }
-}
-
-__global__ void __launch_bounds__(kBottomThreads) k_amg_bottom(BottomArgs A, const CgState *st)
-{
-    pdl_wait();
-    pdl_release();
-    if (st && st->done) return;  // uniform over the cluster: read once before any barrier
-    namespace cg = cooperative_groups;
-    cg::cluster_group cluster = cg::this_cluster();
-    const uint32_t nthr = cluster.num_blocks() * blockDim.x;
-    const uint32_t tid = cluster.block_rank() * blockDim.x + threadIdx.x;
-    const int last = A.count - 1;
-    for (int k = 0; k < last; k++) {  // pre-smoothing, residual, restriction
-        const BottomLevel &L = A.lv[k], &C = A.lv[k + 1];
-        if (A.sweeps == 2) {
-            bottom_sweep(L, L.x1, nullptr, 0.f, false, true, L.x2, tid, nthr);
-            cluster.sync();
-            bottom_sweep(L, L.x2, nullptr, 0.f, false, false, L.r, tid, nthr);
-        } else {
-            bottom_sweep(L, L.x1, nullptr, 0.f, false, false, L.r, tid, nthr);
-        }
-        cluster.sync();
-        for (uint32_t I = tid; I < C.n; I += nthr) {
-            float acc = 0.f;
-            for (uint32_t q = L.agg_ptr[I]; q < L.agg_ptr[I + 1]; q++) acc += __ldcg(L.r + L.agg_rows[q]);
-            __stcg(C.b + I, acc);
-            __stcg(C.x1 + I, C.dw[I] * acc);
-        }
-        cluster.sync();
-    }
-    {  // the coarsest level
-        const BottomLevel &L = A.lv[last];
-        if (A.dense) {
-            for (uint32_t i = tid; i < L.n; i += nthr) {
-                float acc = 0.f;
-                for (uint32_t j = 0; j < L.n; j++) acc = fmaf(A.inv[size_t(i) * L.n + j], __ldcg(L.b + j), acc);
-                __stcg(L.e + i, acc);
-            }
-        } else {  // coarsening stalled above the dense limit: nine damped-Jacobi sweeps from zero
-            float *src = L.x1, *dst = L.x2;
-            for (int k = 0; k < 8; k++) {
-                bottom_sweep(L, src, nullptr, 0.f, false, true, k == 7 ? L.e : dst, tid, nthr);
-                cluster.sync();
-                float *t = src;
-                src = dst;
-                dst = t;
-            }
-        }
-        cluster.sync();
-    }
-    for (int k = last - 1; k >= 0; k--) {  // prolongation and post-smoothing
-        const BottomLevel &L = A.lv[k], &C = A.lv[k + 1];
-        if (A.sweeps == 2) {
-            bottom_sweep(L, L.x2, C.e, A.s, true, true, L.x1, tid, nthr);
-            cluster.sync();
-            bottom_sweep(L, L.x1, nullptr, 0.f, false, true, L.e, tid, nthr);
-        } else {
-            bottom_sweep(L, L.x1, C.e, A.s, true, true, L.e, tid, nthr);
-        }
-        cluster.sync();
-    }
-}
-
 // Sweep over a coarse level (CSR, LANES lanes per row).
 constexpr int kLanes = 4;
 template <int SRC, int OUT>
@@ -1222,8 +1111,10 @@ void fine_sweep(rsg_context *ctx, const FineLaunch<RPW> &f, const SweepArgs &a, 
              partials, ticket, st, mode, rz_out);
 }
 
-// Coarse levels above the cluster limit run on the whole GPU: CSR with kLanes lanes per row (the
-// SELL-32 copy leaves one warp per 32 rows, too few warps for these levels; measured slower).
+// Coarse levels run on the whole GPU: CSR with kLanes lanes per row.  (The SELL-32 copy leaves one warp
+// per 32 rows, too few warps for these levels: measured slower.  One thread-block cluster of 8 CTAs
+// running all levels of up to 32k rows with cluster barriers between steps was slower still: 8 SMs
+// lack the memory-level parallelism for the 276k-entry third level.)
 constexpr bool kCoarseSell = false;
 
 template <int SRC, int OUT>
@@ -1250,57 +1141,9 @@ void down_restrict(rsg_context *ctx, const AmgHierarchy *H, int l, const CgState
              (const uint32_t *)F.agg_rows.p, (const float *)F.r.p, (const float *)C.dw.p, C.b.p, C.x1.p, st);
 }
 
-void bottom_levels(rsg_context *ctx, const AmgHierarchy *H, int l, int sweeps, const CgState *st, bool pdl)
-{
-    BottomArgs A;
-    std::memset(&A, 0, sizeof(A));
-    A.count = H->levels - l;
-    A.sweeps = sweeps;
-    A.s = sweeps == 2 ? kAmgScale2 : kAmgScale1;
-    A.dense = H->dense_coarsest ? 1 : 0;
-    A.inv = H->coarse_inv.p;
-    for (int k = 0; k < A.count; k++) {
-        const AmgLevel &L = H->L[l + k];
-        BottomLevel &B = A.lv[k];
-        B.n = L.n;
-        B.rp = L.rp;
-        B.ci = L.ci;
-        B.val = L.val32;
-        B.dw = L.dw.p;
-        B.b = L.b.p;
-        B.x1 = L.x1.p;
-        B.x2 = L.x2.p;
-        B.r = L.r.p;
-        B.e = L.e.p;
-        if (k + 1 < A.count) {
-            B.agg = L.agg.p;
-            B.agg_ptr = L.agg_ptr.p;
-            B.agg_rows = L.agg_rows.p;
-        }
-    }
-    cudaLaunchAttribute at[2];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = kBottomCtas;
-    at[0].val.clusterDim.y = 1;
-    at[0].val.clusterDim.z = 1;
-    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[1].val.programmaticStreamSerializationAllowed = 1;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(kBottomCtas);
-    cfg.blockDim = dim3(kBottomThreads);
-    cfg.stream = ctx->stream;
-    cfg.attrs = at;
-    cfg.numAttrs = pdl ? 2 : 1;
-    cudaLaunchKernelEx(&cfg, k_amg_bottom, A, st);
-}
-
 void coarse_levels(rsg_context *ctx, const AmgHierarchy *H, int l, int sweeps, const CgState *st, bool pdl)
 {
     const AmgLevel &F = H->L[l];
-    if (F.n <= kBottomRows) {  // this level and every coarser one in one cluster launch
-        bottom_levels(ctx, H, l, sweeps, st, pdl);
-        return;
-    }
     const bool last = (l == H->levels - 1);
     if (last) {
         if (H->dense_coarsest) {
@@ -1445,6 +1288,11 @@ rsg_status amg_vcycle(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H,
                       double *rz_out, bool pdl)
 {
     if (!H || H->levels < 1) return set_error(ctx, RSG_ERR_INVALID_ARG, "amg: no hierarchy");
+    // The V-cycle is a chain of short kernels (the coarse levels' sweeps run a few microseconds), so
+    // each is launched with programmatic dependent launch whatever the caller chose for its own loop
+    // kernels: the next kernel's blocks are scheduled while the current one drains.
+    (void)pdl;
+    pdl = true;
     RSG_RPW_DISPATCH(pick_rpw(A),
                      return vcycle_typed<RPW>(ctx, A, H, r, x0, z, sweeps, partials, ticket, st, mode, rz_out, pdl));
     return RSG_ERR_UNSUPPORTED;
