@@ -542,36 +542,6 @@ __global__ void k_amg_compact(uint32_t nc, const uint32_t *__restrict__ eoff, co
     }
 }
 
-// flags[7] = the largest |value| of the finest matrix's FP32 SELL-32 copy (bit pattern of a
-// non-negative float: ordered as an unsigned integer).
-__global__ void k_amg_absmax(size_t n, const float *__restrict__ v, unsigned int *flags)
-{
-    float m = 0.f;
-    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
-        m = fmaxf(m, fabsf(v[i]));
-    unsigned int u = __float_as_uint(m);
-    u = __reduce_max_sync(0xffffffffu, u);
-    if ((threadIdx.x & 31) == 0 && u) atomicMax(&flags[7], u);
-}
-
-// h = v 2^k in FP16 with 2^k putting the largest magnitude near 2^14 (below the FP16 limit 65504);
-// scale[0] = 2^k, scale[1] = 2^-k.
-__global__ void k_amg_to_half(size_t n, const float *__restrict__ v, const unsigned int *flags, __half *__restrict__ h,
-                              float *__restrict__ scale)
-{
-    const float m = __uint_as_float(flags[7]);
-    int e = 0;
-    if (m > 0.f) frexpf(m, &e);  // m = f 2^e, f in [0.5, 1)
-    const int k = 14 - e;
-    const float up = ldexpf(1.f, k);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        scale[0] = up;
-        scale[1] = ldexpf(1.f, -k);
-    }
-    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
-        h[i] = __float2half_rn(v[i] * up);
-}
-
 // flags[6] = the longest coarse row.
 __global__ void k_amg_row_max(uint32_t nc, const uint32_t *__restrict__ count, unsigned int *flags)
 {
@@ -768,67 +738,6 @@ __global__ void k_amg_prolong(uint32_t n, const float *__restrict__ xs, const ui
     if (st && st->done) return;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         out[i] = fmaf(s, ec[agg[i]], xs[i]);
-}
-
-// Sweep over the finest level with the FP16 copy of its SELL-32 values (FP32 arithmetic; each row's
-// sum is rescaled exactly by the power of two scale[1]).  Layout and loop as for_rows_sell.
-template <int SRC, int OUT, bool FINAL>
-__global__ void __launch_bounds__(kBlock) k_amg_fine_h(Sell<float> S, const __half *__restrict__ hval,
-                                                       const float *__restrict__ scale, SweepArgs a, double *partials,
-                                                       unsigned int *ticket, CgState *st, int mode, double *rz_out)
-{
-    pdl_wait();
-    pdl_release();
-    __shared__ double sh[32];
-    if (st && st->done) return;
-    const float unscale = scale[1];
-    Dot2 rz;
-    const int lane = threadIdx.x & 31;
-    const uint32_t warps_total = gridDim.x * (blockDim.x >> 5);
-    for (uint32_t sl = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); sl < S.n_slices; sl += warps_total) {
-        const uint32_t row0 = sl * 32u, row = row0 + lane;
-        const bool valid = row < S.n;
-        const uint32_t len = valid ? __ldg(&S.rp[row + 1]) - __ldg(&S.rp[row]) : 0u;
-        const uint32_t g4 = __ldg(&S.slice_len4[sl]);
-        const size_t base = size_t(__ldg(&S.slice_ptr[sl])) + 4u * lane;
-        float acc = 0.f;
-#pragma unroll 4
-        for (uint32_t g = 0; g < g4; g++) {
-            const size_t e = base + size_t(g) * 128u;
-            const uint2 hv = __ldcs(reinterpret_cast<const uint2 *>(hval + e));
-            const __half2 h01 = *reinterpret_cast<const __half2 *>(&hv.x), h23 = *reinterpret_cast<const __half2 *>(&hv.y);
-            const float2 f01 = __half22float2(h01), f23 = __half22float2(h23);
-            const float v[4] = {f01.x, f01.y, f23.x, f23.y};
-            uint32_t c[4];
-            if (S.off) {
-                const short4 o = __ldcs(reinterpret_cast<const short4 *>(S.off + e));
-                c[0] = uint32_t(int(row0) + o.x);
-                c[1] = uint32_t(int(row0) + o.y);
-                c[2] = uint32_t(int(row0) + o.z);
-                c[3] = uint32_t(int(row0) + o.w);
-            } else {
-                const uint4 o = __ldcs(reinterpret_cast<const uint4 *>(S.col + e));
-                c[0] = o.x;
-                c[1] = o.y;
-                c[2] = o.z;
-                c[3] = o.w;
-            }
-#pragma unroll
-            for (int t = 0; t < 4; t++)
-                if (4u * g + t < len) acc = fmaf(v[t], sweep_x<SRC>(a, c[t]), acc);
-        }
-        if (valid) {
-            const float res = a.b[row] - acc * unscale;
-            const float o = OUT == kOutRes ? res : fmaf(a.dw[row], res, sweep_x<SRC>(a, row));
-            a.out[row] = o;
-            if (FINAL) rz.add_prod(a.b[row], o);
-        }
-    }
-    if (FINAL) {
-        double accd[1] = {rz.value()};
-        double tot[1];
-        if (grid_sum<1>(accd, partials, ticket, sh, tot) && threadIdx.x == 0) amg_finalize(st, tot[0], mode, rz_out);
-    }
 }
 
 // Sweep over a coarse level (CSR, LANES lanes per row).
@@ -1103,8 +1012,6 @@ void amg_free(AmgHierarchy *H)
         l.s_val.release();
     }
     H->coarse_inv.release();
-    H->fine_h.release();
-    H->fine_scale.release();
     H->T.release();
     H->M1.release();
     H->smask.release();
@@ -1148,16 +1055,6 @@ rsg_status amg_setup(rsg_context *ctx, rsg_csr *A)
     L0.val = A->val;
     L0.val32 = A->val32;
     RSG_TRY(level_vectors(ctx, L0));
-    H->use_half = A->use_sell && A->sell_elems > 0;
-    if (H->use_half) {  // FP16 copy of the SELL-32 values for the finest level's sweeps
-        if (!H->fine_h.ensure(A->sell_elems) || !H->fine_scale.ensure(2))
-            return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: FP16 matrix copy");
-        RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->flags + 7, 0, sizeof(unsigned int), ctx->stream));
-        const int g = ctx->num_sms * 8;
-        k_amg_absmax<<<g, kBlock, 0, ctx->stream>>>(A->sell_elems, A->sval32, H->flags);
-        k_amg_to_half<<<g, kBlock, 0, ctx->stream>>>(A->sell_elems, A->sval32, H->flags, H->fine_h.p, H->fine_scale.p);
-        RSG_CHECK_CUDA(ctx, cudaGetLastError());
-    }
     while (H->levels < kAmgMaxLevels) {
         AmgLevel &F = H->L[H->levels - 1];
         if (F.n <= kAmgCoarsest) {
@@ -1204,20 +1101,14 @@ struct FineLaunch {
     Sell<float> S;
     int use_sell, grid;
     size_t smem;
-    const __half *hval = nullptr;   // FP16 SELL values (the hierarchy's copy), when present
-    const float *hscale = nullptr;
 };
 
 template <int RPW, int SRC, int OUT, bool FINAL>
 void fine_sweep(rsg_context *ctx, const FineLaunch<RPW> &f, const SweepArgs &a, double *partials,
                 unsigned int *ticket, CgState *st, int mode, double *rz_out, bool pdl)
 {
-    if (f.hval)
-        launch_k(ctx->stream, pdl, k_amg_fine_h<SRC, OUT, FINAL>, f.grid, kBlock, 0, f.S, f.hval, f.hscale, a,
-                 partials, ticket, st, mode, rz_out);
-    else
-        launch_k(ctx->stream, pdl, k_amg_fine<RPW, SRC, OUT, FINAL>, f.grid, kBlock, f.smem, f.M, f.S, f.use_sell, a,
-                 partials, ticket, st, mode, rz_out);
+    launch_k(ctx->stream, pdl, k_amg_fine<RPW, SRC, OUT, FINAL>, f.grid, kBlock, f.smem, f.M, f.S, f.use_sell, a,
+             partials, ticket, st, mode, rz_out);
 }
 
 // Coarse levels run on the whole GPU: CSR with kLanes lanes per row.  (The SELL-32 copy leaves one warp
@@ -1295,13 +1186,9 @@ void coarse_levels(rsg_context *ctx, const AmgHierarchy *H, int l, int sweeps, c
 }
 
 template <int RPW>
-FineLaunch<RPW> fine_launch(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H)
+FineLaunch<RPW> fine_launch(rsg_context *ctx, const rsg_csr *A)
 {
     FineLaunch<RPW> f;
-    if (H && H->use_half) {
-        f.hval = H->fine_h.p;
-        f.hscale = H->fine_scale.p;
-    }
     f.M = view<float>(A, true);
     f.S = sell_view<float>(A);
     f.use_sell = A->use_sell;
@@ -1341,7 +1228,7 @@ rsg_status vcycle_typed(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *
         launch_k(ctx->stream, pdl, k_amg_rz, g, kBlock, 0, F.n, r, (const float *)z, partials, ticket, st, mode, rz_out);
         return RSG_OK;
     }
-    const FineLaunch<RPW> f = fine_launch<RPW>(ctx, A, H);
+    const FineLaunch<RPW> f = fine_launch<RPW>(ctx, A);
     const AmgLevel &C = H->L[1];
     const float s = sweeps == 2 ? kAmgScale2 : kAmgScale1;
     float *x1 = F.x1.p, *x2 = F.x2.p;
@@ -1380,10 +1267,10 @@ namespace {
 template <int RPW>
 rsg_status profile_typed_sweep(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H, const float *r, float *z)
 {
-    const FineLaunch<RPW> f = fine_launch<RPW>(ctx, A, H);
+    const FineLaunch<RPW> f = fine_launch<RPW>(ctx, A);
     const AmgLevel &F = H->L[0];
-    SweepArgs a{r, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, z};
-    fine_sweep<RPW, kSrcX, kOutSmooth, false>(ctx, f, a, nullptr, nullptr, nullptr, 0, nullptr, false);
+    SweepArgs a{r, F.dw.p, F.x1.p, H->L[1].e.p, F.agg.p, kAmgScale1, z};
+    fine_sweep<RPW, kSrcXCorr, kOutSmooth, false>(ctx, f, a, nullptr, nullptr, nullptr, 0, nullptr, false);
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
     return RSG_OK;
 }

@@ -10,8 +10,6 @@
 
 #include "krylov.cuh"
 
-#include <cuda_fp16.h>
-
 namespace rsg {
 
 constexpr int kAmgMaxLevels = 12;
@@ -71,12 +69,6 @@ struct AmgLevel {
 
 struct AmgHierarchy {
     int levels = 0;                 // levels in use, the finest included
-    // FP16 copy of the finest matrix's SELL-32 values for the V-cycle sweeps (when the matrix uses
-    // SELL-32), scaled by a power of two so that the largest entry is near 2^14; fine_scale[1] holds
-    // the inverse factor that the sweeps apply to each row sum (exact: a power of two)
-    DevBuf<__half> fine_h;
-    DevBuf<float> fine_scale;
-    bool use_half = false;
     AmgLevel L[kAmgMaxLevels];
     bool dense_coarsest = false;    // the last level is applied through coarse_inv
     DevBuf<float> coarse_inv;       // dense inverse of the last level (row-major)
@@ -112,8 +104,8 @@ rsg_status amg_vcycle(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H,
 inline const float *amg_finest_weights(const AmgHierarchy *H) { return H->L[0].dw.p; }
 inline float *amg_finest_x0(const AmgHierarchy *H) { return H->L[0].x1.p; }
 
-// One launch of a finest-level smoothing sweep (z = x + dw (r - A x), the FP16 values when present),
-// for kernel timing.
+// One launch of the finest level's post-smoothing sweep with the prolongated coarse correction
+// fused into its gather (z = x + dw (r - A x), x = dw r + s P e_c), for kernel timing.
 rsg_status amg_profile_launch(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H, const float *r, float *z);
 
 }  // namespace rsg
