@@ -181,8 +181,8 @@ typedef enum {
     RSG_KERNEL_CG_UPDATE_MIXED = 3,
     RSG_KERNEL_SPMV_FP64 = 4,
     RSG_KERNEL_SPMV_FP32 = 5,
-    RSG_KERNEL_AMG_SWEEP = 6       /* RSG_PREC_AMG: finest-level smoothing sweep with the coarse correction
-                                      fused into its gather (builds A's hierarchy first if it has none) */
+    RSG_KERNEL_AMG_SWEEP = 6       /* RSG_PREC_AMG: a finest-level smoothing sweep x + dw (r - A x) of the
+                                      V-cycle (builds A's hierarchy first if it has none) */
 } rsg_kernel_id;
 RSG_API rsg_status rsg_profile_kernel(rsg_context *ctx, const rsg_csr *A, int32_t kernel, uint32_t reps,
                                       int32_t flush_l2, double *seconds);

@@ -1269,8 +1269,8 @@ rsg_status profile_typed_sweep(rsg_context *ctx, const rsg_csr *A, const AmgHier
 {
     const FineLaunch<RPW> f = fine_launch<RPW>(ctx, A);
     const AmgLevel &F = H->L[0];
-    SweepArgs a{r, F.dw.p, F.x1.p, H->L[1].e.p, F.agg.p, kAmgScale1, z};
-    fine_sweep<RPW, kSrcXCorr, kOutSmooth, false>(ctx, f, a, nullptr, nullptr, nullptr, 0, nullptr, false);
+    SweepArgs a{r, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, z};
+    fine_sweep<RPW, kSrcX, kOutSmooth, false>(ctx, f, a, nullptr, nullptr, nullptr, 0, nullptr, false);
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
     return RSG_OK;
 }

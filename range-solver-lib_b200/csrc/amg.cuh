@@ -104,8 +104,7 @@ rsg_status amg_vcycle(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H,
 inline const float *amg_finest_weights(const AmgHierarchy *H) { return H->L[0].dw.p; }
 inline float *amg_finest_x0(const AmgHierarchy *H) { return H->L[0].x1.p; }
 
-// One launch of the finest level's post-smoothing sweep with the prolongated coarse correction
-// fused into its gather (z = x + dw (r - A x), x = dw r + s P e_c), for kernel timing.
+// One launch of a finest-level smoothing sweep (z = x + dw (r - A x)), for kernel timing.
 rsg_status amg_profile_launch(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H, const float *r, float *z);
 
 }  // namespace rsg
