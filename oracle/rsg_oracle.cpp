@@ -946,12 +946,13 @@ orc_system *orc_assemble_magnetostatics(uint32_t n_nodes, const double *xyz, uin
  * Multilevel aggregation preconditioner (no reference counterpart).  Serial restatement of the
  * CUDA library's set-up (range-solver-lib_b200/csrc/amg.cu): every integer decision and every
  * floating-point sum is taken in the same order, so the hierarchy is identical bit for bit; the
- * V-cycle runs in FP64 here (FP32 on the GPU).
+ * cycle (levels 1..2 as K-cycle levels: two flexible-CG steps) runs in FP64 here (FP32 on the GPU).
  * ------------------------------------------------------------------------------------------------ */
 namespace {
 
 constexpr uint32_t kAmgCoarsest = 128, kAmgMaxEntries = 4096, kAmgUnset = 0xffffffffu;
 constexpr double kAmgTheta = 0.08, kAmgOmega = 2.0 / 3.0, kAmgScale1 = 1.6, kAmgScale2 = 1.8;
+constexpr size_t kAmgKLevels = 2;  /* levels 1..2 are solved by two flexible-CG steps (K-cycle) */
 
 uint32_t amg_hash(uint32_t x)
 {
@@ -1155,12 +1156,58 @@ void amg_sweep(const AmgLev &l, const std::vector<double> &b, const std::vector<
     }
 }
 
+bool amg_k_level(const orc_amg &H, size_t l) { return l >= 1 && l <= kAmgKLevels && l + 1 < H.L.size(); }
+
+void amg_solve_level(const orc_amg &H, size_t lv, const std::vector<double> &b, std::vector<double> &e,
+                     uint32_t sweeps);
+
+/* one cycle on level lv: smoothing from zero, residual, restriction, the coarser level, prolongation
+ * (scaled by 1.6 / 1.8 unless the coarser level is a K-cycle level), smoothing */
 void amg_cycle(const orc_amg &H, size_t lv, const std::vector<double> &b, std::vector<double> &e, uint32_t sweeps)
 {
     const AmgLev &F = H.L[lv];
     const uint32_t n = F.n;
-    e.assign(n, 0.0);
+    const double s = amg_k_level(H, lv + 1) ? 1.0 : (sweeps == 2 ? kAmgScale2 : kAmgScale1);
+    std::vector<double> x(n, 0.0), t(n), r(n);
+    amg_sweep(F, b, x, t, true);           /* x = dw b */
+    x.swap(t);
+    for (uint32_t k = 1; k < sweeps; k++) {
+        amg_sweep(F, b, x, t, true);
+        x.swap(t);
+    }
+    amg_sweep(F, b, x, r, false);
+    const AmgLev &C = H.L[lv + 1];
+    std::vector<double> bc(C.n, 0.0), ec;
+    for (uint32_t I = 0; I < C.n; I++) {
+        double acc = 0.0;
+        for (uint32_t k = F.agg_ptr[I]; k < F.agg_ptr[I + 1]; k++) acc += r[F.agg_rows[k]];
+        bc[I] = acc;
+    }
+    amg_solve_level(H, lv + 1, bc, ec, sweeps);
+    for (uint32_t i = 0; i < n; i++) x[i] += s * ec[F.agg[i]];
+    for (uint32_t k = 0; k < sweeps; k++) {
+        amg_sweep(F, b, x, t, true);
+        x.swap(t);
+    }
+    e = x;
+}
+
+double amg_dot(const std::vector<double> &u, const std::vector<double> &v)
+{
+    double s = 0.0;
+    for (size_t i = 0; i < u.size(); i++) s += u[i] * v[i];
+    return s;
+}
+
+/* e ~ A_lv^-1 b: the dense inverse on the last level, two flexible-CG steps preconditioned by the
+ * cycle on a K-cycle level (Notay's K-cycle), one cycle otherwise */
+void amg_solve_level(const orc_amg &H, size_t lv, const std::vector<double> &b, std::vector<double> &e,
+                     uint32_t sweeps)
+{
+    const AmgLev &F = H.L[lv];
+    const uint32_t n = F.n;
     if (lv + 1 == H.L.size()) {
+        e.assign(n, 0.0);
         if (H.dense) {
             for (uint32_t i = 0; i < n; i++) {
                 double s = 0.0;
@@ -1177,29 +1224,34 @@ void amg_cycle(const orc_amg &H, size_t lv, const std::vector<double> &b, std::v
         }
         return;
     }
-    const double s = sweeps == 2 ? kAmgScale2 : kAmgScale1;
-    std::vector<double> x(n, 0.0), t(n), r(n);
-    amg_sweep(F, b, x, t, true);           /* x = dw b */
-    x.swap(t);
-    for (uint32_t k = 1; k < sweeps; k++) {
-        amg_sweep(F, b, x, t, true);
-        x.swap(t);
+    if (!amg_k_level(H, lv)) {
+        amg_cycle(H, lv, b, e, sweeps);
+        return;
     }
-    amg_sweep(F, b, x, r, false);
-    const AmgLev &C = H.L[lv + 1];
-    std::vector<double> bc(C.n, 0.0), ec;
-    for (uint32_t I = 0; I < C.n; I++) {
-        double acc = 0.0;
-        for (uint32_t k = F.agg_ptr[I]; k < F.agg_ptr[I + 1]; k++) acc += r[F.agg_rows[k]];
-        bc[I] = acc;
+    std::vector<double> c1, c2, v1(n), v2(n), r2(n);
+    auto mul = [&](const std::vector<double> &c, std::vector<double> &v) {
+        for (uint32_t i = 0; i < n; i++) {
+            double acc = 0.0;
+            for (uint32_t j = F.rp[i]; j < F.rp[i + 1]; j++) acc += F.val[j] * c[F.ci[j]];
+            v[i] = acc;
+        }
+    };
+    amg_cycle(H, lv, b, c1, sweeps);
+    mul(c1, v1);
+    const double d1 = amg_dot(c1, v1), t1 = amg_dot(c1, b);
+    const double a1 = d1 > 0.0 ? t1 / d1 : 0.0;
+    for (uint32_t i = 0; i < n; i++) r2[i] = b[i] - a1 * v1[i];
+    amg_cycle(H, lv, r2, c2, sweeps);
+    mul(c2, v2);
+    const double d2 = amg_dot(c2, v2), g = amg_dot(c2, v1), t2 = amg_dot(c2, r2);
+    double g1 = 0.0, a2 = 0.0;
+    if (d1 > 0.0) {
+        const double b2 = d2 - g * g / d1;
+        a2 = b2 > 0.0 ? t2 / b2 : 0.0;
+        g1 = t1 / d1 - g * a2 / d1;
     }
-    amg_cycle(H, lv + 1, bc, ec, sweeps);
-    for (uint32_t i = 0; i < n; i++) x[i] += s * ec[F.agg[i]];
-    for (uint32_t k = 0; k < sweeps; k++) {
-        amg_sweep(F, b, x, t, true);
-        x.swap(t);
-    }
-    e = x;
+    e.assign(n, 0.0);
+    for (uint32_t i = 0; i < n; i++) e[i] = g1 * c1[i] + a2 * c2[i];
 }
 
 }  // namespace
@@ -1260,7 +1312,8 @@ void orc_amg_apply(const orc_amg *h, const double *r, double *z, uint32_t sweeps
         for (uint32_t i = 0; i < F.n; i++) z[i] = F.dw[i] * r[i];
         return;
     }
-    amg_cycle(*h, 0, b, e, sweeps);
+    if (h->L.size() == 1) amg_solve_level(*h, 0, b, e, sweeps);  /* one dense level */
+    else amg_cycle(*h, 0, b, e, sweeps);
     std::memcpy(z, e.data(), F.n * sizeof(double));
 }
 

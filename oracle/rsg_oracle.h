@@ -124,7 +124,8 @@ orc_system *orc_assemble_magnetostatics(uint32_t n_nodes, const double *xyz, uin
 /* Multilevel aggregation preconditioner (no reference counterpart; the checker of the CUDA
  * library's RSG_PREC_AMG): the same aggregation (strength threshold, distance-2 independent roots
  * of hashed priorities in synchronous rounds, joins, singletons), the same Galerkin summation order
- * and stopping rule of the coarsening, and the V-cycle in FP64. */
+ * and stopping rule of the coarsening, and the cycle in FP64 (levels 1 and 2 solved by two
+ * flexible-CG steps each: a K-cycle). */
 typedef struct orc_amg orc_amg;
 orc_amg *orc_amg_build(uint32_t n, const uint32_t *rp, const uint32_t *ci, const double *val);
 uint32_t orc_amg_levels(const orc_amg *h);
@@ -134,7 +135,7 @@ uint64_t orc_amg_nnz(const orc_amg *h, uint32_t level);
 /* agg (rows of the level; not for the last level), row_ptr, col_idx, values: any may be NULL */
 void orc_amg_level(const orc_amg *h, uint32_t level, uint32_t *agg, uint32_t *row_ptr, uint32_t *col_idx,
                    double *values);
-/* z = one V-cycle applied to r (FP64), sweeps 1 or 2 per side */
+/* z = one cycle applied to r (FP64), sweeps 1 or 2 per side */
 void orc_amg_apply(const orc_amg *h, const double *r, double *z, uint32_t sweeps);
 void orc_amg_free(orc_amg *h);
 

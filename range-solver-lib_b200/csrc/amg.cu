@@ -665,7 +665,12 @@ __device__ __forceinline__ float sweep_x(const SweepArgs &a, uint32_t c)
     return x;
 }
 
-__device__ __forceinline__ void amg_finalize(CgState *st, double rz, int mode, double *rz_out)
+// rz = r^T z of the new preconditioned residual; qz = q^T z with q = A p of the last step.  The cycle
+// is a variable preconditioner (its K-cycle levels run flexible-CG steps whose coefficients depend on
+// the input), so the direction update is the flexible (Polak-Ribiere) one: with r_new = r_old - alpha q,
+// beta = z^T (r_new - r_old) / rho = -alpha q^T z / rho.  After a true-residual refresh (r replaced)
+// the mixed-precision refresh rule applies (finalize_check_mixed).
+__device__ __forceinline__ void amg_finalize(CgState *st, double rz, double qz, int mode, double *rz_out)
 {
     if (!st) {
         if (rz_out) *rz_out = rz;
@@ -679,7 +684,7 @@ __device__ __forceinline__ void amg_finalize(CgState *st, double rz, int mode, d
         finalize_check_mixed(st, rz, st->check_rn);
     } else {
         st->rho_new = rz;
-        st->beta = rz / st->rho;
+        st->beta = -st->alpha * qz / st->rho;
     }
 }
 
@@ -687,15 +692,15 @@ __device__ __forceinline__ void amg_finalize(CgState *st, double rz, int mode, d
 // preconditioner; r^T z is reduced and the CG state finalized.
 template <int RPW, int SRC, int OUT, bool FINAL>
 __global__ void __launch_bounds__(kBlock) k_amg_fine(Csr<float> M, Sell<float> S, int use_sell, SweepArgs a,
-                                                     double *partials, unsigned int *ticket, CgState *st, int mode,
-                                                     double *rz_out)
+                                                     const float *qv, double *partials, unsigned int *ticket,
+                                                     CgState *st, int mode, double *rz_out)
 {
     pdl_wait();
     pdl_release();
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double sh[32];
+    __shared__ double sh[64];
     if (st && st->done) return;
-    Dot2 rz;
+    Dot2 rz, qz;
     auto gx = [&](uint32_t c) { return sweep_x<SRC>(a, c); };
     auto epi = [&](uint32_t row, float ax) {
         const float res = a.b[row] - ax;
@@ -703,14 +708,18 @@ __global__ void __launch_bounds__(kBlock) k_amg_fine(Csr<float> M, Sell<float> S
         if (OUT == kOutRes) o = res;
         else o = fmaf(a.dw[row], res, sweep_x<SRC>(a, row));
         a.out[row] = o;
-        if (FINAL) rz.add_prod(a.b[row], o);
+        if (FINAL) {
+            rz.add_prod(a.b[row], o);
+            if (qv) qz.add_prod(qv[row], o);
+        }
     };
     unsigned int *errw = st ? &st->ticket[7] : (ticket ? ticket + 1 : nullptr);
     for_rows_any<float, RPW>(M, S, use_sell != 0, gx, epi, smem_raw, errw, true);
     if (FINAL) {
-        double acc[1] = {rz.value()};
-        double tot[1];
-        if (grid_sum<1>(acc, partials, ticket, sh, tot) && threadIdx.x == 0) amg_finalize(st, tot[0], mode, rz_out);
+        double acc[2] = {rz.value(), qz.value()};
+        double tot[2];
+        if (grid_sum<2>(acc, partials, ticket, sh, tot) && threadIdx.x == 0)
+            amg_finalize(st, tot[0], tot[1], mode, rz_out);
     }
 }
 
@@ -768,6 +777,85 @@ __global__ void __launch_bounds__(kBlock) k_amg_coarse(uint32_t n, const uint32_
     }
 }
 
+// ---- K-cycle: two flexible-CG steps on a coarse level (Notay's K-cycle) ----
+// v = A c (CSR, kLanes lanes per row), with the dot products c.v, c.y1 and (y2 given) c.y2 reduced
+// over the grid into sc[o0], sc[o1], sc[o2].
+template <int NDOT>
+__global__ void __launch_bounds__(kBlock) k_amg_kc_spmv(uint32_t n, const uint32_t *__restrict__ rp,
+                                                        const uint32_t *__restrict__ ci, const float *__restrict__ val,
+                                                        const float *__restrict__ c, float *__restrict__ v,
+                                                        const float *__restrict__ y1, const float *__restrict__ y2,
+                                                        double *partials, unsigned int *ticket, double *sc, int o0,
+                                                        int o1, int o2, const CgState *st)
+{
+    pdl_wait();
+    pdl_release();
+    __shared__ double sh[3 * 32];
+    if (st && st->done) return;
+    const int lane = threadIdx.x & (kLanes - 1);
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t sub = (threadIdx.x & 31) / kLanes;
+    Dot2 d0, d1, d2;
+    for (uint32_t base = gw * (32 / kLanes); base < n; base += warps * (32 / kLanes)) {
+        const uint32_t row = base + sub;
+        float acc = 0.f;
+        if (row < n)
+            for (uint32_t j = rp[row] + lane; j < rp[row + 1]; j += kLanes) acc = fmaf(val[j], c[ci[j]], acc);
+#pragma unroll
+        for (int o = kLanes / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0 && row < n) {
+            v[row] = acc;
+            const float ci_ = c[row];
+            d0.add_prod(ci_, acc);
+            d1.add_prod(ci_, y1[row]);
+            if (NDOT == 3) d2.add_prod(ci_, y2[row]);
+        }
+    }
+    double accd[3] = {d0.value(), d1.value(), d2.value()};
+    double tot[3];
+    if (grid_sum<3>(accd, partials, ticket, sh, tot) && threadIdx.x == 0) {
+        sc[o0] = tot[0];
+        sc[o1] = tot[1];
+        if (NDOT == 3) sc[o2] = tot[2];
+    }
+}
+
+// r2 = b - alpha1 v1 with alpha1 = (c1.b) / (c1.v1); x1 = dw r2 (the next cycle's first smoothing step).
+__global__ void k_amg_kc_r2(uint32_t n, const float *__restrict__ b, const float *__restrict__ v1,
+                            const double *__restrict__ sc, const float *__restrict__ dw, float *__restrict__ r2,
+                            float *__restrict__ x1, const CgState *st)
+{
+    pdl_wait();
+    pdl_release();
+    if (st && st->done) return;
+    const double d1 = sc[0];
+    const float a1 = d1 > 0.0 ? float(sc[1] / d1) : 0.f;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float r = fmaf(-a1, v1[i], b[i]);
+        r2[i] = r;
+        x1[i] = dw[i] * r;
+    }
+}
+
+// e = (alpha1 - g alpha2 / d1) c1 + alpha2 c2: the two-step flexible-CG approximation of A^-1 b.
+__global__ void k_amg_kc_combine(uint32_t n, const float *__restrict__ c1, const float *__restrict__ c2,
+                                 const double *__restrict__ sc, float *__restrict__ e, const CgState *st)
+{
+    pdl_wait();
+    pdl_release();
+    if (st && st->done) return;
+    const double d1 = sc[0], t1 = sc[1], d2 = sc[2], g = sc[3], t2 = sc[4];
+    double g1 = 0.0, a2 = 0.0;
+    if (d1 > 0.0) {
+        const double b2 = d2 - g * g / d1;
+        a2 = b2 > 0.0 ? t2 / b2 : 0.0;
+        g1 = t1 / d1 - g * a2 / d1;
+    }
+    const float fg1 = float(g1), fa2 = float(a2);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        e[i] = fmaf(fg1, c1[i], fa2 * c2[i]);
+}
+
 // b_c[I] = sum of r over the aggregate's rows (ascending order), and the coarse level's first
 // smoothing step x0_c = dw_c b_c.
 __global__ void k_amg_restrict(uint32_t nc, const uint32_t *__restrict__ ptr, const uint32_t *__restrict__ rows,
@@ -816,18 +904,21 @@ __global__ void k_amg_jacobi(uint32_t n, const float *__restrict__ dw, const flo
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) z[i] = dw[i] * r[i];
 }
 
-__global__ void k_amg_rz(uint32_t n, const float *__restrict__ r, const float *__restrict__ z, double *partials,
-                         unsigned int *ticket, CgState *st, int mode, double *rz_out)
+__global__ void k_amg_rz(uint32_t n, const float *__restrict__ r, const float *__restrict__ z, const float *qv,
+                         double *partials, unsigned int *ticket, CgState *st, int mode, double *rz_out)
 {
     pdl_wait();
     pdl_release();
-    __shared__ double sh[32];
+    __shared__ double sh[64];
     if (st && st->done) return;
-    Dot2 rz;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) rz.add_prod(r[i], z[i]);
-    double acc[1] = {rz.value()};
-    double tot[1];
-    if (grid_sum<1>(acc, partials, ticket, sh, tot) && threadIdx.x == 0) amg_finalize(st, tot[0], mode, rz_out);
+    Dot2 rz, qz;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        rz.add_prod(r[i], z[i]);
+        if (qv) qz.add_prod(qv[i], z[i]);
+    }
+    double acc[2] = {rz.value(), qz.value()};
+    double tot[2];
+    if (grid_sum<2>(acc, partials, ticket, sh, tot) && threadIdx.x == 0) amg_finalize(st, tot[0], tot[1], mode, rz_out);
 }
 
 // ---------------------------------------------------------------- host: set-up --------------
@@ -976,11 +1067,14 @@ rsg_status build_galerkin(rsg_context *ctx, AmgHierarchy *H, AmgLevel &F, AmgLev
     return RSG_OK;
 }
 
-rsg_status level_vectors(rsg_context *ctx, AmgLevel &l)
+rsg_status level_vectors(rsg_context *ctx, AmgLevel &l, bool k_buffers)
 {
     if (!l.diag.ensure(l.n) || !l.dw.ensure(l.n) || !l.b.ensure(l.n) || !l.r.ensure(l.n) || !l.x1.ensure(l.n) ||
         !l.x2.ensure(l.n) || !l.e.ensure(l.n))
         return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: level vectors");
+    if (k_buffers && (!l.c1.ensure(l.n) || !l.c2.ensure(l.n) || !l.v1.ensure(l.n) || !l.v2.ensure(l.n) ||
+                      !l.r2.ensure(l.n)))
+        return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: K-cycle vectors");
     k_amg_diag<<<grid_rows(l.n), kBlock, 0, ctx->stream>>>(l.n, l.rp, l.ci, l.val, l.diag.p, l.dw.p);
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
     return RSG_OK;
@@ -1006,6 +1100,11 @@ void amg_free(AmgHierarchy *H)
         l.x1.release();
         l.x2.release();
         l.e.release();
+        l.c1.release();
+        l.c2.release();
+        l.v1.release();
+        l.v2.release();
+        l.r2.release();
         l.s_ptr.release();
         l.s_len4.release();
         l.s_col.release();
@@ -1019,6 +1118,9 @@ void amg_free(AmgHierarchy *H)
     H->u2.release();
     H->u3.release();
     H->scan_blocks.release();
+    H->kc_part.release();
+    H->kc_ticket.release();
+    H->kc_sc.release();
     H->rounds.release();
     H->tcol.release();
     H->tval.release();
@@ -1038,11 +1140,13 @@ rsg_status amg_setup(rsg_context *ctx, rsg_csr *A)
     if (!H) {
         H = new AmgHierarchy;
         if (cudaMalloc(&H->flags, 16 * sizeof(unsigned int)) != cudaSuccess ||
-            cudaMallocHost(&H->flags_h, 16 * sizeof(unsigned int)) != cudaSuccess) {
+            cudaMallocHost(&H->flags_h, 16 * sizeof(unsigned int)) != cudaSuccess || !H->kc_part.ensure(3 * kMaxGrid) ||
+            !H->kc_ticket.ensure(1) || !H->kc_sc.ensure(8 * kAmgMaxLevels)) {
             amg_free(H);
             return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: counters");
         }
         A->amg = H;
+        RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->kc_ticket.p, 0, sizeof(unsigned int), ctx->stream));
     }
     H->mis_rounds = 0;
     H->levels = 1;
@@ -1054,7 +1158,7 @@ rsg_status amg_setup(rsg_context *ctx, rsg_csr *A)
     L0.ci = A->ci;
     L0.val = A->val;
     L0.val32 = A->val32;
-    RSG_TRY(level_vectors(ctx, L0));
+    RSG_TRY(level_vectors(ctx, L0, false));
     while (H->levels < kAmgMaxLevels) {
         AmgLevel &F = H->L[H->levels - 1];
         if (F.n <= kAmgCoarsest) {
@@ -1068,7 +1172,7 @@ rsg_status amg_setup(rsg_context *ctx, rsg_csr *A)
             break;
         AmgLevel &Cl = H->L[H->levels];
         RSG_TRY(build_galerkin(ctx, H, F, Cl, nc, emax, max_size));
-        RSG_TRY(level_vectors(ctx, Cl));
+        RSG_TRY(level_vectors(ctx, Cl, H->levels <= kAmgKLevels));
         H->levels++;
     }
     AmgLevel &last = H->L[H->levels - 1];
@@ -1104,10 +1208,10 @@ struct FineLaunch {
 };
 
 template <int RPW, int SRC, int OUT, bool FINAL>
-void fine_sweep(rsg_context *ctx, const FineLaunch<RPW> &f, const SweepArgs &a, double *partials,
+void fine_sweep(rsg_context *ctx, const FineLaunch<RPW> &f, const SweepArgs &a, const float *qv, double *partials,
                 unsigned int *ticket, CgState *st, int mode, double *rz_out, bool pdl)
 {
-    launch_k(ctx->stream, pdl, k_amg_fine<RPW, SRC, OUT, FINAL>, f.grid, kBlock, f.smem, f.M, f.S, f.use_sell, a,
+    launch_k(ctx->stream, pdl, k_amg_fine<RPW, SRC, OUT, FINAL>, f.grid, kBlock, f.smem, f.M, f.S, f.use_sell, a, qv,
              partials, ticket, st, mode, rz_out);
 }
 
@@ -1141,48 +1245,83 @@ void down_restrict(rsg_context *ctx, const AmgHierarchy *H, int l, const CgState
              (const uint32_t *)F.agg_rows.p, (const float *)F.r.p, (const float *)C.dw.p, C.b.p, C.x1.p, st);
 }
 
-void coarse_levels(rsg_context *ctx, const AmgHierarchy *H, int l, int sweeps, const CgState *st, bool pdl)
+bool k_level(const AmgHierarchy *H, int l) { return l >= 1 && l <= kAmgKLevels && l < H->levels - 1; }
+
+// Scale of the prolongated correction from level l: the K-cycle's flexible-CG steps already scale it.
+float corr_scale(const AmgHierarchy *H, int l, int sweeps)
+{
+    return k_level(H, l) ? 1.f : (sweeps == 2 ? kAmgScale2 : kAmgScale1);
+}
+
+void solve_level(rsg_context *ctx, const AmgHierarchy *H, int l, const float *b, float *e, int sweeps,
+                 const CgState *st, bool pdl);
+
+// One cycle on coarse level l: out ~ A_l^-1 b, with x0 = dw b already in x1.
+void cycle(rsg_context *ctx, const AmgHierarchy *H, int l, const float *b, float *out, int sweeps, const CgState *st,
+           bool pdl)
+{
+    const AmgLevel &F = H->L[l], &C = H->L[l + 1];
+    float *bb = const_cast<float *>(b);
+    if (sweeps == 2) {
+        SweepArgs a1{bb, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, F.x2.p};
+        coarse_sweep<kSrcX, kOutSmooth>(ctx, F, a1, st, pdl);
+        SweepArgs a2{bb, F.dw.p, F.x2.p, nullptr, nullptr, 0.f, F.r.p};
+        coarse_sweep<kSrcX, kOutRes>(ctx, F, a2, st, pdl);
+    } else {
+        SweepArgs a1{bb, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, F.r.p};
+        coarse_sweep<kSrcX, kOutRes>(ctx, F, a1, st, pdl);
+    }
+    down_restrict(ctx, H, l, st, pdl);
+    solve_level(ctx, H, l + 1, C.b.p, C.e.p, sweeps, st, pdl);
+    const float s = corr_scale(H, l + 1, sweeps);
+    if (sweeps == 2) {
+        SweepArgs u1{bb, F.dw.p, F.x2.p, C.e.p, F.agg.p, s, F.x1.p};
+        coarse_sweep<kSrcXCorr, kOutSmooth>(ctx, F, u1, st, pdl);
+        SweepArgs u2{bb, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, out};
+        coarse_sweep<kSrcX, kOutSmooth>(ctx, F, u2, st, pdl);
+    } else {
+        SweepArgs u1{bb, F.dw.p, F.x1.p, C.e.p, F.agg.p, s, out};
+        coarse_sweep<kSrcXCorr, kOutSmooth>(ctx, F, u1, st, pdl);
+    }
+}
+
+// e ~ A_l^-1 b on coarse level l (x0 = dw b already in x1): the dense inverse on the last level, two
+// flexible-CG steps preconditioned by the cycle on a K-cycle level, one cycle otherwise.
+void solve_level(rsg_context *ctx, const AmgHierarchy *H, int l, const float *b, float *e, int sweeps,
+                 const CgState *st, bool pdl)
 {
     const AmgLevel &F = H->L[l];
-    const bool last = (l == H->levels - 1);
-    if (last) {
+    if (l == H->levels - 1) {
         if (H->dense_coarsest) {
-            launch_k(ctx->stream, pdl, k_amg_dense_apply, 1, 256, 0, F.n, (const float *)H->coarse_inv.p,
-                     (const float *)F.b.p, F.e.p, st);
+            launch_k(ctx->stream, pdl, k_amg_dense_apply, 1, 256, 0, F.n, (const float *)H->coarse_inv.p, b, e, st);
         } else {  // coarsening stalled above the dense limit: nine damped-Jacobi sweeps from zero
-            float *src = F.x1.p, *dst = F.x2.p;
+            float *src = F.x1.p, *dst = F.x2.p, *bb = const_cast<float *>(b);
             for (int k = 0; k < 7; k++) {
-                SweepArgs a{F.b.p, F.dw.p, src, nullptr, nullptr, 0.f, dst};
+                SweepArgs a{bb, F.dw.p, src, nullptr, nullptr, 0.f, dst};
                 coarse_sweep<kSrcX, kOutSmooth>(ctx, F, a, st, pdl);
                 std::swap(src, dst);
             }
-            SweepArgs a{F.b.p, F.dw.p, src, nullptr, nullptr, 0.f, F.e.p};
+            SweepArgs a{bb, F.dw.p, src, nullptr, nullptr, 0.f, e};
             coarse_sweep<kSrcX, kOutSmooth>(ctx, F, a, st, pdl);
         }
         return;
     }
-    const AmgLevel &C = H->L[l + 1];
-    const float s = sweeps == 2 ? kAmgScale2 : kAmgScale1;
-    if (sweeps == 2) {
-        SweepArgs a1{F.b.p, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, F.x2.p};
-        coarse_sweep<kSrcX, kOutSmooth>(ctx, F, a1, st, pdl);
-        SweepArgs a2{F.b.p, F.dw.p, F.x2.p, nullptr, nullptr, 0.f, F.r.p};
-        coarse_sweep<kSrcX, kOutRes>(ctx, F, a2, st, pdl);
-    } else {
-        SweepArgs a1{F.b.p, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, F.r.p};
-        coarse_sweep<kSrcX, kOutRes>(ctx, F, a1, st, pdl);
+    if (!k_level(H, l)) {
+        cycle(ctx, H, l, b, e, sweeps, st, pdl);
+        return;
     }
-    down_restrict(ctx, H, l, st, pdl);
-    coarse_levels(ctx, H, l + 1, sweeps, st, pdl);
-    if (sweeps == 2) {
-        SweepArgs u1{F.b.p, F.dw.p, F.x2.p, C.e.p, F.agg.p, s, F.x1.p};
-        coarse_sweep<kSrcXCorr, kOutSmooth>(ctx, F, u1, st, pdl);
-        SweepArgs u2{F.b.p, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, F.e.p};
-        coarse_sweep<kSrcX, kOutSmooth>(ctx, F, u2, st, pdl);
-    } else {
-        SweepArgs u1{F.b.p, F.dw.p, F.x1.p, C.e.p, F.agg.p, s, F.e.p};
-        coarse_sweep<kSrcXCorr, kOutSmooth>(ctx, F, u1, st, pdl);
-    }
+    double *sc = H->kc_sc.p + 8 * l;
+    const int gs = coarse_grid(ctx, F.n), gv = grid_rows(F.n);
+    cycle(ctx, H, l, b, F.c1.p, sweeps, st, pdl);
+    launch_k(ctx->stream, pdl, k_amg_kc_spmv<2>, gs, kBlock, 0, F.n, F.rp, F.ci, F.val32, (const float *)F.c1.p,
+             F.v1.p, b, (const float *)nullptr, H->kc_part.p, H->kc_ticket.p, sc, 0, 1, 0, st);
+    launch_k(ctx->stream, pdl, k_amg_kc_r2, gv, kBlock, 0, F.n, b, (const float *)F.v1.p, (const double *)sc,
+             (const float *)F.dw.p, F.r2.p, F.x1.p, st);
+    cycle(ctx, H, l, F.r2.p, F.c2.p, sweeps, st, pdl);
+    launch_k(ctx->stream, pdl, k_amg_kc_spmv<3>, gs, kBlock, 0, F.n, F.rp, F.ci, F.val32, (const float *)F.c2.p,
+             F.v2.p, (const float *)F.v1.p, (const float *)F.r2.p, H->kc_part.p, H->kc_ticket.p, sc, 2, 3, 4, st);
+    launch_k(ctx->stream, pdl, k_amg_kc_combine, gv, kBlock, 0, F.n, (const float *)F.c1.p, (const float *)F.c2.p,
+             (const double *)sc, e, st);
 }
 
 template <int RPW>
@@ -1208,8 +1347,8 @@ FineLaunch<RPW> fine_launch(rsg_context *ctx, const rsg_csr *A)
 // x0 (= dw r) in the finest level's x1 buffer, computed by the caller or here.
 template <int RPW>
 rsg_status vcycle_typed(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H, const float *r, const float *x0,
-                        float *z, int sweeps, double *partials, unsigned int *ticket, CgState *st, int mode,
-                        double *rz_out, bool pdl)
+                        const float *q, float *z, int sweeps, double *partials, unsigned int *ticket, CgState *st,
+                        int mode, double *rz_out, bool pdl)
 {
     const AmgLevel &F = H->L[0];
     if (!x0) {
@@ -1225,38 +1364,39 @@ rsg_status vcycle_typed(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *
             launch_k(ctx->stream, pdl, k_amg_jacobi, grid_rows(F.n), kBlock, 0, F.n, (const float *)F.dw.p, r, z,
                      (const CgState *)st);
         const int g = std::min(grid_rows(F.n), kMaxGrid);
-        launch_k(ctx->stream, pdl, k_amg_rz, g, kBlock, 0, F.n, r, (const float *)z, partials, ticket, st, mode, rz_out);
+        launch_k(ctx->stream, pdl, k_amg_rz, g, kBlock, 0, F.n, r, (const float *)z, q, partials, ticket, st, mode,
+                 rz_out);
         return RSG_OK;
     }
     const FineLaunch<RPW> f = fine_launch<RPW>(ctx, A);
     const AmgLevel &C = H->L[1];
-    const float s = sweeps == 2 ? kAmgScale2 : kAmgScale1;
     float *x1 = F.x1.p, *x2 = F.x2.p;
     if (sweeps == 2) {
         SweepArgs a1{r, F.dw.p, x0, nullptr, nullptr, 0.f, x2};
-        fine_sweep<RPW, kSrcX, kOutSmooth, false>(ctx, f, a1, partials, ticket, st, mode, rz_out, pdl);
+        fine_sweep<RPW, kSrcX, kOutSmooth, false>(ctx, f, a1, nullptr, partials, ticket, st, mode, rz_out, pdl);
         SweepArgs a2{r, F.dw.p, x2, nullptr, nullptr, 0.f, F.r.p};
-        fine_sweep<RPW, kSrcX, kOutRes, false>(ctx, f, a2, partials, ticket, st, mode, rz_out, pdl);
+        fine_sweep<RPW, kSrcX, kOutRes, false>(ctx, f, a2, nullptr, partials, ticket, st, mode, rz_out, pdl);
     } else {
         SweepArgs a1{r, F.dw.p, x0, nullptr, nullptr, 0.f, F.r.p};
-        fine_sweep<RPW, kSrcX, kOutRes, false>(ctx, f, a1, partials, ticket, st, mode, rz_out, pdl);
+        fine_sweep<RPW, kSrcX, kOutRes, false>(ctx, f, a1, nullptr, partials, ticket, st, mode, rz_out, pdl);
     }
     down_restrict(ctx, H, 0, st, pdl);
-    coarse_levels(ctx, H, 1, sweeps, st, pdl);
+    solve_level(ctx, H, 1, C.b.p, C.e.p, sweeps, st, pdl);
+    const float s = corr_scale(H, 1, sweeps);
     // the coarse correction in its own streaming pass, so that the post-smoothing sweeps gather one vector
     const int gp = std::min(grid_rows(F.n), kMaxGrid);
     if (sweeps == 2) {
         launch_k(ctx->stream, pdl, k_amg_prolong, gp, kBlock, 0, F.n, (const float *)x2, (const uint32_t *)F.agg.p,
                  (const float *)C.e.p, s, x1, (const CgState *)st);
         SweepArgs u1{r, F.dw.p, x1, nullptr, nullptr, 0.f, x2};
-        fine_sweep<RPW, kSrcX, kOutSmooth, false>(ctx, f, u1, partials, ticket, st, mode, rz_out, pdl);
+        fine_sweep<RPW, kSrcX, kOutSmooth, false>(ctx, f, u1, nullptr, partials, ticket, st, mode, rz_out, pdl);
         SweepArgs u2{r, F.dw.p, x2, nullptr, nullptr, 0.f, z};
-        fine_sweep<RPW, kSrcX, kOutSmooth, true>(ctx, f, u2, partials, ticket, st, mode, rz_out, pdl);
+        fine_sweep<RPW, kSrcX, kOutSmooth, true>(ctx, f, u2, q, partials, ticket, st, mode, rz_out, pdl);
     } else {
         launch_k(ctx->stream, pdl, k_amg_prolong, gp, kBlock, 0, F.n, x0, (const uint32_t *)F.agg.p,
                  (const float *)C.e.p, s, x2, (const CgState *)st);
         SweepArgs u1{r, F.dw.p, x2, nullptr, nullptr, 0.f, z};
-        fine_sweep<RPW, kSrcX, kOutSmooth, true>(ctx, f, u1, partials, ticket, st, mode, rz_out, pdl);
+        fine_sweep<RPW, kSrcX, kOutSmooth, true>(ctx, f, u1, q, partials, ticket, st, mode, rz_out, pdl);
     }
     return RSG_OK;
 }
@@ -1270,7 +1410,7 @@ rsg_status profile_typed_sweep(rsg_context *ctx, const rsg_csr *A, const AmgHier
     const FineLaunch<RPW> f = fine_launch<RPW>(ctx, A);
     const AmgLevel &F = H->L[0];
     SweepArgs a{r, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, z};
-    fine_sweep<RPW, kSrcX, kOutSmooth, false>(ctx, f, a, nullptr, nullptr, nullptr, 0, nullptr, false);
+    fine_sweep<RPW, kSrcX, kOutSmooth, false>(ctx, f, a, nullptr, nullptr, nullptr, nullptr, 0, nullptr, false);
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
     return RSG_OK;
 }
@@ -1284,8 +1424,8 @@ rsg_status amg_profile_launch(rsg_context *ctx, const rsg_csr *A, const AmgHiera
 }
 
 rsg_status amg_vcycle(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H, const float *r, const float *x0,
-                      float *z, int sweeps, double *partials, unsigned int *ticket, CgState *st, int mode,
-                      double *rz_out, bool pdl)
+                      const float *q, float *z, int sweeps, double *partials, unsigned int *ticket, CgState *st,
+                      int mode, double *rz_out, bool pdl)
 {
     if (!H || H->levels < 1) return set_error(ctx, RSG_ERR_INVALID_ARG, "amg: no hierarchy");
     // The V-cycle is a chain of short kernels (the coarse levels' sweeps run a few microseconds), so
@@ -1294,7 +1434,8 @@ rsg_status amg_vcycle(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H,
     (void)pdl;
     pdl = true;
     RSG_RPW_DISPATCH(pick_rpw(A),
-                     return vcycle_typed<RPW>(ctx, A, H, r, x0, z, sweeps, partials, ticket, st, mode, rz_out, pdl));
+                     return vcycle_typed<RPW>(ctx, A, H, r, x0, q, z, sweeps, partials, ticket, st, mode, rz_out,
+                                              pdl));
     return RSG_ERR_UNSUPPORTED;
 }
 
@@ -1361,7 +1502,8 @@ rsg_status rsg_amg_apply(rsg_context *ctx, rsg_csr *A, const double *r, double *
     RSG_CHECK_CUDA(ctx, cudaMemsetAsync(scal, 0, 8 * sizeof(double), ctx->stream));
     const int g = std::min(grid_rows(n), kMaxGrid);
     k_amg_d2f<<<g, kBlock, 0, ctx->stream>>>(n, r, L0.b.p);
-    RSG_TRY(amg_vcycle(ctx, A, H, L0.b.p, nullptr, L0.e.p, int(sweeps), partials, ticket, nullptr, 0, scal, false));
+    RSG_TRY(amg_vcycle(ctx, A, H, L0.b.p, nullptr, nullptr, L0.e.p, int(sweeps), partials, ticket, nullptr, 0, scal,
+                       false));
     k_amg_f2d<<<g, kBlock, 0, ctx->stream>>>(n, L0.e.p, z);
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
     RSG_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

@@ -19,6 +19,7 @@ constexpr double kAmgTheta = 0.08;         // strength threshold |a_ij| >= theta
 constexpr float kAmgOmega = 2.0f / 3.0f;   // damped-Jacobi weight of the smoother
 constexpr float kAmgScale1 = 1.6f;         // coarse-correction scale, one smoothing sweep per side
 constexpr float kAmgScale2 = 1.8f;         // coarse-correction scale, two sweeps per side
+constexpr int kAmgKLevels = 2;             // levels 1..kAmgKLevels are solved by two flexible-CG steps (K-cycle)
 constexpr uint32_t kAmgUnset = 0xffffffffu;
 
 // Device buffer that only grows (reallocated when a larger size is asked for).
@@ -60,6 +61,7 @@ struct AmgLevel {
     DevBuf<uint32_t> agg;                  // row of this level -> row of the next level
     DevBuf<uint32_t> agg_ptr, agg_rows;    // next-level row -> rows of this level (ascending)
     DevBuf<float> b, r, x1, x2, e;         // V-cycle vectors; x1 starts as x0 = dw b (b and e unused on level 0)
+    DevBuf<float> c1, c2, v1, v2, r2;      // K-cycle levels: the two flexible-CG steps
     // SELL-32 copy of a coarse level for the sweeps (FP32 values, uint32 columns; see spmv.cuh)
     uint32_t n_slices = 0;
     uint32_t max_row = 0;
@@ -80,6 +82,9 @@ struct AmgHierarchy {
     DevBuf<unsigned int> rounds;    // undecided nodes after each independent-set round
     DevBuf<uint32_t> tcol;          // Galerkin staging: columns
     DevBuf<double> tval;            // Galerkin staging: values
+    DevBuf<double> kc_part;         // K-cycle: grid-reduction partials
+    DevBuf<unsigned int> kc_ticket; // K-cycle: grid-reduction counter (zero between uses)
+    DevBuf<double> kc_sc;           // K-cycle: 8 scalars per level (c1.v1, c1.b, c2.v2, c2.v1, c2.r2)
     unsigned int *flags = nullptr;  // device counters read back by the host (16 words)
     unsigned int *flags_h = nullptr;  // pinned host copy
     double seconds_setup = 0.0;
@@ -91,16 +96,18 @@ void amg_free(AmgHierarchy *H);
 rsg_status amg_setup(rsg_context *ctx, rsg_csr *A);
 AmgHierarchy *amg_of(const rsg_csr *A);
 
-// z = V(r) on the context stream (FP32; sweeps = 1 or 2 smoothing sweeps per side).  The final
-// kernel adds r^T z (compensated) over its grid and, when st is given, finalizes the CG state:
-// mode 0 starts the recurrence (rho = r^T z, beta = 0), mode 1 continues it (beta = rho_new / rho,
-// or the residual-replacement rule after a true-residual check).  Without st the sum goes to
-// *rz_out.  partials holds >= kMaxGrid doubles; ticket is a zeroed grid-reduction counter.
+// z = M(r), one cycle, on the context stream (FP32; sweeps = 1 or 2 smoothing sweeps per side;
+// levels 1..kAmgKLevels solved by two flexible-CG steps, so M varies with r).  The final kernel adds
+// r^T z and q^T z (compensated) over its grid and, when st is given, finalizes the CG state: mode 0
+// starts the recurrence (rho = r^T z, beta = 0), mode 1 continues it with the flexible update
+// beta = -alpha q^T z / rho (or the residual-replacement rule after a true-residual check).  Without st
+// r^T z goes to *rz_out.  partials holds >= 2 kMaxGrid doubles; ticket is a zeroed counter.
 // x0 = (omega / a_ii) r, the first smoothing step, computed by the caller's streaming pass (the CG
 // update / check kernels) in the finest level's x0 buffer (amg_finest_x0), or NULL to compute it here.
+// q (mode 1): the CG's q = A p of the last step, for the flexible direction update.
 rsg_status amg_vcycle(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *H, const float *r, const float *x0,
-                      float *z, int sweeps, double *partials, unsigned int *ticket, CgState *st, int mode,
-                      double *rz_out, bool pdl);
+                      const float *q, float *z, int sweeps, double *partials, unsigned int *ticket, CgState *st,
+                      int mode, double *rz_out, bool pdl);
 inline const float *amg_finest_weights(const AmgHierarchy *H) { return H->L[0].dw.p; }
 inline float *amg_finest_x0(const AmgHierarchy *H) { return H->L[0].x1.p; }
 

@@ -559,8 +559,8 @@ void launch_init(rsg_context *ctx, const CgArgs &a, const Launch &L)
         k_mx_prec<PK><<<L.g_vec, kBlock, 0, ctx->stream>>>(a.A->n, a.P.w, a.P.d32, a.r, a.r32,
                                                           PK == 3 ? a.amg_x0 : a.z32, a.partials, a.st, 0);
     if (PK == 3)  // z0 = V(r0), rho = r0^T z0
-        amg_vcycle(ctx, a.A, a.amg, a.r32, a.amg_x0, a.z32, a.amg_sweeps, a.partials, &a.st->ticket[5], a.st, 0,
-                   nullptr, false);
+        amg_vcycle(ctx, a.A, a.amg, a.r32, a.amg_x0, nullptr, a.z32, a.amg_sweeps, a.partials, &a.st->ticket[5],
+                   a.st, 0, nullptr, false);
 }
 
 template <int RPW, int PK>
@@ -600,8 +600,8 @@ void launch_body(rsg_context *ctx, const CgArgs &a, const Launch &L, cudaGraphCo
                 launch_k(st, pdl, k_mx_prec<PK>, L.g_vec, kBlock, 0, n, a.P.w, a.P.d32, (const double *)nullptr,
                          a.r32, a.z32, a.partials, a.st, 1);
             if (PK == 3)
-                amg_vcycle(ctx, a.A, a.amg, a.r32, a.amg_x0, a.z32, a.amg_sweeps, a.partials, &a.st->ticket[5],
-                           a.st, 1, nullptr, pdl);
+                amg_vcycle(ctx, a.A, a.amg, a.r32, a.amg_x0, a.q32, a.z32, a.amg_sweeps, a.partials,
+                           &a.st->ticket[5], a.st, 1, nullptr, pdl);
         }
     }
     launch_k(st, pdl, k_tail, 1, 32, 0, a.st, h, use_cond);

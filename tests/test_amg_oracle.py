@@ -3,8 +3,9 @@
 Checks the properties the GPU's hierarchy is then compared against bit for bit: every row belongs
 to exactly one aggregate and aggregates are numbered densely; roots are never strong neighbours
 of each other; the coarse matrix equals P^T A P (scipy) with P the aggregate indicator; the dense
-coarsest inverse inverts the last level; the V-cycle is a symmetric positive definite operator;
-and as a CG preconditioner it needs far fewer iterations than Jacobi.
+coarsest inverse inverts the last level; the cycle (a K-cycle: levels 1 and 2 solved by two
+flexible-CG steps) is positive, and as a flexible-CG preconditioner it needs far fewer iterations
+than Jacobi.
 """
 import numpy as np
 import pytest
@@ -42,16 +43,17 @@ def test_hierarchy_shape_and_galerkin(heat24):
     assert np.array_equal(F0.val, A.val)
 
 
-def test_v_cycle_is_spd_and_accelerates_cg(heat24):
+def test_cycle_is_positive_and_accelerates_flexible_cg(heat24):
+    """The cycle's K-cycle levels (two flexible-CG steps) make it a variable preconditioner: positive
+    (u^T M(u) > 0) but not a fixed symmetric matrix, so the outer iteration is flexible CG (the
+    Polak-Ribiere direction update, as the GPU's mixed-precision CG uses with this preconditioner)."""
     A, b, H = heat24
     rng = np.random.default_rng(0)
     u, v = rng.standard_normal(A.n), rng.standard_normal(A.n)
     for sweeps in (1, 2):
-        Mu, Mv = H.apply(u, sweeps), H.apply(v, sweeps)
-        assert abs(v @ Mu - u @ Mv) <= 1e-12 * np.linalg.norm(u) * np.linalg.norm(Mv)
-        assert u @ Mu > 0 and v @ Mv > 0
+        assert u @ H.apply(u, sweeps) > 0 and v @ H.apply(v, sweeps) > 0
     M = _sp(A)
-    for sweeps, bound in ((1, 60), (2, 45)):
+    for sweeps, bound in ((1, 40), (2, 30)):
         x = np.zeros(A.n)
         r = b.copy()
         z = H.apply(r, sweeps)
@@ -66,11 +68,11 @@ def test_v_cycle_is_spd_and_accelerates_cg(heat24):
             if np.linalg.norm(b - M @ x) / bn < 1e-10:
                 break
             z = H.apply(r, sweeps)
-            rz2 = r @ z
-            p = z + (rz2 / rz) * p
-            rz = rz2
+            beta = -al * (q @ z) / rz
+            rz = r @ z
+            p = z + beta * p
         _, sj = O.solve(A, b, prec=1, n_outer=20000, stop_rule="true", rtol=1e-10)
-        assert it <= bound and it * 5 < sj.iterations, (sweeps, it, sj.iterations)
+        assert it <= bound and it * 8 < sj.iterations, (sweeps, it, sj.iterations)
 
 
 def test_small_matrix_is_one_dense_level():
