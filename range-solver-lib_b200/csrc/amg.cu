@@ -749,8 +749,39 @@ __global__ void k_amg_prolong(uint32_t n, const float *__restrict__ xs, const ui
         out[i] = fmaf(s, ec[agg[i]], xs[i]);
 }
 
-// Sweep over a coarse level (CSR, LANES lanes per row).
+// Sweep over a coarse level (CSR, kLanes lanes per row).  Coarse levels are small and latency-bound:
+// each lane first loads up to kChunk column indexes and values of its row, then issues all the
+// gathers, then the multiply-adds, so that a row costs a few round trips instead of one per entry.
 constexpr int kLanes = 4;
+constexpr int kChunk = 8;  // entries per lane per round: rows of up to kLanes * kChunk entries in one round
+
+template <class GX>
+__device__ __forceinline__ float csr_row_dot(const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ci,
+                                             const float *__restrict__ val, uint32_t row, bool valid, int lane,
+                                             GX &gx)
+{
+    float acc = 0.f;
+    const uint32_t beg = valid ? rp[row] : 0u, end = valid ? rp[row + 1] : 0u;
+    for (uint32_t j0 = beg; j0 < end; j0 += kLanes * kChunk) {
+        uint32_t c[kChunk];
+        float v[kChunk], x[kChunk];
+#pragma unroll
+        for (int t = 0; t < kChunk; t++) {
+            const uint32_t j = j0 + uint32_t(lane) + uint32_t(kLanes * t);
+            const bool ok = j < end;
+            c[t] = ok ? ci[j] : row;
+            v[t] = ok ? val[j] : 0.f;
+        }
+#pragma unroll
+        for (int t = 0; t < kChunk; t++) x[t] = v[t] != 0.f ? gx(c[t]) : 0.f;
+#pragma unroll
+        for (int t = 0; t < kChunk; t++) acc = fmaf(v[t], x[t], acc);
+    }
+#pragma unroll
+    for (int o = kLanes / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    return acc;
+}
+
 template <int SRC, int OUT>
 __global__ void __launch_bounds__(kBlock) k_amg_coarse(uint32_t n, const uint32_t *__restrict__ rp,
                                                        const uint32_t *__restrict__ ci, const float *__restrict__ val,
@@ -762,15 +793,13 @@ __global__ void __launch_bounds__(kBlock) k_amg_coarse(uint32_t n, const uint32_
     const int lane = threadIdx.x & (kLanes - 1);
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // warp index
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t sub = (threadIdx.x & 31) / kLanes;                   // row within the warp's group of 4
+    const uint32_t sub = (threadIdx.x & 31) / kLanes;                   // row within the warp's group
+    auto gx = [&](uint32_t c) { return sweep_x<SRC>(a, c); };
     for (uint32_t base = gw * (32 / kLanes); base < n; base += warps * (32 / kLanes)) {
         const uint32_t row = base + sub;
-        float acc = 0.f;
-        if (row < n)
-            for (uint32_t j = rp[row] + lane; j < rp[row + 1]; j += kLanes) acc = fmaf(val[j], sweep_x<SRC>(a, ci[j]), acc);
-#pragma unroll
-        for (int o = kLanes / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0 && row < n) {
+        const bool valid = row < n;
+        const float acc = csr_row_dot(rp, ci, val, row, valid, lane, gx);
+        if (lane == 0 && valid) {
             const float res = a.b[row] - acc;
             a.out[row] = OUT == kOutRes ? res : fmaf(a.dw[row], res, sweep_x<SRC>(a, row));
         }
@@ -796,13 +825,10 @@ __global__ void __launch_bounds__(kBlock) k_amg_kc_spmv(uint32_t n, const uint32
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t sub = (threadIdx.x & 31) / kLanes;
     Dot2 d0, d1, d2;
+    auto gx = [&](uint32_t col) { return c[col]; };
     for (uint32_t base = gw * (32 / kLanes); base < n; base += warps * (32 / kLanes)) {
         const uint32_t row = base + sub;
-        float acc = 0.f;
-        if (row < n)
-            for (uint32_t j = rp[row] + lane; j < rp[row + 1]; j += kLanes) acc = fmaf(val[j], c[ci[j]], acc);
-#pragma unroll
-        for (int o = kLanes / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        const float acc = csr_row_dot(rp, ci, val, row, row < n, lane, gx);
         if (lane == 0 && row < n) {
             v[row] = acc;
             const float ci_ = c[row];
@@ -867,7 +893,18 @@ __global__ void k_amg_restrict(uint32_t nc, const uint32_t *__restrict__ ptr, co
     if (st && st->done) return;
     for (uint32_t I = blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += gridDim.x * blockDim.x) {
         float s = 0.f;
-        for (uint32_t k = ptr[I]; k < ptr[I + 1]; k++) s += r[rows[k]];
+        const uint32_t beg = ptr[I], end = ptr[I + 1];
+        for (uint32_t k0 = beg; k0 < end; k0 += 8) {  // indexes first, then the gathers (in order)
+            uint32_t ix[8];
+            float v[8];
+#pragma unroll
+            for (int t = 0; t < 8; t++) ix[t] = k0 + t < end ? rows[k0 + t] : 0u;
+#pragma unroll
+            for (int t = 0; t < 8; t++) v[t] = k0 + t < end ? r[ix[t]] : 0.f;
+#pragma unroll
+            for (int t = 0; t < 8; t++)
+                if (k0 + t < end) s += v[t];
+        }
         bc[I] = s;
         x0c[I] = dwc[I] * s;
     }
