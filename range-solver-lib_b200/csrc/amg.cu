@@ -650,18 +650,45 @@ enum { kSrcDwB = 0, kSrcX = 1, kSrcDwBCorr = 2, kSrcXCorr = 3 };
 // Output: kOutRes writes r = b - A x, kOutSmooth writes x + dw (b - A x).
 enum { kOutRes = 0, kOutSmooth = 1 };
 
+//   kSrcXCorrK:  x = xs + P (g1 c1 + a2 c2) -- the correction from a K-cycle level, whose two
+//                flexible-CG directions are combined here with the coefficients of its device scalars
+enum { kSrcXCorrK = 4 };
+
 struct SweepArgs {
     const float *b, *dw, *xs, *ec;
     const uint32_t *agg;
     float s;
     float *out;
+    const float *ec2 = nullptr;   // kSrcXCorrK: the second direction (ec holds the first)
+    const double *kc = nullptr;   // kSrcXCorrK: the K-cycle level's scalars
+    float s2 = 0.f;
 };
+
+// Coefficients of the two-step flexible-CG approximation e = g1 c1 + a2 c2 from the scalars
+// sc = {c1.v1, c1.b, c2.v2, c2.v1, c2.r2} (v = A c): a1 = c1.b / c1.v1, b2 = c2.v2 - (c2.v1)^2 / c1.v1,
+// a2 = c2.r2 / b2, g1 = a1 - (c2.v1) a2 / c1.v1.
+__device__ __forceinline__ void kc_coefficients(const double *sc, float &g1, float &a2)
+{
+    const double d1 = sc[0], t1 = sc[1], d2 = sc[2], g = sc[3], t2 = sc[4];
+    double c1 = 0.0, c2 = 0.0;
+    if (d1 > 0.0) {
+        const double b2 = d2 - g * g / d1;
+        c2 = b2 > 0.0 ? t2 / b2 : 0.0;
+        c1 = t1 / d1 - g * c2 / d1;
+    }
+    g1 = float(c1);
+    a2 = float(c2);
+}
 
 template <int SRC>
 __device__ __forceinline__ float sweep_x(const SweepArgs &a, uint32_t c)
 {
     float x = (SRC == kSrcDwB || SRC == kSrcDwBCorr) ? a.dw[c] * a.b[c] : a.xs[c];
     if (SRC == kSrcDwBCorr || SRC == kSrcXCorr) x = fmaf(a.s, a.ec[a.agg[c]], x);
+    if (SRC == kSrcXCorrK) {
+        const uint32_t g = a.agg[c];
+        x = fmaf(a.s, a.ec[g], fmaf(a.s2, a.ec2[g], x));
+    }
     return x;
 }
 
@@ -730,6 +757,7 @@ __global__ void __launch_bounds__(kBlock) k_amg_coarse_sell(Sell<float> S, Sweep
     pdl_wait();
     pdl_release();
     if (st && st->done) return;
+    if (SRC == kSrcXCorrK) kc_coefficients(a.kc, a.s, a.s2);
     auto gx = [&](uint32_t c) { return sweep_x<SRC>(a, c); };
     auto epi = [&](uint32_t row, float ax) {
         const float res = a.b[row] - ax;
@@ -738,15 +766,21 @@ __global__ void __launch_bounds__(kBlock) k_amg_coarse_sell(Sell<float> S, Sweep
     for_rows_sell<float>(S, gx, epi);
 }
 
-// x_out = xs + s P e_c (the prolongated, scaled coarse correction), one streaming pass.
+// x_out = xs + s P e_c (the prolongated, scaled coarse correction), one streaming pass; with kc given
+// (a K-cycle coarse level) x_out = xs + P (g1 c1 + a2 c2), ec = c1, ec2 = c2.
 __global__ void k_amg_prolong(uint32_t n, const float *__restrict__ xs, const uint32_t *__restrict__ agg,
-                              const float *__restrict__ ec, float s, float *__restrict__ out, const CgState *st)
+                              const float *__restrict__ ec, const float *__restrict__ ec2, const double *kc, float s,
+                              float *__restrict__ out, const CgState *st)
 {
     pdl_wait();
     pdl_release();
     if (st && st->done) return;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        out[i] = fmaf(s, ec[agg[i]], xs[i]);
+    float g1 = s, a2 = 0.f;
+    if (kc) kc_coefficients(kc, g1, a2);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t g = agg[i];
+        out[i] = kc ? fmaf(g1, ec[g], fmaf(a2, ec2[g], xs[i])) : fmaf(g1, ec[g], xs[i]);
+    }
 }
 
 // Sweep over a coarse level (CSR, kLanes lanes per row).  Coarse levels are small and latency-bound:
@@ -782,18 +816,14 @@ __device__ __forceinline__ float csr_row_dot(const uint32_t *__restrict__ rp, co
     return acc;
 }
 
+// The rows of one sweep, warp gw of warps (kLanes lanes per row).
 template <int SRC, int OUT>
-__global__ void __launch_bounds__(kBlock) k_amg_coarse(uint32_t n, const uint32_t *__restrict__ rp,
-                                                       const uint32_t *__restrict__ ci, const float *__restrict__ val,
-                                                       SweepArgs a, const CgState *st)
+__device__ __forceinline__ void coarse_rows(uint32_t n, const uint32_t *__restrict__ rp,
+                                            const uint32_t *__restrict__ ci, const float *__restrict__ val,
+                                            const SweepArgs &a, uint32_t gw, uint32_t warps)
 {
-    pdl_wait();
-    pdl_release();
-    if (st && st->done) return;
     const int lane = threadIdx.x & (kLanes - 1);
-    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // warp index
-    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t sub = (threadIdx.x & 31) / kLanes;                   // row within the warp's group
+    const uint32_t sub = (threadIdx.x & 31) / kLanes;  // row within the warp's group
     auto gx = [&](uint32_t c) { return sweep_x<SRC>(a, c); };
     for (uint32_t base = gw * (32 / kLanes); base < n; base += warps * (32 / kLanes)) {
         const uint32_t row = base + sub;
@@ -803,6 +833,142 @@ __global__ void __launch_bounds__(kBlock) k_amg_coarse(uint32_t n, const uint32_
             const float res = a.b[row] - acc;
             a.out[row] = OUT == kOutRes ? res : fmaf(a.dw[row], res, sweep_x<SRC>(a, row));
         }
+    }
+}
+
+template <int SRC, int OUT>
+__global__ void __launch_bounds__(kBlock) k_amg_coarse(uint32_t n, const uint32_t *__restrict__ rp,
+                                                       const uint32_t *__restrict__ ci, const float *__restrict__ val,
+                                                       SweepArgs a, const CgState *st)
+{
+    pdl_wait();
+    pdl_release();
+    if (st && st->done) return;
+    if (SRC == kSrcXCorrK) kc_coefficients(a.kc, a.s, a.s2);
+    coarse_rows<SRC, OUT>(n, rp, ci, val, a, (blockIdx.x * blockDim.x + threadIdx.x) >> 5,
+                          (gridDim.x * blockDim.x) >> 5);
+}
+
+// Residual and restriction in one pass over a coarse level: b_c[I] = sum over the aggregate's rows i
+// of (b_i - (A xs)_i), and x0_c[I] = dw_c[I] b_c[I].  One warp per aggregate: eight row slots of four
+// lanes, a slot taking every eighth row of the aggregate and its four lanes every fourth entry of the
+// row (indexes and values loaded a chunk ahead of the gathers); a fixed shuffle tree adds the lanes.
+// The aggregates of one restriction, warp gw of warps; the restricted residual of aggregate I goes
+// to bc[I] (and x0c[I] = dwc[I] bc[I] when x0c is given).
+__device__ __forceinline__ void res_restrict_rows(uint32_t nc, const uint32_t *__restrict__ ptr,
+                                                  const uint32_t *__restrict__ rows, const uint32_t *__restrict__ rp,
+                                                  const uint32_t *__restrict__ ci, const float *__restrict__ val,
+                                                  const float *__restrict__ b, const float *__restrict__ xs,
+                                                  const float *__restrict__ dwc, float *bc, float *x0c, uint32_t gw,
+                                                  uint32_t warps)
+{
+    const int lane = threadIdx.x & 31, slot = lane >> 2, q = lane & 3;
+    for (uint32_t I = gw; I < nc; I += warps) {
+        float part = 0.f;
+        const uint32_t k1 = ptr[I + 1];
+        for (uint32_t k = ptr[I] + slot; k < k1; k += 8) {
+            const uint32_t row = rows[k];
+            const uint32_t end = rp[row + 1];
+            float acc = 0.f;
+            for (uint32_t j0 = rp[row] + q; j0 < end; j0 += 4 * kChunk) {
+                uint32_t c[kChunk];
+                float v[kChunk], x[kChunk];
+#pragma unroll
+                for (int t = 0; t < kChunk; t++) {
+                    const bool ok = j0 + 4 * t < end;
+                    c[t] = ok ? ci[j0 + 4 * t] : row;
+                    v[t] = ok ? val[j0 + 4 * t] : 0.f;
+                }
+#pragma unroll
+                for (int t = 0; t < kChunk; t++) x[t] = v[t] != 0.f ? xs[c[t]] : 0.f;
+#pragma unroll
+                for (int t = 0; t < kChunk; t++) acc = fmaf(v[t], x[t], acc);
+            }
+            part += (q == 0 ? b[row] : 0.f) - acc;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+        if (lane == 0) {
+            bc[I] = part;
+            if (x0c) x0c[I] = dwc[I] * part;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_amg_res_restrict(uint32_t nc, const uint32_t *__restrict__ ptr,
+                                                             const uint32_t *__restrict__ rows,
+                                                             const uint32_t *__restrict__ rp,
+                                                             const uint32_t *__restrict__ ci,
+                                                             const float *__restrict__ val,
+                                                             const float *__restrict__ b,
+                                                             const float *__restrict__ xs,
+                                                             const float *__restrict__ dwc, float *__restrict__ bc,
+                                                             float *__restrict__ x0c, const CgState *st)
+{
+    pdl_wait();
+    pdl_release();
+    if (st && st->done) return;
+    res_restrict_rows(nc, ptr, rows, rp, ci, val, b, xs, dwc, bc, x0c, (blockIdx.x * blockDim.x + threadIdx.x) >> 5,
+                      (gridDim.x * blockDim.x) >> 5);
+}
+
+// The bottom of the hierarchy in one CTA: the cycle on the last smoothed level l (at most
+// kBottomRows rows), whose next level is inverted densely -- pre-smoothing (two sweeps), residual and
+// restriction into shared memory, the dense coarse solve, the corrected post-smoothing.  Same
+// arithmetic as the separate kernels; __syncthreads orders the phases.
+constexpr uint32_t kBottomRows = 1024;
+constexpr int kBottomThreads = 1024;
+struct BottomArgs {
+    uint32_t n, nc;
+    const uint32_t *rp, *ci, *agg, *ptr, *rows;
+    const float *val, *dw, *inv;
+    const float *b;
+    float *x1, *x2, *out;
+    float s;
+};
+template <int SWEEPS>
+__global__ void __launch_bounds__(kBottomThreads) k_amg_bottom(BottomArgs B, const CgState *st)
+{
+    pdl_wait();
+    pdl_release();
+    if (st && st->done) return;
+    __shared__ float sb[kAmgCoarsest], se[kAmgCoarsest];
+    const uint32_t w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    float *b = const_cast<float *>(B.b);
+    const float *xs = B.x1;
+    if (SWEEPS == 2) {
+        SweepArgs a{b, B.dw, B.x1, nullptr, nullptr, 0.f, B.x2};
+        coarse_rows<kSrcX, kOutSmooth>(B.n, B.rp, B.ci, B.val, a, w, nw);
+        __syncthreads();
+        xs = B.x2;
+    }
+    res_restrict_rows(B.nc, B.ptr, B.rows, B.rp, B.ci, B.val, B.b, xs, nullptr, sb, nullptr, w, nw);
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    for (uint32_t i = w; i < B.nc; i += nw) {
+        float v[kAmgCoarsest / 32];
+#pragma unroll
+        for (int t = 0; t < int(kAmgCoarsest / 32); t++) {
+            const uint32_t j = uint32_t(lane) + 32u * uint32_t(t);
+            v[t] = j < B.nc ? B.inv[size_t(i) * B.nc + j] : 0.f;
+        }
+        float acc = 0.f;
+#pragma unroll
+        for (int t = 0; t < int(kAmgCoarsest / 32); t++) {
+            const uint32_t j = uint32_t(lane) + 32u * uint32_t(t);
+            if (j < B.nc) acc = fmaf(v[t], sb[j], acc);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) se[i] = acc;
+    }
+    __syncthreads();
+    SweepArgs u{b, B.dw, const_cast<float *>(xs), se, B.agg, B.s, SWEEPS == 2 ? B.x1 : B.out};
+    coarse_rows<kSrcXCorr, kOutSmooth>(B.n, B.rp, B.ci, B.val, u, w, nw);
+    if (SWEEPS == 2) {
+        __syncthreads();
+        SweepArgs u2{b, B.dw, B.x1, nullptr, nullptr, 0.f, B.out};
+        coarse_rows<kSrcX, kOutSmooth>(B.n, B.rp, B.ci, B.val, u2, w, nw);
     }
 }
 
@@ -863,25 +1029,6 @@ __global__ void k_amg_kc_r2(uint32_t n, const float *__restrict__ b, const float
     }
 }
 
-// e = (alpha1 - g alpha2 / d1) c1 + alpha2 c2: the two-step flexible-CG approximation of A^-1 b.
-__global__ void k_amg_kc_combine(uint32_t n, const float *__restrict__ c1, const float *__restrict__ c2,
-                                 const double *__restrict__ sc, float *__restrict__ e, const CgState *st)
-{
-    pdl_wait();
-    pdl_release();
-    if (st && st->done) return;
-    const double d1 = sc[0], t1 = sc[1], d2 = sc[2], g = sc[3], t2 = sc[4];
-    double g1 = 0.0, a2 = 0.0;
-    if (d1 > 0.0) {
-        const double b2 = d2 - g * g / d1;
-        a2 = b2 > 0.0 ? t2 / b2 : 0.0;
-        g1 = t1 / d1 - g * a2 / d1;
-    }
-    const float fg1 = float(g1), fa2 = float(a2);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        e[i] = fmaf(fg1, c1[i], fa2 * c2[i]);
-}
-
 // b_c[I] = sum of r over the aggregate's rows (ascending order), and the coarse level's first
 // smoothing step x0_c = dw_c b_c.
 __global__ void k_amg_restrict(uint32_t nc, const uint32_t *__restrict__ ptr, const uint32_t *__restrict__ rows,
@@ -922,8 +1069,18 @@ __global__ void k_amg_dense_apply(uint32_t n, const float *__restrict__ inv, con
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (uint32_t i = warp; i < n; i += nw) {
+        float v[kAmgCoarsest / 32];
+#pragma unroll
+        for (int t = 0; t < int(kAmgCoarsest / 32); t++) {
+            const uint32_t j = uint32_t(lane) + 32u * uint32_t(t);
+            v[t] = j < n ? inv[size_t(i) * n + j] : 0.f;
+        }
         float s = 0.f;
-        for (uint32_t j = lane; j < n; j += 32) s = fmaf(inv[size_t(i) * n + j], sb[j], s);
+#pragma unroll
+        for (int t = 0; t < int(kAmgCoarsest / 32); t++) {
+            const uint32_t j = uint32_t(lane) + 32u * uint32_t(t);
+            if (j < n) s = fmaf(v[t], sb[j], s);
+        }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (lane == 0) e[i] = s;
@@ -1272,9 +1429,7 @@ void coarse_sweep(rsg_context *ctx, const AmgLevel &l, const SweepArgs &a, const
     }
 }
 
-// Level l >= 1 (b and x0 = dw b given by the restriction): pre-smoothing, residual, restriction,
-// the coarser levels, prolongation and post-smoothing into e.  The finest level is done by the caller
-// (fine kernels).  Buffers: x1 holds x0 on entry; with two sweeps x2 holds the pre-smoothed iterate.
+// Restriction of the finest level's residual (written by the fine sweep into r) to level 1's b and x0.
 void down_restrict(rsg_context *ctx, const AmgHierarchy *H, int l, const CgState *st, bool pdl)
 {
     const AmgLevel &F = H->L[l], &C = H->L[l + 1];
@@ -1293,44 +1448,88 @@ float corr_scale(const AmgHierarchy *H, int l, int sweeps)
 void solve_level(rsg_context *ctx, const AmgHierarchy *H, int l, const float *b, float *e, int sweeps,
                  const CgState *st, bool pdl);
 
-// One cycle on coarse level l: out ~ A_l^-1 b, with x0 = dw b already in x1.
+// The prolongated correction from coarse level c into SweepArgs: a K-cycle level's two flexible-CG
+// directions with their coefficients, else the level's e scaled by s.
+void set_correction(const AmgHierarchy *H, int c, int sweeps, SweepArgs &a)
+{
+    const AmgLevel &C = H->L[c];
+    if (k_level(H, c)) {
+        a.ec = C.c1.p;
+        a.ec2 = C.c2.p;
+        a.kc = H->kc_sc.p + 8 * c;
+    } else {
+        a.ec = C.e.p;
+        a.s = sweeps == 2 ? kAmgScale2 : kAmgScale1;
+    }
+}
+
+template <int OUT>
+void coarse_sweep_corr(rsg_context *ctx, const AmgHierarchy *H, int l, SweepArgs a, int sweeps, const CgState *st,
+                       bool pdl)
+{
+    const AmgLevel &F = H->L[l];
+    a.agg = F.agg.p;
+    set_correction(H, l + 1, sweeps, a);
+    if (k_level(H, l + 1)) coarse_sweep<kSrcXCorrK, OUT>(ctx, F, a, st, pdl);
+    else coarse_sweep<kSrcXCorr, OUT>(ctx, F, a, st, pdl);
+}
+
+// Residual of level l from iterate xs, restricted to the next level's b and x0 (one pass).
+void res_restrict(rsg_context *ctx, const AmgHierarchy *H, int l, const float *b, const float *xs, const CgState *st,
+                  bool pdl)
+{
+    const AmgLevel &F = H->L[l], &C = H->L[l + 1];
+    const int g = std::max(1, std::min<int>(int((uint64_t(C.n) * 32 + kBlock - 1) / kBlock), ctx->num_sms * 8));
+    launch_k(ctx->stream, pdl, k_amg_res_restrict, g, kBlock, 0, C.n, (const uint32_t *)F.agg_ptr.p,
+             (const uint32_t *)F.agg_rows.p, F.rp, F.ci, F.val32, b, xs, (const float *)C.dw.p, C.b.p, C.x1.p, st);
+}
+
+// One cycle on coarse level l >= 1: out ~ A_l^-1 b, with x0 = dw b already in x1 (written by the
+// restriction): pre-smoothing, residual and restriction in one pass, the coarser levels, the
+// prolongated correction fused into the first post-smoothing sweep.  With two sweeps x2 holds the
+// pre-smoothed iterate.
 void cycle(rsg_context *ctx, const AmgHierarchy *H, int l, const float *b, float *out, int sweeps, const CgState *st,
            bool pdl)
 {
     const AmgLevel &F = H->L[l], &C = H->L[l + 1];
     float *bb = const_cast<float *>(b);
+    if (l + 1 == H->levels - 1 && H->dense_coarsest && F.n <= kBottomRows) {
+        const BottomArgs B{F.n, C.n, F.rp, F.ci, F.agg.p, F.agg_ptr.p, F.agg_rows.p, F.val32, F.dw.p, H->coarse_inv.p,
+                           b, F.x1.p, F.x2.p, out, sweeps == 2 ? kAmgScale2 : kAmgScale1};
+        if (sweeps == 2) launch_k(ctx->stream, pdl, k_amg_bottom<2>, 1, kBottomThreads, 0, B, st);
+        else launch_k(ctx->stream, pdl, k_amg_bottom<1>, 1, kBottomThreads, 0, B, st);
+        return;
+    }
     if (sweeps == 2) {
         SweepArgs a1{bb, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, F.x2.p};
         coarse_sweep<kSrcX, kOutSmooth>(ctx, F, a1, st, pdl);
-        SweepArgs a2{bb, F.dw.p, F.x2.p, nullptr, nullptr, 0.f, F.r.p};
-        coarse_sweep<kSrcX, kOutRes>(ctx, F, a2, st, pdl);
+        res_restrict(ctx, H, l, b, F.x2.p, st, pdl);
     } else {
-        SweepArgs a1{bb, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, F.r.p};
-        coarse_sweep<kSrcX, kOutRes>(ctx, F, a1, st, pdl);
+        res_restrict(ctx, H, l, b, F.x1.p, st, pdl);
     }
-    down_restrict(ctx, H, l, st, pdl);
     solve_level(ctx, H, l + 1, C.b.p, C.e.p, sweeps, st, pdl);
-    const float s = corr_scale(H, l + 1, sweeps);
     if (sweeps == 2) {
-        SweepArgs u1{bb, F.dw.p, F.x2.p, C.e.p, F.agg.p, s, F.x1.p};
-        coarse_sweep<kSrcXCorr, kOutSmooth>(ctx, F, u1, st, pdl);
+        SweepArgs u1{bb, F.dw.p, F.x2.p, nullptr, nullptr, 0.f, F.x1.p};
+        coarse_sweep_corr<kOutSmooth>(ctx, H, l, u1, sweeps, st, pdl);
         SweepArgs u2{bb, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, out};
         coarse_sweep<kSrcX, kOutSmooth>(ctx, F, u2, st, pdl);
     } else {
-        SweepArgs u1{bb, F.dw.p, F.x1.p, C.e.p, F.agg.p, s, out};
-        coarse_sweep<kSrcXCorr, kOutSmooth>(ctx, F, u1, st, pdl);
+        SweepArgs u1{bb, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, out};
+        coarse_sweep_corr<kOutSmooth>(ctx, H, l, u1, sweeps, st, pdl);
     }
 }
 
-// e ~ A_l^-1 b on coarse level l (x0 = dw b already in x1): the dense inverse on the last level, two
-// flexible-CG steps preconditioned by the cycle on a K-cycle level, one cycle otherwise.
+// e ~ A_l^-1 b on coarse level l (x0 = dw b already in x1): the dense inverse on the last level, one
+// cycle on an ordinary level.  On a K-cycle level two flexible-CG steps preconditioned by the cycle
+// leave their directions in c1, c2 and the scalars in the level's kc_sc slots; the caller's
+// prolongation combines them (e is not written).
 void solve_level(rsg_context *ctx, const AmgHierarchy *H, int l, const float *b, float *e, int sweeps,
                  const CgState *st, bool pdl)
 {
     const AmgLevel &F = H->L[l];
     if (l == H->levels - 1) {
         if (H->dense_coarsest) {
-            launch_k(ctx->stream, pdl, k_amg_dense_apply, 1, 256, 0, F.n, (const float *)H->coarse_inv.p, b, e, st);
+            launch_k(ctx->stream, pdl, k_amg_dense_apply, 1, 1024, 0, F.n, (const float *)H->coarse_inv.p, b, e, st);
         } else {  // coarsening stalled above the dense limit: nine damped-Jacobi sweeps from zero
             float *src = F.x1.p, *dst = F.x2.p, *bb = const_cast<float *>(b);
             for (int k = 0; k < 7; k++) {
@@ -1357,8 +1556,6 @@ void solve_level(rsg_context *ctx, const AmgHierarchy *H, int l, const float *b,
     cycle(ctx, H, l, F.r2.p, F.c2.p, sweeps, st, pdl);
     launch_k(ctx->stream, pdl, k_amg_kc_spmv<3>, gs, kBlock, 0, F.n, F.rp, F.ci, F.val32, (const float *)F.c2.p,
              F.v2.p, (const float *)F.v1.p, (const float *)F.r2.p, H->kc_part.p, H->kc_ticket.p, sc, 2, 3, 4, st);
-    launch_k(ctx->stream, pdl, k_amg_kc_combine, gv, kBlock, 0, F.n, (const float *)F.c1.p, (const float *)F.c2.p,
-             (const double *)sc, e, st);
 }
 
 template <int RPW>
@@ -1395,7 +1592,7 @@ rsg_status vcycle_typed(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *
     }
     if (H->levels < 2) {
         if (H->dense_coarsest)
-            launch_k(ctx->stream, pdl, k_amg_dense_apply, 1, 256, 0, F.n, (const float *)H->coarse_inv.p, r, z,
+            launch_k(ctx->stream, pdl, k_amg_dense_apply, 1, 1024, 0, F.n, (const float *)H->coarse_inv.p, r, z,
                      (const CgState *)st);
         else
             launch_k(ctx->stream, pdl, k_amg_jacobi, grid_rows(F.n), kBlock, 0, F.n, (const float *)F.dw.p, r, z,
@@ -1419,19 +1616,22 @@ rsg_status vcycle_typed(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *
     }
     down_restrict(ctx, H, 0, st, pdl);
     solve_level(ctx, H, 1, C.b.p, C.e.p, sweeps, st, pdl);
+    const bool kc1 = k_level(H, 1);
     const float s = corr_scale(H, 1, sweeps);
+    const float *ec = kc1 ? C.c1.p : C.e.p, *ec2 = kc1 ? C.c2.p : nullptr;
+    const double *kc = kc1 ? H->kc_sc.p + 8 : nullptr;
     // the coarse correction in its own streaming pass, so that the post-smoothing sweeps gather one vector
     const int gp = std::min(grid_rows(F.n), kMaxGrid);
     if (sweeps == 2) {
-        launch_k(ctx->stream, pdl, k_amg_prolong, gp, kBlock, 0, F.n, (const float *)x2, (const uint32_t *)F.agg.p,
-                 (const float *)C.e.p, s, x1, (const CgState *)st);
+        launch_k(ctx->stream, pdl, k_amg_prolong, gp, kBlock, 0, F.n, (const float *)x2, (const uint32_t *)F.agg.p, ec,
+                 ec2, kc, s, x1, (const CgState *)st);
         SweepArgs u1{r, F.dw.p, x1, nullptr, nullptr, 0.f, x2};
         fine_sweep<RPW, kSrcX, kOutSmooth, false>(ctx, f, u1, nullptr, partials, ticket, st, mode, rz_out, pdl);
         SweepArgs u2{r, F.dw.p, x2, nullptr, nullptr, 0.f, z};
         fine_sweep<RPW, kSrcX, kOutSmooth, true>(ctx, f, u2, q, partials, ticket, st, mode, rz_out, pdl);
     } else {
-        launch_k(ctx->stream, pdl, k_amg_prolong, gp, kBlock, 0, F.n, x0, (const uint32_t *)F.agg.p,
-                 (const float *)C.e.p, s, x2, (const CgState *)st);
+        launch_k(ctx->stream, pdl, k_amg_prolong, gp, kBlock, 0, F.n, x0, (const uint32_t *)F.agg.p, ec, ec2, kc, s,
+                 x2, (const CgState *)st);
         SweepArgs u1{r, F.dw.p, x2, nullptr, nullptr, 0.f, z};
         fine_sweep<RPW, kSrcX, kOutSmooth, true>(ctx, f, u1, q, partials, ticket, st, mode, rz_out, pdl);
     }

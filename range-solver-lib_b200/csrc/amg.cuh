@@ -19,7 +19,10 @@ constexpr double kAmgTheta = 0.08;         // strength threshold |a_ij| >= theta
 constexpr float kAmgOmega = 2.0f / 3.0f;   // damped-Jacobi weight of the smoother
 constexpr float kAmgScale1 = 1.6f;         // coarse-correction scale, one smoothing sweep per side
 constexpr float kAmgScale2 = 1.8f;         // coarse-correction scale, two sweeps per side
-constexpr int kAmgKLevels = 2;             // levels 1..kAmgKLevels are solved by two flexible-CG steps (K-cycle)
+#ifndef RSG_AMG_KLEVELS
+#define RSG_AMG_KLEVELS 2
+#endif
+constexpr int kAmgKLevels = RSG_AMG_KLEVELS;  // levels 1..kAmgKLevels are solved by two flexible-CG steps (K-cycle)
 constexpr uint32_t kAmgUnset = 0xffffffffu;
 
 // Device buffer that only grows (reallocated when a larger size is asked for).
