@@ -172,19 +172,40 @@ __global__ void k_amg_diag(uint32_t n, const uint32_t *__restrict__ rp, const ui
     }
 }
 
+// Passes with heavy per-entry work (the FP64 strength test, the coarse-row copy) give each row
+// kRowLanes lanes, entries strided by kRowLanes.  (The light passes -- diagonal, independent-set
+// rounds, joins -- stay one thread per row: with 8 lanes they measured 2-5x slower, the grid of
+// short blocks costing more than the shorter serial loops save.)
+constexpr int kRowLanes = 8;
+
+// f(i, valid, lane) for every row i, kRowLanes lanes each; warps run whole rounds.
+template <class F>
+__device__ __forceinline__ void for_row_groups(uint32_t n, F &&f)
+{
+    const uint32_t lane = threadIdx.x & (kRowLanes - 1);
+    const uint32_t stride = (gridDim.x * blockDim.x) / kRowLanes;
+    for (uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * (32 / kRowLanes); base < n; base += stride) {
+        const uint32_t i = base + (threadIdx.x & 31) / kRowLanes;
+        f(i, i < n, lane);
+    }
+}
+
+inline int grid_groups(uint64_t rows) { return grid_rows(rows * kRowLanes); }
+
 __global__ void k_amg_strength(uint32_t n, const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ci,
                                const double *__restrict__ val, const double *__restrict__ diag, double theta,
                                uint8_t *__restrict__ smask)
 {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for_row_groups(n, [&](uint32_t i, bool ok, uint32_t lane) {
+        if (!ok) return;
         const double di = diag[i];
-        for (uint32_t j = rp[i]; j < rp[i + 1]; j++) {
+        for (uint32_t j = rp[i] + lane; j < rp[i + 1]; j += kRowLanes) {
             const uint32_t c = ci[j];
-            bool s = false;
-            if (c != i && c < n) s = fabs(val[j]) >= theta * sqrt(fabs(di * diag[c])) && val[j] != 0.0;
-            smask[j] = s ? 1 : 0;
+            bool st = false;
+            if (c != i && c < n) st = fabs(val[j]) >= theta * sqrt(fabs(di * diag[c])) && val[j] != 0.0;
+            smask[j] = st ? 1 : 0;
         }
-    }
+    });
 }
 
 __global__ void k_amg_mis_init(uint32_t n, uint64_t *__restrict__ T)
@@ -434,94 +455,154 @@ __global__ void __launch_bounds__(kGalThreads) k_amg_galerkin(uint32_t nc, const
 }
 
 // The same coarse rows with one warp per row and no sort: the warp walks the aggregate's entries in
-// staging order (fine rows ascending, entries in CSR order) 32 at a time, keeps one accumulator per
-// distinct J in shared memory (in order of first occurrence), and adds each 32-entry chunk's values
-// into the accumulators serially in lane order -- so every sum is taken in staging order, as in the
-// sorting kernel above.  The row's (J, sum) pairs are then written in ascending J.  A row with more
-// than kGalUnique distinct columns sets flags[5] (the caller then runs the sorting kernel).
+// staging order (fine rows ascending, entries in CSR order) as one flattened sequence, 32 entries at
+// a time across row boundaries (the indexes, columns and values of kGalAhead chunks loaded before
+// the first is used), keeps one accumulator per distinct J in shared memory (slots in order of first
+// occurrence, found through an open-addressing hash table), and adds each chunk's values into the
+// accumulators serially in lane order -- so every sum is taken in staging order, as in the sorting
+// kernel above.  The row's (J, sum) pairs are then written in ascending J.  A row with more than
+// kGalUnique distinct columns sets flags[5] (the caller then runs the sorting kernel).
 constexpr int kGalWarps = 4;
-constexpr int kGalUnique = 256;
+constexpr int kGalUnique = 128;
+constexpr uint32_t kGalHashBits = 8;
+constexpr uint32_t kGalHash = 1u << kGalHashBits;  // hash slots per warp: load factor <= 1/2, so a probe ends
+constexpr uint32_t kGalEmpty = 0xffffffffu;
+constexpr int kGalAhead = 4;
+__device__ __forceinline__ uint32_t gal_hash(uint32_t J) { return (J * 2654435761u) >> (32 - kGalHashBits); }
 __global__ void __launch_bounds__(32 * kGalWarps) k_amg_galerkin_warp(
     uint32_t nc, const uint32_t *__restrict__ ptr, const uint32_t *__restrict__ rows, const uint32_t *__restrict__ rp,
     const uint32_t *__restrict__ ci, const double *__restrict__ val, const uint32_t *__restrict__ agg,
     const uint32_t *__restrict__ eoff, uint32_t *__restrict__ tcol, double *__restrict__ tval,
     uint32_t *__restrict__ count, unsigned int *flags)
 {
+    static_assert(kGalHash >= 2u * kGalUnique && kGalHash <= 256u, "hash table size");
+    __shared__ uint32_t hkey[kGalWarps][kGalHash];
+    __shared__ uint8_t hslot[kGalWarps][kGalHash];
+    __shared__ uint8_t hpos[kGalWarps][kGalUnique];
     __shared__ uint32_t ucol[kGalWarps][kGalUnique];
     __shared__ double uacc[kGalWarps][kGalUnique];
-    __shared__ uint32_t cslot[kGalWarps][32];
     __shared__ double cval[kGalWarps][32];
+    __shared__ uint32_t rpre[kGalWarps][33], rbeg[kGalWarps][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    uint32_t *uc = ucol[w];
+    uint32_t *hk = hkey[w], *uc = ucol[w], *pre = rpre[w], *beg = rbeg[w];
+    uint8_t *hs = hslot[w], *hp = hpos[w];
     double *ua = uacc[w];
+    for (uint32_t t = lane; t < kGalHash; t += 32) hk[t] = kGalEmpty;
+    __syncwarp();
     for (uint32_t I = blockIdx.x * kGalWarps + w; I < nc; I += gridDim.x * kGalWarps) {
         uint32_t U = 0;
         bool overflow = false;
-        for (uint32_t k = ptr[I]; k < ptr[I + 1] && !overflow; k++) {
-            const uint32_t i = rows[k];
-            for (uint32_t j0 = rp[i]; j0 < rp[i + 1] && !overflow; j0 += 32) {
-                const uint32_t j = j0 + lane;
-                const bool valid = j < rp[i + 1];
-                const uint32_t J = valid ? agg[ci[j]] : kAmgUnset;
-                const double v = valid ? val[j] : 0.0;
-                uint32_t slot = kAmgUnset;
-                if (valid)
-                    for (uint32_t u = 0; u < U; u++)
-                        if (uc[u] == J) {
-                            slot = u;
-                            break;
-                        }
-                // new columns take slots in order of first occurrence (lane order)
-                const bool fresh = valid && slot == kAmgUnset;
-                const unsigned int fresh_mask = __ballot_sync(0xffffffffu, fresh);
-                const unsigned int same = __match_any_sync(0xffffffffu, fresh ? J : kAmgUnset);
-                const int leader = __ffs(same) - 1;
-                const bool is_leader = fresh && leader == lane;
-                const unsigned int leaders = __ballot_sync(0xffffffffu, is_leader);
-                if (U + __popc(leaders) > uint32_t(kGalUnique)) {
-                    overflow = true;
-                    break;
-                }
-                if (is_leader) {
-                    const uint32_t sl = U + __popc(leaders & ((1u << lane) - 1u));
-                    uc[sl] = J;
-                    ua[sl] = 0.0;
-                    slot = sl;
-                }
-                __syncwarp();
-                if (fresh && !is_leader) slot = U + __popc(leaders & ((1u << leader) - 1u));
-                U += __popc(leaders);
-                (void)fresh_mask;
-                cslot[w][lane] = slot;
-                cval[w][lane] = v;
-                __syncwarp();
-                // the lowest lane of each group of equal slots adds the group's values in lane order
-                const unsigned int grp = __match_any_sync(0xffffffffu, slot);
-                if (valid && (__ffs(grp) - 1) == lane) {
-                    double acc = ua[slot];
-                    for (unsigned int m = grp; m; m &= m - 1) acc += cval[w][__ffs(m) - 1];
-                    ua[slot] = acc;
-                }
-                __syncwarp();
+        const uint32_t k0 = ptr[I], k1 = ptr[I + 1];
+        for (uint32_t kb = k0; kb < k1 && !overflow; kb += 32) {
+            // this batch of up to 32 rows: starts and exclusive prefix of lengths
+            const uint32_t nr = min(32u, k1 - kb);
+            uint32_t len = 0, start = 0;
+            if (uint32_t(lane) < nr) {
+                const uint32_t i = rows[kb + lane];
+                start = rp[i];
+                len = rp[i + 1] - start;
             }
-        }
-        if (overflow) {
-            if (lane == 0) {
-                atomicOr(&flags[5], 1u);
-                count[I] = 0;
+            uint32_t inc = len;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += y;
             }
+            const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
+            beg[lane] = start;
+            pre[lane] = inc - len;
+            if (lane == 31) pre[32] = total;
             __syncwarp();
-            continue;
+            for (uint32_t fa = 0; fa < total && !overflow; fa += 32 * kGalAhead) {
+                uint32_t jj[kGalAhead], Jr[kGalAhead];
+                double vr[kGalAhead];
+#pragma unroll
+                for (int t = 0; t < kGalAhead; t++) {
+                    const uint32_t f = fa + 32u * t + uint32_t(lane);
+                    uint32_t lo = 0, hi = nr;  // pre[lo] <= f < pre[hi]
+                    while (hi - lo > 1) {
+                        const uint32_t mid = (lo + hi) >> 1;
+                        if (pre[mid] <= f) lo = mid;
+                        else hi = mid;
+                    }
+                    jj[t] = f < total ? beg[lo] + (f - pre[lo]) : kAmgUnset;
+                }
+#pragma unroll
+                for (int t = 0; t < kGalAhead; t++) {
+                    Jr[t] = jj[t] != kAmgUnset ? ci[jj[t]] : 0u;
+                    vr[t] = jj[t] != kAmgUnset ? val[jj[t]] : 0.0;
+                }
+#pragma unroll
+                for (int t = 0; t < kGalAhead; t++) Jr[t] = jj[t] != kAmgUnset ? agg[Jr[t]] : kAmgUnset;
+#pragma unroll
+                for (int t = 0; t < kGalAhead; t++) {
+                    if (fa + 32u * t >= total || overflow) break;  // warp-uniform
+                    const bool valid = jj[t] != kAmgUnset;
+                    const uint32_t J = Jr[t];
+                    uint32_t slot = kAmgUnset;
+                    if (valid)
+                        for (uint32_t h = gal_hash(J);; h = (h + 1) & (kGalHash - 1)) {
+                            const uint32_t k = hk[h];
+                            if (k == J) {
+                                slot = hs[h];
+                                break;
+                            }
+                            if (k == kGalEmpty) break;
+                        }
+                    __syncwarp();  // every lookup done before this chunk's inserts
+                    // new columns take slots in order of first occurrence (lane order)
+                    const bool fresh = valid && slot == kAmgUnset;
+                    const unsigned int same = __match_any_sync(0xffffffffu, fresh ? J : kAmgUnset);
+                    const int leader = __ffs(same) - 1;
+                    const bool is_leader = fresh && leader == lane;
+                    const unsigned int leaders = __ballot_sync(0xffffffffu, is_leader);
+                    if (U + __popc(leaders) > uint32_t(kGalUnique)) {
+                        overflow = true;
+                        break;
+                    }
+                    if (is_leader) {
+                        const uint32_t sl = U + __popc(leaders & ((1u << lane) - 1u));
+                        uint32_t h = gal_hash(J);
+                        while (atomicCAS(&hk[h], kGalEmpty, J) != kGalEmpty) h = (h + 1) & (kGalHash - 1);
+                        hs[h] = uint8_t(sl);
+                        hp[sl] = uint8_t(h);
+                        uc[sl] = J;
+                        ua[sl] = 0.0;
+                        slot = sl;
+                    }
+                    const uint32_t from_leader = __shfl_sync(0xffffffffu, slot, fresh ? leader : lane);
+                    if (fresh) slot = from_leader;
+                    U += __popc(leaders);
+                    cval[w][lane] = vr[t];
+                    __syncwarp();
+                    // the lowest lane of each group of equal slots adds the group's values in lane order
+                    const unsigned int grp = __match_any_sync(0xffffffffu, slot);
+                    if (valid && (__ffs(grp) - 1) == lane) {
+                        double acc = ua[slot];
+                        for (unsigned int m = grp; m; m &= m - 1) acc += cval[w][__ffs(m) - 1];
+                        ua[slot] = acc;
+                    }
+                    __syncwarp();
+                }
+            }
         }
-        // ascending J: each pair's rank among the row's distinct columns
-        for (uint32_t t = lane; t < U; t += 32) {
-            const uint32_t J = uc[t];
-            uint32_t rank = 0;
-            for (uint32_t u = 0; u < U; u++) rank += uc[u] < J ? 1u : 0u;
-            tcol[size_t(eoff[I]) + rank] = J;
-            tval[size_t(eoff[I]) + rank] = ua[t];
+        if (!overflow) {
+            // ascending J: each pair's rank among the row's distinct columns
+            for (uint32_t t = lane; t < U; t += 32) {
+                const uint32_t J = uc[t];
+                uint32_t rank = 0;
+                for (uint32_t u = 0; u < U; u++) rank += uc[u] < J ? 1u : 0u;
+                tcol[size_t(eoff[I]) + rank] = J;
+                tval[size_t(eoff[I]) + rank] = ua[t];
+            }
         }
-        if (lane == 0) count[I] = U;
+        __syncwarp();
+        // empty the hash table for the next row (the slots in use are listed in hp)
+        for (uint32_t t = lane; t < U; t += 32) hk[hp[t]] = kGalEmpty;
+        if (lane == 0) {
+            count[I] = overflow ? 0u : U;
+            if (overflow) atomicOr(&flags[5], 1u);
+        }
         __syncwarp();
     }
 }
@@ -531,55 +612,16 @@ __global__ void k_amg_compact(uint32_t nc, const uint32_t *__restrict__ eoff, co
                               const double *__restrict__ tval, uint32_t *__restrict__ ci_c, double *__restrict__ val_c,
                               float *__restrict__ val32_c)
 {
-    for (uint32_t I = blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += gridDim.x * blockDim.x) {
-        // (the longest row was recorded by k_amg_row_max)
+    for_row_groups(nc, [&](uint32_t I, bool ok, uint32_t lane) {
+        if (!ok) return;
         const uint32_t src = eoff[I], dst = rp_c[I];
-        for (uint32_t k = 0; k < count[I]; k++) {
+        for (uint32_t k = lane; k < count[I]; k += kRowLanes) {
+            const double v = tval[src + k];
             ci_c[dst + k] = tcol[src + k];
-            val_c[dst + k] = tval[src + k];
-            val32_c[dst + k] = float(tval[src + k]);
+            val_c[dst + k] = v;
+            val32_c[dst + k] = float(v);
         }
-    }
-}
-
-// flags[6] = the longest coarse row.
-__global__ void k_amg_row_max(uint32_t nc, const uint32_t *__restrict__ count, unsigned int *flags)
-{
-    unsigned int m = 0;
-    for (uint32_t I = blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += gridDim.x * blockDim.x) m = max(m, count[I]);
-    m = __reduce_max_sync(0xffffffffu, m);
-    if ((threadIdx.x & 31) == 0 && m) atomicMax(&flags[6], m);
-}
-
-// SELL-32 copy of a coarse level (the layout of spmv.cuh: slice s = rows 32 s .. 32 s + 31, element k
-// of lane l at slice_ptr[s] + (k / 4) 128 + 4 l + k % 4, rows padded to the slice's longest row
-// rounded up to 4).  len4 / elems: per slice; elems is scanned into slice_ptr.
-__global__ void k_amg_sell_len(uint32_t n, uint32_t n_slices, const uint32_t *__restrict__ rp,
-                               uint32_t *__restrict__ len4, uint32_t *__restrict__ elems)
-{
-    for (uint32_t sl = blockIdx.x * blockDim.x + threadIdx.x; sl < n_slices; sl += gridDim.x * blockDim.x) {
-        uint32_t m = 0;
-        for (uint32_t r = sl * 32u; r < min(n, sl * 32u + 32u); r++) m = max(m, rp[r + 1] - rp[r]);
-        const uint32_t l4 = (m + 3u) / 4u;
-        len4[sl] = l4;
-        elems[sl] = l4 * 128u;
-    }
-}
-
-__global__ void k_amg_sell_fill(uint32_t n, const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ci,
-                                const float *__restrict__ val, const uint32_t *__restrict__ sptr,
-                                const uint32_t *__restrict__ len4, uint32_t *__restrict__ scol, float *__restrict__ sval)
-{
-    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
-        const uint32_t sl = row >> 5, lane = row & 31u;
-        const size_t base = size_t(sptr[sl]) + 4u * lane;
-        const uint32_t len = rp[row + 1] - rp[row], padded = len4[sl] * 4u;
-        for (uint32_t k = 0; k < padded; k++) {
-            const size_t e = base + size_t(k >> 2) * 128u + (k & 3u);
-            scol[e] = k < len ? ci[rp[row] + k] : row;
-            sval[e] = k < len ? val[rp[row] + k] : 0.f;
-        }
-    }
+    });
 }
 
 // Dense inverse of the coarsest level (n <= kAmgCoarsest) by in-place Gauss-Jordan elimination in
@@ -748,22 +790,6 @@ __global__ void __launch_bounds__(kBlock) k_amg_fine(Csr<float> M, Sell<float> S
         if (grid_sum<2>(acc, partials, ticket, sh, tot) && threadIdx.x == 0)
             amg_finalize(st, tot[0], tot[1], mode, rz_out);
     }
-}
-
-// Sweep over a coarse level in its SELL-32 copy (one thread per row, as the finest level).
-template <int SRC, int OUT>
-__global__ void __launch_bounds__(kBlock) k_amg_coarse_sell(Sell<float> S, SweepArgs a, const CgState *st)
-{
-    pdl_wait();
-    pdl_release();
-    if (st && st->done) return;
-    if (SRC == kSrcXCorrK) kc_coefficients(a.kc, a.s, a.s2);
-    auto gx = [&](uint32_t c) { return sweep_x<SRC>(a, c); };
-    auto epi = [&](uint32_t row, float ax) {
-        const float res = a.b[row] - ax;
-        a.out[row] = OUT == kOutRes ? res : fmaf(a.dw[row], res, sweep_x<SRC>(a, row));
-    };
-    for_rows_sell<float>(S, gx, epi);
 }
 
 // x_out = xs + s P e_c (the prolongated, scaled coarse correction), one streaming pass; with kc given
@@ -1143,7 +1169,7 @@ rsg_status build_aggregates(rsg_context *ctx, AmgHierarchy *H, AmgLevel &F, uint
     if (!H->T.ensure(n) || !H->M1.ensure(n) || !H->smask.ensure(F.nnz + 1) ||
         !H->u1.ensure(size_t(n) + 1) || !H->u2.ensure(size_t(n) + 1) || !F.agg.ensure(n))
         return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: set-up workspace");
-    k_amg_strength<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, F.val, F.diag.p, kAmgTheta, H->smask.p);
+    k_amg_strength<<<grid_groups(n), kBlock, 0, s>>>(n, F.rp, F.ci, F.val, F.diag.p, kAmgTheta, H->smask.p);
     k_amg_mis_init<<<g, kBlock, 0, s>>>(n, H->T.p);
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
     // synchronous rounds until no node is undecided: launched in batches of kRoundBatch with one
@@ -1169,12 +1195,13 @@ rsg_status build_aggregates(rsg_context *ctx, AmgHierarchy *H, AmgLevel &F, uint
     // root numbering, joins
     k_amg_root_flags<<<g, kBlock, 0, s>>>(n, H->T.p, H->u1.p);
     RSG_TRY(scan_u32(ctx, H, H->u1.p, n, H->u2.p));
-    uint32_t nc = 0;
-    RSG_TRY(read_u32(ctx, H, H->u2.p + n, &nc));
     k_amg_join1<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, H->smask.p, H->T.p, H->u2.p, H->u1.p);
     RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->flags, 0, 4 * sizeof(unsigned int), s));
     k_amg_join2<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, H->smask.p, H->u1.p, F.agg.p, H->flags);
+    // one synchronisation for the number of roots and the nodes left without an aggregate
+    RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(H->flags_h + 8, H->u2.p + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     RSG_TRY(read_flags(ctx, H, 2));
+    uint32_t nc = H->flags_h[8];
     if (H->flags_h[1] > 0) {  // singletons for nodes without any strong path to a root
         k_amg_unset_flags<<<g, kBlock, 0, s>>>(n, F.agg.p, H->u1.p);
         RSG_TRY(scan_u32(ctx, H, H->u1.p, n, H->u2.p));
@@ -1220,25 +1247,23 @@ rsg_status build_galerkin(rsg_context *ctx, AmgHierarchy *H, AmgLevel &F, AmgLev
                           s>>>(nc, F.agg_ptr.p, F.agg_rows.p, F.rp, F.ci, F.val, F.agg.p, H->u1.p, H->tcol.p,
                                H->tval.p, H->u2.p, H->flags);
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
+    // coarse row pointer; one synchronisation for the coarse nnz and the overflow flag
+    if (!Cl.own_rp.ensure(size_t(nc) + 1)) return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: coarse matrix");
+    RSG_TRY(scan_u32(ctx, H, H->u2.p, nc, Cl.own_rp.p));
+    RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(H->flags_h + 9, Cl.own_rp.p + nc, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     RSG_TRY(read_flags(ctx, H, 6));
     if (H->flags_h[5]) {
         cudaFuncSetAttribute(k_amg_galerkin, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         k_amg_galerkin<<<nc, kGalThreads, smem, s>>>(nc, F.agg_ptr.p, F.agg_rows.p, F.rp, F.ci, F.val, F.agg.p,
                                                       H->u1.p, H->tcol.p, H->tval.p, H->u2.p);
         RSG_CHECK_CUDA(ctx, cudaGetLastError());
+        RSG_TRY(scan_u32(ctx, H, H->u2.p, nc, Cl.own_rp.p));
+        RSG_TRY(read_u32(ctx, H, Cl.own_rp.p + nc, &H->flags_h[9]));
     }
-    // coarse row pointer, then compact
-    if (!Cl.own_rp.ensure(size_t(nc) + 1)) return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: coarse matrix");
-    RSG_TRY(scan_u32(ctx, H, H->u2.p, nc, Cl.own_rp.p));
-    RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->flags + 6, 0, sizeof(unsigned int), s));
-    k_amg_row_max<<<std::min(grid_rows(nc), 1024), kBlock, 0, s>>>(nc, H->u2.p, H->flags);
-    RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(H->flags_h + 9, Cl.own_rp.p + nc, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    RSG_TRY(read_flags(ctx, H, 7));  // one synchronisation for the coarse nnz and the longest row
     const uint32_t nnz = H->flags_h[9];
-    Cl.max_row = H->flags_h[6];
     if (!Cl.own_ci.ensure(size_t(nnz) + 1) || !Cl.own_val.ensure(size_t(nnz) + 1) || !Cl.own_val32.ensure(size_t(nnz) + 1))
         return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: coarse matrix");
-    k_amg_compact<<<grid_rows(nc), kBlock, 0, s>>>(nc, H->u1.p, H->u2.p, Cl.own_rp.p, H->tcol.p, H->tval.p,
+    k_amg_compact<<<grid_groups(nc), kBlock, 0, s>>>(nc, H->u1.p, H->u2.p, Cl.own_rp.p, H->tcol.p, H->tval.p,
                                                    Cl.own_ci.p, Cl.own_val.p, Cl.own_val32.p);
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
     Cl.n = nc;
@@ -1247,16 +1272,6 @@ rsg_status build_galerkin(rsg_context *ctx, AmgHierarchy *H, AmgLevel &F, AmgLev
     Cl.ci = Cl.own_ci.p;
     Cl.val = Cl.own_val.p;
     Cl.val32 = Cl.own_val32.p;
-    // SELL-32 copy for the sweeps, sized from the longest row (no further synchronisation)
-    Cl.n_slices = (nc + 31u) / 32u;
-    const size_t cap = size_t(Cl.n_slices) * 128u * ((size_t(Cl.max_row) + 3u) / 4u) + 128u;
-    if (!Cl.s_ptr.ensure(size_t(Cl.n_slices) + 1) || !Cl.s_len4.ensure(Cl.n_slices) || !Cl.s_col.ensure(cap) ||
-        !Cl.s_val.ensure(cap) || !H->u3.ensure(size_t(Cl.n_slices) + 1))
-        return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: coarse SELL copy");
-    k_amg_sell_len<<<grid_rows(Cl.n_slices), kBlock, 0, s>>>(nc, Cl.n_slices, Cl.rp, Cl.s_len4.p, H->u3.p);
-    RSG_TRY(scan_u32(ctx, H, H->u3.p, Cl.n_slices, Cl.s_ptr.p));
-    k_amg_sell_fill<<<grid_rows(nc), kBlock, 0, s>>>(nc, Cl.rp, Cl.ci, Cl.val32, Cl.s_ptr.p, Cl.s_len4.p, Cl.s_col.p,
-                                                     Cl.s_val.p);
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
     return RSG_OK;
 }
@@ -1299,10 +1314,6 @@ void amg_free(AmgHierarchy *H)
         l.v1.release();
         l.v2.release();
         l.r2.release();
-        l.s_ptr.release();
-        l.s_len4.release();
-        l.s_col.release();
-        l.s_val.release();
     }
     H->coarse_inv.release();
     H->T.release();
@@ -1409,24 +1420,15 @@ void fine_sweep(rsg_context *ctx, const FineLaunch<RPW> &f, const SweepArgs &a, 
              partials, ticket, st, mode, rz_out);
 }
 
-// Coarse levels run on the whole GPU: CSR with kLanes lanes per row.  (The SELL-32 copy leaves one warp
+// Coarse levels run on the whole GPU: CSR with kLanes lanes per row.  (A SELL-32 copy leaves one warp
 // per 32 rows, too few warps for these levels: measured slower.  One thread-block cluster of 8 CTAs
 // running all levels of up to 32k rows with cluster barriers between steps was slower still: 8 SMs
 // lack the memory-level parallelism for the 276k-entry third level.)
-constexpr bool kCoarseSell = false;
-
 template <int SRC, int OUT>
 void coarse_sweep(rsg_context *ctx, const AmgLevel &l, const SweepArgs &a, const CgState *st, bool pdl)
 {
-    if (l.n_slices && kCoarseSell) {
-        const Sell<float> S{l.rp, l.s_ptr.p, l.s_len4.p, l.s_val.p, nullptr, l.s_col.p, l.n, l.n_slices};
-        const int g = std::max(1, std::min<int>(int((uint64_t(l.n_slices) * 32 + kBlock - 1) / kBlock),
-                                                ctx->num_sms * 8));
-        launch_k(ctx->stream, pdl, k_amg_coarse_sell<SRC, OUT>, g, kBlock, 0, S, a, st);
-    } else {
-        launch_k(ctx->stream, pdl, k_amg_coarse<SRC, OUT>, coarse_grid(ctx, l.n), kBlock, 0, l.n, l.rp, l.ci, l.val32,
-                 a, st);
-    }
+    launch_k(ctx->stream, pdl, k_amg_coarse<SRC, OUT>, coarse_grid(ctx, l.n), kBlock, 0, l.n, l.rp, l.ci, l.val32, a,
+             st);
 }
 
 // Restriction of the finest level's residual (written by the fine sweep into r) to level 1's b and x0.

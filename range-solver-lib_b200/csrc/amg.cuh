@@ -65,11 +65,6 @@ struct AmgLevel {
     DevBuf<uint32_t> agg_ptr, agg_rows;    // next-level row -> rows of this level (ascending)
     DevBuf<float> b, r, x1, x2, e;         // V-cycle vectors; x1 starts as x0 = dw b (b and e unused on level 0)
     DevBuf<float> c1, c2, v1, v2, r2;      // K-cycle levels: the two flexible-CG steps
-    // SELL-32 copy of a coarse level for the sweeps (FP32 values, uint32 columns; see spmv.cuh)
-    uint32_t n_slices = 0;
-    uint32_t max_row = 0;
-    DevBuf<uint32_t> s_ptr, s_len4, s_col;
-    DevBuf<float> s_val;
 };
 
 struct AmgHierarchy {
