@@ -214,44 +214,102 @@ __global__ void k_amg_mis_init(uint32_t n, uint64_t *__restrict__ T)
         T[i] = (uint64_t(1) << kStateShift) | amg_key(i);
 }
 
-// out_i = max(in_i, max over strong neighbours j of in_j).  Rounds are launched in batches; once a
-// round has left no node undecided (*prev == 0) the later rounds return at once.
+__device__ __forceinline__ uint64_t strong_max(uint32_t i, const uint32_t *__restrict__ rp,
+                                               const uint32_t *__restrict__ ci, const uint8_t *__restrict__ smask,
+                                               const uint64_t *__restrict__ in)
+{
+    uint64_t m = in[i];
+    for (uint32_t j = rp[i]; j < rp[i + 1]; j++)
+        if (smask[j]) m = max(m, in[ci[j]]);
+    return m;
+}
+
+// The decision of an undecided node i from M2_i (the largest tuple within distance 2): a root when
+// it is the node's own tuple, out when it belongs to a root, else still undecided (returns true).
+__device__ __forceinline__ bool mis_decide(uint32_t i, uint64_t t, uint64_t m2, uint64_t *__restrict__ T)
+{
+    if (m2 == t) T[i] = (uint64_t(2) << kStateShift) | amg_key(i);
+    else if (tup_state(m2) == 2) T[i] = amg_key(i);
+    else return true;
+    return false;
+}
+
+// out_i = max(in_i, max over strong neighbours j of in_j), for the nodes the second pass will read:
+// in round 0 all of them, later only those stamped need_i = round by the previous round (the nodes
+// still undecided and their strong neighbours), so late rounds skip most of the graph.  Rounds are
+// launched in batches; once a round has left no node undecided (*prev == 0) the later rounds return
+// at once.
 __global__ void k_amg_nbmax(uint32_t n, const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ci,
                             const uint8_t *__restrict__ smask, const uint64_t *__restrict__ in,
-                            uint64_t *__restrict__ out, const unsigned int *prev)
+                            uint64_t *__restrict__ out, const uint32_t *__restrict__ need, uint32_t round,
+                            const unsigned int *prev)
 {
     if (prev && *prev == 0) return;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint64_t m = in[i];
-        for (uint32_t j = rp[i]; j < rp[i + 1]; j++)
-            if (smask[j]) m = max(m, in[ci[j]]);
-        out[i] = m;
-    }
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (round == 0 || need[i] == round) out[i] = strong_max(i, rp, ci, smask, in);
 }
 
 // Second half of a synchronous round, fused with the decision: for every node still undecided,
-// M2_i = max(M1_i, max over strong neighbours j of M1_j) (decided nodes need no M2); the node becomes
-// a root when M2_i is its own tuple and drops out when M2_i belongs to a root.  *count (zeroed
-// beforehand) receives the number of nodes still undecided; nothing is done once the previous round
-// left none (*prev == 0).
+// M2_i = max(M1_i, max over strong neighbours j of M1_j) (decided nodes need no M2).  A node left
+// undecided stamps itself and its strong neighbours need = round + 1.  *count (zeroed beforehand)
+// receives the number of nodes still undecided; nothing is done once the previous round left none
+// (*prev == 0).
 __global__ void k_amg_mis_round2(uint32_t n, const uint32_t *__restrict__ rp, const uint32_t *__restrict__ ci,
                                  const uint8_t *__restrict__ smask, const uint64_t *__restrict__ M1,
-                                 uint64_t *__restrict__ T, const unsigned int *prev, unsigned int *count)
+                                 uint64_t *__restrict__ T, uint32_t *__restrict__ need, uint32_t round,
+                                 const unsigned int *prev, unsigned int *count)
 {
     if (prev && *prev == 0) return;
     unsigned int left = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint64_t t = T[i];
         if (tup_state(t) != 1) continue;
-        uint64_t m = M1[i];
-        for (uint32_t j = rp[i]; j < rp[i + 1]; j++)
-            if (smask[j]) m = max(m, M1[ci[j]]);
-        if (m == t) T[i] = (uint64_t(2) << kStateShift) | amg_key(i);
-        else if (tup_state(m) == 2) T[i] = amg_key(i);
-        else left++;
+        if (mis_decide(i, t, strong_max(i, rp, ci, smask, M1), T)) {
+            left++;
+            need[i] = round + 1;
+            for (uint32_t j = rp[i]; j < rp[i + 1]; j++)
+                if (smask[j]) need[ci[j]] = round + 1;
+        }
     }
     left = __reduce_add_sync(0xffffffffu, left);
     if ((threadIdx.x & 31) == 0 && left) atomicAdd(count, left);
+}
+
+// All rounds of a small level in one CTA (the passes separated by barriers): out[0] = the rounds
+// run, out[1] = the nodes still undecided after them (0 unless kMaxRounds ran out).
+constexpr uint32_t kMisCtaRows = 4096;
+constexpr int kMisCtaThreads = 1024;
+constexpr uint32_t kMisMaxRounds = 128;
+__global__ void __launch_bounds__(kMisCtaThreads) k_amg_mis_cta(uint32_t n, const uint32_t *__restrict__ rp,
+                                                                const uint32_t *__restrict__ ci,
+                                                                const uint8_t *__restrict__ smask,
+                                                                uint64_t *__restrict__ T, uint64_t *__restrict__ M1,
+                                                                unsigned int *out)
+{
+    __shared__ unsigned int left;
+    uint32_t r = 0;
+    unsigned int l = n;
+    while (r < kMisMaxRounds && l > 0) {
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) M1[i] = strong_max(i, rp, ci, smask, T);
+        if (threadIdx.x == 0) left = 0;
+        __syncthreads();
+        unsigned int mine = 0;
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const uint64_t t = T[i];
+            if (tup_state(t) != 1) continue;
+            if (mis_decide(i, t, strong_max(i, rp, ci, smask, M1), T)) mine++;
+        }
+        mine = __reduce_add_sync(0xffffffffu, mine);
+        if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&left, mine);
+        __syncthreads();
+        l = left;
+        r++;
+        __syncthreads();  // every thread has read left before the next round resets it
+    }
+    if (threadIdx.x == 0) {
+        out[0] = r;
+        out[1] = l;
+    }
 }
 
 __global__ void k_amg_root_flags(uint32_t n, const uint64_t *__restrict__ T, uint32_t *__restrict__ flag)
@@ -1167,31 +1225,43 @@ rsg_status build_aggregates(rsg_context *ctx, AmgHierarchy *H, AmgLevel &F, uint
     const int g = grid_rows(n);
     cudaStream_t s = ctx->stream;
     if (!H->T.ensure(n) || !H->M1.ensure(n) || !H->smask.ensure(F.nnz + 1) ||
-        !H->u1.ensure(size_t(n) + 1) || !H->u2.ensure(size_t(n) + 1) || !F.agg.ensure(n))
+        !H->u1.ensure(size_t(n) + 1) || !H->u2.ensure(size_t(n) + 1) || !H->u3.ensure(size_t(n) + 1) ||
+        !F.agg.ensure(n))
         return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: set-up workspace");
     k_amg_strength<<<grid_groups(n), kBlock, 0, s>>>(n, F.rp, F.ci, F.val, F.diag.p, kAmgTheta, H->smask.p);
     k_amg_mis_init<<<g, kBlock, 0, s>>>(n, H->T.p);
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
-    // synchronous rounds until no node is undecided: launched in batches of kRoundBatch with one
-    // undecided-node counter per round (rounds after the last one needed return at once); the host
-    // reads the batch's last counter
-    constexpr uint32_t kRoundBatch = 8, kMaxRounds = 128;
-    if (!H->rounds.ensure(kMaxRounds)) return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: round counters");
-    RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->rounds.p, 0, kMaxRounds * sizeof(unsigned int), s));
-    uint32_t round = 0;
-    for (;;) {
-        for (uint32_t k = 0; k < kRoundBatch; k++, round++) {
-            const unsigned int *prev = round ? H->rounds.p + round - 1 : nullptr;
-            k_amg_nbmax<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, H->smask.p, H->T.p, H->M1.p, prev);
-            k_amg_mis_round2<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, H->smask.p, H->M1.p, H->T.p, prev,
-                                                  H->rounds.p + round);
-        }
+    if (n <= kMisCtaRows) {  // a small level: every round in one CTA, one synchronisation
+        RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->flags + 10, 0, 2 * sizeof(unsigned int), s));
+        k_amg_mis_cta<<<1, kMisCtaThreads, 0, s>>>(n, F.rp, F.ci, H->smask.p, H->T.p, H->M1.p, H->flags + 10);
         RSG_CHECK_CUDA(ctx, cudaGetLastError());
-        RSG_TRY(read_u32(ctx, H, H->rounds.p + round - 1, &H->flags_h[0]));
-        if (H->flags_h[0] == 0) break;
-        if (round + kRoundBatch > kMaxRounds) return set_error(ctx, RSG_ERR_CUDA, "amg: independent set did not converge");
+        RSG_TRY(read_flags(ctx, H, 12));
+        if (H->flags_h[11] != 0) return set_error(ctx, RSG_ERR_CUDA, "amg: independent set did not converge");
+        H->mis_rounds += H->flags_h[10];
+    } else {
+        // synchronous rounds until no node is undecided: launched in batches of kRoundBatch with one
+        // undecided-node counter per round (rounds after the last one needed return at once); the host
+        // reads the batch's last counter
+        constexpr uint32_t kRoundBatch = 8;
+        if (!H->rounds.ensure(kMisMaxRounds)) return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: round counters");
+        RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->rounds.p, 0, kMisMaxRounds * sizeof(unsigned int), s));
+        RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->u3.p, 0, size_t(n) * sizeof(uint32_t), s));  // round stamps
+        uint32_t round = 0;
+        for (;;) {
+            for (uint32_t k = 0; k < kRoundBatch; k++, round++) {
+                const unsigned int *prev = round ? H->rounds.p + round - 1 : nullptr;
+                k_amg_nbmax<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, H->smask.p, H->T.p, H->M1.p, H->u3.p, round, prev);
+                k_amg_mis_round2<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, H->smask.p, H->M1.p, H->T.p, H->u3.p, round,
+                                                      prev, H->rounds.p + round);
+            }
+            RSG_CHECK_CUDA(ctx, cudaGetLastError());
+            RSG_TRY(read_u32(ctx, H, H->rounds.p + round - 1, &H->flags_h[0]));
+            if (H->flags_h[0] == 0) break;
+            if (round + kRoundBatch > kMisMaxRounds)
+                return set_error(ctx, RSG_ERR_CUDA, "amg: independent set did not converge");
+        }
+        H->mis_rounds += round;
     }
-    H->mis_rounds += round;
     // root numbering, joins
     k_amg_root_flags<<<g, kBlock, 0, s>>>(n, H->T.p, H->u1.p);
     RSG_TRY(scan_u32(ctx, H, H->u1.p, n, H->u2.p));
