@@ -44,11 +44,15 @@ SIGMA = 1.5
 RTOL = 1e-10
 # DRAM bytes of one launch of the headline solver's dominant kernel on heat_lognormal_100, and where
 # each figure comes from (an ncu capture; None where none was taken of the current kernel)
-TRAFFIC = {"mixed_jacobi": 113.65e6, "mixed_amg": None}
+TRAFFIC = {"mixed_jacobi": 113.65e6, "mixed_amg": 120.06e6}
+# trained parameters of the learned preconditioner (bench.py --workload learned --save-model ...)
+LEARNED_MODEL = os.path.join(REPO, "range-solver-lib_b200", "rsg", "models", "heat_family_60.npz")
 TRAFFIC_SOURCE = {
     "mixed_jacobi": ("ncu --set full capture of k_mx_dir on heat_lognormal_100, dram__bytes_read.sum + "
                      "dram__bytes_write.sum of one launch (profiles/k_mx_dir_heat_lognormal_100.md)"),
-    "mixed_amg": None}
+    "mixed_amg": ("ncu --set full capture of k_amg_fine (the cycle's last finest-level sweep) on "
+                  "heat_lognormal_100, dram__bytes_read.sum + dram__bytes_write.sum of one launch "
+                  "(profiles/k_amg_fine_heat_lognormal_100.md)")}
 
 
 def load_peaks() -> tuple[float, str]:
@@ -207,6 +211,34 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         xs_host[key] = x.cpu().numpy()
     x64 = xs_host["fp64_jacobi"]
     err_vs_fp64 = {k: float(np.linalg.norm(v - x64) / np.linalg.norm(x64)) for k, v in xs_host.items()}
+
+    # the learned preconditioner on the same system: flexible CG in FP64 with the trained network as
+    # M (Jacobi fallback), parameters from the committed checkpoint; two solves, L2 flushed, the
+    # faster one reported (not part of the headline choice, which is between the timed solvers)
+    learned = None
+    if args.learned_model and os.path.exists(args.learned_model):
+        from rsg import learned as RL
+        model = RL.Learned.load(ctx, args.learned_model)
+        conf_l = RL.learned_conf(model, rsg.make_conf(n_outer=100000, stop_rule="true", rtol=RTOL))
+        tl = []
+        for _ in range(2):
+            flush.fill_(1)
+            x.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            _, st_l = ctx.solve(A, b, x, conf=conf_l, prec=rsg.PREC_LEARNED)
+            e1.record(stream)
+            e1.synchronize()
+            tl.append(e0.elapsed_time(e1) / 1e3)
+        xs_host["learned_fcg"] = x.cpu().numpy()
+        learned = {"s": min(tl), "iterations": st_l.iterations, "true_relres": st_l.true_relres,
+                   "fallbacks": st_l.fallbacks,
+                   "err_vs_fp64_solution": float(np.linalg.norm(xs_host["learned_fcg"] - x64) / np.linalg.norm(x64)),
+                   "speedup_vs_plain_fp64": times["fp64_jacobi"] / min(tl),
+                   "solver": "flexible CG (FP64) with the learned message-passing preconditioner applied every "
+                             "iteration, Jacobi fallback",
+                   "model": os.path.relpath(args.learned_model, REPO), "model_train_steps": model.step}
+        model.close()
     amg_info = ctx.amg_setup(A)
 
     # dominant kernels, timed live (HBM-bound: L2 flushed before each launch)
@@ -232,18 +264,16 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
 
     # launches per solve: setup (norm, 2 scalings, Jacobi, FP32 copy, init residual + z, fold,
     # unscale, true residual) + per 2-iteration graph body (3 kernels per iteration + tail); the
-    # multilevel preconditioner adds its V-cycle per iteration (2 sweeps + 1 restriction per level
-    # and side, the dense coarsest solve) and its set-up kernels
+    # multilevel preconditioner adds one cycle per application (once at the start and once per
+    # iteration) and its set-up, both as counted by the library (rsg_amg_info)
     def launches(key):
         st = stats[key]
         bodies = (st.iterations + 1) // 2
         base = 10 + bodies * 7 + (0 if key == "fp64_jacobi" else 1)
         if key != "mixed_amg":
             return base
-        L, nu = amg_info["levels"], args.amg_sweeps
-        per_cycle = (L - 1) * (2 * nu + 1) + 1
-        setup = 4 + (L - 1) * (14 + 6 * amg_info["mis_rounds"] // max(L - 1, 1))
-        return base + per_cycle * (st.iterations + 1) + setup
+        per_cycle = amg_info["cycle_launches"][args.amg_sweeps - 1]
+        return base + per_cycle * (st.iterations + 1) + amg_info["setup_launches"]
 
     # end to end through the reference-facing API with pinned host buffers
     rp_h, ci_h, val_h = A.to_host()
@@ -271,7 +301,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         "by_spmv64": nnz * 10 + 4 * (n + 1) + 2 * n * 8, "traffic": traffic, "n": n, "nnz": nnz,
         "asm_ms": float(np.median(asm_ms[1:])), "asm_host_ms": float(np.median(asm_host_ms[1:])),
         "clocks": sampler.summary(), "e2e_s": e2e_s, "tune": tune, "amg_info": amg_info,
-        "h2d": int(nnz * 8 + 2 * n * 8), "d2h": int(n * 8), "launches": launches(best),
+        "h2d": int(nnz * 8 + 2 * n * 8), "d2h": int(n * 8), "launches": launches(best), "learned": learned,
         "ctx": ctx, "A": A, "b": b, "rp": rp_h, "ci": ci_h, "val": val_h, "xs": xs_host, "problem": p,
     }
     return out
@@ -358,8 +388,13 @@ def main():
     ap.add_argument("--batch-mode", default="shard", choices=["shard", "replicas"],
                     help="batch256: shard one batch of 256 systems across the ranks (default), or solve 256 "
                          "systems on every rank")
-    ap.add_argument("--amg-sweeps", type=int, default=2, choices=[1, 2],
-                    help="damped-Jacobi sweeps per side of the multilevel preconditioner's V-cycle")
+    ap.add_argument("--amg-sweeps", type=int, default=1, choices=[1, 2],
+                    help="damped-Jacobi sweeps per side of the multilevel preconditioner's cycle (1: fewer "
+                         "launches per iteration, measured faster than 2 at 100^3)")
+    ap.add_argument("--learned-model", default=LEARNED_MODEL,
+                    help="heat100: trained learned-preconditioner parameters (.npz) for the learned FCG row; "
+                         "'' skips it")
+    ap.add_argument("--save-model", default="", help="learned: write the trained parameters (.npz) here")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="heat100: keep the built-in launch shapes")
     ap.add_argument("--workload", default="heat100",
@@ -482,6 +517,8 @@ def main():
                    "speedup_vs_plain_fp64": times["fp64_jacobi"] / times[best],
                    "target_3x_over_plain_fp64_met": times["fp64_jacobi"] / times[best] >= 3.0,
                    "solvers": per_solver, "amg_hierarchy": r["amg_info"], "amg_sweeps": args.amg_sweeps,
+                   "learned_fcg": (dict(r["learned"], err_vs_oracle=parity.get("err_vs_oracle_learned_fcg")
+                                        if parity else None) if r["learned"] else None),
                    "assembly_numeric_s": r["asm_ms"] / 1e3,
                    "assembly_numeric_from_host_arrays_s": r["asm_host_ms"] / 1e3,
                    "autotune": r["tune"]},
@@ -798,6 +835,9 @@ def run_other(args, rank, world, local_rank, threads):
                                       base=base)
         torch.cuda.synchronize()
         t_train = time.perf_counter() - t0
+        if args.save_model:
+            os.makedirs(os.path.dirname(os.path.abspath(args.save_model)), exist_ok=True)
+            model.save(args.save_model, with_adam=False)
         methods = ("pcg", "fcg", "gmres", "fgmres", "pcg_x0")
         ev = RL.evaluate_heat_family(ctx, model, args.learned_hex, range(args.eval_seeds), rtol=RTOL, base=base,
                                      methods=methods)

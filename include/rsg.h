@@ -37,7 +37,8 @@ typedef enum {
     RSG_ERR_CUDA = -2,
     RSG_ERR_OUT_OF_MEMORY = -3,
     RSG_ERR_UNSUPPORTED = -4,
-    RSG_ERR_SINGULAR = -5,      /* singular block in block-Jacobi (RRMatrix::invert failure) */
+    RSG_ERR_SINGULAR = -5,      /* singular block in block-Jacobi (RRMatrix::invert failure); a zero norm
+                                   (breakdown) in an eigenvalue driver */
     RSG_ERR_TIMEOUT = -6
 } rsg_status;
 
@@ -91,7 +92,7 @@ typedef struct {
                                    (slower than evict_first on SELL-32 in measurements, so not applied there) */
     int32_t  autotune;          /* 1: autotune A's launch shapes on its first solve (rsg_autotune, with the
                                    cache file named by the RSG_TUNE_CACHE environment variable if set) */
-    int32_t  amg_sweeps;        /* RSG_PREC_AMG: damped-Jacobi sweeps per side of the V-cycle, 1 or 2 (0: 2) */
+    int32_t  amg_sweeps;        /* RSG_PREC_AMG: damped-Jacobi sweeps per side of the cycle, 1 or 2 (0: 1) */
     int32_t  reserved[4];
 } rsg_solver_conf;
 
@@ -201,6 +202,41 @@ RSG_API rsg_status rsg_solve_multi(rsg_context *ctx, rsg_csr *A, const rsg_solve
                                    uint32_t k, const double *B, double *X, int32_t memory, rsg_stats *per_rhs,
                                    rsg_stats *summary);
 
+/* ---- eigenvalues of the pencil (M, K) ----
+ * Replaces REigenValueSolver::solve (src/reigenvaluesolver.cpp:40-110) with its three methods:
+ * Lanczos (:119-210, with qlDecomposition :420-497), Arnoldi (:211-294, with qrDecomposition
+ * :499-592) and the Rayleigh quotient iteration (:295-392).  Every solve of a step is rsg_solve with
+ * *conf and Jacobi (as the reference passes R_MATRIX_PRECONDITIONER_JACOBI), its x the previous
+ * step's vector as the reference's is; the vectors stay on the device.  Results follow the
+ * reference's solve(): with more than one value, d_i = |1/d_i| sorted ascending (after the
+ * reference's swap of the first two) and the eigenvectors reordered by the same permutation; the
+ * Lanczos values are the Lanczos diagonal (the reference's QL step ends before any rotation);
+ * Rayleigh returns its shift mu and vector.  M and K: CSR handles of one size (Rayleigh: one
+ * pattern).  start: n host values, the reference's random start vector rand()/RAND_MAX (normalised
+ * here).  values: n_eigen (Rayleigh: 1) host doubles; vectors (Arnoldi, Rayleigh; may be NULL):
+ * the same count of rows of n doubles.  A zero norm met on the way returns RSG_ERR_SINGULAR. */
+typedef enum {
+    RSG_EIGEN_LANCZOS = 0,      /* REigenValueSolverConf::Lanczos */
+    RSG_EIGEN_ARNOLDI = 1,      /* REigenValueSolverConf::Arnoldi */
+    RSG_EIGEN_RAYLEIGH = 2      /* REigenValueSolverConf::Rayleigh */
+} rsg_eigen_method;
+typedef struct {
+    int32_t  method;            /* rsg_eigen_method */
+    uint32_t n_eigen;           /* getNEigenValues (Lanczos, Arnoldi) */
+    uint32_t n_iterations;      /* getNIterations: QR sweeps (Arnoldi), iterations (Rayleigh) */
+    uint32_t reserved;
+    double   cvg;               /* getSolverCvgValue: QR subdiagonal bound, Rayleigh |mu - mu_old| */
+    double   mu0;               /* Rayleigh: the first shift (the reference draws 1e9 rand()/RAND_MAX) */
+} rsg_eigen_conf;
+typedef struct {
+    uint32_t n_values;          /* values written */
+    uint32_t solves;            /* linear solves run */
+    uint64_t iterations;        /* their Krylov iterations in total */
+} rsg_eigen_stats;
+RSG_API rsg_status rsg_eigen_solve(rsg_context *ctx, const rsg_csr *M, rsg_csr *K, const rsg_eigen_conf *econf,
+                                   const rsg_solver_conf *conf, const double *start, double *values,
+                                   double *vectors, rsg_eigen_stats *stats);
+
 /* Autotuner (no counterpart in the reference, whose loops are OpenMP).  Picks
  * A's layout (SELL-32, or the CSR stream with a rows-per-warp chunk) and the
  * grid sizes of the CG loop's two kernels per iteration (fused direction +
@@ -252,17 +288,19 @@ RSG_API rsg_status rsg_selftest_wait_timeout(rsg_context *ctx, uint32_t polls);
  * matrix's current values at every rsg_solve that asks for it: aggregates rooted at a distance-2
  * independent set of the strength graph (|a_ij| >= 0.08 sqrt(|a_ii a_jj|)), piecewise-constant
  * prolongation, Galerkin coarse matrices added in a fixed order (deterministic), down to at most
- * 128 rows, inverted densely.  Applied as a symmetric FP32 V-cycle (damped Jacobi, weight 2/3, with
- * conf.amg_sweeps sweeps per side and a coarse correction scaled by 1.6 / 1.8) inside the
- * mixed-precision CG (precision MIXED, stop_rule TRUE_RELRES), which keeps the result at FP64 accuracy. */
+ * 128 rows, inverted densely.  Applied as an FP32 cycle (damped Jacobi, weight 2/3, with
+ * conf.amg_sweeps sweeps per side and a coarse correction scaled by 1.6 / 1.8; levels 1 and 2 solved
+ * by two flexible-CG steps each, a K-cycle) inside the mixed-precision CG (precision MIXED, stop_rule
+ * TRUE_RELRES), whose direction update is then the flexible one; the result keeps FP64 accuracy. */
 typedef struct {
     uint32_t levels;            /* levels including the finest */
     uint32_t dense_coarsest;    /* 1: the last level is applied through its dense inverse */
     uint32_t rows[16];
     uint64_t nnz[16];
     uint32_t mis_rounds;        /* synchronous rounds of the independent-set construction, all levels */
-    uint32_t reserved;
+    uint32_t setup_launches;    /* kernel launches of the set-up */
     double   seconds_setup;     /* wall time of the set-up */
+    uint32_t cycle_launches[2]; /* kernel launches of one cycle inside CG, with 1 / 2 smoothing sweeps */
 } rsg_amg_info;
 /* Build (or rebuild) A's hierarchy from A's current values; info may be NULL. */
 RSG_API rsg_status rsg_amg_setup(rsg_context *ctx, rsg_csr *A, rsg_amg_info *info);

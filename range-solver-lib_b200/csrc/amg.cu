@@ -140,6 +140,18 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(const uint32_t *__r
     }
 }
 
+// Launch accounting: every kernel launch of this file is counted (rsg_amg_info reports the set-up's
+// launches); a dry run of the cycle skips its launches and only counts them.
+thread_local uint32_t t_launches = 0;
+thread_local bool t_dry = false;
+inline void count_launch() { ++t_launches; }
+template <class... P, class... A>
+void amg_launch(cudaStream_t stream, bool pdl, void (*k)(P...), dim3 grid, int block, size_t smem, A &&...args)
+{
+    ++t_launches;
+    if (!t_dry) launch_k(stream, pdl, k, grid, block, smem, std::forward<A>(args)...);
+}
+
 // Exclusive scan of in[0..n) into out[0..n]; the total lands in *total_dev (device word).
 rsg_status scan_u32(rsg_context *ctx, AmgHierarchy *H, const uint32_t *in, uint32_t n, uint32_t *out)
 {
@@ -149,8 +161,11 @@ rsg_status scan_u32(rsg_context *ctx, AmgHierarchy *H, const uint32_t *in, uint3
         return RSG_OK;
     }
     if (!H->scan_blocks.ensure(nb)) return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: scan workspace");
+    count_launch();
     k_scan_tiles<<<nb, kScanThreads, 0, ctx->stream>>>(in, n, H->scan_blocks.p);
+    count_launch();
     k_scan_sums<<<1, kScanThreads, 0, ctx->stream>>>(H->scan_blocks.p, nb);
+    count_launch();
     k_scan_apply<<<nb, kScanThreads, 0, ctx->stream>>>(in, n, H->scan_blocks.p, out);
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
     return RSG_OK;
@@ -1228,11 +1243,14 @@ rsg_status build_aggregates(rsg_context *ctx, AmgHierarchy *H, AmgLevel &F, uint
         !H->u1.ensure(size_t(n) + 1) || !H->u2.ensure(size_t(n) + 1) || !H->u3.ensure(size_t(n) + 1) ||
         !F.agg.ensure(n))
         return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: set-up workspace");
+    count_launch();
     k_amg_strength<<<grid_groups(n), kBlock, 0, s>>>(n, F.rp, F.ci, F.val, F.diag.p, kAmgTheta, H->smask.p);
+    count_launch();
     k_amg_mis_init<<<g, kBlock, 0, s>>>(n, H->T.p);
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
     if (n <= kMisCtaRows) {  // a small level: every round in one CTA, one synchronisation
         RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->flags + 10, 0, 2 * sizeof(unsigned int), s));
+        count_launch();
         k_amg_mis_cta<<<1, kMisCtaThreads, 0, s>>>(n, F.rp, F.ci, H->smask.p, H->T.p, H->M1.p, H->flags + 10);
         RSG_CHECK_CUDA(ctx, cudaGetLastError());
         RSG_TRY(read_flags(ctx, H, 12));
@@ -1250,7 +1268,9 @@ rsg_status build_aggregates(rsg_context *ctx, AmgHierarchy *H, AmgLevel &F, uint
         for (;;) {
             for (uint32_t k = 0; k < kRoundBatch; k++, round++) {
                 const unsigned int *prev = round ? H->rounds.p + round - 1 : nullptr;
+                count_launch();
                 k_amg_nbmax<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, H->smask.p, H->T.p, H->M1.p, H->u3.p, round, prev);
+                count_launch();
                 k_amg_mis_round2<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, H->smask.p, H->M1.p, H->T.p, H->u3.p, round,
                                                       prev, H->rounds.p + round);
             }
@@ -1263,18 +1283,23 @@ rsg_status build_aggregates(rsg_context *ctx, AmgHierarchy *H, AmgLevel &F, uint
         H->mis_rounds += round;
     }
     // root numbering, joins
+    count_launch();
     k_amg_root_flags<<<g, kBlock, 0, s>>>(n, H->T.p, H->u1.p);
     RSG_TRY(scan_u32(ctx, H, H->u1.p, n, H->u2.p));
+    count_launch();
     k_amg_join1<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, H->smask.p, H->T.p, H->u2.p, H->u1.p);
     RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->flags, 0, 4 * sizeof(unsigned int), s));
+    count_launch();
     k_amg_join2<<<g, kBlock, 0, s>>>(n, F.rp, F.ci, H->smask.p, H->u1.p, F.agg.p, H->flags);
     // one synchronisation for the number of roots and the nodes left without an aggregate
     RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(H->flags_h + 8, H->u2.p + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     RSG_TRY(read_flags(ctx, H, 2));
     uint32_t nc = H->flags_h[8];
     if (H->flags_h[1] > 0) {  // singletons for nodes without any strong path to a root
+        count_launch();
         k_amg_unset_flags<<<g, kBlock, 0, s>>>(n, F.agg.p, H->u1.p);
         RSG_TRY(scan_u32(ctx, H, H->u1.p, n, H->u2.p));
+        count_launch();
         k_amg_singletons<<<g, kBlock, 0, s>>>(n, nc, H->u2.p, F.agg.p);
         nc += H->flags_h[1];
     }
@@ -1282,11 +1307,14 @@ rsg_status build_aggregates(rsg_context *ctx, AmgHierarchy *H, AmgLevel &F, uint
     if (!F.agg_ptr.ensure(size_t(nc) + 1) || !F.agg_rows.ensure(n) || !H->u3.ensure(size_t(nc) + 1))
         return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: aggregate lists");
     RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->u3.p, 0, size_t(nc) * sizeof(uint32_t), s));
+    count_launch();
     k_amg_count<<<g, kBlock, 0, s>>>(n, F.agg.p, H->u3.p);
     RSG_TRY(scan_u32(ctx, H, H->u3.p, nc, F.agg_ptr.p));
     RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->u3.p, 0, size_t(nc) * sizeof(uint32_t), s));
+    count_launch();
     k_amg_fill<<<g, kBlock, 0, s>>>(n, F.agg.p, F.agg_ptr.p, H->u3.p, F.agg_rows.p);
     RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->flags + 2, 0, 2 * sizeof(unsigned int), s));
+    count_launch();
     k_amg_sort_agg<<<grid_rows(nc), kBlock, 0, s>>>(nc, F.agg_ptr.p, F.agg_rows.p, F.rp, H->u3.p, H->flags);
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
     RSG_TRY(read_flags(ctx, H, 4));
@@ -1313,6 +1341,7 @@ rsg_status build_galerkin(rsg_context *ctx, AmgHierarchy *H, AmgLevel &F, AmgLev
     // one warp per coarse row; rows with more distinct columns than the warp kernel keeps fall back to
     // the sorting kernel (one CTA per row) for the whole level
     RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->flags + 5, 0, sizeof(unsigned int), s));
+    count_launch();
     k_amg_galerkin_warp<<<int(std::min<uint64_t>((nc + kGalWarps - 1) / kGalWarps, 65535ull * 8)), 32 * kGalWarps, 0,
                           s>>>(nc, F.agg_ptr.p, F.agg_rows.p, F.rp, F.ci, F.val, F.agg.p, H->u1.p, H->tcol.p,
                                H->tval.p, H->u2.p, H->flags);
@@ -1324,6 +1353,7 @@ rsg_status build_galerkin(rsg_context *ctx, AmgHierarchy *H, AmgLevel &F, AmgLev
     RSG_TRY(read_flags(ctx, H, 6));
     if (H->flags_h[5]) {
         cudaFuncSetAttribute(k_amg_galerkin, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        count_launch();
         k_amg_galerkin<<<nc, kGalThreads, smem, s>>>(nc, F.agg_ptr.p, F.agg_rows.p, F.rp, F.ci, F.val, F.agg.p,
                                                       H->u1.p, H->tcol.p, H->tval.p, H->u2.p);
         RSG_CHECK_CUDA(ctx, cudaGetLastError());
@@ -1333,6 +1363,7 @@ rsg_status build_galerkin(rsg_context *ctx, AmgHierarchy *H, AmgLevel &F, AmgLev
     const uint32_t nnz = H->flags_h[9];
     if (!Cl.own_ci.ensure(size_t(nnz) + 1) || !Cl.own_val.ensure(size_t(nnz) + 1) || !Cl.own_val32.ensure(size_t(nnz) + 1))
         return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: coarse matrix");
+    count_launch();
     k_amg_compact<<<grid_groups(nc), kBlock, 0, s>>>(nc, H->u1.p, H->u2.p, Cl.own_rp.p, H->tcol.p, H->tval.p,
                                                    Cl.own_ci.p, Cl.own_val.p, Cl.own_val32.p);
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
@@ -1354,6 +1385,7 @@ rsg_status level_vectors(rsg_context *ctx, AmgLevel &l, bool k_buffers)
     if (k_buffers && (!l.c1.ensure(l.n) || !l.c2.ensure(l.n) || !l.v1.ensure(l.n) || !l.v2.ensure(l.n) ||
                       !l.r2.ensure(l.n)))
         return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: K-cycle vectors");
+    count_launch();
     k_amg_diag<<<grid_rows(l.n), kBlock, 0, ctx->stream>>>(l.n, l.rp, l.ci, l.val, l.diag.p, l.dw.p);
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
     return RSG_OK;
@@ -1411,6 +1443,7 @@ AmgHierarchy *amg_of(const rsg_csr *A) { return static_cast<AmgHierarchy *>(A->a
 rsg_status amg_setup(rsg_context *ctx, rsg_csr *A)
 {
     const auto t0 = std::chrono::steady_clock::now();
+    const uint32_t launches0 = t_launches;
     AmgHierarchy *H = amg_of(A);
     if (!H) {
         H = new AmgHierarchy;
@@ -1456,11 +1489,23 @@ rsg_status amg_setup(rsg_context *ctx, rsg_csr *A)
             return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: coarse inverse");
         const size_t smem = size_t(last.n) * last.n * sizeof(double);
         cudaFuncSetAttribute(k_amg_dense_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        count_launch();
         k_amg_dense_inverse<<<1, 512, smem, ctx->stream>>>(last.n, last.rp, last.ci, last.val, H->coarse_inv.p);
         RSG_CHECK_CUDA(ctx, cudaGetLastError());
     }
     RSG_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     H->seconds_setup = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    H->setup_launches = t_launches - launches0;
+    // launches of one cycle as the CG loop applies it, for one and two sweeps (dry runs: nothing launched)
+    for (int nu = 1; nu <= 2; nu++) {
+        const uint32_t c0 = t_launches;
+        t_dry = true;
+        const rsg_status st = amg_vcycle(ctx, A, H, nullptr, H->L[0].x1.p, nullptr, nullptr, nu, nullptr, nullptr,
+                                         nullptr, 1, nullptr, true);
+        t_dry = false;
+        RSG_TRY(st);
+        H->cycle_launches[nu - 1] = t_launches - c0;
+    }
     return RSG_OK;
 }
 
@@ -1486,7 +1531,7 @@ template <int RPW, int SRC, int OUT, bool FINAL>
 void fine_sweep(rsg_context *ctx, const FineLaunch<RPW> &f, const SweepArgs &a, const float *qv, double *partials,
                 unsigned int *ticket, CgState *st, int mode, double *rz_out, bool pdl)
 {
-    launch_k(ctx->stream, pdl, k_amg_fine<RPW, SRC, OUT, FINAL>, f.grid, kBlock, f.smem, f.M, f.S, f.use_sell, a, qv,
+    amg_launch(ctx->stream, pdl, k_amg_fine<RPW, SRC, OUT, FINAL>, f.grid, kBlock, f.smem, f.M, f.S, f.use_sell, a, qv,
              partials, ticket, st, mode, rz_out);
 }
 
@@ -1497,7 +1542,7 @@ void fine_sweep(rsg_context *ctx, const FineLaunch<RPW> &f, const SweepArgs &a, 
 template <int SRC, int OUT>
 void coarse_sweep(rsg_context *ctx, const AmgLevel &l, const SweepArgs &a, const CgState *st, bool pdl)
 {
-    launch_k(ctx->stream, pdl, k_amg_coarse<SRC, OUT>, coarse_grid(ctx, l.n), kBlock, 0, l.n, l.rp, l.ci, l.val32, a,
+    amg_launch(ctx->stream, pdl, k_amg_coarse<SRC, OUT>, coarse_grid(ctx, l.n), kBlock, 0, l.n, l.rp, l.ci, l.val32, a,
              st);
 }
 
@@ -1505,7 +1550,7 @@ void coarse_sweep(rsg_context *ctx, const AmgLevel &l, const SweepArgs &a, const
 void down_restrict(rsg_context *ctx, const AmgHierarchy *H, int l, const CgState *st, bool pdl)
 {
     const AmgLevel &F = H->L[l], &C = H->L[l + 1];
-    launch_k(ctx->stream, pdl, k_amg_restrict, grid_rows(C.n), kBlock, 0, C.n, (const uint32_t *)F.agg_ptr.p,
+    amg_launch(ctx->stream, pdl, k_amg_restrict, grid_rows(C.n), kBlock, 0, C.n, (const uint32_t *)F.agg_ptr.p,
              (const uint32_t *)F.agg_rows.p, (const float *)F.r.p, (const float *)C.dw.p, C.b.p, C.x1.p, st);
 }
 
@@ -1552,7 +1597,7 @@ void res_restrict(rsg_context *ctx, const AmgHierarchy *H, int l, const float *b
 {
     const AmgLevel &F = H->L[l], &C = H->L[l + 1];
     const int g = std::max(1, std::min<int>(int((uint64_t(C.n) * 32 + kBlock - 1) / kBlock), ctx->num_sms * 8));
-    launch_k(ctx->stream, pdl, k_amg_res_restrict, g, kBlock, 0, C.n, (const uint32_t *)F.agg_ptr.p,
+    amg_launch(ctx->stream, pdl, k_amg_res_restrict, g, kBlock, 0, C.n, (const uint32_t *)F.agg_ptr.p,
              (const uint32_t *)F.agg_rows.p, F.rp, F.ci, F.val32, b, xs, (const float *)C.dw.p, C.b.p, C.x1.p, st);
 }
 
@@ -1568,8 +1613,8 @@ void cycle(rsg_context *ctx, const AmgHierarchy *H, int l, const float *b, float
     if (l + 1 == H->levels - 1 && H->dense_coarsest && F.n <= kBottomRows) {
         const BottomArgs B{F.n, C.n, F.rp, F.ci, F.agg.p, F.agg_ptr.p, F.agg_rows.p, F.val32, F.dw.p, H->coarse_inv.p,
                            b, F.x1.p, F.x2.p, out, sweeps == 2 ? kAmgScale2 : kAmgScale1};
-        if (sweeps == 2) launch_k(ctx->stream, pdl, k_amg_bottom<2>, 1, kBottomThreads, 0, B, st);
-        else launch_k(ctx->stream, pdl, k_amg_bottom<1>, 1, kBottomThreads, 0, B, st);
+        if (sweeps == 2) amg_launch(ctx->stream, pdl, k_amg_bottom<2>, 1, kBottomThreads, 0, B, st);
+        else amg_launch(ctx->stream, pdl, k_amg_bottom<1>, 1, kBottomThreads, 0, B, st);
         return;
     }
     if (sweeps == 2) {
@@ -1601,7 +1646,7 @@ void solve_level(rsg_context *ctx, const AmgHierarchy *H, int l, const float *b,
     const AmgLevel &F = H->L[l];
     if (l == H->levels - 1) {
         if (H->dense_coarsest) {
-            launch_k(ctx->stream, pdl, k_amg_dense_apply, 1, 1024, 0, F.n, (const float *)H->coarse_inv.p, b, e, st);
+            amg_launch(ctx->stream, pdl, k_amg_dense_apply, 1, 1024, 0, F.n, (const float *)H->coarse_inv.p, b, e, st);
         } else {  // coarsening stalled above the dense limit: nine damped-Jacobi sweeps from zero
             float *src = F.x1.p, *dst = F.x2.p, *bb = const_cast<float *>(b);
             for (int k = 0; k < 7; k++) {
@@ -1621,12 +1666,12 @@ void solve_level(rsg_context *ctx, const AmgHierarchy *H, int l, const float *b,
     double *sc = H->kc_sc.p + 8 * l;
     const int gs = coarse_grid(ctx, F.n), gv = grid_rows(F.n);
     cycle(ctx, H, l, b, F.c1.p, sweeps, st, pdl);
-    launch_k(ctx->stream, pdl, k_amg_kc_spmv<2>, gs, kBlock, 0, F.n, F.rp, F.ci, F.val32, (const float *)F.c1.p,
+    amg_launch(ctx->stream, pdl, k_amg_kc_spmv<2>, gs, kBlock, 0, F.n, F.rp, F.ci, F.val32, (const float *)F.c1.p,
              F.v1.p, b, (const float *)nullptr, H->kc_part.p, H->kc_ticket.p, sc, 0, 1, 0, st);
-    launch_k(ctx->stream, pdl, k_amg_kc_r2, gv, kBlock, 0, F.n, b, (const float *)F.v1.p, (const double *)sc,
+    amg_launch(ctx->stream, pdl, k_amg_kc_r2, gv, kBlock, 0, F.n, b, (const float *)F.v1.p, (const double *)sc,
              (const float *)F.dw.p, F.r2.p, F.x1.p, st);
     cycle(ctx, H, l, F.r2.p, F.c2.p, sweeps, st, pdl);
-    launch_k(ctx->stream, pdl, k_amg_kc_spmv<3>, gs, kBlock, 0, F.n, F.rp, F.ci, F.val32, (const float *)F.c2.p,
+    amg_launch(ctx->stream, pdl, k_amg_kc_spmv<3>, gs, kBlock, 0, F.n, F.rp, F.ci, F.val32, (const float *)F.c2.p,
              F.v2.p, (const float *)F.v1.p, (const float *)F.r2.p, H->kc_part.p, H->kc_ticket.p, sc, 2, 3, 4, st);
 }
 
@@ -1658,19 +1703,19 @@ rsg_status vcycle_typed(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *
 {
     const AmgLevel &F = H->L[0];
     if (!x0) {
-        launch_k(ctx->stream, pdl, k_amg_jacobi, grid_rows(F.n), kBlock, 0, F.n, (const float *)F.dw.p, r, F.x1.p,
+        amg_launch(ctx->stream, pdl, k_amg_jacobi, grid_rows(F.n), kBlock, 0, F.n, (const float *)F.dw.p, r, F.x1.p,
                  (const CgState *)st);
         x0 = F.x1.p;
     }
     if (H->levels < 2) {
         if (H->dense_coarsest)
-            launch_k(ctx->stream, pdl, k_amg_dense_apply, 1, 1024, 0, F.n, (const float *)H->coarse_inv.p, r, z,
+            amg_launch(ctx->stream, pdl, k_amg_dense_apply, 1, 1024, 0, F.n, (const float *)H->coarse_inv.p, r, z,
                      (const CgState *)st);
         else
-            launch_k(ctx->stream, pdl, k_amg_jacobi, grid_rows(F.n), kBlock, 0, F.n, (const float *)F.dw.p, r, z,
+            amg_launch(ctx->stream, pdl, k_amg_jacobi, grid_rows(F.n), kBlock, 0, F.n, (const float *)F.dw.p, r, z,
                      (const CgState *)st);
         const int g = std::min(grid_rows(F.n), kMaxGrid);
-        launch_k(ctx->stream, pdl, k_amg_rz, g, kBlock, 0, F.n, r, (const float *)z, q, partials, ticket, st, mode,
+        amg_launch(ctx->stream, pdl, k_amg_rz, g, kBlock, 0, F.n, r, (const float *)z, q, partials, ticket, st, mode,
                  rz_out);
         return RSG_OK;
     }
@@ -1695,14 +1740,14 @@ rsg_status vcycle_typed(rsg_context *ctx, const rsg_csr *A, const AmgHierarchy *
     // the coarse correction in its own streaming pass, so that the post-smoothing sweeps gather one vector
     const int gp = std::min(grid_rows(F.n), kMaxGrid);
     if (sweeps == 2) {
-        launch_k(ctx->stream, pdl, k_amg_prolong, gp, kBlock, 0, F.n, (const float *)x2, (const uint32_t *)F.agg.p, ec,
+        amg_launch(ctx->stream, pdl, k_amg_prolong, gp, kBlock, 0, F.n, (const float *)x2, (const uint32_t *)F.agg.p, ec,
                  ec2, kc, s, x1, (const CgState *)st);
         SweepArgs u1{r, F.dw.p, x1, nullptr, nullptr, 0.f, x2};
         fine_sweep<RPW, kSrcX, kOutSmooth, false>(ctx, f, u1, nullptr, partials, ticket, st, mode, rz_out, pdl);
         SweepArgs u2{r, F.dw.p, x2, nullptr, nullptr, 0.f, z};
         fine_sweep<RPW, kSrcX, kOutSmooth, true>(ctx, f, u2, q, partials, ticket, st, mode, rz_out, pdl);
     } else {
-        launch_k(ctx->stream, pdl, k_amg_prolong, gp, kBlock, 0, F.n, x0, (const uint32_t *)F.agg.p, ec, ec2, kc, s,
+        amg_launch(ctx->stream, pdl, k_amg_prolong, gp, kBlock, 0, F.n, x0, (const uint32_t *)F.agg.p, ec, ec2, kc, s,
                  x2, (const CgState *)st);
         SweepArgs u1{r, F.dw.p, x2, nullptr, nullptr, 0.f, z};
         fine_sweep<RPW, kSrcX, kOutSmooth, true>(ctx, f, u1, q, partials, ticket, st, mode, rz_out, pdl);
@@ -1771,7 +1816,10 @@ rsg_status rsg_amg_setup(rsg_context *ctx, rsg_csr *A, rsg_amg_info *info)
             info->nnz[l] = H->L[l].nnz;
         }
         info->mis_rounds = H->mis_rounds;
+        info->setup_launches = H->setup_launches;
         info->seconds_setup = H->seconds_setup;
+        info->cycle_launches[0] = H->cycle_launches[0];
+        info->cycle_launches[1] = H->cycle_launches[1];
     }
     return RSG_OK;
 }
@@ -1810,9 +1858,11 @@ rsg_status rsg_amg_apply(rsg_context *ctx, rsg_csr *A, const double *r, double *
     unsigned int *ticket = reinterpret_cast<unsigned int *>(scal + 4);
     RSG_CHECK_CUDA(ctx, cudaMemsetAsync(scal, 0, 8 * sizeof(double), ctx->stream));
     const int g = std::min(grid_rows(n), kMaxGrid);
+    count_launch();
     k_amg_d2f<<<g, kBlock, 0, ctx->stream>>>(n, r, L0.b.p);
     RSG_TRY(amg_vcycle(ctx, A, H, L0.b.p, nullptr, nullptr, L0.e.p, int(sweeps), partials, ticket, nullptr, 0, scal,
                        false));
+    count_launch();
     k_amg_f2d<<<g, kBlock, 0, ctx->stream>>>(n, L0.e.p, z);
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
     RSG_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

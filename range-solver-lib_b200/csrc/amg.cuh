@@ -4,8 +4,9 @@
 // (src/rmatrixpreconditioner.cpp).  The hierarchy is built on the GPU from the matrix's current
 // values (strength of connection, aggregates rooted at a distance-2 independent set of hashed
 // priorities, piecewise-constant prolongation, Galerkin coarse matrices summed in a fixed order,
-// dense inverse of the coarsest level) and applied as a symmetric FP32 V-cycle with damped-Jacobi
-// smoothing and a scaled coarse correction, so that CG sees one fixed SPD operator.
+// dense inverse of the coarsest level) and applied as an FP32 cycle with damped-Jacobi smoothing and a
+// scaled coarse correction; levels 1..kAmgKLevels are solved by two flexible-CG steps each (K-cycle),
+// so the outer CG uses the flexible direction update.
 #pragma once
 
 #include "krylov.cuh"
@@ -87,6 +88,8 @@ struct AmgHierarchy {
     unsigned int *flags_h = nullptr;  // pinned host copy
     double seconds_setup = 0.0;
     uint32_t mis_rounds = 0;
+    uint32_t setup_launches = 0;         // kernel launches of the last set-up
+    uint32_t cycle_launches[2] = {0, 0};  // kernel launches of one cycle inside CG, one / two sweeps
 };
 
 void amg_free(AmgHierarchy *H);

@@ -239,7 +239,7 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
         }
         a.P = P;
         a.amg = prec_type == RSG_PREC_AMG ? amg_of(A) : nullptr;
-        a.amg_sweeps = c.amg_sweeps == 1 ? 1 : 2;
+        a.amg_sweeps = c.amg_sweeps == 2 ? 2 : 1;
         if (a.amg) {
             a.P.d32 = amg_finest_weights(a.amg);  // omega / a_ii: the V-cycle's first smoothing step
             a.amg_x0 = amg_finest_x0(a.amg);

@@ -17,7 +17,8 @@ from . import _lib
 from ._lib import (BREAKDOWN, ERR_INVALID_ARG, ERR_SINGULAR, ERR_UNSUPPORTED, MEM_DEVICE, MEM_HOST, NOT_CONVERGED,
                    OK, PREC_AMG, PREC_BLOCK_JACOBI, PREC_JACOBI, PREC_LEARNED, PREC_NONE, PRECISION_FP64,
                    PRECISION_MIXED,
-                   SOLVER_CG, SOLVER_GMRES, STOP_REFERENCE, STOP_TRUE_RELRES, RsgError, SolverConf, Stats, Time)
+                   SOLVER_CG, SOLVER_GMRES, STOP_REFERENCE, STOP_TRUE_RELRES, RsgError, SolverConf, Stats, Time,
+                   EIGEN_ARNOLDI, EIGEN_LANCZOS, EIGEN_RAYLEIGH)
 
 __all__ = ["Context", "Matrix", "Assembly", "Batch", "make_conf", "RsgError", "SolverConf", "Stats", "Solver"]
 
@@ -39,7 +40,7 @@ def make_conf(solver: str | int = "cg", n_outer: int = 1000, n_inner: int = 30, 
               precision: str | int = "fp64", scale_equations: bool = True, reliable_delta: float = 1e-3,
               flexible: bool = False, use_graph: bool = True, check_interval: int = 16,
               output_frequency: int = 0, output_file: str | None = None,
-              l2_resident_f32: bool = False, autotune: bool = False, amg_sweeps: int = 2) -> SolverConf:
+              l2_resident_f32: bool = False, autotune: bool = False, amg_sweeps: int = 1) -> SolverConf:
     c = SolverConf()
     _lib.load().rsg_conf_default(C.byref(c))
     c.solver_type = solver if isinstance(solver, int) else {"cg": SOLVER_CG, "gmres": SOLVER_GMRES}[solver]
@@ -167,7 +168,25 @@ class Context:
         self.check(self.lib.rsg_amg_setup(self.h, A.h, C.byref(info)), "amg_setup")
         L = info.levels
         return {"levels": L, "dense_coarsest": bool(info.dense_coarsest), "rows": list(info.rows[:L]),
-                "nnz": list(info.nnz[:L]), "mis_rounds": info.mis_rounds, "seconds_setup": info.seconds_setup}
+                "nnz": list(info.nnz[:L]), "mis_rounds": info.mis_rounds, "seconds_setup": info.seconds_setup,
+                "setup_launches": info.setup_launches, "cycle_launches": list(info.cycle_launches)}
+
+    def eigen_solve(self, M: "Matrix", K: "Matrix", start, method: int = _lib.EIGEN_LANCZOS, n_eigen: int = 4,
+                    n_iterations: int = 100, cvg: float = 1e-8, mu0: float = 0.0, conf=None):
+        """Eigenvalues of the pencil (M, K) by REigenValueSolver's methods (rsg_eigen_solve): returns
+        (values, vectors or None, stats dict).  start: the n start values (the reference draws them
+        with rand() / RAND_MAX); conf: the linear solves' configuration (default: CG, Jacobi,
+        FP64 true relative residual 1e-12)."""
+        start = np.ascontiguousarray(start, np.float64)
+        ec = _lib.EigenConf(method=method, n_eigen=n_eigen, n_iterations=n_iterations, cvg=cvg, mu0=mu0)
+        conf = conf if conf is not None else make_conf(n_outer=100000, stop_rule="true", rtol=1e-12)
+        nv = 1 if method == _lib.EIGEN_RAYLEIGH else min(n_eigen, K.n)
+        values = np.empty(nv, np.float64)
+        vectors = None if method == _lib.EIGEN_LANCZOS else np.empty((nv, K.n), np.float64)
+        st = _lib.EigenStats()
+        self.check(self.lib.rsg_eigen_solve(self.h, M.h, K.h, C.byref(ec), C.byref(conf), _ptr(start), _ptr(values),
+                                            None if vectors is None else _ptr(vectors), C.byref(st)), "eigen_solve")
+        return values, vectors, {"n_values": st.n_values, "solves": st.solves, "iterations": st.iterations}
 
     def amg_level(self, A: "Matrix", level: int, n_rows: int, nnz: int, with_agg: bool = True):
         """(agg or None, row_ptr, col_idx, values) of one level of A's last hierarchy."""

@@ -127,9 +127,28 @@ class AmgInfo(C.Structure):
         ("rows", C.c_uint32 * 16),
         ("nnz", C.c_uint64 * 16),
         ("mis_rounds", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("setup_launches", C.c_uint32),
         ("seconds_setup", C.c_double),
+        ("cycle_launches", C.c_uint32 * 2),
     ]
+
+
+class EigenConf(C.Structure):
+    _fields_ = [
+        ("method", C.c_int32),
+        ("n_eigen", C.c_uint32),
+        ("n_iterations", C.c_uint32),
+        ("reserved", C.c_uint32),
+        ("cvg", C.c_double),
+        ("mu0", C.c_double),
+    ]
+
+
+class EigenStats(C.Structure):
+    _fields_ = [("n_values", C.c_uint32), ("solves", C.c_uint32), ("iterations", C.c_uint64)]
+
+
+EIGEN_LANCZOS, EIGEN_ARNOLDI, EIGEN_RAYLEIGH = 0, 1, 2
 
 
 class Time(C.Structure):
@@ -176,6 +195,8 @@ SIGNATURES = {
     "rsg_batch_autotune": (C.c_int, [_P, _P, C.POINTER(TuneInfo)]),
     "rsg_profile_kernel": (C.c_int, [_P, _P, C.c_int32, C.c_uint32, C.c_int32, _DP]),
     "rsg_amg_setup": (C.c_int, [_P, _P, C.POINTER(AmgInfo)]),
+    "rsg_eigen_solve": (C.c_int, [_P, _P, _P, C.POINTER(EigenConf), C.POINTER(SolverConf), _P, _P, _P,
+                                  C.POINTER(EigenStats)]),
     "rsg_amg_level": (C.c_int, [_P, _P, C.c_uint32, _P, _P, _P, _P]),
     "rsg_amg_apply": (C.c_int, [_P, _P, _P, _P, C.c_uint32]),
     "rsg_true_relres_noalloc": (C.c_int, [C.c_uint32, _P, _P, _P, _P, _P, _P, _P]),

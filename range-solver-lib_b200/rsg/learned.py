@@ -59,10 +59,12 @@ class Learned:
             raise ValueError(f"expected {self.n_params} values, got {v.size}")
         self.ctx.check(self.ctx.lib.rsg_learned_set_params(self.ctx.h, self.h, _ptr(v), which), "learned_set")
 
-    def save(self, path: str):
+    def save(self, path: str, with_adam: bool = True):
+        """Parameters (and, with_adam, the Adam moments to resume training) as a compressed .npz."""
         self._info()
-        np.savez(path, layers=self.layers, hidden=self.hidden, step=self.step, params=self.get(PARAMS),
-                 adam_m=self.get(ADAM_M), adam_v=self.get(ADAM_V))
+        extra = {"adam_m": self.get(ADAM_M), "adam_v": self.get(ADAM_V)} if with_adam else {}
+        np.savez_compressed(path, layers=self.layers, hidden=self.hidden, step=self.step, params=self.get(PARAMS),
+                            **extra)
 
     @classmethod
     def load(cls, ctx, path: str) -> "Learned":
@@ -71,8 +73,9 @@ class Learned:
         if int(d["hidden"]) != m.hidden:
             raise ValueError(f"checkpoint hidden width {int(d['hidden'])} != library width {m.hidden}")
         m.set(d["params"], PARAMS)
-        m.set(d["adam_m"], ADAM_M)
-        m.set(d["adam_v"], ADAM_V)
+        if "adam_m" in d.files:  # inference-only checkpoints carry the parameters alone
+            m.set(d["adam_m"], ADAM_M)
+            m.set(d["adam_v"], ADAM_V)
         ctx.check(ctx.lib.rsg_learned_set_step(m.h, int(d["step"])), "learned_set_step")
         m._info()
         return m

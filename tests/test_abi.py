@@ -59,7 +59,7 @@ def test_rsg_package_fails_loudly_without_library(tmp_path, monkeypatch):
 def test_struct_layouts_match_header(tmp_path):
     """The ctypes mirrors of the public structs have the C compiler's size and field offsets."""
     structs = {"rsg_solver_conf": _lib.SolverConf, "rsg_stats": _lib.Stats, "rsg_time": _lib.Time,
-               "rsg_tune_info": _lib.TuneInfo, "rsg_model_groups": _lib.ModelGroups}
+               "rsg_tune_info": _lib.TuneInfo, "rsg_model_groups": _lib.ModelGroups, "rsg_amg_info": _lib.AmgInfo}
     lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "rsg.h"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')

@@ -94,6 +94,17 @@ def test_amg_mixed_cg_matches_oracle(ctx, case, sweeps):
     # blocks and the hierarchy does not beat Jacobi there (measured 658 against 637 iterations)
 
 
+def test_amg_info_counts_launches(ctx):
+    A, _ = O.assemble_heat(W.heat_cube(30, sigma=1.5, seed=9, source="random"))
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    info = ctx.amg_setup(M)
+    c1, c2 = info["cycle_launches"]
+    # per level below the finest at least a restriction and a corrected sweep; two sweeps add launches
+    assert c1 >= 2 * (info["levels"] - 1) and c2 > c1
+    assert info["setup_launches"] >= 10 * (info["levels"] - 1)
+    assert ctx.amg_setup(M)["cycle_launches"] == [c1, c2]
+
+
 def test_amg_rejects_unsupported_modes(ctx):
     A, b = O.assemble_heat(W.heat_cube(6, sigma=1.0, seed=1, source="random"))
     M = ctx.matrix(A.rp, A.ci, A.val)

@@ -6,6 +6,8 @@ Tolerances: the FP32 CUDA-core forward matches the float64 oracle to 1e-5
 reach the FP64 true relative residual they were asked for.
 """
 
+import os
+
 import numpy as np
 import pytest
 
@@ -144,8 +146,19 @@ def test_checkpoint_roundtrip(ctx, torch_cuda, tmp_path):
     m2.apply(M, rd, z2)
     ctx.sync()
     assert torch.equal(z1, z2)
+    # an inference-only checkpoint carries the parameters alone and applies the same network
+    path2 = str(tmp_path / "params.npz")
+    m.save(path2, with_adam=False)
+    assert "adam_m" not in np.load(path2).files
+    m3 = RL.Learned.load(ctx, path2)
+    np.testing.assert_array_equal(m3.get(RL.PARAMS), m.get(RL.PARAMS))
+    z3 = torch.empty_like(rd)
+    m3.apply(M, rd, z3)
+    ctx.sync()
+    assert torch.equal(z1, z3)
     m.close()
     m2.close()
+    m3.close()
 
 
 @pytest.mark.parametrize("solver", ["cg", "gmres"])
@@ -221,3 +234,24 @@ def test_ablation_trained_network_cuts_iterations(ctx, torch_cuda):
     model.close()
     for asm, _ in keep:
         asm.close()
+
+
+def test_committed_model_cuts_iterations(ctx):
+    """The parameters shipped in rsg/models (trained by `bench.py --workload learned --train-seeds
+    1000 --save-model ...` on the 60^3 heat family) load, and flexible CG with them needs fewer
+    iterations than Jacobi-PCG on a held-out seed of the family at its own mesh size (2.7x fewer
+    on eight held-out seeds when measured), at the same FP64 true residual."""
+    path = os.path.join(os.path.dirname(RL.__file__), "models", "heat_family_60.npz")
+    model = RL.Learned.load(ctx, path)
+    assert model.layers == 6 and model.step > 0
+    base = W.heat_cube(60, sigma=1.0, seed=0, source="random")
+    p = W.reseed_heat(base, sigma=RL.family_sigma(7), seed=7)
+    A, b = O.assemble_heat(p)
+    M = ctx.matrix(A.rp, A.ci, A.val)
+    conf = rsg.make_conf(n_outer=20000, stop_rule="true", rtol=1e-10)
+    x_l, st_l = ctx.solve(M, b, conf=RL.learned_conf(model, conf), prec=rsg.PREC_LEARNED)
+    x_j, st_j = ctx.solve(M, b, conf=conf, prec=rsg.PREC_JACOBI)
+    assert st_l.converged == 1 and O.true_relres(A, b, x_l) <= 1e-10 * 1.01
+    assert st_j.converged == 1
+    assert st_l.iterations * 2 < st_j.iterations, (st_l.iterations, st_j.iterations)
+    model.close()
