@@ -318,3 +318,120 @@ def assemble_magnetostatics(p) -> tuple[CSR, np.ndarray]:
     h = lib().orc_assemble_magnetostatics(m.n_nodes, _ptr(xyz), m.n_tets, _ptr(tets), _ptr(j), _ptr(a), _ptr(book),
                                           p.n_free)
     return _system(h)
+
+
+# ---- eigenvalues of the pencil (M, K): REigenValueSolver restated (src/reigenvaluesolver.cpp) ----
+EIGEN_LANCZOS, EIGEN_ARNOLDI, EIGEN_RAYLEIGH = 0, 1, 2
+
+
+def _sdot(x: np.ndarray, y: np.ndarray) -> float:
+    """Sum of products in index order (RRVector::dot)."""
+    return float(np.cumsum(x * y)[-1]) if len(x) else 0.0
+
+
+def _qr_iteration(H: np.ndarray, n_iterations: int, cvg: float):
+    """qrDecomposition (src/reigenvaluesolver.cpp:499-592): unshifted QR iteration by classical
+    Gram-Schmidt, A <- R Q, V <- V Q, until every subdiagonal entry is at most cvg."""
+    m = H.shape[0]
+    A = H.copy()
+    V = np.zeros((m, m))
+    Q = np.zeros((m, m))
+    R = np.zeros((m, m))
+    for it in range(n_iterations):
+        for i in range(m):
+            a = A[:, i].copy()
+            u = a.copy()
+            for j in range(i):
+                e = Q[:, j]
+                u = u - _sdot(a, e) * e
+            nu = np.sqrt(_sdot(u, u))
+            if nu == 0.0:
+                raise RuntimeError("QR iteration met a dependent column")
+            Q[:, i] = u * (1.0 / nu)
+        for i in range(m):
+            e = Q[:, i]
+            for j in range(i, m):
+                R[i, j] = _sdot(A[:, j], e)
+        A = np.array([[_sdot(R[r, :], Q[:, c]) for c in range(m)] for r in range(m)])
+        V = Q.copy() if it == 0 else np.array([[_sdot(V[r, :], Q[:, c]) for c in range(m)] for r in range(m)])
+        if all(abs(A[i, i - 1]) <= cvg for i in range(1, m)):
+            break
+    return np.diag(A).copy(), V
+
+
+def eigen_solve(M: CSR, K: CSR, method: int, n_eigen: int, start: np.ndarray, *, mu0: float = 0.0,
+                n_iterations: int = 100, eig_cvg: float = 1e-8, **solve_kw):
+    """REigenValueSolver::solve restated (src/reigenvaluesolver.cpp:40-110 and the three methods);
+    every linear solve is the oracle's RMatrixSolver::solve with Jacobi and solve_kw, its x the
+    previous vector as in the reference.  start: the n start values (normalised here); eig_cvg: the
+    eigenvalue solver's own bound (QR subdiagonal, Rayleigh |mu - mu_old|).  Returns
+    (values, vectors or None, number of solves)."""
+    conf = make_conf(**solve_kw)
+    n = K.n
+    v = np.array(start, np.float64, copy=True)
+    v = v / np.sqrt(_sdot(v, v))
+    solves = 0
+    vec = None
+    if method == EIGEN_LANCZOS:  # :119-210; qlDecomposition (:420-497) leaves d unchanged
+        ne = min(n_eigen, n)
+        d, e = np.zeros(ne), np.zeros(ne + 1)
+        vo, w = np.zeros(n), np.zeros(n)
+        for i in range(ne):
+            b = spmv(M, v)
+            if i > 0:
+                b = b - spmv(K, vo) * e[i]
+            w, _ = solve(K, b, w, prec=1, conf=conf)
+            solves += 1
+            d[i] = _sdot(w, v)
+            if i + 1 < ne:
+                w = w - d[i] * v
+                e[i + 1] = np.sqrt(_sdot(w, w))
+                vo = v
+                v = w / e[i + 1]
+    elif method == EIGEN_ARNOLDI:  # :211-294
+        ne = min(n_eigen, n)
+        H = np.zeros((ne, ne))
+        Qa = np.zeros((n, ne))
+        Qa[:, 0] = v
+        q = v.copy()
+        for i in range(1, ne + 1):
+            q, _ = solve(K, spmv(M, Qa[:, i - 1].copy()), q, prec=1, conf=conf)
+            solves += 1
+            for j in range(i):
+                H[j, i - 1] = _sdot(Qa[:, j], q)
+                q = q - H[j, i - 1] * Qa[:, j]
+            if i < ne:
+                H[i, i - 1] = np.sqrt(_sdot(q, q))
+                Qa[:, i] = q / H[i, i - 1]
+        d, V = _qr_iteration(H, n_iterations, eig_cvg)
+        vec = (Qa @ V).T.copy()
+    else:  # Rayleigh quotient iteration, :295-392 (M and K on one pattern)
+        m2 = M.val.copy()
+        c, dd = np.zeros(n), np.zeros(n)
+        b = v
+        mu = mu0
+        for it in range(n_iterations):
+            muo = mu
+            kv = K.val * mu
+            m2 = np.where(kv != 0.0, m2 + kv, m2)
+            f = spmv(CSR(n, K.rp, K.ci, kv), b)
+            c, _ = solve(CSR(n, M.rp, M.ci, m2), f, c, prec=1, conf=conf)
+            f = f * (1.0 / np.sqrt(_sdot(c, c)))
+            b, _ = solve(M, f, b, prec=1, conf=conf)
+            kv = -1.0 * K.val * mu
+            m2 = np.where(kv != 0.0, m2 + kv, m2)
+            dd, _ = solve(K, spmv(CSR(n, M.rp, M.ci, m2), b), dd, prec=1, conf=conf)
+            solves += 3
+            mu = _sdot(dd, b) / _sdot(b, b)
+            if it > 0 and abs(muo - mu) < eig_cvg:
+                break
+        d = np.array([mu])
+        vec = b[None, :].copy()
+    if len(d) > 1:  # solve(), :90-110
+        d = np.abs(1.0 / d)
+        d[0], d[1] = d[1], d[0]
+        order = np.argsort(d, kind="stable")
+        d = d[order]
+        if vec is not None:
+            vec = vec[order]
+    return d, vec, solves

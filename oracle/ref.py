@@ -1,7 +1,8 @@
 """ctypes wrapper of the reference's own solver, compiled from its sources (TEST INFRASTRUCTURE ONLY).
 
 `make -C oracle ref` compiles the reference project's src/rmatrixsolver.cpp,
-src/rmatrixpreconditioner.cpp, src/riterationinfo.cpp and src/riterationinfovalue.cpp unchanged
+src/rmatrixpreconditioner.cpp, src/riterationinfo.cpp, src/riterationinfovalue.cpp and
+src/reigenvaluesolver.cpp unchanged
 against the stand-in headers in oracle/ref_shim/ into oracle/_ref/libref_solver.so (see
 oracle/ref_driver.cpp).  Only tests/ and bench.py's reference arm use it, as the checker of the
 oracle's restatement and of the CUDA library, and as the timed CPU baseline.  It is built where the
@@ -44,8 +45,37 @@ def lib():
         L.ref_solve.restype = C.c_int
         L.ref_solve.argtypes = [P, P, P, C.c_int, C.c_int, C.c_uint, C.c_uint, C.c_uint, C.c_double, C.c_char_p,
                                 C.c_int, C.POINTER(RefResult)]
+        L.ref_rand_start.argtypes = [C.c_uint, C.c_uint32, P, C.POINTER(C.c_double)]
+        L.ref_eigen.restype = C.c_int
+        L.ref_eigen.argtypes = [P, P, C.c_int, C.c_uint, C.c_uint, C.c_double, C.c_uint, C.c_uint, C.c_double,
+                                C.c_int, C.c_uint32, P, P, C.POINTER(RefResult)]
         _LIB = L
     return _LIB
+
+
+LANCZOS, ARNOLDI, RAYLEIGH = 0, 1, 2
+
+
+def rand_start(seed: int, n: int):
+    """The start vector and Rayleigh shift REigenValueSolver draws with rand() after srand(seed)."""
+    start = np.empty(n, np.float64)
+    mu = C.c_double()
+    lib().ref_rand_start(seed, n, _p(start), C.byref(mu))
+    return start, mu.value
+
+
+def eigen(M: "RefMatrix", K: "RefMatrix", method: int, n_eigen: int, *, n_iterations: int = 100,
+          cvg: float = 1e-8, seed: int = 1, n_outer: int = 100000, solver_cvg: float = 1e-13, threads: int = 1):
+    """REigenValueSolver::solve(M, K, d, ev) after srand(seed) -> (d, ev or None, RefResult)."""
+    nv = 1 if method == RAYLEIGH else min(n_eigen, K.n)
+    d = np.empty(nv, np.float64)
+    ev = np.zeros((nv, K.n), np.float64)
+    res = RefResult()
+    rc = lib().ref_eigen(M.h, K.h, method, n_eigen, n_iterations, cvg, seed, n_outer, solver_cvg, threads, nv,
+                         _p(d), _p(ev), C.byref(res))
+    if rc < 0:
+        raise RuntimeError(f"reference eigen solve failed: {res.message.decode(errors='replace')}")
+    return d[:rc], (None if method == LANCZOS else ev[:rc]), res
 
 
 def _p(a: np.ndarray):

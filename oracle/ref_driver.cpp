@@ -1,8 +1,8 @@
 // C driver around the reference's own solver sources (TEST INFRASTRUCTURE ONLY).
 //
 // oracle/Makefile's `ref` target compiles the reference project's src/rmatrixsolver.cpp,
-// src/rmatrixpreconditioner.cpp, src/riterationinfo.cpp and src/riterationinfovalue.cpp
-// unchanged, from where they lie, against the stand-in headers in oracle/ref_shim/ (range-base-lib,
+// src/rmatrixpreconditioner.cpp, src/riterationinfo.cpp, src/riterationinfovalue.cpp and
+// src/reigenvaluesolver.cpp unchanged, from where they lie, against the stand-in headers in oracle/ref_shim/ (range-base-lib,
 // range-model-lib and the few Qt classes they name are not part of the reference), together with
 // this file, into oracle/_ref/libref_solver.so.  Tests use it to check the oracle's restatement and
 // the CUDA library against the reference's own RMatrixSolver::solve; bench.py's reference arm
@@ -11,6 +11,7 @@
 // The iteration count and the last error come from RIterationInfo::printIteration, which reports
 // every iteration through RLogger::info when the output frequency is 1: the logger stand-in below
 // picks the values out of that one format's arguments.
+#include <algorithm>
 #include <chrono>
 #include <cstdarg>
 #include <cstdint>
@@ -23,6 +24,7 @@
 
 #include <omp.h>
 
+#include "reigenvaluesolver.h"
 #include "rmatrixsolver.h"
 
 namespace {
@@ -155,6 +157,59 @@ int ref_solve(void *handle, const double *b, double *x, int solver_type, int pre
         out->error = g_log.error;
         out->trend = g_log.trend;
         return 0;
+    } catch (const std::exception &e) {
+        std::snprintf(out->message, sizeof(out->message), "%s", e.what());
+        return -1;
+    }
+}
+
+// The start values REigenValueSolver draws (src/reigenvaluesolver.cpp:125-128, 222-225, 306-311)
+// after srand(seed): n values rand()/RAND_MAX, then (Rayleigh) the shift 1e9 rand()/RAND_MAX.
+void ref_rand_start(unsigned seed, uint32_t n, double *start, double *mu)
+{
+    std::srand(seed);
+    for (uint32_t i = 0; i < n; i++) start[i] = double(std::rand()) / double(RAND_MAX);
+    *mu = 1.0e9 * double(std::rand()) / double(RAND_MAX);
+}
+
+// REigenValueSolver::solve(M, K, d, ev) after srand(seed), its matrix solves configured as ref_solve
+// configures CG.  values: up to n_values doubles; vectors (may be NULL): rows of n doubles.
+// Returns the number of values, or -1 with the RError text in out->message.
+int ref_eigen(void *m_handle, void *k_handle, int method, unsigned n_eigen, unsigned n_iterations, double cvg,
+              unsigned seed, unsigned n_outer, double solver_cvg, int threads, uint32_t n_values, double *values,
+              double *vectors, ref_result *out)
+{
+    std::memset(out, 0, sizeof(*out));
+    struct TeamSize {
+        int prev = omp_get_max_threads();
+        ~TeamSize() { omp_set_num_threads(prev); }
+    } team;
+    if (threads > 0) omp_set_num_threads(threads);
+    const RSparseMatrix &M = *static_cast<RSparseMatrix *>(m_handle);
+    const RSparseMatrix &K = *static_cast<RSparseMatrix *>(k_handle);
+    try {
+        REigenValueSolverConf ec;
+        ec.method = REigenValueSolverConf::Method(method);
+        ec.setNEigenValues(n_eigen);
+        ec.setNIterations(n_iterations);
+        ec.setSolverCvgValue(cvg);
+        RMatrixSolverConf conf(RMatrixSolverConf::CG);
+        conf.setNOuterIterations(n_outer);
+        conf.setSolverCvgValue(solver_cvg);
+        conf.setOutputFrequency(1);
+        REigenValueSolver solver(ec, conf);
+        RRVector d;
+        RRMatrix ev;
+        std::srand(seed);
+        const auto t0 = std::chrono::steady_clock::now();
+        solver.solve(M, K, d, ev);
+        out->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        const uint32_t nd = std::min<uint32_t>(n_values, d.getNRows());
+        for (uint32_t i = 0; i < nd; i++) values[i] = d[i];
+        if (vectors)
+            for (uint32_t r = 0; r < std::min<uint32_t>(nd, ev.getNRows()); r++)
+                for (uint32_t c = 0; c < ev.getNColumns(); c++) vectors[size_t(r) * ev.getNColumns() + c] = ev[r][c];
+        return int(d.getNRows());
     } catch (const std::exception &e) {
         std::snprintf(out->message, sizeof(out->message), "%s", e.what());
         return -1;

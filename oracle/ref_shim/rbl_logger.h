@@ -10,6 +10,8 @@ class RLogger
         static void info(const char *format, ...) __attribute__((format(printf, 1, 2)));
         static void warning(const char *format, ...) __attribute__((format(printf, 1, 2)));
         static void error(const char *format, ...) __attribute__((format(printf, 1, 2)));
+        static void indent() {}
+        static void unindent() {}
 };
 
 #endif

@@ -1,7 +1,8 @@
 // Stand-ins for range-base-lib's RRVector and RRMatrix (TEST INFRASTRUCTURE): dense FP64 vector
-// and row-major matrix with the members the reference's solver sources call.  invert() is
-// Gauss-Jordan elimination with partial pivoting (range-base-lib's own method is not published
-// with the reference); a singular matrix throws RError.
+// and row-major matrix with the members the reference's solver and eigenvalue sources call.
+// invert() is Gauss-Jordan elimination with partial pivoting (range-base-lib's own method is not
+// published with the reference); a singular matrix throws RError.  dot / norm / mlt sum in index
+// order; normalize() divides by the norm.
 #ifndef REF_SHIM_RBL_RMATRIX_H
 #define REF_SHIM_RBL_RMATRIX_H
 
@@ -45,6 +46,23 @@ class RRVector
             for (double e : x.v) s += e * e;
             return std::sqrt(s);
         }
+
+        //! Sum of products in index order.
+        static double dot(const RRVector &x, const RRVector &y)
+        {
+            double s = 0.0;
+            for (size_t i = 0; i < x.v.size(); i++) s += x.v[i] * y.v[i];
+            return s;
+        }
+
+        //! Divides every element by the Euclidean norm (left as is when the norm is zero); returns the norm.
+        double normalize()
+        {
+            const double nrm = euclideanNorm(*this);
+            if (nrm != 0.0)
+                for (double &e : v) e /= nrm;
+            return nrm;
+        }
 };
 
 class RRMatrix
@@ -72,6 +90,27 @@ class RRMatrix
         void fill(double value)
         {
             for (RRVector &r : rows) r.fill(value);
+        }
+
+        void transpose()
+        {
+            RRMatrix t(nColumns, uint(rows.size()), 0.0);
+            for (uint i = 0; i < rows.size(); i++)
+                for (uint j = 0; j < nColumns; j++) t[j][i] = rows[i][j];
+            *this = t;
+        }
+
+        //! c = a b, each entry summed over the inner index in ascending order.
+        static void mlt(const RRMatrix &a, const RRMatrix &b, RRMatrix &c)
+        {
+            RRMatrix r(a.getNRows(), b.getNColumns(), 0.0);
+            for (uint i = 0; i < a.getNRows(); i++)
+                for (uint j = 0; j < b.getNColumns(); j++) {
+                    double s = 0.0;
+                    for (uint k = 0; k < a.getNColumns(); k++) s += a[i][k] * b[k][j];
+                    r[i][j] = s;
+                }
+            c = r;
         }
 
         void invert()

@@ -6,6 +6,7 @@
 
 #include <vector>
 
+#include "rbl_rmatrix.h"
 #include "rbl_utils.h"
 
 template <typename T>
@@ -25,6 +26,13 @@ class RSparseVector
             values.assign(val, val + n);
         }
         void setValue(uint position, const T &value) { values[position] = value; }
+        void insert(uint index, const T &value)
+        {
+            uint p = 0;
+            while (p < indexes.size() && indexes[p] < index) p++;
+            indexes.insert(indexes.begin() + p, index);
+            values.insert(values.begin() + p, value);
+        }
 };
 
 class RSparseMatrix
@@ -56,6 +64,37 @@ class RSparseMatrix
             return false;
         }
         double getValue(uint row, uint position) const { return rows[row].getValue(position); }
+
+        std::vector<uint> getRowIndexes(uint row) const
+        {
+            std::vector<uint> out(rows[row].size());
+            for (uint j = 0; j < out.size(); j++) out[j] = rows[row].getIndex(j);
+            return out;
+        }
+
+        //! Adds value to entry (row, column), inserting it in column order when it is not stored.
+        void addValue(uint row, uint column, double value)
+        {
+            uint position = 0;
+            if (findColumnPosition(row, column, position)) {
+                RSparseVector<double> &r = rows[row];
+                r.setValue(position, r.getValue(position) + value);
+            } else {
+                rows[row].insert(column, value);
+            }
+        }
+
+        //! y = A x, every row summed over its stored entries in column order.
+        static void mlt(const RSparseMatrix &a, const RRVector &x, RRVector &y)
+        {
+            y.resize(a.getNRows());
+            for (uint i = 0; i < a.getNRows(); i++) {
+                const RSparseVector<double> &r = a.rows[i];
+                double s = 0.0;
+                for (uint j = 0; j < r.size(); j++) s += r.getValue(j) * x[r.getIndex(j)];
+                y[i] = s;
+            }
+        }
 };
 
 #endif
