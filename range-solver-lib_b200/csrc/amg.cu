@@ -1025,12 +1025,56 @@ struct BottomArgs {
     float *x1, *x2, *out;
     float s;
 };
-template <int SWEEPS>
+// Words of shared memory the staged form needs (matrix, aggregate lists and the level's vectors).
+inline size_t bottom_stage_words(uint32_t n, uint32_t nc, uint64_t nnz) { return size_t(n) * 7 + 2 * nnz + nc + 8; }
+constexpr size_t kBottomStageBytes = 160 * 1024;
+
+// STAGE: the level's matrix, aggregate lists, diagonal weights and vectors are first copied into
+// shared memory by the whole CTA (the static parts before waiting on the previous kernel, so the
+// copy overlaps its tail), and every phase then reads shared memory instead of chaining L2 round
+// trips.  Same arithmetic either way.
+template <int SWEEPS, bool STAGE>
 __global__ void __launch_bounds__(kBottomThreads) k_amg_bottom(BottomArgs B, const CgState *st)
 {
-    pdl_wait();
-    pdl_release();
-    if (st && st->done) return;
+    extern __shared__ __align__(16) uint32_t stage[];
+    if (STAGE) {
+        const uint32_t n = B.n, nc = B.nc, nnz = B.rp[n] - B.rp[0], r0 = B.rp[0];
+        uint32_t *rp = stage, *ci = rp + n + 1, *agg = ci + nnz, *ptr = agg + n, *rows = ptr + nc + 1;
+        float *val = reinterpret_cast<float *>(rows + n), *dw = val + nnz, *b = dw + n, *x1 = b + n, *x2 = x1 + n;
+        for (uint32_t i = threadIdx.x; i <= n; i += blockDim.x) rp[i] = B.rp[i] - r0;
+        for (uint32_t j = threadIdx.x; j < nnz; j += blockDim.x) {
+            ci[j] = B.ci[r0 + j];
+            val[j] = B.val[r0 + j];
+        }
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            agg[i] = B.agg[i];
+            rows[i] = B.rows[i];
+            dw[i] = B.dw[i];
+        }
+        for (uint32_t i = threadIdx.x; i <= nc; i += blockDim.x) ptr[i] = B.ptr[i];
+        pdl_wait();
+        pdl_release();
+        if (st && st->done) return;
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            b[i] = B.b[i];
+            x1[i] = B.x1[i];
+        }
+        __syncthreads();
+        B.rp = rp;
+        B.ci = ci;
+        B.agg = agg;
+        B.ptr = ptr;
+        B.rows = rows;
+        B.val = val;
+        B.dw = dw;
+        B.b = b;
+        B.x1 = x1;
+        B.x2 = x2;
+    } else {
+        pdl_wait();
+        pdl_release();
+        if (st && st->done) return;
+    }
     __shared__ float sb[kAmgCoarsest], se[kAmgCoarsest];
     const uint32_t w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     float *b = const_cast<float *>(B.b);
@@ -1613,8 +1657,15 @@ void cycle(rsg_context *ctx, const AmgHierarchy *H, int l, const float *b, float
     if (l + 1 == H->levels - 1 && H->dense_coarsest && F.n <= kBottomRows) {
         const BottomArgs B{F.n, C.n, F.rp, F.ci, F.agg.p, F.agg_ptr.p, F.agg_rows.p, F.val32, F.dw.p, H->coarse_inv.p,
                            b, F.x1.p, F.x2.p, out, sweeps == 2 ? kAmgScale2 : kAmgScale1};
-        if (sweeps == 2) amg_launch(ctx->stream, pdl, k_amg_bottom<2>, 1, kBottomThreads, 0, B, st);
-        else amg_launch(ctx->stream, pdl, k_amg_bottom<1>, 1, kBottomThreads, 0, B, st);
+        const size_t sm = bottom_stage_words(F.n, C.n, F.nnz) * sizeof(uint32_t);
+        if (sm <= kBottomStageBytes) {
+            auto k = sweeps == 2 ? k_amg_bottom<2, true> : k_amg_bottom<1, true>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kBottomStageBytes));
+            amg_launch(ctx->stream, pdl, k, 1, kBottomThreads, sm, B, st);
+        } else {
+            amg_launch(ctx->stream, pdl, sweeps == 2 ? k_amg_bottom<2, false> : k_amg_bottom<1, false>, 1,
+                       kBottomThreads, 0, B, st);
+        }
         return;
     }
     if (sweeps == 2) {
