@@ -690,7 +690,8 @@ rsg_status gnn_forward(rsg_context *ctx, rsg_learned *G, const rsg_csr *A, const
         float *m = train ? G->m[l] : G->m[0];
         const float *W = G->params + off_layer(l), *b = W + size_t(K2) * H;
         k_gnn_spmm<<<gs, kBlock, 0, sm>>>(n, A->rp, A->ci, G->ew, hin, m);
-        if (tensor_cores) k_gnn_dense_tc<<<gt, 32 * kTcWarps, 0, sm>>>(n, hin, m, W, b, hout);
+        if (tensor_cores && train) RSG_TRY(gnn_train_dense_umma(ctx, n, hin, m, W, b, hout));
+        else if (tensor_cores) k_gnn_dense_tc<<<gt, 32 * kTcWarps, 0, sm>>>(n, hin, m, W, b, hout);
         else k_gnn_dense_f32<<<gf, kBlock, 0, sm>>>(n, hin, m, W, b, hout);
     }
     const float *hl = train ? G->h[G->L] : G->h[G->L & 1];
@@ -736,8 +737,13 @@ rsg_status gnn_loss_grad(rsg_context *ctx, rsg_learned *G, const rsg_csr *A, con
     float *g = G->gh, *g2 = G->gh2;
     for (int l = L - 1; l >= 0; l--) {
         const float *W = G->params + off_layer(l), *b = W + size_t(K2) * H;
-        k_gnn_layer_bwd<<<gb, 256, kBwdSmem, sm>>>(n, G->h[l], G->m[l], W, b, g, G->dz, g2, G->gm);
-        k_gnn_layer_wgrad<<<nb, kBlock, 0, sm>>>(n, G->h[l], G->m[l], G->dz, G->blk);
+        if (tensor_cores) {
+            RSG_TRY(gnn_train_bwd_umma(ctx, n, G->h[l], G->m[l], W, b, g, G->dz, g2, G->gm));
+            RSG_TRY(gnn_train_wgrad_umma(ctx, n, G->h[l], G->m[l], G->dz, G->blk, nb));
+        } else {
+            k_gnn_layer_bwd<<<gb, 256, kBwdSmem, sm>>>(n, G->h[l], G->m[l], W, b, g, G->dz, g2, G->gm);
+            k_gnn_layer_wgrad<<<nb, kBlock, 0, sm>>>(n, G->h[l], G->m[l], G->dz, G->blk);
+        }
         k_gnn_sum_blocks<<<32, kBlock, 0, sm>>>(G->blk, nb, K2 * H + H, G->grad + off_layer(l));
         // g_prev += W^T-graph gm (the graph weights are symmetric): reuse the SpMM into gm, then add
         k_gnn_spmm<<<gs, kBlock, 0, sm>>>(n, A->rp, A->ci, G->ew, G->gm, G->dz);

@@ -50,6 +50,15 @@ rsg_status gnn_loss_grad(rsg_context *ctx, rsg_learned *G, const rsg_csr *A, con
 rsg_status gnn_forward_umma(rsg_context *ctx, rsg_learned *G, const rsg_csr *A, const double *r, double *z,
                             const double *xyz, const float *rms);
 bool gnn_umma_setup(rsg_context *ctx, int *grid);
+// Training layers on the tensor cores (tcgen05, BF16 operands, FP32 accumulation; gnn_umma.cu):
+// h_out = h + relu([h, m] W + b); the data backward (dz = g [z + b > 0] to dz, g_prev = g + (dz W^T)[:, :H],
+// gm = (dz W^T)[:, H:]); the weight gradient as nblk blocks of partial sums (K2*H + H each).
+rsg_status gnn_train_dense_umma(rsg_context *ctx, uint32_t n, const float *h, const float *m, const float *W,
+                                const float *b, float *hout);
+rsg_status gnn_train_bwd_umma(rsg_context *ctx, uint32_t n, const float *hp, const float *m, const float *W,
+                              const float *b, const float *g, float *dz, float *gprev, float *gm);
+rsg_status gnn_train_wgrad_umma(rsg_context *ctx, uint32_t n, const float *hp, const float *m, const float *dz,
+                                float *blk, int nblk);
 void rsg_axpy_f32(rsg_context *ctx, size_t n, float a, const float *x, float *y);
 
 struct FcgResult {

@@ -360,4 +360,476 @@ rsg_status gnn_forward_umma(rsg_context *ctx, rsg_learned *G, const rsg_csr *A, 
     return RSG_OK;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Training on the 5th-generation tensor cores (BF16 operands, FP32 accumulation in TMEM).
+//   forward:  h_out = h + relu([h, m] W + b)                 (M=128 rows, N=64, K=128)
+//   backward: z = [h_prev, m] W (recomputed), dz = g [z + b > 0],
+//             [g_prev - g | g_m] = dz W^T                    (M=128 rows, N=128, K=64)
+//   weights:  dW = [h_prev, m]^T dz over a contiguous row range per CTA, accumulated in TMEM across
+//             its 128-row tiles                               (M=128 features, N=64, K=128 rows)
+// The activations stay FP32 in global memory; each tile is rounded to BF16 when it is staged.
+namespace {
+
+constexpr uint32_t kSBO64 = (H / 8) * 128;  // K = 64 tiles: 8 core matrices per 8-row group
+constexpr uint32_t kTile64Bytes = kTileRows * H * 2;  // 16 KB
+
+__device__ __forceinline__ uint32_t tile_off_s(uint32_t row, uint32_t k, uint32_t sbo)
+{
+    return (row >> 3) * sbo + (k >> 3) * kLBO + (row & 7) * 16 + (k & 7) * 2;
+}
+
+__device__ __forceinline__ uint64_t smem_desc_s(uint32_t saddr, uint32_t sbo)
+{
+    return uint64_t((saddr & 0x3FFFFu) >> 4) | (uint64_t(kLBO >> 4) << 16) | (uint64_t(sbo >> 4) << 32) |
+           (uint64_t(1) << 46);
+}
+
+// kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, both K-major, N and M as given
+__host__ __device__ constexpr uint32_t idesc_bf16(uint32_t m, uint32_t n)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((m >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16_id(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                             uint32_t accumulate)
+{
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t *slot, uint32_t cols)
+{
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
+                 "r"(cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_free(uint32_t tmem, uint32_t cols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(cols) : "memory");
+}
+
+// Stages rows r0 .. r0+127 of X = [a | b] (two n x 64 FP32 arrays) as a BF16 K-major A tile
+// (M = 128 rows, K = 128); rows past n are zero.
+__device__ __forceinline__ void stage_rows_ab(unsigned char *At, uint32_t r0, uint32_t n, const float *a,
+                                              const float *b)
+{
+    for (uint32_t e = threadIdx.x; e < kTileRows * (K2 / 8); e += blockDim.x) {
+        const uint32_t trow = e / (K2 / 8), k8 = e % (K2 / 8), row = r0 + trow;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (row < n) {
+            const float *src = k8 < H / 8 ? a + size_t(row) * H + k8 * 8 : b + size_t(row) * H + (k8 - H / 8) * 8;
+            const float4 x0 = *reinterpret_cast<const float4 *>(src);
+            const float4 x1 = *reinterpret_cast<const float4 *>(src + 4);
+            v = make_uint4(pack2(x0.x, x0.y), pack2(x0.z, x0.w), pack2(x1.x, x1.y), pack2(x1.z, x1.w));
+        }
+        *reinterpret_cast<uint4 *>(At + tile_off(trow, k8 * 8)) = v;
+    }
+}
+
+// B = W^T (N = 64 output columns x K = 128), BF16, K-major (W: K2 x H row-major)
+__device__ __forceinline__ void stage_wt(unsigned char *Bt, const float *W)
+{
+    for (int e = threadIdx.x; e < K2 * H; e += blockDim.x) {
+        const int k = e / H, c = e % H;
+        *reinterpret_cast<__nv_bfloat16 *>(Bt + tile_off(c, k)) = __float2bfloat16_rn(W[e]);
+    }
+}
+
+// forward: h_out = h + relu([h, m] W + b) for 128-row tiles (FP32 in and out)
+constexpr uint32_t kFwdOffB = kATileBytes;
+constexpr uint32_t kFwdOffBias = kFwdOffB + kBTileBytes;
+constexpr uint32_t kFwdOffBar = kFwdOffBias + H * 4;
+constexpr uint32_t kFwdOffTmem = kFwdOffBar + 16;
+constexpr uint32_t kFwdSmem = kFwdOffTmem + 16;
+
+__global__ void __launch_bounds__(kThreads) k_gnn_dense_umma(uint32_t n, const float *__restrict__ h,
+                                                              const float *__restrict__ m,
+                                                              const float *__restrict__ W,
+                                                              const float *__restrict__ bias,
+                                                              float *__restrict__ h_out, unsigned int *err)
+{
+    extern __shared__ __align__(1024) unsigned char sm[];
+    unsigned char *At = sm, *Bt = sm + kFwdOffB;
+    float *bs = reinterpret_cast<float *>(sm + kFwdOffBias);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + kFwdOffBar);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + kFwdOffTmem);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    stage_wt(Bt, W);
+    if (tid < H) bs[tid] = bias[tid];
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    if (warp == 0) tmem_alloc(tslot, kTmemCols);
+    fence_async_shared();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const uint32_t tiles = (n + kTileRows - 1) / kTileRows;
+    const int quarter = warp & 3, half = warp >> 2;
+    uint32_t phase = 0;
+    bool in_flight = false, failed = false;
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const uint32_t r0 = tile * kTileRows;
+        stage_rows_ab(At, r0, n, h, m);
+        fence_async_shared();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(At), b0 = smem_u32(Bt);
+#pragma unroll
+            for (int ks = 0; ks < K2 / 16; ks++)
+                umma_bf16(tmem, smem_desc(a0 + ks * 2 * kLBO), smem_desc(b0 + ks * 2 * kLBO), ks > 0 ? 1u : 0u);
+            umma_commit(bar);
+        }
+        in_flight = true;
+        const bool ok = mbar_wait(bar, phase, err);
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        in_flight = false;
+        phase ^= 1u;
+        tc_fence_after();
+        const uint32_t row = r0 + uint32_t(quarter * 32 + lane);
+        uint32_t v[32];
+        tmem_ld32(tmem + (uint32_t(quarter * 32) << 16) + uint32_t(half * 32), v);
+        if (row < n) {
+#pragma unroll
+            for (int c4 = 0; c4 < 8; c4++) {
+                const int c = half * 32 + c4 * 4;
+                const float4 hv = *reinterpret_cast<const float4 *>(h + size_t(row) * H + c);
+                float4 o;
+                o.x = hv.x + fmaxf(__uint_as_float(v[c4 * 4]) + bs[c], 0.f);
+                o.y = hv.y + fmaxf(__uint_as_float(v[c4 * 4 + 1]) + bs[c + 1], 0.f);
+                o.z = hv.z + fmaxf(__uint_as_float(v[c4 * 4 + 2]) + bs[c + 2], 0.f);
+                o.w = hv.w + fmaxf(__uint_as_float(v[c4 * 4 + 3]) + bs[c + 3], 0.f);
+                *reinterpret_cast<float4 *>(h_out + size_t(row) * H + c) = o;
+            }
+        }
+        tc_fence_before();
+        __syncthreads();  // the A tile and TMEM are free for the next tile
+    }
+    if (failed && in_flight && tid == 0) mbar_wait(bar, phase, nullptr);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_free(tmem, kTmemCols);
+    }
+}
+
+// backward (data): per 128-row tile, D1 = [h_prev, m] W^T-tile product (z without bias, TMEM
+// columns 0..63); dz = g [z + b > 0] (FP32 to dz_out, BF16 into A2); D2 = dz W^T (TMEM columns
+// 64..191): g_prev = g + D2[:, :64], gm = D2[:, 64:].
+constexpr uint32_t kBwdTmemCols = 256;
+constexpr uint32_t kBwOffB1 = kATileBytes;                  // W^T: N = 64 x K = 128
+constexpr uint32_t kBwOffA2 = kBwOffB1 + kBTileBytes;       // dz: M = 128 x K = 64
+constexpr uint32_t kBwOffB2 = kBwOffA2 + kTile64Bytes;      // W: N = 128 x K = 64
+constexpr uint32_t kBwOffBias = kBwOffB2 + K2 * H * 2;
+constexpr uint32_t kBwOffBar = kBwOffBias + H * 4;
+constexpr uint32_t kBwOffTmem = kBwOffBar + 16;
+constexpr uint32_t kBwdUmmaSmem = kBwOffTmem + 16;
+
+__global__ void __launch_bounds__(kThreads) k_gnn_bwd_umma(uint32_t n, const float *__restrict__ hp,
+                                                            const float *__restrict__ m, const float *__restrict__ W,
+                                                            const float *__restrict__ bias,
+                                                            const float *__restrict__ g, float *__restrict__ dz_out,
+                                                            float *__restrict__ gprev, float *__restrict__ gm,
+                                                            unsigned int *err)
+{
+    extern __shared__ __align__(1024) unsigned char sm[];
+    unsigned char *A1 = sm, *B1 = sm + kBwOffB1, *A2 = sm + kBwOffA2, *B2 = sm + kBwOffB2;
+    float *bs = reinterpret_cast<float *>(sm + kBwOffBias);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + kBwOffBar);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + kBwOffTmem);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    stage_wt(B1, W);
+    for (int e = tid; e < K2 * H; e += kThreads) {  // B2 = W (N = K2 input features x K = H outputs)
+        const int kin = e / H, c = e % H;
+        *reinterpret_cast<__nv_bfloat16 *>(B2 + tile_off_s(kin, c, kSBO64)) = __float2bfloat16_rn(W[e]);
+    }
+    if (tid < H) bs[tid] = bias[tid];
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    if (warp == 0) tmem_alloc(tslot, kBwdTmemCols);
+    fence_async_shared();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot, tmem2 = tmem + H;
+    const uint32_t tiles = (n + kTileRows - 1) / kTileRows;
+    const int quarter = warp & 3, half = warp >> 2;
+    constexpr uint32_t kId2 = idesc_bf16(kTileRows, K2);
+    uint32_t phase = 0;
+    bool in_flight = false, failed = false;
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const uint32_t r0 = tile * kTileRows;
+        const uint32_t trow = uint32_t(quarter * 32 + lane), row = r0 + trow;
+        stage_rows_ab(A1, r0, n, hp, m);
+        fence_async_shared();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(A1), b0 = smem_u32(B1);
+#pragma unroll
+            for (int ks = 0; ks < K2 / 16; ks++)
+                umma_bf16(tmem, smem_desc(a0 + ks * 2 * kLBO), smem_desc(b0 + ks * 2 * kLBO), ks > 0 ? 1u : 0u);
+            umma_commit(bar);
+        }
+        in_flight = true;
+        bool ok = mbar_wait(bar, phase, err);
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        in_flight = false;
+        phase ^= 1u;
+        tc_fence_after();
+        {  // dz = g [z + b > 0]
+            uint32_t v[32];
+            tmem_ld32(tmem + (uint32_t(quarter * 32) << 16) + uint32_t(half * 32), v);
+#pragma unroll
+            for (int c8 = 0; c8 < 4; c8++) {
+                const int cb = half * 32 + c8 * 8;
+                float d[8];
+#pragma unroll
+                for (int t = 0; t < 8; t++) {
+                    const int c = cb + t;
+                    d[t] = (row < n && __uint_as_float(v[c8 * 8 + t]) + bs[c] > 0.f) ? g[size_t(row) * H + c] : 0.f;
+                }
+                if (row < n) {
+                    float4 *dst = reinterpret_cast<float4 *>(dz_out + size_t(row) * H + cb);
+                    dst[0] = make_float4(d[0], d[1], d[2], d[3]);
+                    dst[1] = make_float4(d[4], d[5], d[6], d[7]);
+                }
+                *reinterpret_cast<uint4 *>(A2 + tile_off_s(trow, uint32_t(cb), kSBO64)) =
+                    make_uint4(pack2(d[0], d[1]), pack2(d[2], d[3]), pack2(d[4], d[5]), pack2(d[6], d[7]));
+            }
+        }
+        fence_async_shared();
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(A2), b0 = smem_u32(B2);
+#pragma unroll
+            for (int ks = 0; ks < H / 16; ks++)
+                umma_bf16_id(tmem2, smem_desc_s(a0 + ks * 2 * kLBO, kSBO64), smem_desc_s(b0 + ks * 2 * kLBO, kSBO64),
+                             kId2, ks > 0 ? 1u : 0u);
+            umma_commit(bar);
+        }
+        in_flight = true;
+        ok = mbar_wait(bar, phase, err);
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        in_flight = false;
+        phase ^= 1u;
+        tc_fence_after();
+#pragma unroll
+        for (int part = 0; part < 2; part++) {  // warp half covers D2 columns 64 half .. +64
+            const int cb = half * 64 + part * 32;
+            uint32_t v[32];
+            tmem_ld32(tmem2 + (uint32_t(quarter * 32) << 16) + uint32_t(cb), v);
+            if (row < n) {
+#pragma unroll
+                for (int c4 = 0; c4 < 8; c4++) {
+                    const int c = cb + c4 * 4;
+                    float4 o = make_float4(__uint_as_float(v[c4 * 4]), __uint_as_float(v[c4 * 4 + 1]),
+                                           __uint_as_float(v[c4 * 4 + 2]), __uint_as_float(v[c4 * 4 + 3]));
+                    if (c < H) {
+                        const float4 gv = *reinterpret_cast<const float4 *>(g + size_t(row) * H + c);
+                        o.x += gv.x;
+                        o.y += gv.y;
+                        o.z += gv.z;
+                        o.w += gv.w;
+                        *reinterpret_cast<float4 *>(gprev + size_t(row) * H + c) = o;
+                    } else {
+                        *reinterpret_cast<float4 *>(gm + size_t(row) * H + (c - H)) = o;
+                    }
+                }
+            }
+        }
+        tc_fence_before();
+        __syncthreads();  // A1, A2 and TMEM free for the next tile
+    }
+    if (failed && in_flight && tid == 0) mbar_wait(bar, phase, nullptr);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_free(tmem, kBwdTmemCols);
+    }
+}
+
+// weight gradient: dW = X^T dz (X = [h_prev, m]) and db = column sums of dz over a contiguous row
+// range per CTA, its 128-row tiles accumulated in one TMEM accumulator (M = 128 features,
+// N = 64 columns, K = 128 rows per tile); db in FP32 on CUDA cores, rows in order.  Output: one
+// block of K2*H + H partial sums per CTA (summed in CTA order by k_gnn_sum_blocks).
+constexpr uint32_t kWgOffB = kATileBytes;  // dz^T: N = 64 x K = 128 rows
+constexpr uint32_t kWgOffBar = kWgOffB + kBTileBytes;
+constexpr uint32_t kWgOffTmem = kWgOffBar + 16;
+constexpr uint32_t kWgUmmaSmem = kWgOffTmem + 16;
+
+__global__ void __launch_bounds__(kThreads) k_gnn_wgrad_umma(uint32_t n, const float *__restrict__ hp,
+                                                              const float *__restrict__ m, const float *__restrict__ dz,
+                                                              float *__restrict__ blk, unsigned int *err)
+{
+    extern __shared__ __align__(1024) unsigned char sm[];
+    unsigned char *At = sm, *Bt = sm + kWgOffB;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + kWgOffBar);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + kWgOffTmem);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t rows_per = (n + gridDim.x - 1) / gridDim.x;
+    const uint32_t r0 = min(n, blockIdx.x * rows_per), r1 = min(n, r0 + rows_per);
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    if (warp == 0) tmem_alloc(tslot, kTmemCols);
+    fence_async_shared();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    float db = 0.f;  // threads 0..63: column tid of db
+    uint32_t phase = 0;
+    bool in_flight = false, failed = false, any = false;
+    for (uint32_t t0 = r0; t0 < r1; t0 += kTileRows) {
+        const uint32_t cnt = min(uint32_t(kTileRows), r1 - t0);
+        // A = X^T (row = feature k2, k = tile row), B = dz^T (row = column c, k = tile row)
+        for (uint32_t e = tid; e < kTileRows * (K2 / 8); e += kThreads) {
+            const uint32_t rr = e / (K2 / 8), k8 = e % (K2 / 8);
+            float x[8];
+            if (rr < cnt) {
+                const float *src = k8 < H / 8 ? hp + size_t(t0 + rr) * H + k8 * 8 : m + size_t(t0 + rr) * H + (k8 - H / 8) * 8;
+                const float4 x0 = *reinterpret_cast<const float4 *>(src), x1 = *reinterpret_cast<const float4 *>(src + 4);
+                x[0] = x0.x; x[1] = x0.y; x[2] = x0.z; x[3] = x0.w; x[4] = x1.x; x[5] = x1.y; x[6] = x1.z; x[7] = x1.w;
+            } else {
+#pragma unroll
+                for (int t = 0; t < 8; t++) x[t] = 0.f;
+            }
+#pragma unroll
+            for (int t = 0; t < 8; t++)
+                *reinterpret_cast<__nv_bfloat16 *>(At + tile_off(k8 * 8 + t, rr)) = __float2bfloat16_rn(x[t]);
+        }
+        for (uint32_t e = tid; e < kTileRows * (H / 8); e += kThreads) {
+            const uint32_t rr = e / (H / 8), c8 = e % (H / 8);
+            float d[8];
+            if (rr < cnt) {
+                const float4 d0 = *reinterpret_cast<const float4 *>(dz + size_t(t0 + rr) * H + c8 * 8);
+                const float4 d1 = *reinterpret_cast<const float4 *>(dz + size_t(t0 + rr) * H + c8 * 8 + 4);
+                d[0] = d0.x; d[1] = d0.y; d[2] = d0.z; d[3] = d0.w; d[4] = d1.x; d[5] = d1.y; d[6] = d1.z; d[7] = d1.w;
+            } else {
+#pragma unroll
+                for (int t = 0; t < 8; t++) d[t] = 0.f;
+            }
+#pragma unroll
+            for (int t = 0; t < 8; t++)
+                *reinterpret_cast<__nv_bfloat16 *>(Bt + tile_off(c8 * 8 + t, rr)) = __float2bfloat16_rn(d[t]);
+        }
+        if (tid < H)
+            for (uint32_t rr = 0; rr < cnt; rr++) db += dz[size_t(t0 + rr) * H + tid];
+        fence_async_shared();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(At), b0 = smem_u32(Bt);
+#pragma unroll
+            for (int ks = 0; ks < kTileRows / 16; ks++)
+                umma_bf16(tmem, smem_desc(a0 + ks * 2 * kLBO), smem_desc(b0 + ks * 2 * kLBO),
+                          (any || ks > 0) ? 1u : 0u);
+            umma_commit(bar);
+        }
+        any = true;
+        in_flight = true;
+        const bool ok = mbar_wait(bar, phase, err);
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        in_flight = false;
+        phase ^= 1u;
+        tc_fence_before();
+        __syncthreads();  // the tiles are free for the next rows
+    }
+    float *out = blk + size_t(blockIdx.x) * (K2 * H + H);
+    if (!failed) {
+        tc_fence_after();
+        const int quarter = warp & 3, half = warp >> 2;
+        const uint32_t k2 = uint32_t(quarter * 32 + lane);
+        uint32_t v[32];
+        if (any) tmem_ld32(tmem + (uint32_t(quarter * 32) << 16) + uint32_t(half * 32), v);
+#pragma unroll
+        for (int j = 0; j < 32; j++) out[size_t(k2) * H + half * 32 + j] = any ? __uint_as_float(v[j]) : 0.f;
+        if (tid < H) out[K2 * H + tid] = db;
+    }
+    if (failed && in_flight && tid == 0) mbar_wait(bar, phase, nullptr);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_free(tmem, kTmemCols);
+    }
+}
+
+}  // namespace
+
+// Host wrappers of the training kernels (grids: persistent over tiles for the forward and the
+// data backward, gnn grad blocks for the weight gradient).
+static bool train_umma_attr(rsg_context *ctx)
+{
+    static bool done = false;
+    if (done) return true;
+    const std::pair<const void *, uint32_t> ks[] = {{(const void *)k_gnn_dense_umma, kFwdSmem},
+                                                    {(const void *)k_gnn_bwd_umma, kBwdUmmaSmem},
+                                                    {(const void *)k_gnn_wgrad_umma, kWgUmmaSmem}};
+    for (const auto &k : ks)
+        if (cudaFuncSetAttribute(k.first, cudaFuncAttributeMaxDynamicSharedMemorySize, int(k.second)) != cudaSuccess)
+            return false;
+    done = true;
+    return true;
+}
+
+rsg_status gnn_train_dense_umma(rsg_context *ctx, uint32_t n, const float *h, const float *m, const float *W,
+                                const float *b, float *hout)
+{
+    if (!train_umma_attr(ctx)) return set_error(ctx, RSG_ERR_CUDA, "learned: tensor-core training set-up");
+    const uint32_t tiles = (n + kTileRows - 1) / kTileRows;
+    const int g = int(std::max<uint32_t>(1, std::min<uint32_t>(tiles, uint32_t(ctx->num_sms) * 4)));
+    k_gnn_dense_umma<<<g, kThreads, kFwdSmem, ctx->stream>>>(n, h, m, W, b, hout, ctx->errw);
+    RSG_CHECK_CUDA(ctx, cudaGetLastError());
+    return RSG_OK;
+}
+
+rsg_status gnn_train_bwd_umma(rsg_context *ctx, uint32_t n, const float *hp, const float *m, const float *W,
+                              const float *b, const float *g, float *dz, float *gprev, float *gm)
+{
+    if (!train_umma_attr(ctx)) return set_error(ctx, RSG_ERR_CUDA, "learned: tensor-core training set-up");
+    const uint32_t tiles = (n + kTileRows - 1) / kTileRows;
+    const int gr = int(std::max<uint32_t>(1, std::min<uint32_t>(tiles, uint32_t(ctx->num_sms) * 2)));
+    k_gnn_bwd_umma<<<gr, kThreads, kBwdUmmaSmem, ctx->stream>>>(n, hp, m, W, b, g, dz, gprev, gm, ctx->errw);
+    RSG_CHECK_CUDA(ctx, cudaGetLastError());
+    return RSG_OK;
+}
+
+rsg_status gnn_train_wgrad_umma(rsg_context *ctx, uint32_t n, const float *hp, const float *m, const float *dz,
+                                float *blk, int nblk)
+{
+    if (!train_umma_attr(ctx)) return set_error(ctx, RSG_ERR_CUDA, "learned: tensor-core training set-up");
+    k_gnn_wgrad_umma<<<nblk, kThreads, kWgUmmaSmem, ctx->stream>>>(n, hp, m, dz, blk, ctx->errw);
+    RSG_CHECK_CUDA(ctx, cudaGetLastError());
+    return RSG_OK;
+}
+
 }  // namespace rsg

@@ -2,7 +2,8 @@
 
 Tolerances: the FP32 CUDA-core forward matches the float64 oracle to 1e-5
 (relative 2-norm); the BF16 tensor-core forward to 3e-2; the FP32 gradient to
-2e-3 (norm-wise, per parameter block).  Solves with the learned preconditioner
+2e-3 (norm-wise, per parameter block); the tcgen05 (BF16) gradient to 3e-2 per
+block and 5e-3 overall.  Solves with the learned preconditioner
 reach the FP64 true relative residual they were asked for.
 """
 
@@ -111,6 +112,13 @@ def test_gradient_matches_oracle(ctx, model, torch_cuda):
     for name, a, b in _blocks(3):
         assert rel_err(g[a:b], want_g[a:b]) < 2e-3, name
     assert rel_err(g, want_g) < 1e-3
+    # the tcgen05 path: BF16 operands (8-bit mantissa) in the forward, data-backward and weight-gradient
+    # products, FP32 accumulation.  Measured on B200: loss 7e-6, gradient 1.7e-3, worst block 1.2e-2.
+    loss_t, g_t = model.loss_grad(M, rd, xd, tensor_cores=True)
+    assert abs(loss_t - want_loss) / want_loss < 1e-4
+    for name, a, b in _blocks(3):
+        assert rel_err(g_t[a:b], want_g[a:b]) < 3e-2, name
+    assert rel_err(g_t, want_g) < 5e-3
 
 
 def test_train_step_reduces_loss(ctx, torch_cuda):
