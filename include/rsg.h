@@ -93,7 +93,10 @@ typedef struct {
     int32_t  autotune;          /* 1: autotune A's launch shapes on its first solve (rsg_autotune, with the
                                    cache file named by the RSG_TUNE_CACHE environment variable if set) */
     int32_t  amg_sweeps;        /* RSG_PREC_AMG: damped-Jacobi sweeps per side of the cycle, 1 or 2 (0: 1) */
-    int32_t  reserved[4];
+    int32_t  persistent;        /* CG with none / Jacobi in graph mode: run the loop as one persistent cooperative
+                                   kernel (same results bit for bit): 0 = for systems up to 131,072 rows,
+                                   1 = whenever the device allows it, -1 = never */
+    int32_t  reserved[3];
 } rsg_solver_conf;
 
 typedef struct {

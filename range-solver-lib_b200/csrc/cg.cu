@@ -687,7 +687,18 @@ rsg_status run_typed(rsg_context *ctx, const CgArgs &a, double *seconds)
     launch_init<RPW, PK>(ctx, a, L);
     RSG_CHECK_CUDA(ctx, cudaGetLastError());
 
-    if (a.use_graph) {
+    const bool persist_ok = a.use_graph && (PK == 0 || PK == 1) && a.A->use_sell && a.persistent >= 0 &&
+                            (a.persistent > 0 || a.A->n <= kPersistRows);
+    bool persisted = false;
+    if (persist_ok)
+        RSG_TRY(cg_persist_run(ctx, a, a.mixed ? L.g_dir32 : L.g_dir64, a.mixed ? L.g_upd32 : L.g_upd64, L.g_spmv64,
+                               &persisted));
+    if (persisted) {
+        if (a.mixed) k_mx_fold<<<L.g_vec, kBlock, 0, ctx->stream>>>(a.A->n, a.x, a.y32, a.st);
+        RSG_CHECK_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
+        const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) return set_error(ctx, RSG_ERR_CUDA, "solve: %s", cudaGetErrorString(e));
+    } else if (a.use_graph) {
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         const bool pdl = pdl_for(a.A, a.mixed);

@@ -37,6 +37,7 @@ struct rsg_context {
     double *pinned = nullptr;         // small pinned host buffer for readbacks (64 doubles)
     unsigned int *errw = nullptr;     // device word: set when a kernel's bounded wait ran out
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    double *persist = nullptr;        // persistent CG loop: phase partials and barrier words (cg_persist.cu)
 };
 
 struct rsg_csr {

@@ -87,6 +87,7 @@ void rsg_context_destroy(rsg_context *ctx)
     if (ctx->ws.base) cudaFree(ctx->ws.base);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     if (ctx->errw) cudaFree(ctx->errw);
+    if (ctx->persist) cudaFree(ctx->persist);
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);

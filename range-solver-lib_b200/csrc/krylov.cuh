@@ -64,6 +64,7 @@ struct CgArgs {
     const AmgHierarchy *amg;      // kind 3: the matrix's hierarchy
     int amg_sweeps;               // kind 3: smoothing sweeps per side of the V-cycle (1 or 2)
     float *amg_x0;                // kind 3: omega D^-1 r, written by the update / check kernels (P.d32 = omega / a_ii)
+    int persistent = 0;           // the loop as one cooperative kernel: 1 when possible, 0 small systems, -1 never
 };
 
 rsg_status autotune_run(rsg_context *ctx, rsg_csr *A, const char *cache_path);
@@ -93,6 +94,13 @@ void launch_k(cudaStream_t stream, bool pdl, void (*k)(P...), dim3 grid, int blo
 }
 
 rsg_status cg_run(rsg_context *ctx, const CgArgs &a, double *seconds);
+// The CG loop as one persistent cooperative kernel (cg_persist.cu), bit for bit the graph loop's
+// results with the same grids; *ran = false when it could not be launched (nothing was).
+rsg_status cg_persist_run(rsg_context *ctx, const CgArgs &a, int g_dir, int g_upd, int g_chk, bool *ran);
+// Rows up to which the loop runs persistent by default (conf.persistent = 0): measured per CG
+// iteration, graph loop -> persistent, FP64 / mixed: 8k rows 17.3 -> 12.2 / 17.1 -> 11.3 us;
+// 65k rows 18.4 -> 14.1 / 18.4 -> 12.4 us; 266k rows 29.0 -> 36.9 / 24.5 -> 24.4 us.
+constexpr uint32_t kPersistRows = 131072;
 
 // ---------------- state transitions (thread 0 of the last block) ----------------
 

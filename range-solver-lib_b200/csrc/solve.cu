@@ -219,6 +219,7 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
         a.q = arena_take<double>(ctx, n);
         a.mixed = mixed;
         a.use_graph = c.use_graph != 0;
+        a.persistent = c.persistent;
         a.check_interval = std::max<uint32_t>(2, c.check_interval);
         RSG_CHECK_CUDA(ctx, cudaMemsetAsync(a.p0, 0, size_t(n) * sizeof(double), ctx->stream));
         RSG_CHECK_CUDA(ctx, cudaMemsetAsync(a.p1, 0, size_t(n) * sizeof(double), ctx->stream));

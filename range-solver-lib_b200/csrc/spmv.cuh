@@ -413,12 +413,14 @@ __device__ __forceinline__ void ld4(const float *p, float (&v)[4])
     v[3] = a.w;
 }
 
+// The rows of virtual block vb of a grid of vgrid blocks (a persistent kernel runs several virtual
+// blocks per CTA with the same row assignment, and so the same sums, as a grid of vgrid blocks).
 template <typename V, class GX, class EPI>
-__device__ __forceinline__ void for_rows_sell(const Sell<V> &M, GX &gx, EPI &epi)
+__device__ __forceinline__ void for_rows_sell_v(const Sell<V> &M, GX &gx, EPI &epi, uint32_t vb, uint32_t vgrid)
 {
     const int lane = threadIdx.x & 31;
-    const uint32_t warps_total = gridDim.x * (blockDim.x >> 5);
-    for (uint32_t s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); s < M.n_slices; s += warps_total) {
+    const uint32_t warps_total = vgrid * (blockDim.x >> 5);
+    for (uint32_t s = vb * (blockDim.x >> 5) + (threadIdx.x >> 5); s < M.n_slices; s += warps_total) {
         const uint32_t row0 = s * 32u, row = row0 + lane;
         const bool valid = row < M.n;
         const uint32_t len = valid ? __ldg(&M.rp[row + 1]) - __ldg(&M.rp[row]) : 0u;
@@ -450,6 +452,12 @@ __device__ __forceinline__ void for_rows_sell(const Sell<V> &M, GX &gx, EPI &epi
         }
         if (valid) epi(row, acc);
     }
+}
+
+template <typename V, class GX, class EPI>
+__device__ __forceinline__ void for_rows_sell(const Sell<V> &M, GX &gx, EPI &epi)
+{
+    for_rows_sell_v<V>(M, gx, epi, blockIdx.x, gridDim.x);
 }
 
 template <typename V>

@@ -40,7 +40,8 @@ def make_conf(solver: str | int = "cg", n_outer: int = 1000, n_inner: int = 30, 
               precision: str | int = "fp64", scale_equations: bool = True, reliable_delta: float = 1e-3,
               flexible: bool = False, use_graph: bool = True, check_interval: int = 16,
               output_frequency: int = 0, output_file: str | None = None,
-              l2_resident_f32: bool = False, autotune: bool = False, amg_sweeps: int = 1) -> SolverConf:
+              l2_resident_f32: bool = False, autotune: bool = False, amg_sweeps: int = 1,
+              persistent: int = 0) -> SolverConf:
     c = SolverConf()
     _lib.load().rsg_conf_default(C.byref(c))
     c.solver_type = solver if isinstance(solver, int) else {"cg": SOLVER_CG, "gmres": SOLVER_GMRES}[solver]
@@ -63,6 +64,7 @@ def make_conf(solver: str | int = "cg", n_outer: int = 1000, n_inner: int = 30, 
     c.l2_resident_f32 = 1 if l2_resident_f32 else 0
     c.autotune = 1 if autotune else 0
     c.amg_sweeps = amg_sweeps
+    c.persistent = persistent
     return c
 
 

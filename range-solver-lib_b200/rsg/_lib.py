@@ -57,7 +57,8 @@ class SolverConf(C.Structure):
         ("l2_resident_f32", C.c_int32),
         ("autotune", C.c_int32),
         ("amg_sweeps", C.c_int32),
-        ("reserved", C.c_int32 * 4),
+        ("persistent", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 
