@@ -746,10 +746,17 @@ rsg_status run_typed(rsg_context *ctx, const CgArgs &a, double *seconds)
 
 namespace {
 
+// Evicts L2 by reading a buffer larger than it.  A read leaves clean lines behind; writing the
+// buffer instead left up to 126 MB of dirty lines whose write-back then overlapped the timed kernel
+// and was charged to it.  The store happens only if the XOR of the buffer hits one given value.
 __global__ void k_flush(uint4 *buf, size_t n16, unsigned int salt)
 {
-    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n16; i += size_t(gridDim.x) * blockDim.x)
-        buf[i] = make_uint4(salt, salt, salt, salt);
+    unsigned int acc = 0;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n16; i += size_t(gridDim.x) * blockDim.x) {
+        const uint4 v = buf[i];
+        acc ^= v.x ^ v.y ^ v.z ^ v.w;
+    }
+    if (acc == (salt | 0x80000000u) + 0x9e3779b9u) buf[0].x = acc;
 }
 
 template <int RPW>
