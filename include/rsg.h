@@ -205,6 +205,33 @@ RSG_API rsg_status rsg_solve_multi(rsg_context *ctx, rsg_csr *A, const rsg_solve
                                    uint32_t k, const double *B, double *X, int32_t memory, rsg_stats *per_rhs,
                                    rsg_stats *summary);
 
+/* ---- pattern-cached assembly of caller-computed element matrices ----
+ * Replaces RSolverFluid::buildSparseMatrixPattern / assemblyMatrix (src/rsolverfluid.cpp:2305-2419),
+ * the fluid solver's assembly of its element matrices (4 DOFs per node there; any count here).
+ * rsg_scatter_plan_create builds, on the host, the CSR pattern of every active element's enabled DOFs
+ * (rows and columns ascending, values zero) and, for every stored entry and every right-hand-side
+ * row, the list of element contributions in element order; rsg_scatter_assemble then forms the values
+ * on the GPU, one thread per entry adding its contributions in that order -- the order of the
+ * reference's serial element loop, so the result is the same bit for bit (no atomics).
+ * Mesh: element e has nodes elem_nodes[elem_begin[e] .. elem_begin[e+1]); elem_active[e] != 0 marks
+ * the elements the reference assembles (computable volumes, surfaces with a free-pressure condition).
+ * book[node * dofs_per_node + c]: the DOF's equation number (< n_free), or 0xffffffff when disabled.
+ * Ae / fe (host or device per `memory`): for every ACTIVE element in element order, its dense
+ * (dofs_per_node * nodes)^2 matrix (row-major, local DOF = node slot * dofs_per_node + component) and
+ * its (dofs_per_node * nodes) vector, concatenated; rsg_scatter_plan_info gives the two totals. */
+typedef struct rsg_scatter_plan rsg_scatter_plan;
+RSG_API rsg_status rsg_scatter_plan_create(rsg_context *ctx, uint32_t dofs_per_node, uint32_t n_elements,
+                                           const uint32_t *elem_begin, const uint32_t *elem_nodes,
+                                           const uint8_t *elem_active, uint32_t n_nodes, const uint32_t *book,
+                                           uint32_t n_free, rsg_scatter_plan **out);
+RSG_API rsg_status rsg_scatter_plan_info(const rsg_scatter_plan *plan, uint64_t *ae_values, uint64_t *fe_values,
+                                         uint64_t *nnz);
+/* A: created on the first call (*A == NULL), its values replaced afterwards (same pattern); b_device:
+ * n_free doubles, overwritten. */
+RSG_API rsg_status rsg_scatter_assemble(rsg_context *ctx, rsg_scatter_plan *plan, const double *Ae,
+                                        const double *fe, int32_t memory, rsg_csr **A, double *b_device);
+RSG_API void       rsg_scatter_plan_destroy(rsg_context *ctx, rsg_scatter_plan *plan);
+
 /* ---- eigenvalues of the pencil (M, K) ----
  * Replaces REigenValueSolver::solve (src/reigenvaluesolver.cpp:40-110) with its three methods:
  * Lanczos (:119-210, with qlDecomposition :420-497), Arnoldi (:211-294, with qrDecomposition

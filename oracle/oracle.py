@@ -90,6 +90,9 @@ def lib():
         L.orc_amg_free.argtypes = [_P]
         L.orc_node_book_generic.restype = C.c_uint32
         L.orc_node_book_generic.argtypes = [C.c_uint32, C.c_uint32, _P, _P, C.c_uint32, _P, _P, _P, _P, _P]
+        L.orc_scatter_assemble.restype = C.c_uint64
+        L.orc_scatter_assemble.argtypes = [C.c_uint32, C.c_uint32, _P, _P, _P, C.c_uint32, _P, C.c_uint32, _P, _P,
+                                           _P, _P, _P, _P]
         L.orc_node_book_stress.restype = C.c_uint32
         L.orc_node_book_stress.argtypes = [C.c_uint32, C.c_uint32, _P, _P, C.c_uint32, _P, _P, _P, _P, _P, _P]
         L.orc_system_n.restype = C.c_uint32
@@ -435,3 +438,22 @@ def eigen_solve(M: CSR, K: CSR, method: int, n_eigen: int, start: np.ndarray, *,
         if vec is not None:
             vec = vec[order]
     return d, vec, solves
+
+
+def scatter_assemble(d: int, elem_begin, elem_nodes, elem_active, n_nodes: int, book, n_free: int, Ae, fe):
+    """RSolverFluid::buildSparseMatrixPattern + assemblyMatrix (src/rsolverfluid.cpp:2305-2419) restated:
+    (CSR, b) of the active elements' blocks Ae / fe (concatenated in element order)."""
+    eb = np.ascontiguousarray(elem_begin, np.uint32)
+    en = np.ascontiguousarray(elem_nodes, np.uint32)
+    act = None if elem_active is None else np.ascontiguousarray(elem_active, np.uint8)
+    bk = np.ascontiguousarray(book, np.uint32)
+    ae = np.ascontiguousarray(Ae, np.float64)
+    fv = np.ascontiguousarray(fe, np.float64)
+    args = (d, len(eb) - 1, _ptr(eb), _ptr(en), None if act is None else _ptr(act), n_nodes, _ptr(bk), n_free)
+    nnz = lib().orc_scatter_assemble(*args, None, None, None, None, None, None)
+    rp = np.empty(n_free + 1, np.uint32)
+    ci = np.empty(nnz, np.uint32)
+    val = np.empty(nnz, np.float64)
+    b = np.empty(n_free, np.float64)
+    lib().orc_scatter_assemble(*args, _ptr(ae), _ptr(fv), _ptr(rp), _ptr(ci), _ptr(val), _ptr(b))
+    return CSR(n_free, rp, ci, val), b

@@ -13,6 +13,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <vector>
 
 namespace {
@@ -1318,5 +1319,57 @@ void orc_amg_apply(const orc_amg *h, const double *r, double *z, uint32_t sweeps
 }
 
 void orc_amg_free(orc_amg *h) { delete h; }
+
+// RSolverFluid::buildSparseMatrixPattern (src/rsolverfluid.cpp:2305-2397) and assemblyMatrix (:2399-2419):
+// rows as ordered maps column -> value; the pattern pass inserts zeros for every pair of an active
+// element's enabled DOFs, the assembly pass adds each active element's matrix and vector in element
+// order.  Ae / fe hold the active elements' blocks concatenated in element order.
+uint64_t orc_scatter_assemble(uint32_t d, uint32_t ne, const uint32_t *elem_begin, const uint32_t *elem_nodes,
+                              const uint8_t *elem_active, uint32_t n_nodes, const uint32_t *book, uint32_t n_free,
+                              const double *Ae, const double *fe, uint32_t *rp, uint32_t *ci, double *val, double *b)
+{
+    (void)n_nodes;
+    std::vector<std::map<uint32_t, double>> A(n_free);
+    std::vector<double> bp(n_free, 0.0);
+    std::vector<std::vector<uint32_t>> active(ne), vpos(ne);  // local DOF, equation row
+    for (uint32_t e = 0; e < ne; e++) {
+        if (elem_active && !elem_active[e]) continue;
+        for (uint32_t m = 0; m < elem_begin[e + 1] - elem_begin[e]; m++)
+            for (uint32_t i = 0; i < d; i++) {
+                const uint32_t mp = book[size_t(elem_nodes[elem_begin[e] + m]) * d + i];
+                if (mp == 0xffffffffu) continue;
+                active[e].push_back(m * d + i);
+                vpos[e].push_back(mp);
+            }
+        for (uint32_t r : vpos[e])
+            for (uint32_t c : vpos[e]) A[r].emplace(c, 0.0);
+    }
+    if (Ae && fe) {
+        size_t ae_off = 0, fe_off = 0;
+        for (uint32_t e = 0; e < ne; e++) {
+            if (elem_active && !elem_active[e]) continue;
+            const size_t nd = size_t(elem_begin[e + 1] - elem_begin[e]) * d;
+            for (size_t a = 0; a < active[e].size(); a++) {
+                bp[vpos[e][a]] += fe[fe_off + active[e][a]];
+                for (size_t c = 0; c < active[e].size(); c++)
+                    A[vpos[e][a]][vpos[e][c]] += Ae[ae_off + active[e][a] * nd + active[e][c]];
+            }
+            ae_off += nd * nd;
+            fe_off += nd;
+        }
+    }
+    uint64_t nnz = 0;
+    for (uint32_t r = 0; r < n_free; r++) {
+        if (rp) rp[r] = uint32_t(nnz);
+        for (const auto &kv : A[r]) {
+            if (ci) ci[nnz] = kv.first;
+            if (val) val[nnz] = kv.second;
+            nnz++;
+        }
+    }
+    if (rp) rp[n_free] = uint32_t(nnz);
+    if (b) std::copy(bp.begin(), bp.end(), b);
+    return nnz;
+}
 
 }  // extern "C"

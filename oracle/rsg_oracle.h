@@ -139,6 +139,13 @@ void orc_amg_level(const orc_amg *h, uint32_t level, uint32_t *agg, uint32_t *ro
 void orc_amg_apply(const orc_amg *h, const double *r, double *z, uint32_t sweeps);
 void orc_amg_free(orc_amg *h);
 
+/* RSolverFluid::buildSparseMatrixPattern + assemblyMatrix (src/rsolverfluid.cpp:2305-2419): the pattern
+ * of the active elements' enabled DOFs, then every active element's Ae / fe added in element order.
+ * Returns nnz; rp / ci / val / b are filled when non-NULL (call once with NULLs to size them). */
+uint64_t orc_scatter_assemble(uint32_t d, uint32_t n_elements, const uint32_t *elem_begin, const uint32_t *elem_nodes,
+                              const uint8_t *elem_active, uint32_t n_nodes, const uint32_t *book, uint32_t n_free,
+                              const double *Ae, const double *fe, uint32_t *rp, uint32_t *ci, double *val, double *b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -20,7 +20,7 @@ from ._lib import (BREAKDOWN, ERR_INVALID_ARG, ERR_SINGULAR, ERR_UNSUPPORTED, ME
                    SOLVER_CG, SOLVER_GMRES, STOP_REFERENCE, STOP_TRUE_RELRES, RsgError, SolverConf, Stats, Time,
                    EIGEN_ARNOLDI, EIGEN_LANCZOS, EIGEN_RAYLEIGH)
 
-__all__ = ["Context", "Matrix", "Assembly", "Batch", "make_conf", "RsgError", "SolverConf", "Stats", "Solver"]
+__all__ = ["Context", "Matrix", "Assembly", "ScatterPlan", "Batch", "make_conf", "RsgError", "SolverConf", "Stats", "Solver"]
 
 
 def _ptr(a) -> C.c_void_p:
@@ -488,6 +488,61 @@ class Assembly:
             self.A = None
         if self.h and self.ctx.h:
             self.ctx.lib.rsg_assembly_destroy(self.ctx.h, self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ScatterPlan:
+    """Pattern-cached assembly of caller-computed element matrices (rsg_scatter_plan):
+    RSolverFluid::buildSparseMatrixPattern / assemblyMatrix (src/rsolverfluid.cpp:2305-2419).  The plan
+    holds the pattern of the active elements' enabled DOFs and, per entry, its contributions in
+    element order; assemble() adds the element blocks on the GPU in that order."""
+
+    def __init__(self, ctx: Context, dofs_per_node: int, elem_begin, elem_nodes, elem_active, n_nodes: int, book,
+                 n_free: int):
+        self.ctx = ctx
+        eb = np.ascontiguousarray(elem_begin, np.uint32)
+        en = np.ascontiguousarray(elem_nodes, np.uint32)
+        act = None if elem_active is None else np.ascontiguousarray(elem_active, np.uint8)
+        bk = np.ascontiguousarray(book, np.uint32)
+        h = C.c_void_p()
+        ctx.check(ctx.lib.rsg_scatter_plan_create(ctx.h, dofs_per_node, len(eb) - 1, _ptr(eb), _ptr(en),
+                                                  None if act is None else _ptr(act), n_nodes, _ptr(bk), n_free,
+                                                  C.byref(h)), "scatter_plan_create")
+        self.h = h
+        ae, fe, nnz = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        ctx.check(ctx.lib.rsg_scatter_plan_info(h, C.byref(ae), C.byref(fe), C.byref(nnz)), "scatter_plan_info")
+        self.ae_values, self.fe_values, self.nnz, self.n_free = ae.value, fe.value, nnz.value, n_free
+        self.A: Matrix | None = None
+
+    def assemble(self, Ae, fe, b_dev=None) -> Matrix:
+        """Element blocks (host numpy arrays, or device tensors) -> the plan's matrix (created on first
+        use) and, when b_dev is given (device, n_free doubles), the right-hand side."""
+        dev = _is_device(Ae)
+        if not dev:
+            Ae = np.ascontiguousarray(Ae, np.float64)
+            fe = np.ascontiguousarray(fe, np.float64)
+        hA = C.c_void_p(self.A.h.value if self.A is not None else 0)
+        self.ctx.check(self.ctx.lib.rsg_scatter_assemble(self.ctx.h, self.h, _ptr(Ae), _ptr(fe),
+                                                         MEM_DEVICE if dev else MEM_HOST, C.byref(hA),
+                                                         _ptr(b_dev)), "scatter_assemble")
+        if self.A is None:
+            self.A = Matrix(self.ctx, hA)
+        else:
+            self.A.refresh_info()
+        return self.A
+
+    def close(self):
+        if self.A is not None:
+            self.A.close()
+            self.A = None
+        if self.h and self.ctx.h:
+            self.ctx.lib.rsg_scatter_plan_destroy(self.ctx.h, self.h)
         self.h = None
 
     def __del__(self):

@@ -221,6 +221,10 @@ SIGNATURES = {
                                              _PP]),
     "rsg_assembly_destroy": (None, [_P, _P]),
     "rsg_assembly_info": (C.c_int, [_P, _U32P, _U64P]),
+    "rsg_scatter_plan_create": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, _P, _P, C.c_uint32, _P, C.c_uint32, _PP]),
+    "rsg_scatter_plan_info": (C.c_int, [_P, _U64P, _U64P, _U64P]),
+    "rsg_scatter_assemble": (C.c_int, [_P, _P, _P, _P, C.c_int32, _PP, _P]),
+    "rsg_scatter_plan_destroy": (None, [_P, _P]),
     "rsg_assembly_scatter": (C.c_int, [_P, _P, _P, _P]),
     "rsg_assembly_create_magnetostatics": (C.c_int, [_P, C.c_uint32, _P, C.c_uint32, _P, _P, C.c_uint32, _P]),
     "rsg_assemble_magnetostatics": (C.c_int, [_P, _P, _P, _P, C.c_int32, _P, _P]),
