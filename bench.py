@@ -295,7 +295,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         A.update_values(val_pin)  # the reference re-reads A's values on every solve (src/rmatrixsolver.cpp:56-97)
-        xs, st_e = ctx.solve(A, b_pin, x_pin, conf=solvers[best][0], prec=solvers[best][1])
+        xs, st_e = ctx.solve(A, b_pin, x_pin, conf=solvers[best][0], prec=solvers[best][1], inplace=True)
         t1 = time.perf_counter()
         if i > 0:
             e2e.append(t1 - t0)

@@ -124,8 +124,10 @@ class Context:
 
     # ---- solve ----
     def solve(self, A: "Matrix", b, x=None, conf: SolverConf | None = None, prec: int = PREC_JACOBI,
-              block_size: int = 1, allow=(OK, NOT_CONVERGED, BREAKDOWN)):
-        """RMatrixSolver::solve: returns (x, Stats).  Device arrays are updated in place."""
+              block_size: int = 1, allow=(OK, NOT_CONVERGED, BREAKDOWN), inplace: bool = False):
+        """RMatrixSolver::solve: returns (x, Stats).  Device arrays are updated in place; a host x is
+        copied first unless inplace=True (then a C-contiguous float64 x is the in/out array itself, as
+        the C ABI's x is -- which keeps a pinned x pinned)."""
         conf = conf or make_conf()
         st = Stats()
         if _is_device(b):
@@ -135,7 +137,10 @@ class Context:
                                    C.byref(st))
         else:
             b = np.ascontiguousarray(b, np.float64)
-            x = np.zeros(A.n) if x is None else np.array(x, np.float64, copy=True)
+            if inplace and isinstance(x, np.ndarray) and x.dtype == np.float64 and x.flags.c_contiguous:
+                pass
+            else:
+                x = np.zeros(A.n) if x is None else np.array(x, np.float64, copy=True)
             s = self.lib.rsg_solve(self.h, A.h, C.byref(conf), prec, block_size, _ptr(b), _ptr(x), MEM_HOST,
                                    C.byref(st))
         self.check(s, "solve", allow)
