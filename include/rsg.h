@@ -62,7 +62,12 @@ typedef enum {
 
 typedef enum {
     RSG_PRECISION_FP64 = 0,     /* everything in FP64 */
-    RSG_PRECISION_MIXED = 1     /* FP32 inner Krylov, FP64 residual/solution (reliable updates) */
+    RSG_PRECISION_MIXED = 1,    /* FP32 inner Krylov, FP64 residual/solution (reliable updates) */
+    RSG_PRECISION_AUTO = 2      /* CG: mixed precision, continuing in FP64 from the current x when a residual
+                                   refresh finds the FP32 recurrence more than 2x off the true residual (stiff
+                                   systems, where FP32 matrix values cost iterations); TRUE_RELRES rule.  It
+                                   recovers part of mixed precision's loss there; FP64 stays the choice when
+                                   the system is known to be stiff */
 } rsg_precision;
 
 typedef enum { RSG_MEM_HOST = 0, RSG_MEM_DEVICE = 1 } rsg_memory;
@@ -113,7 +118,8 @@ typedef struct {
     int32_t  converged;
     int32_t  status;            /* rsg_status of the solve */
     uint32_t fallbacks;         /* learned preconditioner: steps that fell back to Jacobi */
-    uint32_t reserved[5];
+    uint32_t fp64_iterations;   /* RSG_PRECISION_AUTO: iterations run in FP64 after the switch (0: none) */
+    uint32_t reserved[4];
 } rsg_stats;
 
 typedef struct rsg_context rsg_context;

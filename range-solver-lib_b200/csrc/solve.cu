@@ -102,10 +102,14 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
     const bool learned = prec_type == RSG_PREC_LEARNED;
     if (learned) c.flexible = 1;
     if (c.autotune && !A->tune.valid) RSG_TRY(autotune_run(ctx, A, std::getenv("RSG_TUNE_CACHE")));
-    if (c.precision == RSG_PRECISION_MIXED && c.stop_rule != RSG_STOP_TRUE_RELRES)
+    if (c.precision == RSG_PRECISION_AUTO && (c.solver_type != RSG_SOLVER_CG || prec_type == RSG_PREC_AMG || learned))
+        return set_error(ctx, RSG_ERR_UNSUPPORTED, "precision AUTO is for CG with NONE, JACOBI or BLOCK_JACOBI");
+    if ((c.precision == RSG_PRECISION_MIXED || c.precision == RSG_PRECISION_AUTO) && c.stop_rule != RSG_STOP_TRUE_RELRES)
         return set_error(ctx, RSG_ERR_INVALID_ARG, "mixed precision requires stop_rule TRUE_RELRES");
+    if (c.precision < RSG_PRECISION_FP64 || c.precision > RSG_PRECISION_AUTO)
+        return set_error(ctx, RSG_ERR_INVALID_ARG, "Invalid precision '%d'", c.precision);
     const uint32_t n = A->n;
-    const bool mixed = c.precision == RSG_PRECISION_MIXED;
+    const bool mixed = c.precision == RSG_PRECISION_MIXED || c.precision == RSG_PRECISION_AUTO;
     const bool gmres = c.solver_type == RSG_SOLVER_GMRES;
     const uint32_t w = prec_type == RSG_PREC_BLOCK_JACOBI ? block_width(n, block_size) : 1;
     const uint32_t max_it = std::max<uint32_t>(c.n_outer, 1);
@@ -259,17 +263,45 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
         h.history = hist;
         h.trend_hist = thist;
         h.evict_first32 = c.l2_resident_f32 ? 0 : 1;
+        h.auto_switch = c.precision == RSG_PRECISION_AUTO ? 1 : 0;
+        const CgState h_init = h;
         RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(cst, &h, sizeof(h), cudaMemcpyHostToDevice, ctx->stream));
         RSG_TRY(cg_run(ctx, a, &solve_seconds));
         RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(&h, cst, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
         RSG_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-        st_out.iterations = h.it;
-        st_out.outer = h.n_updates;
+        uint32_t logged = h.it, outer = h.n_updates;
+        if (h.switched) {
+            // precision AUTO: the FP32 recurrence drifted -- continue in FP64 from the folded x with the
+            // iterations left (fresh directions; the history continues where it stopped)
+            const uint32_t used = h.it;
+            CgArgs a64 = a;
+            a64.mixed = false;
+            CgState h2 = h_init;
+            h2.auto_switch = 0;
+            h2.max_it = max_it > used ? max_it - used : 1;
+            h2.body_limit = h2.max_it / 2 + 16;
+            h2.history = hist ? hist + used : nullptr;
+            h2.trend_hist = thist ? thist + used : nullptr;
+            RSG_CHECK_CUDA(ctx, cudaMemsetAsync(a64.p0, 0, size_t(n) * sizeof(double), ctx->stream));
+            RSG_CHECK_CUDA(ctx, cudaMemsetAsync(a64.p1, 0, size_t(n) * sizeof(double), ctx->stream));
+            RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(cst, &h2, sizeof(h2), cudaMemcpyHostToDevice, ctx->stream));
+            double s2 = 0.0;
+            RSG_TRY(cg_run(ctx, a64, &s2));
+            solve_seconds += s2;
+            RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(&h, cst, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+            RSG_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            st_out.fp64_iterations = h.it;
+            logged = used + h.it;
+            outer += h.n_updates;
+        }
+        st_out.iterations = logged;
+        st_out.outer = outer;
         st_out.error = h.error;
         st_out.trend = h.trend;
         st_out.converged = h.converged;
         solve_status = h.ticket[7] ? RSG_ERR_TIMEOUT : rsg_status(h.status);
         if (want_hist) {
+            h.it = logged;
             std::vector<double> e(h.it), t(h.it);
             cudaMemcpy(e.data(), hist, h.it * sizeof(double), cudaMemcpyDeviceToHost);
             cudaMemcpy(t.data(), thist, h.it * sizeof(double), cudaMemcpyDeviceToHost);

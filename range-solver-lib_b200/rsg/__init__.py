@@ -16,7 +16,7 @@ import numpy as np
 from . import _lib
 from ._lib import (BREAKDOWN, ERR_INVALID_ARG, ERR_SINGULAR, ERR_UNSUPPORTED, MEM_DEVICE, MEM_HOST, NOT_CONVERGED,
                    OK, PREC_AMG, PREC_BLOCK_JACOBI, PREC_JACOBI, PREC_LEARNED, PREC_NONE, PRECISION_FP64,
-                   PRECISION_MIXED,
+                   PRECISION_MIXED, PRECISION_AUTO,
                    SOLVER_CG, SOLVER_GMRES, STOP_REFERENCE, STOP_TRUE_RELRES, RsgError, SolverConf, Stats, Time,
                    EIGEN_ARNOLDI, EIGEN_LANCZOS, EIGEN_RAYLEIGH)
 
@@ -53,7 +53,8 @@ def make_conf(solver: str | int = "cg", n_outer: int = 1000, n_inner: int = 30, 
                                                                  "true": STOP_TRUE_RELRES}[stop_rule]
     c.rtol = rtol
     c.precision = precision if isinstance(precision, int) else {"fp64": PRECISION_FP64,
-                                                                 "mixed": PRECISION_MIXED}[precision]
+                                                                 "mixed": PRECISION_MIXED,
+                                                                 "auto": PRECISION_AUTO}[precision]
     c.scale_equations = 1 if scale_equations else 0
     c.reliable_delta = reliable_delta
     c.flexible = 1 if flexible else 0

@@ -29,7 +29,7 @@ ERR_TIMEOUT = -6
 SOLVER_CG, SOLVER_GMRES = 0, 1
 PREC_NONE, PREC_JACOBI, PREC_BLOCK_JACOBI, PREC_LEARNED, PREC_AMG = 0, 1, 2, 3, 4
 STOP_REFERENCE, STOP_TRUE_RELRES = 0, 1
-PRECISION_FP64, PRECISION_MIXED = 0, 1
+PRECISION_FP64, PRECISION_MIXED, PRECISION_AUTO = 0, 1, 2
 MEM_HOST, MEM_DEVICE = 0, 1
 NOALLOC_MAX_ROWS = 2097152
 BC_DISPLACEMENT, BC_DISPLACEMENT_NORMAL, BC_DISPLACEMENT_ROLLER = 1, 2, 4
@@ -77,7 +77,8 @@ class Stats(C.Structure):
         ("converged", C.c_int32),
         ("status", C.c_int32),
         ("fallbacks", C.c_uint32),
-        ("reserved", C.c_uint32 * 5),
+        ("fp64_iterations", C.c_uint32),
+        ("reserved", C.c_uint32 * 4),
     ]
 
     def as_dict(self) -> dict:
