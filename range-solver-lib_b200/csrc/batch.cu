@@ -8,12 +8,17 @@
 // every 32-row SELL slice belongs to exactly one system.  Each system keeps its
 // own CG state (the same CgState and transitions as the single-system solver:
 // stop on FP64 true relative residual, FP64 or mixed precision with reliable
-// updates).  Per iteration the same three kernels as the single-system solver
-// run over all slices; slices of converged systems are skipped; each slice
-// writes its partial sums, and the warp that finishes a system's last slice
-// adds that system's slice partials in slice order and advances the system's
-// state.  The loop is one CUDA graph `while` node; the tail kernel keeps it
-// running while any system is active.
+// updates).  Per iteration the same three phases as the single-system solver
+// (direction + SpMV, update, residual check) run over the slices of a list of
+// systems: the active systems for the first two, and for the check only the
+// systems whose update asked for one (a refresh or a convergence claim) -- the
+// check is an FP64 SpMV, and spread over all active systems' slices its few
+// listed systems would leave most warps idle and a few working through long
+// runs of slices.  Each slice writes its partial sums; one block per listed
+// system then adds them in slice order and advances the system's state, and the
+// last of those blocks after an update builds the check list.  The loop is one
+// CUDA graph `while` node; the tail kernel rebuilds the active list and keeps
+// the loop running while any system is active.
 #include "krylov.cuh"
 
 #include <algorithm>
@@ -44,6 +49,7 @@ struct BatchCtl {
     uint32_t body_limit;
     int32_t timeout;
     int32_t pad;
+    uint32_t arrive;  // blocks of the update reduction that have finished (reset by the last)
 };
 
 struct BView {
@@ -59,6 +65,54 @@ struct Active {
     uint32_t *sys;       // [capacity]
     uint32_t *prefix;    // [capacity + 1]
 };
+
+// Block-wide (blockDim.x == kBlock): lists in order the systems in_sys[0..n_in) (0..n_in when in_sys
+// is null) that keep(system) accepts, with the exclusive prefix of their slice counts.  Every
+// thread calls it; keep must give the same answer on both of its calls.
+template <class KEEP>
+__device__ __forceinline__ void build_list(uint32_t n_in, const uint32_t *in_sys, const uint32_t *sys_slice,
+                                           Active *out, KEEP keep)
+{
+    __shared__ uint32_t cnt_sys[kBlock], cnt_sl[kBlock];
+    const uint32_t t = threadIdx.x, per = (n_in + blockDim.x - 1) / blockDim.x;
+    const uint32_t i0 = min(n_in, t * per), i1 = min(n_in, i0 + per);
+    uint32_t ns = 0, nsl = 0;
+    for (uint32_t i = i0; i < i1; i++) {
+        const uint32_t sys = in_sys ? in_sys[i] : i;
+        if (keep(sys)) {
+            ns++;
+            nsl += sys_slice[sys + 1] - sys_slice[sys];
+        }
+    }
+    cnt_sys[t] = ns;
+    cnt_sl[t] = nsl;
+    __syncthreads();
+    if (t == 0) {  // exclusive scan (blockDim entries)
+        uint32_t a = 0, b = 0;
+        for (uint32_t k = 0; k < blockDim.x; k++) {
+            const uint32_t x = cnt_sys[k], y = cnt_sl[k];
+            cnt_sys[k] = a;
+            cnt_sl[k] = b;
+            a += x;
+            b += y;
+        }
+        out->n_sys = a;
+        out->n_slices = b;
+        out->prefix[a] = b;
+    }
+    __syncthreads();
+    uint32_t o = cnt_sys[t], pre = cnt_sl[t];
+    for (uint32_t i = i0; i < i1; i++) {
+        const uint32_t sys = in_sys ? in_sys[i] : i;
+        if (keep(sys)) {
+            out->sys[o] = sys;
+            out->prefix[o] = pre;
+            pre += sys_slice[sys + 1] - sys_slice[sys];
+            o++;
+        }
+    }
+    __syncthreads();
+}
 
 // SELL row product of this lane's row in slice s.
 template <typename V, class GX>
@@ -144,32 +198,14 @@ __device__ __forceinline__ void batch_loop(const BView &B, const Active *L, CgSt
 }
 
 // One block per listed system: adds the system's slice partials in a fixed order
-// and applies the state transition `kind` (the same transitions as the
+// and applies the state transition KIND (the same transitions as the
 // single-system solver).
 enum RedKind { RED_INIT_RES = 0, RED_INIT_Z, RED_DIR64, RED_DIR32, RED_UPD64, RED_UPD32, RED_CHK64, RED_CHK32, RED_TRUE };
 
 template <int NV, int KIND>
-__global__ void __launch_bounds__(kBlock) bk_reduce(BView B, const Active *L, CgState *S, const double *part,
-                                                    double *relres)
+__device__ __forceinline__ void finalize(CgState *st, const double (&acc)[NV], double *relres, uint32_t sys)
 {
-    __shared__ double sh[NV * 32];
-    if (blockIdx.x >= L->n_sys) return;
-    const uint32_t sys = L->sys[blockIdx.x];
-    CgState *st = &S[sys];
-    const bool skip = (KIND == RED_INIT_RES || KIND == RED_TRUE) ? false
-                      : (KIND == RED_CHK64 || KIND == RED_CHK32) ? (st->done || !st->need_check)
-                                                                 : st->done != 0;
-    if (skip) return;
-    const uint32_t b0 = B.sys_slice[sys], b1 = B.sys_slice[sys + 1];
-    double acc[NV];
-#pragma unroll
-    for (int q = 0; q < NV; q++) acc[q] = 0.0;
-    for (uint32_t s = b0 + threadIdx.x; s < b1; s += blockDim.x)
-#pragma unroll
-        for (int q = 0; q < NV; q++) acc[q] += part[size_t(s) * NV + q];
-    block_sum<NV>(acc, sh);
-    if (threadIdx.x != 0) return;
-    if (KIND == RED_INIT_RES) {
+    if constexpr (KIND == RED_INIT_RES) {
         st->rn = sqrt(acc[0]);
         st->bn = sqrt(acc[1]);
         st->max_r = st->rn;
@@ -179,12 +215,12 @@ __global__ void __launch_bounds__(kBlock) bk_reduce(BView B, const Active *L, Cg
             st->converged = 1;
             st->status = isfinite(st->rn) ? RSG_OK : RSG_BREAKDOWN;
         }
-    } else if (KIND == RED_INIT_Z) {
+    } else if constexpr (KIND == RED_INIT_Z) {
         st->rho = st->rho_new = acc[0];
         st->beta = 0.0;
-    } else if (KIND == RED_DIR64 || KIND == RED_DIR32) {
+    } else if constexpr (KIND == RED_DIR64 || KIND == RED_DIR32) {
         double pq = acc[0];
-        if (KIND == RED_DIR32) {
+        if constexpr (KIND == RED_DIR32) {
             if (pq == 0.0) pq = 1e-300;
         } else {
             pq = clamp_pq(pq, st->eps);
@@ -193,17 +229,56 @@ __global__ void __launch_bounds__(kBlock) bk_reduce(BView B, const Active *L, Cg
         st->rho = st->rho_new;
         st->alpha = st->rho / pq;
         st->fold = 0;
-    } else if (KIND == RED_UPD64) {
+    } else if constexpr (KIND == RED_UPD64) {
         finalize_update64(st, acc[0], acc[1], acc[2]);
-    } else if (KIND == RED_UPD32) {
+    } else if constexpr (KIND == RED_UPD32) {
         finalize_update_mixed(st, acc[0], acc[1]);
-    } else if (KIND == RED_CHK64) {
+    } else if constexpr (KIND == RED_CHK64) {
         finalize_check64(st, acc[0], sqrt(acc[1]));
-    } else if (KIND == RED_CHK32) {
+    } else if constexpr (KIND == RED_CHK32) {
         finalize_check_mixed(st, acc[0], sqrt(acc[1]));
     } else {
         relres[sys] = acc[1] > 0.0 ? sqrt(acc[0] / acc[1]) : sqrt(acc[0]);
     }
+}
+
+template <int NV, int KIND>
+__global__ void __launch_bounds__(kBlock) bk_reduce(BView B, const Active *L, CgState *S, const double *part,
+                                                    double *relres, Active *L_chk = nullptr, uint32_t *arrive = nullptr)
+{
+    __shared__ double sh[NV * 32];
+    __shared__ uint32_t last_sh;
+    if (blockIdx.x < L->n_sys) {
+        const uint32_t sys = L->sys[blockIdx.x];
+        CgState *st = &S[sys];
+        const bool skip = (KIND == RED_INIT_RES || KIND == RED_TRUE) ? false
+                          : (KIND == RED_CHK64 || KIND == RED_CHK32) ? (st->done || !st->need_check)
+                                                                     : st->done != 0;
+        if (!skip) {
+            const uint32_t b0 = B.sys_slice[sys], b1 = B.sys_slice[sys + 1];
+            double acc[NV];
+#pragma unroll
+            for (int q = 0; q < NV; q++) acc[q] = 0.0;
+            for (uint32_t s = b0 + threadIdx.x; s < b1; s += blockDim.x)
+#pragma unroll
+                for (int q = 0; q < NV; q++) acc[q] += part[size_t(s) * NV + q];
+            block_sum<NV>(acc, sh);
+            if (threadIdx.x == 0) finalize<NV, KIND>(st, acc, relres, sys);
+        }
+    }
+    if (!L_chk) return;
+    // after an update: the last block to finish lists the systems that asked for a check
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last_sh = atomicAdd(arrive, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last_sh) return;
+    __threadfence();
+    build_list(L->n_sys, L->sys, B.sys_slice, L_chk,
+               [&](uint32_t i) { return __ldcg(&S[i].done) == 0 && __ldcg(&S[i].need_check) != 0; });
+    if (threadIdx.x == 0) *arrive = 0;
 }
 
 #define BATCH_ROWS_LOOP                                                                                      \
@@ -385,48 +460,14 @@ __global__ void bk_true_res(Sell<double> M, BView B, const Active *L, const doub
         });
 }
 
-// Loop control: rebuilds the list of active systems (block-wide scan), keeps the
-// graph's while node running while any system is active, enforces the hard limit.
+// Loop control: rebuilds the list of active systems, keeps the graph's while node
+// running while any system is active, enforces the hard limit.
 __global__ void __launch_bounds__(kBlock) bk_tail(const CgState *S, const uint32_t *sys_slice, uint32_t n_sys,
                                                   Active *L, BatchCtl *ctl, cudaGraphConditionalHandle h,
                                                   int use_cond)
 {
-    __shared__ uint32_t cnt_sys[kBlock], cnt_sl[kBlock];
-    const uint32_t t = threadIdx.x, per = (n_sys + blockDim.x - 1) / blockDim.x;
-    const uint32_t i0 = min(n_sys, t * per), i1 = min(n_sys, i0 + per);
-    uint32_t ns = 0, nsl = 0;
-    for (uint32_t i = i0; i < i1; i++)
-        if (!S[i].done) {
-            ns++;
-            nsl += sys_slice[i + 1] - sys_slice[i];
-        }
-    cnt_sys[t] = ns;
-    cnt_sl[t] = nsl;
-    __syncthreads();
-    if (t == 0) {  // exclusive scan (blockDim entries)
-        uint32_t a = 0, b = 0;
-        for (uint32_t k = 0; k < blockDim.x; k++) {
-            const uint32_t x = cnt_sys[k], y = cnt_sl[k];
-            cnt_sys[k] = a;
-            cnt_sl[k] = b;
-            a += x;
-            b += y;
-        }
-        L->n_sys = a;
-        L->n_slices = b;
-    }
-    __syncthreads();
-    uint32_t o = cnt_sys[t], pre = cnt_sl[t];
-    for (uint32_t i = i0; i < i1; i++)
-        if (!S[i].done) {
-            L->sys[o] = i;
-            L->prefix[o] = pre;
-            pre += sys_slice[i + 1] - sys_slice[i];
-            o++;
-        }
-    __syncthreads();
-    if (t == 0) {
-        L->prefix[L->n_sys] = L->n_slices;
+    build_list(n_sys, nullptr, sys_slice, L, [&](uint32_t i) { return S[i].done == 0; });
+    if (threadIdx.x == 0) {
         const uint32_t bc = ++ctl->body_count;
         int keep = L->n_sys > 0;
         if (keep && bc >= ctl->body_limit) {
@@ -590,7 +631,7 @@ rsg_status rsg_batch_solve(rsg_context *ctx, rsg_batch *B, const rsg_solver_conf
     const uint32_t max_it = std::max<uint32_t>(conf->n_outer, 1);
     const size_t vn = arena_bytes(n, sizeof(double)), vf = arena_bytes(n, sizeof(float));
     size_t bytes = 8 * vn + arena_bytes(size_t(nsl) * 3, sizeof(double)) + arena_bytes(ns, sizeof(CgState)) +
-                   2 * arena_bytes(1, sizeof(Active)) + 4 * arena_bytes(size_t(ns) + 1, sizeof(uint32_t)) +
+                   3 * arena_bytes(1, sizeof(Active)) + 6 * arena_bytes(size_t(ns) + 1, sizeof(uint32_t)) +
                    arena_bytes(ns, sizeof(double)) + arena_bytes(1, sizeof(BatchCtl)) + 2 * arena_bytes(B->user_rows, 8);
     if (mixed) bytes += 7 * vf;
     RSG_TRY(arena_reserve(ctx, bytes));
@@ -604,6 +645,8 @@ rsg_status rsg_batch_solve(rsg_context *ctx, rsg_batch *B, const rsg_solver_conf
     Active *L_all = arena_take<Active>(ctx, 1), *L_act = arena_take<Active>(ctx, 1);
     uint32_t *la_sys = arena_take<uint32_t>(ctx, size_t(ns) + 1), *la_pre = arena_take<uint32_t>(ctx, size_t(ns) + 1);
     uint32_t *lb_sys = arena_take<uint32_t>(ctx, size_t(ns) + 1), *lb_pre = arena_take<uint32_t>(ctx, size_t(ns) + 1);
+    Active *L_chk = arena_take<Active>(ctx, 1);  // systems that asked for a check (built by the update reduction)
+    uint32_t *lc_sys = arena_take<uint32_t>(ctx, size_t(ns) + 1), *lc_pre = arena_take<uint32_t>(ctx, size_t(ns) + 1);
     double *bu = memory == RSG_MEM_HOST ? arena_take<double>(ctx, B->user_rows) : const_cast<double *>(b);
     double *xu = memory == RSG_MEM_HOST ? arena_take<double>(ctx, B->user_rows) : x;
     float *r32 = nullptr, *z32 = nullptr, *pa = nullptr, *pb = nullptr, *q32 = nullptr, *y32 = nullptr, *d32 = nullptr;
@@ -657,7 +700,7 @@ rsg_status rsg_batch_solve(rsg_context *ctx, rsg_batch *B, const rsg_solver_conf
         h.stop_rule = RSG_STOP_TRUE_RELRES;
         std::vector<CgState> hs(ns, h);
         RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(S, hs.data(), ns * sizeof(CgState), cudaMemcpyHostToDevice, sm));
-        BatchCtl c = {0, max_it / 2 + 16, 0, 1};
+        BatchCtl c = {0, max_it / 2 + 16, 0, 1, 0};
         RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(ctl, &c, sizeof(c), cudaMemcpyHostToDevice, sm));
         // both lists start with every system
         std::vector<uint32_t> ids(ns), pre(size_t(ns) + 1);
@@ -666,13 +709,14 @@ rsg_status rsg_batch_solve(rsg_context *ctx, rsg_batch *B, const rsg_solver_conf
             pre[i] = B->pad_begin[i] / 32;
         }
         pre[ns] = nsl;
-        Active la = {ns, nsl, la_sys, la_pre}, lb = {ns, nsl, lb_sys, lb_pre};
+        Active la = {ns, nsl, la_sys, la_pre}, lb = {ns, nsl, lb_sys, lb_pre}, lc = {0, 0, lc_sys, lc_pre};
         RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(la_sys, ids.data(), ns * 4, cudaMemcpyHostToDevice, sm));
         RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(la_pre, pre.data(), (size_t(ns) + 1) * 4, cudaMemcpyHostToDevice, sm));
         RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(lb_sys, ids.data(), ns * 4, cudaMemcpyHostToDevice, sm));
         RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(lb_pre, pre.data(), (size_t(ns) + 1) * 4, cudaMemcpyHostToDevice, sm));
         RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(L_all, &la, sizeof(Active), cudaMemcpyHostToDevice, sm));
         RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(L_act, &lb, sizeof(Active), cudaMemcpyHostToDevice, sm));
+        RSG_CHECK_CUDA(ctx, cudaMemcpyAsync(L_chk, &lc, sizeof(Active), cudaMemcpyHostToDevice, sm));
         RSG_CHECK_CUDA(ctx, cudaStreamSynchronize(sm));
     }
     const BView V{B->d_slice_sys, B->d_sys_slice, nsl, ns};
@@ -702,20 +746,20 @@ rsg_status rsg_batch_solve(rsg_context *ctx, rsg_batch *B, const rsg_solver_conf
                 bk_dir<double, false><<<g, kBlock, 0, sm>>>(M64, V, L_act, z, po, pn, q, xp, nullptr, part, S);
                 bk_reduce<1, RED_DIR64><<<gr, kBlock, 0, sm>>>(V, L_act, S, part, nullptr);
                 bk_update<double, false><<<g, kBlock, 0, sm>>>(V, L_act, n, jac ? d : nullptr, pn, q, xp, r, z, part, S);
-                bk_reduce<3, RED_UPD64><<<gr, kBlock, 0, sm>>>(V, L_act, S, part, nullptr);
-                bk_check<false><<<g, kBlock, 0, sm>>>(M64, V, L_act, jac ? d : nullptr, nullptr, bp, xp, nullptr, r, z,
+                bk_reduce<3, RED_UPD64><<<gr, kBlock, 0, sm>>>(V, L_act, S, part, nullptr, L_chk, &ctl->arrive);
+                bk_check<false><<<g, kBlock, 0, sm>>>(M64, V, L_chk, jac ? d : nullptr, nullptr, bp, xp, nullptr, r, z,
                                                      nullptr, nullptr, part, S);
-                bk_reduce<2, RED_CHK64><<<gr, kBlock, 0, sm>>>(V, L_act, S, part, nullptr);
+                bk_reduce<2, RED_CHK64><<<gr, kBlock, 0, sm>>>(V, L_chk, S, part, nullptr);
             } else {
                 float *po = half ? pb : pa, *pn = half ? pa : pb;
                 bk_dir<float, true><<<g, kBlock, 0, sm>>>(M32, V, L_act, z32, po, pn, q32, xp, y32, part, S);
                 bk_reduce<1, RED_DIR32><<<gr, kBlock, 0, sm>>>(V, L_act, S, part, nullptr);
                 bk_update<float, true><<<g, kBlock, 0, sm>>>(V, L_act, n, jac ? d32 : nullptr, pn, q32, y32, r32, z32, part,
                                                             S);
-                bk_reduce<3, RED_UPD32><<<gr, kBlock, 0, sm>>>(V, L_act, S, part, nullptr);
-                bk_check<true><<<g, kBlock, 0, sm>>>(M64, V, L_act, nullptr, jac ? d32 : nullptr, bp, xp, y32, r, z, r32,
+                bk_reduce<3, RED_UPD32><<<gr, kBlock, 0, sm>>>(V, L_act, S, part, nullptr, L_chk, &ctl->arrive);
+                bk_check<true><<<g, kBlock, 0, sm>>>(M64, V, L_chk, nullptr, jac ? d32 : nullptr, bp, xp, y32, r, z, r32,
                                                     z32, part, S);
-                bk_reduce<2, RED_CHK32><<<gr, kBlock, 0, sm>>>(V, L_act, S, part, nullptr);
+                bk_reduce<2, RED_CHK32><<<gr, kBlock, 0, sm>>>(V, L_chk, S, part, nullptr);
             }
         }
         bk_tail<<<1, kBlock, 0, sm>>>(S, B->d_sys_slice, ns, L_act, ctl, h, use_cond);

@@ -91,8 +91,9 @@ def _coupled(ctx, A1, A2):
 
 
 def test_batch_autotune_keeps_results(ctx):
-    """The batch autotuner only changes launch shapes: tuned solves reach the same tolerance
-    and agree with the untuned ones to rounding."""
+    """The batch autotuner only changes launch shapes: every slice's partial sums and every
+    system's sums of them are formed in the same order whatever the grid, so tuned solves give
+    the untuned solutions bit for bit."""
     sys_ = systems([(6, 1.0, 11), (12, 1.2, 12), (4, 0.8, 13), (9, 1.0, 14)])
     batch = rsg.Batch(ctx, [(A.rp, A.ci, A.val) for A, _ in sys_])
     b = np.concatenate([bb for _, bb in sys_])
@@ -109,4 +110,4 @@ def test_batch_autotune_keeps_results(ctx):
             assert summ.status == rsg.OK and summ.true_relres <= 1e-10
             results[(tag, precision)] = x
     for precision in ("fp64", "mixed"):
-        assert rel_err(results[("tuned", precision)], results[("default", precision)]) < 1e-8
+        assert np.array_equal(results[("tuned", precision)], results[("default", precision)])
