@@ -337,9 +337,16 @@ typedef struct {
     uint32_t setup_launches;    /* kernel launches of the set-up */
     double   seconds_setup;     /* wall time of the set-up */
     uint32_t cycle_launches[2]; /* kernel launches of one cycle inside CG, with 1 / 2 smoothing sweeps */
+    uint32_t persist_level;     /* first level (<= 32768 rows) whose visits run as one persistent
+                                   cooperative kernel each (rsg_amg_setup_conf with persistent > 0);
+                                   0 when every cycle kernel is launched */
 } rsg_amg_info;
 /* Build (or rebuild) A's hierarchy from A's current values; info may be NULL. */
 RSG_API rsg_status rsg_amg_setup(rsg_context *ctx, rsg_csr *A, rsg_amg_info *info);
+/* The same, built as rsg_solve builds it for conf (conf->persistent > 0: the levels of at most 32768
+ * rows below the finest run as one persistent cooperative kernel per visit; NULL: as rsg_amg_setup). */
+RSG_API rsg_status rsg_amg_setup_conf(rsg_context *ctx, rsg_csr *A, const rsg_solver_conf *conf,
+                                      rsg_amg_info *info);
 /* Copy level `level` of the last hierarchy to host arrays (any may be NULL): agg (rows of the level)
  * maps each row to its aggregate, the row of level + 1 (not for the last level); row_ptr / col_idx /
  * values are the level's CSR (level 0: A itself). */

@@ -28,6 +28,7 @@
 //   into the gather; the finest level reads the matrix's FP32 SELL-32 (or CSR-stream) copy, the
 //   coarse levels their CSR with 8 lanes per row.
 #include "amg.cuh"
+#include "grid_sync.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -782,9 +783,20 @@ struct SweepArgs {
 // Coefficients of the two-step flexible-CG approximation e = g1 c1 + a2 c2 from the scalars
 // sc = {c1.v1, c1.b, c2.v2, c2.v1, c2.r2} (v = A c): a1 = c1.b / c1.v1, b2 = c2.v2 - (c2.v1)^2 / c1.v1,
 // a2 = c2.r2 / b2, g1 = a1 - (c2.v1) a2 / c1.v1.
+// Loads of vectors: COH (the persistent coarse-level kernel, whose phases read what other CTAs wrote
+// earlier in the same launch) reads through L2 (ld.global.cg); the separate kernels load plainly.
+template <bool COH, typename T>
+__device__ __forceinline__ T ldv(const T *p)
+{
+    if constexpr (COH) return __ldcg(p);
+    else return *p;
+}
+
+template <bool COH = false>
 __device__ __forceinline__ void kc_coefficients(const double *sc, float &g1, float &a2)
 {
-    const double d1 = sc[0], t1 = sc[1], d2 = sc[2], g = sc[3], t2 = sc[4];
+    const double d1 = ldv<COH>(sc), t1 = ldv<COH>(sc + 1), d2 = ldv<COH>(sc + 2), g = ldv<COH>(sc + 3),
+                 t2 = ldv<COH>(sc + 4);
     double c1 = 0.0, c2 = 0.0;
     if (d1 > 0.0) {
         const double b2 = d2 - g * g / d1;
@@ -795,14 +807,14 @@ __device__ __forceinline__ void kc_coefficients(const double *sc, float &g1, flo
     a2 = float(c2);
 }
 
-template <int SRC>
+template <int SRC, bool COH = false>
 __device__ __forceinline__ float sweep_x(const SweepArgs &a, uint32_t c)
 {
-    float x = (SRC == kSrcDwB || SRC == kSrcDwBCorr) ? a.dw[c] * a.b[c] : a.xs[c];
-    if (SRC == kSrcDwBCorr || SRC == kSrcXCorr) x = fmaf(a.s, a.ec[a.agg[c]], x);
+    float x = (SRC == kSrcDwB || SRC == kSrcDwBCorr) ? a.dw[c] * ldv<COH>(a.b + c) : ldv<COH>(a.xs + c);
+    if (SRC == kSrcDwBCorr || SRC == kSrcXCorr) x = fmaf(a.s, ldv<COH>(a.ec + a.agg[c]), x);
     if (SRC == kSrcXCorrK) {
         const uint32_t g = a.agg[c];
-        x = fmaf(a.s, a.ec[g], fmaf(a.s2, a.ec2[g], x));
+        x = fmaf(a.s, ldv<COH>(a.ec + g), fmaf(a.s2, ldv<COH>(a.ec2 + g), x));
     }
     return x;
 }
@@ -916,21 +928,21 @@ __device__ __forceinline__ float csr_row_dot(const uint32_t *__restrict__ rp, co
 }
 
 // The rows of one sweep, warp gw of warps (kLanes lanes per row).
-template <int SRC, int OUT>
+template <int SRC, int OUT, bool COH = false>
 __device__ __forceinline__ void coarse_rows(uint32_t n, const uint32_t *__restrict__ rp,
                                             const uint32_t *__restrict__ ci, const float *__restrict__ val,
                                             const SweepArgs &a, uint32_t gw, uint32_t warps)
 {
     const int lane = threadIdx.x & (kLanes - 1);
     const uint32_t sub = (threadIdx.x & 31) / kLanes;  // row within the warp's group
-    auto gx = [&](uint32_t c) { return sweep_x<SRC>(a, c); };
+    auto gx = [&](uint32_t c) { return sweep_x<SRC, COH>(a, c); };
     for (uint32_t base = gw * (32 / kLanes); base < n; base += warps * (32 / kLanes)) {
         const uint32_t row = base + sub;
         const bool valid = row < n;
         const float acc = csr_row_dot(rp, ci, val, row, valid, lane, gx);
         if (lane == 0 && valid) {
-            const float res = a.b[row] - acc;
-            a.out[row] = OUT == kOutRes ? res : fmaf(a.dw[row], res, sweep_x<SRC>(a, row));
+            const float res = ldv<COH>(a.b + row) - acc;
+            a.out[row] = OUT == kOutRes ? res : fmaf(a.dw[row], res, sweep_x<SRC, COH>(a, row));
         }
     }
 }
@@ -954,12 +966,12 @@ __global__ void __launch_bounds__(kBlock) k_amg_coarse(uint32_t n, const uint32_
 // row (indexes and values loaded a chunk ahead of the gathers); a fixed shuffle tree adds the lanes.
 // The aggregates of one restriction, warp gw of warps; the restricted residual of aggregate I goes
 // to bc[I] (and x0c[I] = dwc[I] bc[I] when x0c is given).
+template <bool COH = false>
 __device__ __forceinline__ void res_restrict_rows(uint32_t nc, const uint32_t *__restrict__ ptr,
                                                   const uint32_t *__restrict__ rows, const uint32_t *__restrict__ rp,
                                                   const uint32_t *__restrict__ ci, const float *__restrict__ val,
-                                                  const float *__restrict__ b, const float *__restrict__ xs,
-                                                  const float *__restrict__ dwc, float *bc, float *x0c, uint32_t gw,
-                                                  uint32_t warps)
+                                                  const float *b, const float *xs, const float *__restrict__ dwc,
+                                                  float *bc, float *x0c, uint32_t gw, uint32_t warps)
 {
     const int lane = threadIdx.x & 31, slot = lane >> 2, q = lane & 3;
     for (uint32_t I = gw; I < nc; I += warps) {
@@ -979,11 +991,11 @@ __device__ __forceinline__ void res_restrict_rows(uint32_t nc, const uint32_t *_
                     v[t] = ok ? val[j0 + 4 * t] : 0.f;
                 }
 #pragma unroll
-                for (int t = 0; t < kChunk; t++) x[t] = v[t] != 0.f ? xs[c[t]] : 0.f;
+                for (int t = 0; t < kChunk; t++) x[t] = v[t] != 0.f ? ldv<COH>(xs + c[t]) : 0.f;
 #pragma unroll
                 for (int t = 0; t < kChunk; t++) acc = fmaf(v[t], x[t], acc);
             }
-            part += (q == 0 ? b[row] : 0.f) - acc;
+            part += (q == 0 ? ldv<COH>(b + row) : 0.f) - acc;
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
@@ -1258,6 +1270,168 @@ __global__ void k_amg_rz(uint32_t n, const float *__restrict__ r, const float *_
     if (grid_sum<2>(acc, partials, ticket, sh, tot) && threadIdx.x == 0) amg_finalize(st, tot[0], tot[1], mode, rz_out);
 }
 
+// ---- the coarse levels of one cycle in one persistent kernel ----
+// Below kCoarsePersistRows rows a level's kernels are chains of a few L2 round trips each; launched
+// one by one, the launch and the wait for the predecessor cost as much as the work.  From the first
+// level at or below that size, solve_level's whole recursion (cycles, K-cycle steps, the dense coarse
+// solve) runs as one cooperative launch: the host records the phases it would launch, in order, as a
+// program (CoarsePhase), and the kernel runs them with a grid barrier between phases.  Each phase does
+// what the separate kernel does, with the same per-row (per-aggregate) arithmetic; the K-cycle dot
+// products keep the separate kernel's grid as virtual blocks and its per-block partial sums, and the
+// last CTA at the barrier adds the partials in the separate kernel's order (grid_sum), so the cycle
+// gives the same bits either way.  The bottom level's cycle runs as its separate phases (restriction,
+// dense solve, corrected sweep), the same arithmetic as the fused one-CTA kernel.
+#ifndef RSG_COARSE_CTAS_PER_SM
+#define RSG_COARSE_CTAS_PER_SM 1
+#endif
+constexpr int kCoarseCtasPerSm = RSG_COARSE_CTAS_PER_SM;
+constexpr uint32_t kCoarsePersistRows = 32768;
+
+enum CoarseOp : uint32_t {
+    CP_SWEEP_X = 0,   // coarse_rows<kSrcX, kOutSmooth>
+    CP_SWEEP_CORR,    // coarse_rows<kSrcXCorr, kOutSmooth>
+    CP_SWEEP_CORRK,   // coarse_rows<kSrcXCorrK, kOutSmooth> (coefficients from a.kc)
+    CP_RES_RESTRICT,  // res_restrict_rows: a.b, a.xs -> bc, x0c
+    CP_DENSE,         // dense coarse solve: a.out = inv a.b
+    CP_KC_SPMV2,      // K-cycle: v = A c, sc[o0] = c.v, sc[o1] = c.y1
+    CP_KC_SPMV3,      //          ... and sc[o2] = c.y2
+    CP_KC_R2,         // K-cycle: r2 = a.b - a1 v1 (a1 from sc), x1 = dw r2
+};
+
+struct CoarsePhase {
+    uint32_t op, n, nc, vgrid;          // rows; coarse rows (restriction); the K-cycle SpMV's grid
+    const uint32_t *rp, *ci;            // the level's matrix
+    const float *val;
+    const uint32_t *ptr, *rows;         // restriction: aggregate lists
+    const float *dwc;                   // restriction: the coarse level's weights
+    float *bc, *x0c;                    // restriction outputs; K-cycle r2: r2 and x1
+    const float *inv;                   // dense solve
+    const float *c, *y1, *y2;           // K-cycle SpMV operands (r2: c = v1)
+    float *v;                           // K-cycle SpMV output
+    double *sc;                         // K-cycle scalars of the level
+    int32_t o0, o1, o2, pad;
+    SweepArgs a;
+};
+
+__device__ __forceinline__ void dense_rows(uint32_t n, const float *__restrict__ inv, const float *b, float *e,
+                                           float *sb, uint32_t gw, uint32_t warps)
+{
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sb[i] = __ldcg(b + i);
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    for (uint32_t i = gw; i < n; i += warps) {
+        float v[kAmgCoarsest / 32];
+#pragma unroll
+        for (int t = 0; t < int(kAmgCoarsest / 32); t++) {
+            const uint32_t j = uint32_t(lane) + 32u * uint32_t(t);
+            v[t] = j < n ? inv[size_t(i) * n + j] : 0.f;
+        }
+        float s = 0.f;
+#pragma unroll
+        for (int t = 0; t < int(kAmgCoarsest / 32); t++) {
+            const uint32_t j = uint32_t(lane) + 32u * uint32_t(t);
+            if (j < n) s = fmaf(v[t], sb[j], s);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) e[i] = s;
+    }
+}
+
+// k_amg_kc_spmv's work for its virtual blocks vb = blockIdx.x, blockIdx.x + gridDim.x, ... < vgrid:
+// the same rows per thread, the same compensated sums, the block's partials at part[3 vb + k].
+template <int NDOT>
+__device__ __forceinline__ void kc_spmv_blocks(const CoarsePhase &p, double *part, double *sh)
+{
+    const int lane = threadIdx.x & (kLanes - 1);
+    const uint32_t sub = (threadIdx.x & 31) / kLanes, vwarps = (p.vgrid * blockDim.x) >> 5;
+    const float *c = p.c;
+    auto gx = [&](uint32_t col) { return __ldcg(c + col); };
+    for (uint32_t vb = blockIdx.x; vb < p.vgrid; vb += gridDim.x) {
+        const uint32_t gw = (vb * blockDim.x + threadIdx.x) >> 5;
+        Dot2 d0, d1, d2;
+        for (uint32_t base = gw * (32 / kLanes); base < p.n; base += vwarps * (32 / kLanes)) {
+            const uint32_t row = base + sub;
+            const float acc = csr_row_dot(p.rp, p.ci, p.val, row, row < p.n, lane, gx);
+            if (lane == 0 && row < p.n) {
+                p.v[row] = acc;
+                const float ci_ = __ldcg(c + row);
+                d0.add_prod(ci_, acc);
+                d1.add_prod(ci_, __ldcg(p.y1 + row));
+                if (NDOT == 3) d2.add_prod(ci_, __ldcg(p.y2 + row));
+            }
+        }
+        double accd[3] = {d0.value(), d1.value(), d2.value()};
+        block_sum<3>(accd, sh);
+        if (threadIdx.x == 0)
+#pragma unroll
+            for (int k = 0; k < 3; k++) part[size_t(vb) * 3 + k] = accd[k];
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_amg_coarse_persist(const CoarsePhase *prog, uint32_t n_phases,
+                                                               double *part, unsigned int *bar, const CgState *st,
+                                                               unsigned int *err)
+{
+    __shared__ __align__(16) unsigned char ph_raw[sizeof(CoarsePhase)];
+    __shared__ double sh[3 * 32];
+    __shared__ float sb[kAmgCoarsest];
+    if (st && st->done) return;  // written before this launch only: the same answer in every CTA
+    const CoarsePhase &p = *reinterpret_cast<const CoarsePhase *>(ph_raw);
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t i = 0; i < n_phases; i++) {
+        __syncthreads();
+        {
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(prog + i);
+            uint32_t *dst = reinterpret_cast<uint32_t *>(ph_raw);
+            for (uint32_t w = threadIdx.x; w < uint32_t(sizeof(CoarsePhase) / 4); w += blockDim.x) dst[w] = src[w];
+        }
+        __syncthreads();
+        const uint32_t op = p.op;
+        if (op == CP_SWEEP_X) {
+            coarse_rows<kSrcX, kOutSmooth, true>(p.n, p.rp, p.ci, p.val, p.a, gw, warps);
+        } else if (op == CP_SWEEP_CORR) {
+            coarse_rows<kSrcXCorr, kOutSmooth, true>(p.n, p.rp, p.ci, p.val, p.a, gw, warps);
+        } else if (op == CP_SWEEP_CORRK) {
+            SweepArgs a = p.a;
+            kc_coefficients<true>(a.kc, a.s, a.s2);
+            coarse_rows<kSrcXCorrK, kOutSmooth, true>(p.n, p.rp, p.ci, p.val, a, gw, warps);
+        } else if (op == CP_RES_RESTRICT) {
+            res_restrict_rows<true>(p.nc, p.ptr, p.rows, p.rp, p.ci, p.val, p.a.b, p.a.xs, p.dwc, p.bc, p.x0c, gw,
+                                    warps);
+        } else if (op == CP_DENSE) {
+            dense_rows(p.n, p.inv, p.a.b, p.a.out, sb, gw, warps);
+        } else if (op == CP_KC_SPMV2 || op == CP_KC_SPMV3) {
+            if (op == CP_KC_SPMV2) kc_spmv_blocks<2>(p, part, sh);
+            else kc_spmv_blocks<3>(p, part, sh);
+            // the last CTA to arrive adds the partials in grid_sum's order and stores the scalars
+            auto last = [&]() {
+                double acc[3] = {0.0, 0.0, 0.0};
+                for (uint32_t b = threadIdx.x; b < p.vgrid; b += blockDim.x)
+#pragma unroll
+                    for (int k = 0; k < 3; k++) acc[k] += __ldcg(&part[size_t(b) * 3 + k]);
+                block_sum<3>(acc, sh);
+                if (threadIdx.x == 0) {
+                    p.sc[p.o0] = acc[0];
+                    p.sc[p.o1] = acc[1];
+                    if (op == CP_KC_SPMV3) p.sc[p.o2] = acc[2];
+                }
+            };
+            if (!grid_barrier(bar, err, last)) return;
+            continue;
+        } else if (op == CP_KC_R2) {
+            const double d1 = __ldcg(p.sc), t1 = __ldcg(p.sc + 1);
+            const float a1 = d1 > 0.0 ? float(t1 / d1) : 0.f;
+            for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < p.n; k += gridDim.x * blockDim.x) {
+                const float r = fmaf(-a1, __ldcg(p.c + k), __ldcg(p.a.b + k));
+                p.bc[k] = r;
+                p.x0c[k] = p.a.dw[k] * r;
+            }
+        }
+        if (i + 1 < n_phases && !grid_barrier(bar, err)) return;
+    }
+}
+
 // ---------------------------------------------------------------- host: set-up --------------
 
 rsg_status read_flags(rsg_context *ctx, AmgHierarchy *H, int count)
@@ -1470,6 +1644,8 @@ void amg_free(AmgHierarchy *H)
     H->u3.release();
     H->scan_blocks.release();
     H->kc_part.release();
+    H->persist_prog.release();
+    H->persist_bar.release();
     H->kc_ticket.release();
     H->kc_sc.release();
     H->rounds.release();
@@ -1484,7 +1660,11 @@ void amg_release(void *h) { amg_free(static_cast<AmgHierarchy *>(h)); }
 
 AmgHierarchy *amg_of(const rsg_csr *A) { return static_cast<AmgHierarchy *>(A->amg); }
 
-rsg_status amg_setup(rsg_context *ctx, rsg_csr *A)
+namespace {
+rsg_status build_persist(rsg_context *ctx, AmgHierarchy *H, bool want);
+}  // namespace
+
+rsg_status amg_setup(rsg_context *ctx, rsg_csr *A, bool persistent)
 {
     const auto t0 = std::chrono::steady_clock::now();
     const uint32_t launches0 = t_launches;
@@ -1540,6 +1720,7 @@ rsg_status amg_setup(rsg_context *ctx, rsg_csr *A)
     RSG_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     H->seconds_setup = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     H->setup_launches = t_launches - launches0;
+    RSG_TRY(build_persist(ctx, H, persistent));
     // launches of one cycle as the CG loop applies it, for one and two sweeps (dry runs: nothing launched)
     for (int nu = 1; nu <= 2; nu++) {
         const uint32_t c0 = t_launches;
@@ -1691,10 +1872,16 @@ void cycle(rsg_context *ctx, const AmgHierarchy *H, int l, const float *b, float
 // cycle on an ordinary level.  On a K-cycle level two flexible-CG steps preconditioned by the cycle
 // leave their directions in c1, c2 and the scalars in the level's kc_sc slots; the caller's
 // prolongation combines them (e is not written).
+void coarse_persist(rsg_context *ctx, const AmgHierarchy *H, int sweeps, const CgState *st);
+
 void solve_level(rsg_context *ctx, const AmgHierarchy *H, int l, const float *b, float *e, int sweeps,
                  const CgState *st, bool pdl)
 {
     const AmgLevel &F = H->L[l];
+    if (l == H->persist_level && b == F.b.p && e == F.e.p) {  // the recorded program of this visit
+        coarse_persist(ctx, H, sweeps, st);
+        return;
+    }
     if (l == H->levels - 1) {
         if (H->dense_coarsest) {
             amg_launch(ctx->stream, pdl, k_amg_dense_apply, 1, 1024, 0, F.n, (const float *)H->coarse_inv.p, b, e, st);
@@ -1724,6 +1911,230 @@ void solve_level(rsg_context *ctx, const AmgHierarchy *H, int l, const float *b,
     cycle(ctx, H, l, F.r2.p, F.c2.p, sweeps, st, pdl);
     amg_launch(ctx->stream, pdl, k_amg_kc_spmv<3>, gs, kBlock, 0, F.n, F.rp, F.ci, F.val32, (const float *)F.c2.p,
              F.v2.p, (const float *)F.v1.p, (const float *)F.r2.p, H->kc_part.p, H->kc_ticket.p, sc, 2, 3, 4, st);
+}
+
+// ---- the small coarse levels as one persistent kernel: program recording, probe, launch ----
+
+// Records, in launch order, the phases solve_level(l) launches (the bottom level's cycle as its
+// separate phases).  Mirrors cycle / solve_level / coarse_sweep_corr / res_restrict above.
+struct CoarseProgram {
+    rsg_context *ctx;
+    const AmgHierarchy *H;
+    int sweeps;
+    std::vector<CoarsePhase> ph;
+
+    void sweep(int src, const AmgLevel &l, const SweepArgs &a)
+    {
+        CoarsePhase p{};
+        p.op = src == kSrcX ? CP_SWEEP_X : src == kSrcXCorr ? CP_SWEEP_CORR : CP_SWEEP_CORRK;
+        p.n = l.n;
+        p.rp = l.rp;
+        p.ci = l.ci;
+        p.val = l.val32;
+        p.a = a;
+        ph.push_back(p);
+    }
+    void sweep_corr(int l, SweepArgs a)
+    {
+        const AmgLevel &F = H->L[l];
+        a.agg = F.agg.p;
+        set_correction(H, l + 1, sweeps, a);
+        sweep(k_level(H, l + 1) ? kSrcXCorrK : kSrcXCorr, F, a);
+    }
+    void res_restrict(int l, const float *b, const float *xs)
+    {
+        const AmgLevel &F = H->L[l], &C = H->L[l + 1];
+        CoarsePhase p{};
+        p.op = CP_RES_RESTRICT;
+        p.n = F.n;
+        p.nc = C.n;
+        p.rp = F.rp;
+        p.ci = F.ci;
+        p.val = F.val32;
+        p.ptr = F.agg_ptr.p;
+        p.rows = F.agg_rows.p;
+        p.dwc = C.dw.p;
+        p.bc = C.b.p;
+        p.x0c = C.x1.p;
+        p.a.b = b;
+        p.a.xs = xs;
+        ph.push_back(p);
+    }
+    void kc_spmv(const AmgLevel &F, int ndot, const float *c, float *v, const float *y1, const float *y2, double *sc,
+                 int o0, int o1, int o2)
+    {
+        CoarsePhase p{};
+        p.op = ndot == 2 ? CP_KC_SPMV2 : CP_KC_SPMV3;
+        p.n = F.n;
+        p.vgrid = uint32_t(coarse_grid(ctx, F.n));
+        p.rp = F.rp;
+        p.ci = F.ci;
+        p.val = F.val32;
+        p.c = c;
+        p.v = v;
+        p.y1 = y1;
+        p.y2 = y2;
+        p.sc = sc;
+        p.o0 = o0;
+        p.o1 = o1;
+        p.o2 = o2;
+        ph.push_back(p);
+    }
+    void cycle(int l, const float *b, float *out)
+    {
+        const AmgLevel &F = H->L[l], &C = H->L[l + 1];
+        float *bb = const_cast<float *>(b);
+        if (sweeps == 2) {
+            sweep(kSrcX, F, SweepArgs{bb, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, F.x2.p});
+            res_restrict(l, b, F.x2.p);
+        } else {
+            res_restrict(l, b, F.x1.p);
+        }
+        solve_level(l + 1, C.b.p, C.e.p);
+        if (sweeps == 2) {
+            sweep_corr(l, SweepArgs{bb, F.dw.p, F.x2.p, nullptr, nullptr, 0.f, F.x1.p});
+            sweep(kSrcX, F, SweepArgs{bb, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, out});
+        } else {
+            sweep_corr(l, SweepArgs{bb, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, out});
+        }
+    }
+    void solve_level(int l, const float *b, float *e)
+    {
+        const AmgLevel &F = H->L[l];
+        if (l == H->levels - 1) {
+            if (H->dense_coarsest) {
+                CoarsePhase p{};
+                p.op = CP_DENSE;
+                p.n = F.n;
+                p.inv = H->coarse_inv.p;
+                p.a.b = b;
+                p.a.out = e;
+                ph.push_back(p);
+            } else {
+                float *src = F.x1.p, *dst = F.x2.p, *bb = const_cast<float *>(b);
+                for (int k = 0; k < 7; k++) {
+                    sweep(kSrcX, F, SweepArgs{bb, F.dw.p, src, nullptr, nullptr, 0.f, dst});
+                    std::swap(src, dst);
+                }
+                sweep(kSrcX, F, SweepArgs{bb, F.dw.p, src, nullptr, nullptr, 0.f, e});
+            }
+            return;
+        }
+        if (!k_level(H, l)) {
+            cycle(l, b, e);
+            return;
+        }
+        double *sc = H->kc_sc.p + 8 * l;
+        cycle(l, b, F.c1.p);
+        kc_spmv(F, 2, F.c1.p, F.v1.p, b, nullptr, sc, 0, 1, 0);
+        CoarsePhase r{};
+        r.op = CP_KC_R2;
+        r.n = F.n;
+        r.a.b = b;
+        r.a.dw = F.dw.p;
+        r.c = F.v1.p;
+        r.sc = sc;
+        r.bc = F.r2.p;
+        r.x0c = F.x1.p;
+        ph.push_back(r);
+        cycle(l, F.r2.p, F.c2.p);
+        kc_spmv(F, 3, F.c2.p, F.v2.p, F.v1.p, F.r2.p, sc, 2, 3, 4);
+    }
+};
+
+__global__ void k_coop_probe(unsigned int *) {}
+
+// Whether this device runs a cooperative launch captured in a CUDA graph (the CG loop's body is one):
+// one tiny captured launch on a private stream, cached in the context.
+bool coop_graph_supported(rsg_context *ctx)
+{
+    if (ctx->coop_graph >= 0) return ctx->coop_graph != 0;
+    int coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device);
+    bool ok = coop != 0;
+    cudaStream_t s = nullptr;
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    if (ok) ok = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess;
+    if (ok) ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+        cudaLaunchAttribute at;
+        at.id = cudaLaunchAttributeCooperative;
+        at.val.cooperative = 1;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(2);
+        cfg.blockDim = dim3(32);
+        cfg.stream = s;
+        cfg.attrs = &at;
+        cfg.numAttrs = 1;
+        const cudaError_t le = cudaLaunchKernelEx(&cfg, k_coop_probe, (unsigned int *)nullptr);
+        const cudaError_t ee = cudaStreamEndCapture(s, &g);
+        ok = le == cudaSuccess && ee == cudaSuccess && g && cudaGraphInstantiate(&ge, g, 0) == cudaSuccess &&
+             cudaGraphLaunch(ge, s) == cudaSuccess && cudaStreamSynchronize(s) == cudaSuccess;
+    }
+    if (ge) cudaGraphExecDestroy(ge);
+    if (g) cudaGraphDestroy(g);
+    if (s) cudaStreamDestroy(s);
+    (void)cudaGetLastError();
+    ctx->coop_graph = ok ? 1 : 0;
+    return ok;
+}
+
+// Picks the first level (below the finest) of at most kCoarsePersistRows rows that has a coarser
+// level, records its programs for one and two sweeps and uploads them; persist_level stays 0 when
+// the kernel is not wanted or cannot run.
+rsg_status build_persist(rsg_context *ctx, AmgHierarchy *H, bool want)
+{
+    H->persist_level = 0;
+    H->persist_grid = 0;
+    if (!want) return RSG_OK;
+    int l0 = 0;
+    for (int l = 1; l + 1 < H->levels; l++)
+        if (H->L[l].n <= kCoarsePersistRows) {
+            l0 = l;
+            break;
+        }
+    if (l0 == 0 || !coop_graph_supported(ctx)) return RSG_OK;
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_amg_coarse_persist, kBlock, 0) != cudaSuccess || occ < 1) {
+        (void)cudaGetLastError();
+        return RSG_OK;
+    }
+    std::vector<CoarsePhase> all;
+    for (int nu = 1; nu <= 2; nu++) {
+        CoarseProgram P{ctx, H, nu, {}};
+        P.solve_level(l0, H->L[l0].b.p, H->L[l0].e.p);
+        H->persist_len[nu - 1] = uint32_t(P.ph.size());
+        all.insert(all.end(), P.ph.begin(), P.ph.end());
+    }
+    const size_t bytes = all.size() * sizeof(CoarsePhase);
+    if (!H->persist_prog.ensure(bytes) || !H->persist_bar.ensure(4))
+        return set_error(ctx, RSG_ERR_OUT_OF_MEMORY, "amg: persistent cycle program");
+    RSG_CHECK_CUDA(ctx, cudaMemcpy(H->persist_prog.p, all.data(), bytes, cudaMemcpyHostToDevice));
+    RSG_CHECK_CUDA(ctx, cudaMemsetAsync(H->persist_bar.p, 0, 4 * sizeof(unsigned int), ctx->stream));
+    H->persist_grid = std::min(occ, kCoarseCtasPerSm) * ctx->num_sms;
+    H->persist_level = l0;
+    return RSG_OK;
+}
+
+// solve_level(l) from the recorded program: one cooperative launch (counted like the others).
+void coarse_persist(rsg_context *ctx, const AmgHierarchy *H, int sweeps, const CgState *st)
+{
+    ++t_launches;
+    if (t_dry) return;
+    const uint32_t k = sweeps == 2 ? 1 : 0;
+    const CoarsePhase *prog = reinterpret_cast<const CoarsePhase *>(H->persist_prog.p) + (k ? H->persist_len[0] : 0);
+    unsigned int *err = st ? const_cast<unsigned int *>(&st->ticket[7]) : ctx->errw;
+    cudaLaunchAttribute at;
+    at.id = cudaLaunchAttributeCooperative;
+    at.val.cooperative = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(unsigned(H->persist_grid));
+    cfg.blockDim = dim3(kBlock);
+    cfg.stream = ctx->stream;
+    cfg.attrs = &at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_amg_coarse_persist, prog, H->persist_len[k], H->kc_part.p, H->persist_bar.p, st, err);
 }
 
 template <int RPW>
@@ -1854,9 +2265,14 @@ extern "C" {
 
 rsg_status rsg_amg_setup(rsg_context *ctx, rsg_csr *A, rsg_amg_info *info)
 {
+    return rsg_amg_setup_conf(ctx, A, nullptr, info);
+}
+
+rsg_status rsg_amg_setup_conf(rsg_context *ctx, rsg_csr *A, const rsg_solver_conf *conf, rsg_amg_info *info)
+{
     if (!ctx || !A) return set_error(ctx, RSG_ERR_INVALID_ARG, "amg_setup: bad arguments");
     RSG_CHECK_CUDA(ctx, cudaSetDevice(ctx->device));
-    RSG_TRY(amg_setup(ctx, A));
+    RSG_TRY(amg_setup(ctx, A, conf && conf->persistent > 0));
     if (info) {
         const AmgHierarchy *H = amg_of(A);
         std::memset(info, 0, sizeof(*info));
@@ -1871,6 +2287,7 @@ rsg_status rsg_amg_setup(rsg_context *ctx, rsg_csr *A, rsg_amg_info *info)
         info->seconds_setup = H->seconds_setup;
         info->cycle_launches[0] = H->cycle_launches[0];
         info->cycle_launches[1] = H->cycle_launches[1];
+        info->persist_level = uint32_t(H->persist_level);
     }
     return RSG_OK;
 }

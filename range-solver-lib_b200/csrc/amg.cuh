@@ -90,11 +90,21 @@ struct AmgHierarchy {
     uint32_t mis_rounds = 0;
     uint32_t setup_launches = 0;         // kernel launches of the last set-up
     uint32_t cycle_launches[2] = {0, 0};  // kernel launches of one cycle inside CG, one / two sweeps
+    // Levels from persist_level on (0: none) run as one persistent cooperative kernel per visit: the
+    // phase programs it runs for one and two sweeps (recorded from the cycle's own recursion), its
+    // CTA count and its barrier words.
+    int persist_level = 0;
+    int persist_grid = 0;
+    DevBuf<uint8_t> persist_prog;
+    uint32_t persist_len[2] = {0, 0};
+    DevBuf<unsigned int> persist_bar;
 };
 
 void amg_free(AmgHierarchy *H);
 // (Re)builds A's hierarchy from A's current values; A owns it afterwards (freed with A).
-rsg_status amg_setup(rsg_context *ctx, rsg_csr *A);
+// persistent: run the small coarse levels of each cycle as one persistent kernel (when the device
+// can capture a cooperative launch in a graph); false (the default) launches their kernels one by one.
+rsg_status amg_setup(rsg_context *ctx, rsg_csr *A, bool persistent = false);
 AmgHierarchy *amg_of(const rsg_csr *A);
 
 // z = M(r), one cycle, on the context stream (FP32; sweeps = 1 or 2 smoothing sweeps per side;

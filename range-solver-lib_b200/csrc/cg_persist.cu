@@ -17,14 +17,13 @@
 //
 // Barrier waits are bounded: a CTA that waits longer than kBarrierPolls polls flags the context's
 // error word, marks the state RSG_ERR_TIMEOUT and leaves; the others then time out as well.
+#include "grid_sync.cuh"
 #include "krylov.cuh"
 
 #include <algorithm>
 
 namespace rsg {
 namespace {
-
-constexpr uint32_t kBarrierPolls = 1u << 24;  // ~ seconds of polling with the back-off below
 
 struct PersistArgs {
     Sell<double> S64;
@@ -36,49 +35,10 @@ struct PersistArgs {
     float *r32, *z32, *p32a, *p32b, *q32, *y32;
     double *part_dir, *part_upd, *part_chk;  // per-virtual-block partials of the three phases
     CgState *st;
-    unsigned int *bar;                       // [0] arrivals, [1] generation
+    unsigned int *bar;                       // [0] arrivals, [1] generation, [2] abort (grid_sync.cuh)
     uint32_t g_dir, g_upd, g_chk;           // the graph loop's grids (virtual)
     unsigned int *err;
 };
-
-__device__ __forceinline__ unsigned int ld_acquire(const unsigned int *p)
-{
-    unsigned int v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-// Grid barrier (all CTAs co-resident: cooperative launch).  Returns false in every thread of a CTA
-// whose wait ran out.
-__device__ __forceinline__ bool grid_barrier(unsigned int *bar, unsigned int *err)
-{
-    __shared__ int ok_sh;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        const unsigned int gen = ld_acquire(bar + 1);
-        __threadfence();
-        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            uint32_t t = 0;
-            while (ld_acquire(bar + 1) == gen) {
-                if (++t >= kBarrierPolls) {
-                    ok = 0;
-                    atomicOr(err, 1u);
-                    break;
-                }
-                if (t > 4096) __nanosleep(64);
-            }
-        }
-        __threadfence();
-        ok_sh = ok;
-    }
-    __syncthreads();
-    return ok_sh != 0;
-}
 
 // The graph kernels' last-block sum of G per-block partials (NV each): strided over the threads,
 // then the block reduction -- the same order as grid_sum (common.cuh).  Valid in thread 0.
@@ -441,7 +401,7 @@ rsg_status cg_persist_run(rsg_context *ctx, const CgArgs &a, int g_dir, int g_up
     }
     double *part = ctx->persist;
     unsigned int *bar = reinterpret_cast<unsigned int *>(part + size_t(6) * kMaxGrid);
-    RSG_CHECK_CUDA(ctx, cudaMemsetAsync(bar, 0, sizeof(unsigned int), ctx->stream));  // no arrivals pending
+    RSG_CHECK_CUDA(ctx, cudaMemsetAsync(bar, 0, 3 * sizeof(unsigned int), ctx->stream));  // no arrivals, no abort
     PersistArgs pa;
     pa.S64 = sell_view<double>(a.A);
     pa.S32 = sell_view<float>(a.A);

@@ -38,6 +38,7 @@ struct rsg_context {
     unsigned int *errw = nullptr;     // device word: set when a kernel's bounded wait ran out
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     double *persist = nullptr;        // persistent CG loop: phase partials and barrier words (cg_persist.cu)
+    int coop_graph = -1;              // a cooperative launch can be captured in a graph: -1 not probed, 0 no, 1 yes
 };
 
 struct rsg_csr {

@@ -159,7 +159,7 @@ extern "C" rsg_status rsg_solve(rsg_context *ctx, rsg_csr *A, const rsg_solver_c
     P.kind = learned ? RSG_PREC_JACOBI : (prec_type == RSG_PREC_AMG ? 3 : prec_type);
     P.w = w;
     if (prec_type == RSG_PREC_AMG) {
-        RSG_TRY(amg_setup(ctx, A));  // rebuilt from the current values on every solve
+        RSG_TRY(amg_setup(ctx, A, c.persistent > 0));  // rebuilt from the current values on every solve
     } else if (prec_type == RSG_PREC_JACOBI || learned) {
         RSG_TRY(jacobi_build(ctx, A, d));
     } else if (prec_type == RSG_PREC_BLOCK_JACOBI) {

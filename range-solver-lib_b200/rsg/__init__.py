@@ -170,14 +170,19 @@ class Context:
         return X, list(per), summ
 
     # ---- multilevel aggregation preconditioner ----
-    def amg_setup(self, A: "Matrix") -> dict:
-        """Build A's hierarchy from its current values (rsg_amg_setup); returns its shape."""
+    def amg_setup(self, A: "Matrix", conf: SolverConf | None = None) -> dict:
+        """Build A's hierarchy from its current values (rsg_amg_setup, or rsg_amg_setup_conf: as a
+        solve with conf builds it); returns its shape."""
         info = _lib.AmgInfo()
-        self.check(self.lib.rsg_amg_setup(self.h, A.h, C.byref(info)), "amg_setup")
+        if conf is None:
+            self.check(self.lib.rsg_amg_setup(self.h, A.h, C.byref(info)), "amg_setup")
+        else:
+            self.check(self.lib.rsg_amg_setup_conf(self.h, A.h, C.byref(conf), C.byref(info)), "amg_setup")
         L = info.levels
         return {"levels": L, "dense_coarsest": bool(info.dense_coarsest), "rows": list(info.rows[:L]),
                 "nnz": list(info.nnz[:L]), "mis_rounds": info.mis_rounds, "seconds_setup": info.seconds_setup,
-                "setup_launches": info.setup_launches, "cycle_launches": list(info.cycle_launches)}
+                "setup_launches": info.setup_launches, "cycle_launches": list(info.cycle_launches),
+                "persist_level": info.persist_level}
 
     def eigen_solve(self, M: "Matrix", K: "Matrix", start, method: int = _lib.EIGEN_LANCZOS, n_eigen: int = 4,
                     n_iterations: int = 100, cvg: float = 1e-8, mu0: float = 0.0, conf=None):

@@ -132,6 +132,7 @@ class AmgInfo(C.Structure):
         ("setup_launches", C.c_uint32),
         ("seconds_setup", C.c_double),
         ("cycle_launches", C.c_uint32 * 2),
+        ("persist_level", C.c_uint32),
     ]
 
 
@@ -197,6 +198,7 @@ SIGNATURES = {
     "rsg_batch_autotune": (C.c_int, [_P, _P, C.POINTER(TuneInfo)]),
     "rsg_profile_kernel": (C.c_int, [_P, _P, C.c_int32, C.c_uint32, C.c_int32, _DP]),
     "rsg_amg_setup": (C.c_int, [_P, _P, C.POINTER(AmgInfo)]),
+    "rsg_amg_setup_conf": (C.c_int, [_P, _P, C.POINTER(SolverConf), C.POINTER(AmgInfo)]),
     "rsg_eigen_solve": (C.c_int, [_P, _P, _P, C.POINTER(EigenConf), C.POINTER(SolverConf), _P, _P, _P,
                                   C.POINTER(EigenStats)]),
     "rsg_amg_level": (C.c_int, [_P, _P, C.c_uint32, _P, _P, _P, _P]),

@@ -100,9 +100,16 @@ def test_amg_info_counts_launches(ctx):
     info = ctx.amg_setup(M)
     c1, c2 = info["cycle_launches"]
     # per level below the finest at least a restriction and a corrected sweep; two sweeps add launches
+    assert info["persist_level"] == 0
     assert c1 >= 2 * (info["levels"] - 1) and c2 > c1
     assert info["setup_launches"] >= 10 * (info["levels"] - 1)
     assert ctx.amg_setup(M)["cycle_launches"] == [c1, c2]
+    # with the persistent coarse levels, level 1 (~3k rows) and everything below it is one kernel: the
+    # cycle launches the finest sweeps (one or two per side), the restriction, that kernel and the
+    # prolongation
+    info_p = ctx.amg_setup(M, conf=rsg.make_conf(persistent=1))
+    assert info_p["levels"] >= 3 and info_p["persist_level"] == 1
+    assert info_p["cycle_launches"] == [5, 7]
 
 
 def test_amg_rejects_unsupported_modes(ctx):
