@@ -403,7 +403,10 @@ def main():
                          "'' skips it")
     ap.add_argument("--save-model", default="", help="learned: write the trained parameters (.npz) here")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-autotune", action="store_true", help="heat100: keep the built-in launch shapes")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="heat100, batch256: keep the built-in launch shapes")
+    ap.add_argument("--batch-precisions", default="fp64,mixed",
+                    help="batch256: the precisions to time (comma-separated; the fastest gives the value)")
     ap.add_argument("--workload", default="heat100",
                     choices=["heat100", "stress", "batch256", "transient40", "learned", "gmres100", "multi100",
                              "magneto64"],
@@ -786,12 +789,12 @@ def run_other(args, rank, world, local_rank, threads):
             rhs.append(bb.cpu().numpy())
             asm.close()
         batch = rsg.Batch(ctx, systems)
-        tune = batch.autotune()  # launch shapes of the batch loop (set-up, not timed)
+        tune = batch.autotune() if not args.no_autotune else None  # launch shapes of the batch loop (set-up)
         b_all = torch.from_numpy(np.concatenate(rhs)).cuda()
         x_all = torch.zeros_like(b_all)
         res = {}
         worst = 0.0
-        for precision in ("fp64", "mixed"):
+        for precision in args.batch_precisions.split(","):
             conf = rsg.make_conf(n_outer=100000, stop_rule="true", rtol=RTOL, precision=precision,
                                  use_graph=not args.host_loop)
             for _ in range(args.warmup):

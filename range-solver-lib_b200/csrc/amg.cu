@@ -1023,6 +1023,69 @@ __global__ void __launch_bounds__(kBlock) k_amg_res_restrict(uint32_t nc, const 
                       (gridDim.x * blockDim.x) >> 5);
 }
 
+// k_amg_kc_r2 folded into the restriction that follows it (one sweep per side): the K-cycle's second
+// right-hand side r2 = b - a1 v1 and its first smoothing step x1 = dw r2 are formed where the
+// restriction reads them -- for the gathered columns on the fly, for the aggregate's own rows also
+// stored (each row belongs to one aggregate) for the cycle's later steps.  The same expressions as
+// k_amg_kc_r2, so the same bits.
+__global__ void __launch_bounds__(kBlock) k_amg_res_restrict_kc(uint32_t nc, const uint32_t *__restrict__ ptr,
+                                                                const uint32_t *__restrict__ rows,
+                                                                const uint32_t *__restrict__ rp,
+                                                                const uint32_t *__restrict__ ci,
+                                                                const float *__restrict__ val,
+                                                                const float *__restrict__ b,
+                                                                const float *__restrict__ v1,
+                                                                const double *__restrict__ sc,
+                                                                const float *__restrict__ dw,
+                                                                const float *__restrict__ dwc, float *__restrict__ bc,
+                                                                float *__restrict__ x0c, float *__restrict__ r2,
+                                                                float *__restrict__ x1, const CgState *st)
+{
+    pdl_wait();
+    pdl_release();
+    if (st && st->done) return;
+    const double d1 = sc[0];
+    const float a1 = d1 > 0.0 ? float(sc[1] / d1) : 0.f;
+    const int lane = threadIdx.x & 31, slot = lane >> 2, q = lane & 3;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; I < nc; I += warps) {
+        float part = 0.f;
+        const uint32_t k1 = ptr[I + 1];
+        for (uint32_t k = ptr[I] + slot; k < k1; k += 8) {
+            const uint32_t row = rows[k];
+            const uint32_t end = rp[row + 1];
+            float acc = 0.f;
+            for (uint32_t j0 = rp[row] + q; j0 < end; j0 += 4 * kChunk) {
+                uint32_t c[kChunk];
+                float v[kChunk], x[kChunk];
+#pragma unroll
+                for (int t = 0; t < kChunk; t++) {
+                    const bool ok = j0 + 4 * t < end;
+                    c[t] = ok ? ci[j0 + 4 * t] : row;
+                    v[t] = ok ? val[j0 + 4 * t] : 0.f;
+                }
+#pragma unroll
+                for (int t = 0; t < kChunk; t++) x[t] = v[t] != 0.f ? dw[c[t]] * fmaf(-a1, v1[c[t]], b[c[t]]) : 0.f;
+#pragma unroll
+                for (int t = 0; t < kChunk; t++) acc = fmaf(v[t], x[t], acc);
+            }
+            float r = 0.f;
+            if (q == 0) {
+                r = fmaf(-a1, v1[row], b[row]);
+                r2[row] = r;
+                x1[row] = dw[row] * r;
+            }
+            part += r - acc;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+        if (lane == 0) {
+            bc[I] = part;
+            x0c[I] = dwc[I] * part;
+        }
+    }
+}
+
 // The bottom of the hierarchy in one CTA: the cycle on the last smoothed level l (at most
 // kBottomRows rows), whose next level is inverted densely -- pre-smoothing (two sweeps), residual and
 // restriction into shared memory, the dense coarse solve, the corrected post-smoothing.  Same
@@ -1826,16 +1889,34 @@ void res_restrict(rsg_context *ctx, const AmgHierarchy *H, int l, const float *b
              (const uint32_t *)F.agg_rows.p, F.rp, F.ci, F.val32, b, xs, (const float *)C.dw.p, C.b.p, C.x1.p, st);
 }
 
+// Whether the cycle on level l runs as the one-CTA bottom kernel.
+bool bottom_cycle(const AmgHierarchy *H, int l)
+{
+    return l + 1 == H->levels - 1 && H->dense_coarsest && H->L[l].n <= kBottomRows;
+}
+
 // One cycle on coarse level l >= 1: out ~ A_l^-1 b, with x0 = dw b already in x1 (written by the
 // restriction): pre-smoothing, residual and restriction in one pass, the coarser levels, the
 // prolongated correction fused into the first post-smoothing sweep.  With two sweeps x2 holds the
-// pre-smoothed iterate.
+// pre-smoothed iterate.  kc_b (one sweep, not the bottom cycle): b is the K-cycle's r2 = kc_b - a1 v1,
+// still to be formed together with x1 by the restriction (k_amg_res_restrict_kc).
 void cycle(rsg_context *ctx, const AmgHierarchy *H, int l, const float *b, float *out, int sweeps, const CgState *st,
-           bool pdl)
+           bool pdl, const float *kc_b = nullptr)
 {
     const AmgLevel &F = H->L[l], &C = H->L[l + 1];
     float *bb = const_cast<float *>(b);
-    if (l + 1 == H->levels - 1 && H->dense_coarsest && F.n <= kBottomRows) {
+    if (kc_b) {
+        const int g = std::max(1, std::min<int>(int((uint64_t(C.n) * 32 + kBlock - 1) / kBlock), ctx->num_sms * 8));
+        amg_launch(ctx->stream, pdl, k_amg_res_restrict_kc, g, kBlock, 0, C.n, (const uint32_t *)F.agg_ptr.p,
+                   (const uint32_t *)F.agg_rows.p, F.rp, F.ci, F.val32, kc_b, (const float *)F.v1.p,
+                   (const double *)(H->kc_sc.p + 8 * l), (const float *)F.dw.p, (const float *)C.dw.p, C.b.p, C.x1.p,
+                   F.r2.p, F.x1.p, st);
+        solve_level(ctx, H, l + 1, C.b.p, C.e.p, sweeps, st, pdl);
+        SweepArgs u1{bb, F.dw.p, F.x1.p, nullptr, nullptr, 0.f, out};
+        coarse_sweep_corr<kOutSmooth>(ctx, H, l, u1, sweeps, st, pdl);
+        return;
+    }
+    if (bottom_cycle(H, l)) {
         const BottomArgs B{F.n, C.n, F.rp, F.ci, F.agg.p, F.agg_ptr.p, F.agg_rows.p, F.val32, F.dw.p, H->coarse_inv.p,
                            b, F.x1.p, F.x2.p, out, sweeps == 2 ? kAmgScale2 : kAmgScale1};
         const size_t sm = bottom_stage_words(F.n, C.n, F.nnz) * sizeof(uint32_t);
@@ -1906,9 +1987,12 @@ void solve_level(rsg_context *ctx, const AmgHierarchy *H, int l, const float *b,
     cycle(ctx, H, l, b, F.c1.p, sweeps, st, pdl);
     amg_launch(ctx->stream, pdl, k_amg_kc_spmv<2>, gs, kBlock, 0, F.n, F.rp, F.ci, F.val32, (const float *)F.c1.p,
              F.v1.p, b, (const float *)nullptr, H->kc_part.p, H->kc_ticket.p, sc, 0, 1, 0, st);
-    amg_launch(ctx->stream, pdl, k_amg_kc_r2, gv, kBlock, 0, F.n, b, (const float *)F.v1.p, (const double *)sc,
-             (const float *)F.dw.p, F.r2.p, F.x1.p, st);
-    cycle(ctx, H, l, F.r2.p, F.c2.p, sweeps, st, pdl);
+    // with one sweep the next cycle starts with the restriction, which forms r2 and x1 itself
+    const bool fold = sweeps == 1 && !bottom_cycle(H, l);
+    if (!fold)
+        amg_launch(ctx->stream, pdl, k_amg_kc_r2, gv, kBlock, 0, F.n, b, (const float *)F.v1.p, (const double *)sc,
+                   (const float *)F.dw.p, F.r2.p, F.x1.p, st);
+    cycle(ctx, H, l, F.r2.p, F.c2.p, sweeps, st, pdl, fold ? b : nullptr);
     amg_launch(ctx->stream, pdl, k_amg_kc_spmv<3>, gs, kBlock, 0, F.n, F.rp, F.ci, F.val32, (const float *)F.c2.p,
              F.v2.p, (const float *)F.v1.p, (const float *)F.r2.p, H->kc_part.p, H->kc_ticket.p, sc, 2, 3, 4, st);
 }
