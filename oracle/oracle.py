@@ -49,7 +49,11 @@ class OrcStats(C.Structure):
 
 
 class OrcTime(C.Structure):
-    _fields_ = [("transient", C.c_int32), ("alpha", C.c_double), ("dt", C.c_double)]
+    _fields_ = [("transient", C.c_int32), ("alpha", C.c_double), ("dt", C.c_double), ("mass_rule", C.c_int32)]
+
+
+# quadrature of the P1 mass integral (orc_time.mass_rule)
+MASS_EXACT, MASS_CENTROID, MASS_LUMPED = 0, 1, 2
 
 
 _P = C.c_void_p
@@ -278,8 +282,10 @@ def _system(h) -> tuple[CSR, np.ndarray]:
     return CSR(n, rp, ci, val), b
 
 
-def assemble_heat(p) -> tuple[CSR, np.ndarray]:
-    """RSolverHeat::prepare + assemblyMatrix restated for a rsg.workloads.HeatProblem."""
+def assemble_heat(p, mass_rule: int = MASS_EXACT) -> tuple[CSR, np.ndarray]:
+    """RSolverHeat::prepare + assemblyMatrix restated for a rsg.workloads.HeatProblem.  mass_rule picks
+    the quadrature of the transient mass integral, which the reference takes from range-model-lib's
+    tetrahedron rule (absent here): exact (the default, as the GPU assembly), centroid or lumped."""
     m = p.mesh
     xyz = np.ascontiguousarray(m.xyz, np.float64)
     tets = np.ascontiguousarray(m.tets, np.uint32)
@@ -288,14 +294,36 @@ def assemble_heat(p) -> tuple[CSR, np.ndarray]:
     rc = np.ascontiguousarray(p.rhoc_e, np.float64)
     nt = np.ascontiguousarray(p.node_t, np.float64)
     book = np.ascontiguousarray(p.book, np.uint32)
-    tm = OrcTime(1 if p.transient else 0, p.alpha, p.dt)
+    tm = OrcTime(1 if p.transient else 0, p.alpha, p.dt, mass_rule)
     h = lib().orc_assemble_heat(m.n_nodes, _ptr(xyz), m.n_tets, _ptr(tets), _ptr(k), _ptr(q), _ptr(rc), _ptr(nt),
                                 _ptr(book), p.n_free, C.byref(tm))
     return _system(h)
 
 
-def assemble_stress(p) -> tuple[CSR, np.ndarray]:
-    """RSolverStress::prepare + assemblyMatrix restated for a rsg.workloads.StressProblem."""
+def transient_heat(p, steps: int, *, mass_rule: int = MASS_EXACT, rtol: float = 1e-12) -> list[np.ndarray]:
+    """The reference's transient time loop for heat (src/rsolver.cpp:106-144: every step re-assembles
+    with the previous step's temperatures, src/rsolverheat.cpp:768-779, and solves with CG + Jacobi,
+    the previous solution as the initial guess).  Returns the node temperatures after each step; p is
+    not modified."""
+    import copy
+    q = copy.copy(p)
+    q.node_t = np.array(p.node_t, np.float64, copy=True)
+    free = q.book != 0xFFFFFFFF
+    idx = q.book[free].astype(np.int64)
+    out = []
+    for _ in range(steps):
+        A, b = assemble_heat(q, mass_rule)
+        x0 = np.empty(A.n)
+        x0[idx] = q.node_t[free]
+        x, st = solve(A, b, x0, prec=1, n_outer=100000, stop_rule="true", rtol=rtol)
+        q.node_t[free] = x[idx]
+        out.append(q.node_t.copy())
+    return out
+
+
+def assemble_stress(p, mass_rule: int = MASS_EXACT) -> tuple[CSR, np.ndarray]:
+    """RSolverStress::prepare + assemblyMatrix restated for a rsg.workloads.StressProblem (mass_rule as
+    for assemble_heat)."""
     m = p.mesh
     arrs = [np.ascontiguousarray(a, np.float64) for a in (m.xyz, p.e_mod, p.nu, p.rho_e, p.gravity, p.texp_e,
                                                           p.dtemp_e, p.traction, p.node_u)]
@@ -303,7 +331,7 @@ def assemble_stress(p) -> tuple[CSR, np.ndarray]:
     tets = np.ascontiguousarray(m.tets, np.uint32)
     tris = np.ascontiguousarray(p.tris, np.uint32)
     book = np.ascontiguousarray(p.book, np.uint32)
-    tm = OrcTime(1 if p.transient else 0, p.alpha, p.dt)
+    tm = OrcTime(1 if p.transient else 0, p.alpha, p.dt, mass_rule)
     h = lib().orc_assemble_stress(m.n_nodes, _ptr(xyz), m.n_tets, _ptr(tets), _ptr(e), _ptr(nu), _ptr(rho), _ptr(g),
                                   _ptr(te), _ptr(dte), tris.shape[0], _ptr(tris), _ptr(tr), _ptr(nu_), _ptr(book),
                                   p.n_free, C.byref(tm))

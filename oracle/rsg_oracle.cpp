@@ -709,6 +709,14 @@ void orc_system_copy(const orc_system *s, uint32_t *rp, uint32_t *ci, double *va
 }
 void orc_system_free(orc_system *s) { delete s; }
 
+/* The mass integral int N_m N_n over a tetrahedron of volume V under the quadrature rule of orc_time. */
+static double tet_mass(int rule, double V, int m, int n)
+{
+    if (rule == 1) return V / 16.0;
+    if (rule == 2) return m == n ? V / 4.0 : 0.0;
+    return V * (m == n ? 2.0 : 1.0) / 20.0;
+}
+
 orc_system *orc_assemble_heat(uint32_t n_nodes, const double *xyz, uint32_t n_tets, const uint32_t *tets,
                               const double *k_e, const double *q_e, const double *rhoc_e, const double *node_t,
                               const uint32_t *book, uint32_t n_free, const orc_time *time)
@@ -728,7 +736,7 @@ orc_system *orc_assemble_heat(uint32_t n_nodes, const double *xyz, uint32_t n_te
         for (int m = 0; m < 4; m++) {
             for (int n = 0; n < 4; n++) {
                 Ke[m][n] = (G[m][0] * G[n][0] + G[m][1] * G[n][1] + G[m][2] * G[n][2]) * k_e[e] * V;
-                Me[m][n] = transient ? rhoc_e[e] * V * (m == n ? 2.0 : 1.0) / 20.0 : 0.0;
+                Me[m][n] = transient ? rhoc_e[e] * tet_mass(time->mass_rule, V, m, n) : 0.0;
             }
             fe[m] = q_e[e] * V / 4.0;
         }
@@ -873,7 +881,7 @@ orc_system *orc_assemble_stress(uint32_t n_nodes, const double *xyz, uint32_t n_
         if (transient)
             for (int m = 0; m < 4; m++)
                 for (int n = 0; n < 4; n++) {
-                    double value = rho_e[e] * V * (m == n ? 2.0 : 1.0) / 20.0;
+                    double value = rho_e[e] * tet_mass(time->mass_rule, V, m, n);
                     for (int k = 0; k < 3; k++) Me[(3 * m + k) * 12 + 3 * n + k] = value;
                 }
         for (int m = 0; m < 4; m++)

@@ -100,6 +100,9 @@ typedef struct {
     int32_t transient;        /* time solver enabled */
     double  alpha;            /* time-march approximation coefficient (1 = backward Euler) */
     double  dt;
+    int32_t mass_rule;        /* quadrature of the mass integral N N^T over a tetrahedron: 0 exact
+                                 (V (1 + d_mn) / 20, any rule of degree >= 2), 1 one centroid point
+                                 (V / 16 for every pair), 2 row-sum lumped (V / 4 on the diagonal) */
 } orc_time;
 
 orc_system *orc_assemble_heat(uint32_t n_nodes, const double *xyz, uint32_t n_tets, const uint32_t *tets,
