@@ -405,6 +405,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
                     help="heat100, batch256: keep the built-in launch shapes")
+    ap.add_argument("--batch-systems", type=int, default=256,
+                    help="batch256: solve the first K systems of the draw (a smaller case for profiling)")
     ap.add_argument("--batch-precisions", default="fp64,mixed",
                     help="batch256: the precisions to time (comma-separated; the fastest gives the value)")
     ap.add_argument("--workload", default="heat100",
@@ -775,10 +777,11 @@ def run_other(args, rank, world, local_rank, threads):
         # every rank); with --batch-mode shard the systems are partitioned across ranks by estimated
         # work (strong scaling: the same 256 systems whatever N), with replicas every rank solves its
         # own 256 (weak scaling)
-        sizes = np.random.default_rng(1000 + (rank if args.batch_mode == "replicas" else 0)).integers(8, 61, 256)
-        seeds = [(10000 * rank if args.batch_mode == "replicas" else 0) + i for i in range(256)]
+        ns = max(1, min(256, args.batch_systems))
+        sizes = np.random.default_rng(1000 + (rank if args.batch_mode == "replicas" else 0)).integers(8, 61, 256)[:ns]
+        seeds = [(10000 * rank if args.batch_mode == "replicas" else 0) + i for i in range(ns)]
         costs = [D.estimated_cost(15 * (int(nh) + 1) ** 3, (int(nh) + 1) ** 3) for nh in sizes]
-        mine = D.shard_systems(costs, world)[rank] if args.batch_mode == "shard" else list(range(256))
+        mine = D.shard_systems(costs, world)[rank] if args.batch_mode == "shard" else list(range(ns))
         systems, rhs = [], []
         for i in mine:
             p = W.heat_cube(int(sizes[i]), sigma=1.0, seed=seeds[i], source="random")
@@ -814,17 +817,17 @@ def run_other(args, rank, world, local_rank, threads):
         # every system converged on every rank (one reduction, after the timed regions)
         worst_all = max_over_ranks(worst)
         t_best = min(r["s"] for r in res.values())
-        total = 256 * (world if args.batch_mode == "replicas" else 1)
-        line.update({"metric": "systems solved per second to FP64 rel. residual 1e-10 (256 uneven heat systems"
+        total = ns * (world if args.batch_mode == "replicas" else 1)
+        line.update({"metric": f"systems solved per second to FP64 rel. residual 1e-10 ({ns} uneven heat systems"
                                + (" per GPU)" if args.batch_mode == "replicas" else ", sharded across the GPUs)"),
                      "value": total / t_best, "unit": "systems/s", "ms_per_step": t_best * 1e3,
                      "higher_is_better": True, "dtype": "f64 / f32-inner",
                      "scaling": "weak" if args.batch_mode == "replicas" else "strong",
-                     "config": {"workload": "batch256_heat_8to60", "rows_this_rank": batch.rows,
+                     "config": {"workload": f"batch{ns}_heat_8to60", "rows_this_rank": batch.rows,
                                 "nnz_this_rank": batch.nnz, "systems_this_rank": len(mine), "autotune": tune,
                                 "worst_true_relres_all_ranks": worst_all,
                                 "parallelism": (f"independent replicas x{world}" if args.batch_mode == "replicas"
-                                                else f"256 systems sharded over {world} ranks by estimated work "
+                                                else f"{ns} systems sharded over {world} ranks by estimated work "
                                                      "(rsg.distributed.shard_systems), no collective in the solve"),
                                 "variants": res}})
         if world == 1 and not args.no_cpu_baseline:
