@@ -26,7 +26,11 @@
 //   aggregate, in ascending row order), the coarse level, prolongation scaled by s, post-smoothing
 //   with the same sweeps.  Every sweep is one pass over the level's matrix with the smoother fused
 //   into the gather; the finest level reads the matrix's FP32 SELL-32 (or CSR-stream) copy, the
-//   coarse levels their CSR with 8 lanes per row.
+//   coarse levels their CSR with 4 lanes per row.  Levels 1..kAmgKLevels are solved by two
+//   flexible-CG steps each (K-cycle); the last smoothed level and the dense coarse solve run as one
+//   single-CTA kernel.  Each step is its own kernel, launched with programmatic dependent launch; on
+//   request (conf.persistent > 0) the levels of at most kCoarsePersistRows rows run instead as one
+//   persistent cooperative kernel per visit, with the same bits (measured slower on B200).
 #include "amg.cuh"
 #include "grid_sync.cuh"
 
