@@ -27,3 +27,22 @@ def test_reference_arm_json_line():
     assert d["cpu_baseline"]["kind"] == ("reference" if R.available() else "port")
     assert d["e2e"] == {"value": d["value"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert d["config"]["workload"] == "heat_lognormal_10" and d["config"]["true_relres"] <= 1e-10
+
+
+def test_reference_arm_under_torchrun_prints_once():
+    """Launched like the driver launches N > 1 (torchrun, one process per GPU): rank 0 alone runs the
+    reference arm and prints its line; the other rank exits 0 without work."""
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    env = dict(os.environ, RSG_BENCH_N="8")
+    out = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+                          "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.join(REPO, "bench.py"),
+                          "--impl", "reference", "--gpus", "2", "--steps", "2", "--warmup", "3"],
+                         capture_output=True, text=True, env=env, timeout=600, cwd=REPO)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.strip().splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["config"]["workload"] == "heat_lognormal_8"
